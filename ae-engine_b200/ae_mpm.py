@@ -1,0 +1,446 @@
+"""ctypes binding of libae_mpm.so (include/ae_mpm.h) for tests, benchmarks and Python callers.
+
+Particle state crosses the boundary in the reference's MpssBuffer layout
+(ae_particle/src/mpss.rs:105-157): pos/vel as [f32;3], strain (F) and c (APIC C) as row-major
+[f32;9], jacobian and mass as f32, material_idx as u16.  `Particles` holds those arrays as numpy.
+
+There is no CPU fallback: if the library is missing or no CUDA device is usable, the calls
+raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libae_mpm.so")
+
+OK, EINVAL, ENOMEM, ENAN, ETIMEOUT, EBUDGET, ECUDA, EDOMAIN, ENOTFOUND, EAGAIN = range(10)
+STATUS = {OK: "OK", EINVAL: "EINVAL", ENOMEM: "ENOMEM", ENAN: "ENAN", ETIMEOUT: "ETIMEOUT", EBUDGET: "EBUDGET",
+          ECUDA: "ECUDA", EDOMAIN: "EDOMAIN", ENOTFOUND: "ENOTFOUND", EAGAIN: "EAGAIN"}
+
+# ConstitutiveModel (ae_particle/src/constitutive.rs:12-27) and the physics-mode materials
+NEO_HOOKEAN, DRUCKER_PRAGER, VON_MISES, NEWTONIAN_FLUID, COROTATED, FIXED_COROTATED, RIGID = range(7)
+PHYS_JELLY, PHYS_SNOW, PHYS_FLUID = 16, 17, 18
+MODE_PHYSICS, MODE_REFERENCE, MODE_VELOCITY_ONLY = 0, 1, 2
+WALL_STICKY, WALL_SLIP = 0, 1
+P2G_AUTO, P2G_TILE, P2G_WARP_AGG, P2G_GLOBAL = 0, 1, 2, 3
+
+
+class MpmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("%s: %s" % (STATUS.get(code, code), msg))
+        self.code = code
+
+
+class Material(C.Structure):
+    _fields_ = [("young_modulus", C.c_float), ("poisson_ratio", C.c_float), ("yield_stress", C.c_float),
+                ("hardening", C.c_float), ("density", C.c_float), ("friction_angle", C.c_float),
+                ("cohesion", C.c_float), ("model", C.c_int32), ("theta_c", C.c_float), ("theta_s", C.c_float),
+                ("hardening_xi", C.c_float), ("bulk_modulus", C.c_float)]
+
+
+class Config(C.Structure):
+    _fields_ = [("grid_dx", C.c_float), ("grid_size", C.c_uint64 * 3), ("substeps", C.c_uint64),
+                ("gravity", C.c_float * 3), ("damping", C.c_float), ("enable_plasticity", C.c_uint8),
+                ("enable_contact", C.c_uint8), ("use_sparse_grid", C.c_uint8)]
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_uint64), ("ny", C.c_uint64), ("nz", C.c_uint64), ("dx", C.c_float),
+                ("origin", C.c_float * 3)]
+
+
+class ParticlesView(C.Structure):
+    _fields_ = [("pos", C.c_void_p), ("vel", C.c_void_p), ("strain", C.c_void_p), ("jacobian", C.c_void_p),
+                ("c", C.c_void_p), ("mass", C.c_void_p), ("material_idx", C.c_void_p)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("n", C.c_uint32 * 3), ("dx", C.c_float), ("origin", C.c_float * 3),
+                ("gravity", C.c_float * 3), ("dt", C.c_float), ("wall_mode", C.c_int32),
+                ("wall_margin", C.c_int32), ("restitution", C.c_float), ("damping", C.c_float),
+                ("wall_origin", C.c_int32), ("n_materials", C.c_uint32), ("materials", C.POINTER(Material)),
+                ("max_particles", C.c_uint64)]
+
+
+class ExecOpts(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("deterministic", C.c_int32), ("sort_interval", C.c_int32),
+                ("p2g_variant", C.c_int32), ("block_threads", C.c_int32), ("use_graph", C.c_int32),
+                ("track_totals", C.c_int32), ("svd_fp64_fallback", C.c_int32)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("p2g_variant", C.c_int32), ("block_threads", C.c_int32), ("sort_interval", C.c_int32),
+                ("us_per_substep", C.c_float)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("substeps_per_tick", C.c_uint32), ("max_scenes", C.c_uint32),
+                ("exec", ExecOpts)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("request_id", C.c_uint64), ("status", C.c_int32), ("submit_s", C.c_double),
+                ("admit_s", C.c_double), ("done_s", C.c_double)]
+
+
+# every function include/ae_mpm.h declares: name -> (restype, argtypes)
+_P = C.c_void_p
+SIGNATURES = {
+    "ae_mpm_abi_version": (C.c_int, []),
+    "ae_mpm_exec_opts_default": (None, [C.POINTER(ExecOpts)]),
+    "ae_mpm_ctx_create": (C.c_int, [C.c_int, C.POINTER(_P)]),
+    "ae_mpm_ctx_destroy": (None, [_P]),
+    "ae_mpm_last_error": (C.c_char_p, [_P]),
+    "ae_mpm_step_parallel_with_grid": (C.c_int, [_P, C.POINTER(ParticlesView), C.c_uint64, C.POINTER(Grid),
+                                                 C.POINTER(Config), C.POINTER(Material), C.c_uint32,
+                                                 C.POINTER(C.c_int32), C.c_uint32, C.c_float,
+                                                 C.POINTER(C.c_uint64), C.c_uint64]),
+    "ae_mpm_step_velocity_only_parallel": (C.c_int, [_P, C.POINTER(ParticlesView), C.c_uint64, C.POINTER(Grid),
+                                                     C.POINTER(Config), C.c_float, C.POINTER(C.c_uint64),
+                                                     C.c_uint64]),
+    "ae_mpm_grid_download": (C.c_int, [_P, _P, _P, C.c_uint64]),
+    "ae_mpm_world_create": (C.c_int, [_P, C.POINTER(SceneDesc), C.c_uint32, C.POINTER(ExecOpts), C.POINTER(_P)]),
+    "ae_mpm_world_destroy": (C.c_int, [_P]),
+    "ae_mpm_world_upload": (C.c_int, [_P, C.c_uint32, C.POINTER(ParticlesView), C.c_uint64]),
+    "ae_mpm_world_upload_f64": (C.c_int, [_P, C.c_uint32, C.POINTER(ParticlesView), C.c_uint64]),
+    "ae_mpm_world_step": (C.c_int, [_P, C.c_uint32]),
+    "ae_mpm_world_sync": (C.c_int, [_P]),
+    "ae_mpm_world_download": (C.c_int, [_P, C.c_uint32, C.POINTER(ParticlesView)]),
+    "ae_mpm_world_download_f64": (C.c_int, [_P, C.c_uint32, C.POINTER(ParticlesView)]),
+    "ae_mpm_world_totals": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_double)]),
+    "ae_mpm_world_errors": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
+    "ae_mpm_world_launch_count": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
+    "ae_mpm_world_stage_times": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_double)]),
+    "ae_mpm_world_stream": (_P, [_P]),
+    "ae_mpm_world_particles": (C.c_uint64, [_P]),
+    "ae_mpm_radix_sort_keys": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, _P, _P]),
+    "ae_mpm_world_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(TuneResult)]),
+    "ae_mpm_server_create": (C.c_int, [_P, C.POINTER(ServerOpts), C.POINTER(_P)]),
+    "ae_mpm_server_submit": (C.c_int, [_P, C.POINTER(SceneDesc), C.POINTER(ParticlesView), C.c_uint64, C.c_uint32,
+                                       C.POINTER(ParticlesView), C.POINTER(C.c_uint64)]),
+    "ae_mpm_server_cancel": (C.c_int, [_P, C.c_uint64]),
+    "ae_mpm_server_poll": (C.c_int, [_P, C.POINTER(RequestResult), C.c_uint32, C.POINTER(C.c_uint32)]),
+    "ae_mpm_server_drain": (C.c_int, [_P, C.c_double]),
+    "ae_mpm_server_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
+                                      C.POINTER(C.c_uint64)]),
+    "ae_mpm_server_destroy": (C.c_int, [_P]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Loads the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError("libae_mpm.so is not built (%s): run __graft_entry__.build()" % path)
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exec_opts(**kw) -> ExecOpts:
+    o = ExecOpts()
+    load().ae_mpm_exec_opts_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def material(young_modulus=1e6, poisson_ratio=0.3, yield_stress=1e4, hardening=0.01, density=1000.0,
+             friction_angle=35.0, cohesion=0.0, model=NEO_HOOKEAN, theta_c=2.5e-2, theta_s=7.5e-3,
+             hardening_xi=10.0, bulk_modulus=0.0) -> Material:
+    return Material(young_modulus, poisson_ratio, yield_stress, hardening, density, friction_angle, cohesion,
+                    model, theta_c, theta_s, hardening_xi, bulk_modulus)
+
+
+@dataclass
+class Particles:
+    """Particle arrays in the reference layout (float32 or float64)."""
+    pos: np.ndarray
+    vel: np.ndarray
+    F: np.ndarray
+    J: np.ndarray
+    C: np.ndarray
+    mass: np.ndarray
+    mat: np.ndarray
+
+    @staticmethod
+    def empty(n: int, dtype=np.float32) -> "Particles":
+        F = np.zeros((n, 9), dtype)
+        F[:, [0, 4, 8]] = 1
+        return Particles(np.zeros((n, 3), dtype), np.zeros((n, 3), dtype), F, np.ones(n, dtype),
+                         np.zeros((n, 9), dtype), np.ones(n, dtype), np.zeros(n, np.uint16))
+
+    @property
+    def n(self) -> int:
+        return int(self.pos.shape[0])
+
+    @property
+    def dtype(self):
+        return self.pos.dtype
+
+    def astype(self, dtype) -> "Particles":
+        return Particles(*(np.ascontiguousarray(a.astype(dtype)) for a in
+                           (self.pos, self.vel, self.F, self.J, self.C, self.mass)), self.mat.copy())
+
+    def copy(self) -> "Particles":
+        return Particles(self.pos.copy(), self.vel.copy(), self.F.copy(), self.J.copy(), self.C.copy(),
+                         self.mass.copy(), self.mat.copy())
+
+    def subset(self, idx) -> "Particles":
+        return Particles(self.pos[idx].copy(), self.vel[idx].copy(), self.F[idx].copy(), self.J[idx].copy(),
+                         self.C[idx].copy(), self.mass[idx].copy(), self.mat[idx].copy())
+
+    def check(self) -> None:
+        for name in ("pos", "vel", "F", "J", "C", "mass", "mat"):
+            a = getattr(self, name)
+            if not a.flags["C_CONTIGUOUS"]:
+                setattr(self, name, np.ascontiguousarray(a))
+
+    def view(self) -> ParticlesView:
+        self.check()
+        return ParticlesView(self.pos.ctypes.data, self.vel.ctypes.data, self.F.ctypes.data, self.J.ctypes.data,
+                             self.C.ctypes.data, self.mass.ctypes.data, self.mat.ctypes.data)
+
+
+@dataclass
+class Scene:
+    """Python form of ae_mpm_scene_desc."""
+    n: tuple
+    dx: float
+    dt: float
+    materials: list
+    mode: int = MODE_PHYSICS
+    origin: tuple = (0.0, 0.0, 0.0)
+    gravity: tuple = (0.0, -9.8, 0.0)
+    wall_mode: int = WALL_STICKY
+    wall_margin: int = 3
+    restitution: float = 0.0
+    damping: float = 0.995
+    wall_origin: int = 1
+    max_particles: int = 0
+    _mats: object = field(default=None, repr=False)
+
+    def desc(self) -> SceneDesc:
+        arr = (Material * len(self.materials))(*self.materials)
+        self._mats = arr
+        return SceneDesc(self.mode, (C.c_uint32 * 3)(*self.n), self.dx, (C.c_float * 3)(*self.origin),
+                         (C.c_float * 3)(*self.gravity), self.dt, self.wall_mode, self.wall_margin,
+                         self.restitution, self.damping, self.wall_origin, len(self.materials),
+                         C.cast(arr, C.POINTER(Material)), self.max_particles)
+
+
+class Context:
+    def __init__(self, device: int = 0):
+        lib = load()
+        h = C.c_void_p()
+        rc = lib.ae_mpm_ctx_create(device, C.byref(h))
+        if rc != OK:
+            raise MpmError(rc, "ae_mpm_ctx_create(%d) failed (no usable CUDA device?)" % device)
+        self.h = h
+        self.lib = lib
+
+    def close(self):
+        if self.h:
+            self.lib.ae_mpm_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc: int) -> int:
+        if rc != OK:
+            raise MpmError(rc, self.lib.ae_mpm_last_error(self.h).decode())
+        return rc
+
+    # -- drop-in entry points ----------------------------------------------------------------
+    def step_parallel_with_grid(self, p: Particles, grid: Grid, config: Config, materials, models, total_dt,
+                                indices) -> None:
+        mats = (Material * max(len(materials), 1))(*materials)
+        mods = (C.c_int32 * max(len(models), 1))(*models)
+        idx = np.ascontiguousarray(np.asarray(indices, np.uint64))
+        v = p.view()
+        self.check(self.lib.ae_mpm_step_parallel_with_grid(
+            self.h, C.byref(v), p.n, C.byref(grid), C.byref(config), mats, len(materials), mods, len(models),
+            total_dt, idx.ctypes.data_as(C.POINTER(C.c_uint64)), idx.size))
+
+    def step_velocity_only_parallel(self, p: Particles, grid: Grid, config: Config, total_dt, indices) -> None:
+        idx = np.ascontiguousarray(np.asarray(indices, np.uint64))
+        v = p.view()
+        self.check(self.lib.ae_mpm_step_velocity_only_parallel(
+            self.h, C.byref(v), p.n, C.byref(grid), C.byref(config), total_dt,
+            idx.ctypes.data_as(C.POINTER(C.c_uint64)), idx.size))
+
+    def grid_download(self, nx, ny, nz):
+        m = np.zeros(nx * ny * nz, np.float32)
+        v = np.zeros((nx * ny * nz, 3), np.float32)
+        self.check(self.lib.ae_mpm_grid_download(self.h, m.ctypes.data, v.ctypes.data, m.size))
+        return m, v
+
+    def radix_sort(self, keys: np.ndarray, key_bits: int):
+        keys = np.ascontiguousarray(keys, np.uint32)
+        sk = np.empty_like(keys)
+        perm = np.empty_like(keys)
+        self.check(self.lib.ae_mpm_radix_sort_keys(self.h, keys.ctypes.data, keys.size, key_bits,
+                                                   sk.ctypes.data, perm.ctypes.data))
+        return sk, perm
+
+
+class World:
+    """Device-resident scenes stepped in lockstep (batched path; one scene = plain path)."""
+
+    def __init__(self, ctx: Context, scenes, opts: ExecOpts | None = None):
+        self.ctx = ctx
+        self.scenes = list(scenes)
+        descs = (SceneDesc * len(self.scenes))(*[s.desc() for s in self.scenes])
+        self._descs = descs
+        h = C.c_void_p()
+        ctx.check(ctx.lib.ae_mpm_world_create(ctx.h, descs, len(self.scenes),
+                                              C.byref(opts) if opts is not None else None, C.byref(h)))
+        self.h = h
+        self.f64 = opts is not None and opts.precision == 64
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.ae_mpm_world_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, scene: int, p: Particles) -> None:
+        want = np.float64 if self.f64 else np.float32
+        if p.dtype != want:
+            raise TypeError("world precision needs %s particles" % np.dtype(want).name)
+        v = p.view()
+        fn = self.ctx.lib.ae_mpm_world_upload_f64 if self.f64 else self.ctx.lib.ae_mpm_world_upload
+        self.ctx.check(fn(self.h, scene, C.byref(v), p.n))
+        self._keep = p
+
+    def download(self, scene: int, n: int) -> Particles:
+        p = Particles.empty(n, np.float64 if self.f64 else np.float32)
+        v = p.view()
+        fn = self.ctx.lib.ae_mpm_world_download_f64 if self.f64 else self.ctx.lib.ae_mpm_world_download
+        self.ctx.check(fn(self.h, scene, C.byref(v)))
+        return p
+
+    def download_into(self, scene: int, p: Particles) -> None:
+        v = p.view()
+        fn = self.ctx.lib.ae_mpm_world_download_f64 if self.f64 else self.ctx.lib.ae_mpm_world_download
+        self.ctx.check(fn(self.h, scene, C.byref(v)))
+
+    def step(self, n: int) -> None:
+        self.ctx.check(self.ctx.lib.ae_mpm_world_step(self.h, n))
+
+    def sync(self, raise_on_error: bool = True) -> int:
+        rc = self.ctx.lib.ae_mpm_world_sync(self.h)
+        if raise_on_error:
+            self.ctx.check(rc)
+        return rc
+
+    def totals(self, scene: int) -> np.ndarray:
+        out = (C.c_double * 5)()
+        self.ctx.check(self.ctx.lib.ae_mpm_world_totals(self.h, scene, out))
+        return np.array(out[:])
+
+    def errors(self, scene: int):
+        w = C.c_uint32()
+        c = (C.c_uint64 * 3)()
+        self.ctx.check(self.ctx.lib.ae_mpm_world_errors(self.h, scene, C.byref(w), c))
+        return int(w.value), [int(x) for x in c]
+
+    def launches(self) -> int:
+        n = C.c_uint64()
+        self.ctx.check(self.ctx.lib.ae_mpm_world_launch_count(self.h, C.byref(n)))
+        return int(n.value)
+
+    def stage_times(self, n: int) -> dict:
+        """Mean per-substep device time of each stage (us), measured with CUDA events."""
+        out = (C.c_double * 5)()
+        self.ctx.check(self.ctx.lib.ae_mpm_world_stage_times(self.h, n, out))
+        return dict(zip(("sort", "p2g", "grid", "g2p", "substep"), out[:]))
+
+    def stream(self) -> int:
+        return int(self.ctx.lib.ae_mpm_world_stream(self.h) or 0)
+
+    def particles(self) -> int:
+        return int(self.ctx.lib.ae_mpm_world_particles(self.h))
+
+    def autotune(self, substeps_per_trial: int = 8) -> TuneResult:
+        r = TuneResult()
+        self.ctx.check(self.ctx.lib.ae_mpm_world_autotune(self.h, substeps_per_trial, C.byref(r)))
+        return r
+
+
+class Server:
+    """Continuous-batching server (ae_mpm_server_*)."""
+
+    def __init__(self, ctx: Context, hbm_budget_bytes=0, substeps_per_tick=10, max_scenes=4096,
+                 exec_options: ExecOpts | None = None):
+        self.ctx = ctx
+        o = ServerOpts(hbm_budget_bytes, substeps_per_tick, max_scenes, exec_options or exec_opts())
+        h = C.c_void_p()
+        ctx.check(ctx.lib.ae_mpm_server_create(ctx.h, C.byref(o), C.byref(h)))
+        self.h = h
+        self._pending = {}
+
+    def submit(self, scene: Scene, p: Particles, substeps: int) -> int:
+        out = Particles.empty(p.n)
+        vin, vout = p.view(), out.view()
+        d = scene.desc()
+        rid = C.c_uint64()
+        self.ctx.check(self.ctx.lib.ae_mpm_server_submit(self.h, C.byref(d), C.byref(vin), p.n, substeps,
+                                                         C.byref(vout), C.byref(rid)))
+        self._pending[int(rid.value)] = (out, scene)
+        return int(rid.value)
+
+    def cancel(self, rid: int) -> int:
+        return self.ctx.lib.ae_mpm_server_cancel(self.h, rid)
+
+    def poll(self, max_n: int = 256):
+        res = (RequestResult * max_n)()
+        n = C.c_uint32()
+        rc = self.ctx.lib.ae_mpm_server_poll(self.h, res, max_n, C.byref(n))
+        out = []
+        for i in range(n.value if rc == OK else 0):
+            r = res[i]
+            parts, _ = self._pending.pop(int(r.request_id), (None, None))
+            out.append((int(r.request_id), int(r.status), r.submit_s, r.admit_s, r.done_s, parts))
+        return out
+
+    def drain(self, timeout_s: float = 60.0) -> int:
+        return self.ctx.lib.ae_mpm_server_drain(self.h, timeout_s)
+
+    def stats(self):
+        rb, rs, tk, ps = C.c_uint64(), C.c_uint32(), C.c_uint64(), C.c_uint64()
+        self.ctx.check(self.ctx.lib.ae_mpm_server_stats(self.h, C.byref(rb), C.byref(rs), C.byref(tk), C.byref(ps)))
+        return dict(resident_bytes=rb.value, resident_scenes=rs.value, ticks=tk.value, particle_substeps=ps.value)
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.ae_mpm_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

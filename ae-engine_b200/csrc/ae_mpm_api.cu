@@ -1,0 +1,473 @@
+// ae_mpm_api.cu -- C ABI of libae_mpm.so (declared in include/ae_mpm.h).
+//
+// The drop-in entry points keep the reference's call shape (caller-owned MpssBuffer arrays,
+// particle_indices, MpmConfig, material/model tables) and move the selected particles through
+// one device-resident world per context, re-created only when the grid size or particle count
+// changes.  Nothing here falls back to CPU arithmetic: without a usable CUDA device every entry
+// point that computes returns AE_MPM_ECUDA.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ae_mpm.h"
+#include "mpm_world.cuh"
+#include "radix_sort.cuh"
+
+using aemp::WorldBase;
+
+struct ae_mpm_ctx {
+  int device = 0;
+  std::string err = "ok";
+  // drop-in world cache
+  WorldBase* dropin = nullptr;
+  std::string dropin_sig;
+  std::vector<ae_mpm_material> dropin_mats;
+  // pinned staging for gathers through particle_indices
+  float* pin = nullptr;
+  size_t pin_bytes = 0;
+  // radix sort API scratch
+  aemp::SortScratch sort;
+  uint32_t* sort_keys = nullptr;
+  uint64_t sort_keys_cap = 0;
+  // autotune cache: workload signature -> choice
+  std::map<std::string, ae_mpm_tune_result> tuned;
+};
+
+struct ae_mpm_world {
+  ae_mpm_ctx* ctx;
+  WorldBase* w;
+  std::string sig;  // workload signature for the autotune cache
+};
+
+namespace aemp {
+int ctx_device(const ae_mpm_ctx* ctx) { return ctx ? ctx->device : 0; }
+}  // namespace aemp
+
+namespace {
+
+int fail(ae_mpm_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int set_device(ae_mpm_ctx* ctx) {
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  return AE_MPM_OK;
+}
+
+std::string world_signature(const ae_mpm_scene_desc* s, uint32_t n, const ae_mpm_exec_opts& o) {
+  // scene count, total particles, grid sizes and the material models of the batch
+  uint64_t parts = 0;
+  std::string g;
+  for (uint32_t i = 0; i < n; ++i) {
+    parts += s[i].max_particles;
+    if (i < 8) g += std::to_string(s[i].n[0]) + "x" + std::to_string(s[i].n[1]) + "x" + std::to_string(s[i].n[2]) + ",";
+  }
+  uint32_t models = 0;
+  for (uint32_t i = 0; i < n; ++i)
+    for (uint32_t k = 0; k < s[i].n_materials; ++k) models |= 1u << (s[i].materials[k].model & 31);
+  int bucket = 0;
+  while ((1ull << bucket) < parts) ++bucket;
+  return "m" + std::to_string(s[0].mode) + "p" + std::to_string(o.precision) + "d" + std::to_string(o.deterministic) +
+         "s" + std::to_string(n) + "n" + std::to_string(bucket) + "g" + g + "k" + std::to_string(models);
+}
+
+int ensure_pinned(ae_mpm_ctx* ctx, size_t bytes) {
+  if (bytes <= ctx->pin_bytes) return AE_MPM_OK;
+  if (ctx->pin) cudaFreeHost(ctx->pin);
+  ctx->pin = nullptr;
+  ctx->pin_bytes = 0;
+  cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&ctx->pin), bytes, cudaHostAllocDefault);
+  if (e != cudaSuccess) return fail(ctx, AE_MPM_ENOMEM, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+  ctx->pin_bytes = bytes;
+  return AE_MPM_OK;
+}
+
+// reference-layout view over the pinned staging for n particles
+ae_mpm_particles pinned_view(ae_mpm_ctx* ctx, uint64_t n) {
+  ae_mpm_particles v;
+  float* p = ctx->pin;
+  v.pos = p;
+  v.vel = p + 3 * n;
+  v.strain = p + 6 * n;
+  v.jacobian = p + 15 * n;
+  v.c = p + 16 * n;
+  v.mass = p + 25 * n;
+  v.material_idx = reinterpret_cast<uint16_t*>(p + 26 * n);
+  return v;
+}
+
+int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64_t capacity, const ae_mpm_grid* grid,
+               const ae_mpm_config* config, const std::vector<ae_mpm_material>& mats, float total_dt,
+               const uint64_t* idx, uint64_t n) {
+  if (config->substeps == 0) return AE_MPM_OK;  // `for _ in 0..0` runs no substep
+  if (grid->nx == 0 || grid->ny == 0 || grid->nz == 0 || grid->nx > (1u << 20) || grid->ny > (1u << 20) ||
+      grid->nz > (1u << 20))
+    return fail(ctx, AE_MPM_EINVAL, "grid needs 1..2^20 nodes per axis");
+  if (!(grid->dx > 0.0f)) return fail(ctx, AE_MPM_EINVAL, "grid dx must be positive");
+  if (!buffer->pos || !buffer->vel || !buffer->mass ||
+      (mode == AE_MPM_MODE_REFERENCE && (!buffer->strain || !buffer->jacobian || !buffer->c || !buffer->material_idx)))
+    return fail(ctx, AE_MPM_EINVAL, "particle buffer has a null array");
+  for (uint64_t k = 0; k < n; ++k)
+    if (idx[k] >= capacity) return fail(ctx, AE_MPM_EINVAL, "particle index " + std::to_string(idx[k]) + " >= capacity");
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  ae_mpm_scene_desc d{};
+  d.mode = mode;
+  d.n[0] = uint32_t(grid->nx);
+  d.n[1] = uint32_t(grid->ny);
+  d.n[2] = uint32_t(grid->nz);
+  d.dx = grid->dx;
+  for (int a = 0; a < 3; ++a) {
+    d.origin[a] = grid->origin[a];
+    d.gravity[a] = config->gravity[a];
+  }
+  d.dt = total_dt / float(config->substeps);
+  d.damping = config->damping;
+  d.wall_origin = n >= 50000 ? 1 : 0;  // mpm_solver.rs:1077 switches to the parallel path
+  d.wall_margin = 0;
+  d.n_materials = uint32_t(mats.size());
+  d.materials = mats.data();
+  d.max_particles = n;
+  ae_mpm_exec_opts o;
+  ae_mpm_exec_opts_default(&o);
+  std::string sig = world_signature(&d, 1, o) + "|" + std::to_string(mats.size());
+  if (!ctx->dropin || ctx->dropin_sig != sig) {
+    delete ctx->dropin;
+    ctx->dropin = nullptr;
+    auto it = ctx->tuned.find(world_signature(&d, 1, o));
+    if (it != ctx->tuned.end()) {
+      o.p2g_variant = it->second.p2g_variant;
+      o.block_threads = it->second.block_threads;
+      o.sort_interval = it->second.sort_interval;
+    }
+    std::string why;
+    int st = 0;
+    ctx->dropin = aemp::make_world(&d, 1, o, why, &st);
+    if (!ctx->dropin) return fail(ctx, st ? st : AE_MPM_ECUDA, why);
+    ctx->dropin_sig = sig;
+  } else {
+    rc = ctx->dropin->set_scene_params(0, d);
+    if (rc) return fail(ctx, rc, ctx->dropin->err);
+  }
+  // gather the selected particles into pinned staging
+  rc = ensure_pinned(ctx, sizeof(float) * 26 * n + sizeof(uint16_t) * n + 64);
+  if (rc) return rc;
+  ae_mpm_particles v = pinned_view(ctx, n);
+  for (uint64_t k = 0; k < n; ++k) {
+    const uint64_t i = idx[k];
+    std::memcpy(v.pos + 3 * k, buffer->pos + 3 * i, 3 * sizeof(float));
+    std::memcpy(v.vel + 3 * k, buffer->vel + 3 * i, 3 * sizeof(float));
+    v.mass[k] = buffer->mass[i];
+    if (buffer->strain) {
+      std::memcpy(v.strain + 9 * k, buffer->strain + 9 * i, 9 * sizeof(float));
+    } else {
+      for (int q = 0; q < 9; ++q) v.strain[9 * k + q] = (q % 4 == 0) ? 1.0f : 0.0f;
+    }
+    if (buffer->c) {
+      std::memcpy(v.c + 9 * k, buffer->c + 9 * i, 9 * sizeof(float));
+    } else {
+      std::memset(v.c + 9 * k, 0, 9 * sizeof(float));
+    }
+    v.jacobian[k] = buffer->jacobian ? buffer->jacobian[i] : 1.0f;
+    v.material_idx[k] = buffer->material_idx ? buffer->material_idx[i] : 0;
+  }
+  WorldBase* w = ctx->dropin;
+  if ((rc = w->upload(0, &v, n, false)) || (rc = w->step(uint32_t(config->substeps))) || (rc = w->download(0, &v, false)))
+    return fail(ctx, rc, w->err);
+  for (uint64_t k = 0; k < n; ++k) {
+    const uint64_t i = idx[k];
+    std::memcpy(buffer->pos + 3 * i, v.pos + 3 * k, 3 * sizeof(float));
+    std::memcpy(buffer->vel + 3 * i, v.vel + 3 * k, 3 * sizeof(float));
+    if (mode == AE_MPM_MODE_REFERENCE) {
+      std::memcpy(buffer->strain + 9 * i, v.strain + 9 * k, 9 * sizeof(float));
+      std::memcpy(buffer->c + 9 * i, v.c + 9 * k, 9 * sizeof(float));
+      buffer->jacobian[i] = v.jacobian[k];
+    }
+  }
+  return AE_MPM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ae_mpm_abi_version(void) { return AE_MPM_ABI_VERSION; }
+
+void ae_mpm_exec_opts_default(ae_mpm_exec_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->precision = 32;
+  o->deterministic = 0;
+  o->sort_interval = 1;
+  o->p2g_variant = AE_MPM_P2G_AUTO;
+  o->block_threads = 0;
+  o->use_graph = 1;
+  o->track_totals = 0;
+  o->svd_fp64_fallback = 1;
+}
+
+int ae_mpm_ctx_create(int device, ae_mpm_ctx** out) {
+  if (!out) return AE_MPM_EINVAL;
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) return AE_MPM_ECUDA;
+  if (device < 0 || device >= count) return AE_MPM_EINVAL;
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return AE_MPM_ECUDA;
+  auto* c = new ae_mpm_ctx();
+  c->device = device;
+  *out = c;
+  return AE_MPM_OK;
+}
+
+void ae_mpm_ctx_destroy(ae_mpm_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  delete ctx->dropin;
+  if (ctx->pin) cudaFreeHost(ctx->pin);
+  aemp::sort_scratch_free(ctx->sort);
+  cudaFree(ctx->sort_keys);
+  delete ctx;
+}
+
+const char* ae_mpm_last_error(const ae_mpm_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int ae_mpm_step_parallel_with_grid(ae_mpm_ctx* ctx, const ae_mpm_particles* buffer, uint64_t capacity,
+                                   const ae_mpm_grid* grid, const ae_mpm_config* config,
+                                   const ae_mpm_material* material_table, uint32_t n_materials,
+                                   const int32_t* model_table, uint32_t n_models, float total_dt,
+                                   const uint64_t* particle_indices, uint64_t n_indices) {
+  if (!ctx) return AE_MPM_EINVAL;
+  if (n_indices == 0) return AE_MPM_OK;  // mpm_solver.rs:1072-1074
+  if (!buffer || !grid || !config || !particle_indices) return fail(ctx, AE_MPM_EINVAL, "null argument");
+  if (n_materials == 0 || !material_table)
+    return fail(ctx, AE_MPM_EINVAL, "material_table is empty (the reference indexes material_table[0])");
+  if (n_models > 0 && !model_table) return fail(ctx, AE_MPM_EINVAL, "model_table is null");
+  // effective (params, model) per material index, with the reference's fallbacks
+  // (mpm_solver.rs:840-841: params default to material_table[0], model to NeoHookean)
+  const uint32_t ne = std::max(n_materials, n_models);
+  std::vector<ae_mpm_material> mats(ne);
+  for (uint32_t k = 0; k < ne; ++k) {
+    mats[k] = material_table[k < n_materials ? k : 0];
+    mats[k].model = k < n_models ? model_table[k] : AE_MPM_NEO_HOOKEAN;
+    if (mats[k].model < AE_MPM_NEO_HOOKEAN || mats[k].model > AE_MPM_RIGID)
+      return fail(ctx, AE_MPM_EINVAL, "model_table holds a value that is not a ConstitutiveModel");
+  }
+  return dropin_run(ctx, AE_MPM_MODE_REFERENCE, buffer, capacity, grid, config, mats, total_dt, particle_indices,
+                    n_indices);
+}
+
+int ae_mpm_step_velocity_only_parallel(ae_mpm_ctx* ctx, const ae_mpm_particles* buffer, uint64_t capacity,
+                                       const ae_mpm_grid* grid, const ae_mpm_config* config, float total_dt,
+                                       const uint64_t* particle_indices, uint64_t n_indices) {
+  if (!ctx) return AE_MPM_EINVAL;
+  if (n_indices == 0) return AE_MPM_OK;  // mpm_solver.rs:1344-1346
+  if (!buffer || !grid || !config || !particle_indices) return fail(ctx, AE_MPM_EINVAL, "null argument");
+  std::vector<ae_mpm_material> mats(1);
+  std::memset(&mats[0], 0, sizeof(mats[0]));
+  mats[0].density = 1.0f;
+  mats[0].young_modulus = 1.0f;
+  mats[0].model = AE_MPM_NEO_HOOKEAN;  // unused: the velocity-only substep has no stress
+  return dropin_run(ctx, AE_MPM_MODE_VELOCITY_ONLY, buffer, capacity, grid, config, mats, total_dt, particle_indices,
+                    n_indices);
+}
+
+int ae_mpm_grid_download(ae_mpm_ctx* ctx, float* mass, float* vel, uint64_t n_nodes) {
+  if (!ctx) return AE_MPM_EINVAL;
+  if (!ctx->dropin) return fail(ctx, AE_MPM_EINVAL, "no drop-in step has run on this context");
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  rc = ctx->dropin->grid_download(0, mass, vel, n_nodes);
+  return rc ? fail(ctx, rc, ctx->dropin->err) : AE_MPM_OK;
+}
+
+int ae_mpm_world_create(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32_t n_scenes,
+                        const ae_mpm_exec_opts* opts, ae_mpm_world** out) {
+  if (!ctx || !out) return AE_MPM_EINVAL;
+  *out = nullptr;
+  if (!scenes || n_scenes == 0) return fail(ctx, AE_MPM_EINVAL, "no scenes");
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  ae_mpm_exec_opts o;
+  if (opts)
+    o = *opts;
+  else
+    ae_mpm_exec_opts_default(&o);
+  if (o.precision != 64) o.precision = 32;
+  auto it = ctx->tuned.find(world_signature(scenes, n_scenes, o));
+  if (it != ctx->tuned.end()) {
+    if (o.p2g_variant == AE_MPM_P2G_AUTO) o.p2g_variant = it->second.p2g_variant;
+    if (o.block_threads == 0) o.block_threads = it->second.block_threads;
+    if (opts == nullptr || opts->p2g_variant == AE_MPM_P2G_AUTO) o.sort_interval = it->second.sort_interval;
+  }
+  if (o.p2g_variant == AE_MPM_P2G_AUTO) o.p2g_variant = AE_MPM_P2G_TILE;
+  if (o.block_threads == 0) o.block_threads = 256;
+  std::string why;
+  int st = 0;
+  WorldBase* w = aemp::make_world(scenes, n_scenes, o, why, &st);
+  if (!w) return fail(ctx, st ? st : AE_MPM_ECUDA, why);
+  *out = new ae_mpm_world{ctx, w, world_signature(scenes, n_scenes, o)};
+  return AE_MPM_OK;
+}
+
+int ae_mpm_world_destroy(ae_mpm_world* world) {
+  if (!world) return AE_MPM_EINVAL;
+  cudaSetDevice(world->ctx->device);
+  delete world->w;
+  delete world;
+  return AE_MPM_OK;
+}
+
+#define AE_WORLD_CALL(expr)                                 \
+  do {                                                      \
+    if (!world) return AE_MPM_EINVAL;                       \
+    int rc_ = set_device(world->ctx);                       \
+    if (rc_) return rc_;                                    \
+    rc_ = (expr);                                           \
+    if (rc_) return fail(world->ctx, rc_, world->w->err);   \
+    return AE_MPM_OK;                                       \
+  } while (0)
+
+int ae_mpm_world_upload(ae_mpm_world* world, uint32_t scene, const ae_mpm_particles* host, uint64_t n) {
+  if (world && !host) return fail(world->ctx, AE_MPM_EINVAL, "null particle view");
+  AE_WORLD_CALL(world->w->upload(scene, host, n, false));
+}
+int ae_mpm_world_upload_f64(ae_mpm_world* world, uint32_t scene, const ae_mpm_particles_f64* host, uint64_t n) {
+  if (world && !host) return fail(world->ctx, AE_MPM_EINVAL, "null particle view");
+  AE_WORLD_CALL(world->w->upload(scene, host, n, true));
+}
+int ae_mpm_world_step(ae_mpm_world* world, uint32_t n_substeps) { AE_WORLD_CALL(world->w->step(n_substeps)); }
+int ae_mpm_world_sync(ae_mpm_world* world) { AE_WORLD_CALL(world->w->sync()); }
+int ae_mpm_world_download(ae_mpm_world* world, uint32_t scene, ae_mpm_particles* host) {
+  if (world && !host) return fail(world->ctx, AE_MPM_EINVAL, "null particle view");
+  AE_WORLD_CALL(world->w->download(scene, host, false));
+}
+int ae_mpm_world_download_f64(ae_mpm_world* world, uint32_t scene, ae_mpm_particles_f64* host) {
+  if (world && !host) return fail(world->ctx, AE_MPM_EINVAL, "null particle view");
+  AE_WORLD_CALL(world->w->download(scene, host, true));
+}
+int ae_mpm_world_totals(ae_mpm_world* world, uint32_t scene, double out[5]) {
+  if (world && !out) return fail(world->ctx, AE_MPM_EINVAL, "null output");
+  AE_WORLD_CALL(world->w->totals(scene, out));
+}
+int ae_mpm_world_errors(ae_mpm_world* world, uint32_t scene, uint32_t* error_word, uint64_t counters[3]) {
+  AE_WORLD_CALL(world->w->errors(scene, error_word, counters));
+}
+
+int ae_mpm_world_stage_times(ae_mpm_world* world, uint32_t n_substeps, double out_us[5]) {
+  if (world && !out_us) return fail(world->ctx, AE_MPM_EINVAL, "null output");
+  AE_WORLD_CALL(world->w->stage_times(n_substeps, out_us));
+}
+
+int ae_mpm_world_launch_count(const ae_mpm_world* world, uint64_t* launches) {
+  if (!world || !launches) return AE_MPM_EINVAL;
+  *launches = world->w->last_launches();
+  return AE_MPM_OK;
+}
+
+void* ae_mpm_world_stream(ae_mpm_world* world) { return world ? static_cast<void*>(world->w->stream()) : nullptr; }
+
+uint64_t ae_mpm_world_particles(const ae_mpm_world* world) { return world ? world->w->particles() : 0; }
+
+int ae_mpm_radix_sort_keys(ae_mpm_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t key_bits,
+                           uint32_t* sorted_keys_out, uint32_t* perm_out) {
+  if (!ctx) return AE_MPM_EINVAL;
+  if (n == 0) return AE_MPM_OK;
+  if (!keys || !sorted_keys_out || !perm_out || key_bits == 0 || key_bits > 32 || n >= (1ull << 32))
+    return fail(ctx, AE_MPM_EINVAL, "bad radix sort arguments");
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  if (ctx->sort.n_cap < n) {
+    cudaError_t e = aemp::sort_scratch_alloc(ctx->sort, n);
+    if (e != cudaSuccess) return fail(ctx, AE_MPM_ENOMEM, cudaGetErrorString(e));
+  }
+  if (ctx->sort_keys_cap < n) {
+    cudaFree(ctx->sort_keys);
+    ctx->sort_keys = nullptr;
+    ctx->sort_keys_cap = 0;
+    cudaError_t e = cudaMalloc(&ctx->sort_keys, sizeof(uint32_t) * n);
+    if (e != cudaSuccess) return fail(ctx, AE_MPM_ENOMEM, cudaGetErrorString(e));
+    ctx->sort_keys_cap = n;
+  }
+  cudaError_t e = cudaMemcpy(ctx->sort_keys, keys, sizeof(uint32_t) * n, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, cudaGetErrorString(e));
+  const uint32_t *sk = nullptr, *pm = nullptr;
+  aemp::radix_sort_pairs(ctx->sort_keys, n, int(key_bits), ctx->sort, 0, &sk, &pm);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(sorted_keys_out, sk, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(perm_out, pm, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, cudaGetErrorString(e));
+  return AE_MPM_OK;
+}
+
+// Autotuner: P2G variant x particles per block x sort interval, timed with CUDA events on the
+// world's stream from the same starting state (snapshot restored between trials).
+int ae_mpm_world_autotune(ae_mpm_world* world, uint32_t substeps_per_trial, ae_mpm_tune_result* out) {
+  if (!world) return AE_MPM_EINVAL;
+  ae_mpm_ctx* ctx = world->ctx;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  WorldBase* w = world->w;
+  if (substeps_per_trial == 0) substeps_per_trial = 8;
+  const ae_mpm_exec_opts saved = w->opts();
+  if ((rc = w->snapshot(false))) return fail(ctx, rc, w->err);
+  std::vector<int> variants = {AE_MPM_P2G_TILE, AE_MPM_P2G_WARP_AGG, AE_MPM_P2G_GLOBAL};
+  std::vector<int> threads = {128, 256};
+  std::vector<int> intervals = {1, 2, 4, 8};
+  if (saved.deterministic) {
+    variants = {saved.p2g_variant};
+    intervals = {1};
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  ae_mpm_tune_result best{saved.p2g_variant, saved.block_threads, saved.sort_interval, 1e30f};
+  for (int v : variants)
+    for (int t : threads)
+      for (int si : intervals) {
+        w->opts().p2g_variant = v;
+        w->opts().block_threads = t;
+        w->opts().sort_interval = si;
+        w->invalidate_graph();
+        if ((rc = w->snapshot(true))) break;
+        // warm-up reaches the graph path too; each trial then times whole graph periods
+        uint32_t trial = std::max<uint32_t>(substeps_per_trial, uint32_t(2 * si));
+        if ((rc = w->step(trial))) break;
+        cudaStream_t s = w->stream();
+        cudaEventRecord(e0, s);
+        if ((rc = w->step(trial))) break;
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        float us = 1000.0f * ms / float(trial);
+        if (us < best.us_per_substep) best = ae_mpm_tune_result{v, t, si, us};
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) {
+    w->opts() = saved;
+    w->invalidate_graph();
+    w->snapshot(true);
+    return fail(ctx, rc, w->err);
+  }
+  w->opts().p2g_variant = best.p2g_variant;
+  w->opts().block_threads = best.block_threads;
+  w->opts().sort_interval = best.sort_interval;
+  w->invalidate_graph();
+  if ((rc = w->snapshot(true))) return fail(ctx, rc, w->err);
+  ctx->tuned[world->sig] = best;
+  if (out) *out = best;
+  return AE_MPM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1906 @@
+// mpm_world.cu -- the MPM substep on sm_100a: kernels and the world driver.
+//
+// Substep (every scene of a world at once):
+//   sort     radix sort of cell keys -> perm (sorted position -> storage slot)
+//   P2G      one block per chunk of sorted particles; the chunk's stencil bounding box is a
+//            shared-memory tile with halo that absorbs all same-cell contributions, then is
+//            flushed with 16-byte vector atomics (red.global.add.v4.f32) into the grid
+//   grid     one pass over the blocks P2G touched: momentum -> velocity, gravity, walls;
+//            clears the accumulator and the touched flags for the next substep
+//   G2P      one thread per sorted particle: gather, APIC C, F update and material return
+//            mapping, written to the other particle buffer in sorted order (the reorder costs
+//            nothing extra), plus the next substep's cell key
+// Deterministic mode replaces P2G's float atomics with per-cell fixed-order sums and a per-node
+// fixed-order gather (no float atomics anywhere), so two runs are bitwise identical.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <memory>
+
+#include "mpm_world.cuh"
+
+namespace aemp {
+
+// ============================================================================================
+// device helpers
+// ============================================================================================
+template <class T>
+struct Bits;
+template <>
+struct Bits<float> {
+  static __device__ __forceinline__ float pack(uint32_t u) { return __uint_as_float(u); }
+  static __device__ __forceinline__ uint32_t unpack(float f) { return __float_as_uint(f); }
+};
+template <>
+struct Bits<double> {
+  static __device__ __forceinline__ double pack(uint32_t u) { return __longlong_as_double((long long)u); }
+  static __device__ __forceinline__ uint32_t unpack(double d) { return uint32_t(__double_as_longlong(d)); }
+};
+
+__device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ double4 ld4(const double4* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  double2 a = __ldg(q), b = __ldg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 mk4(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
+__device__ __forceinline__ double4 mk4(double a, double b, double c, double d) { return make_double4(a, b, c, d); }
+
+__device__ __forceinline__ void atomic_add4(float4* p, float a, float b, float c, float d) {
+  atomicAdd(p, make_float4(a, b, c, d));  // one 16-byte vector reduction (sm_90+)
+}
+__device__ __forceinline__ void atomic_add4(double4* p, double a, double b, double c, double d) {
+  atomicAdd(&p->x, a);
+  atomicAdd(&p->y, b);
+  atomicAdd(&p->z, c);
+  atomicAdd(&p->w, d);
+}
+
+template <class T>
+__device__ __forceinline__ int floor_to_int(T v) {
+  if (v != v) return 0;  // NaN -> 0, as Rust's `as isize`
+  v = t_clamp(v, T(-1.0e9), T(1.0e9));
+  return int(t_floor(v));
+}
+
+template <class T>
+__device__ __forceinline__ uint32_t node_index(const SceneDev<T>& sc, int i, int j, int k) {
+  uint32_t b = (uint32_t(k >> 2) * uint32_t(sc.nb[1]) + uint32_t(j >> 2)) * uint32_t(sc.nb[0]) + uint32_t(i >> 2);
+  return (sc.blk_off + b) * 64u + ((uint32_t(k & 3) << 4) | (uint32_t(j & 3) << 2) | uint32_t(i & 3));
+}
+
+template <class T>
+__device__ __forceinline__ T sel3(const T* a, int i) {
+  return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]);
+}
+
+// cell key of a position: physics mode base clamped into the grid; reference modes base clamped
+// at 0 (Grid::pos_to_grid, mpm_solver.rs:161-175) and the dead key when the stencil is off-grid
+template <class T>
+__device__ __forceinline__ uint32_t cell_key(const SceneDev<T>& sc, int mode, T x, T y, T z) {
+  T p[3] = {x, y, z};
+  int b[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    int g = floor_to_int((p[a] - sc.origin[a]) * sc.inv_dx - T(0.5));
+    if (mode == AE_MPM_MODE_PHYSICS) {
+      g = min(max(g, 0), sc.n[a] - 1);
+    } else {
+      g = max(g, 0);
+      if (g >= sc.n[a]) return sc.dead_key;
+    }
+    b[a] = g;
+  }
+  return node_index(sc, b[0], b[1], b[2]);
+}
+
+template <class T>
+__device__ __forceinline__ void mark_block(const WorldDev<T>& w, uint32_t gb) {
+  volatile uint32_t* f = w.blk_flag + gb;
+  if (*f == 0u && atomicExch(w.blk_flag + gb, 1u) == 0u) {
+    uint32_t slot = atomicAdd(w.touched_count, 1u);
+    w.touched[slot] = gb;
+  }
+}
+
+template <class T>
+__device__ __forceinline__ const MatDev& mat_of(const WorldDev<T>& w, const SceneDev<T>& sc, uint32_t m) {
+  return w.mats[sc.mat_off + (m < sc.n_mat ? m : sc.n_mat)];
+}
+
+// ============================================================================================
+// per-particle P2G setup
+// ============================================================================================
+template <class T>
+struct P2GPart {
+  int g[3];     // stencil base node per axis (nodes g..g+2)
+  T w[3][3];    // per-axis weights
+  T o[3][3];    // physics: (k - fx) dx;  reference: node position - particle position
+  T dw[3][3];   // reference: N'(k - fx) / dx
+  T m;
+  T v[3];       // physics: m v;  reference/velonly: v
+  T A[9];       // physics: m C - 4 dt V0/dx^2 tau;  reference: C
+  T sv[9];      // reference: dt * V * sigma
+};
+
+template <class T, int MODE>
+__device__ __forceinline__ void p2g_setup(const WorldDev<T>& w, const SceneDev<T>& sc, uint32_t src, P2GPart<T>& p) {
+  using V4 = typename V4T<T>::type;
+  const V4 a0 = ld4(w.in[0] + src);
+  const V4 a4 = ld4(w.in[4] + src);
+  T x[3] = {a0.x, a0.y, a0.z};
+  p.m = a0.w;
+  if (MODE == AE_MPM_MODE_VELOCITY_ONLY) {
+    p.v[0] = a4.x;
+    p.v[1] = a4.y;
+    p.v[2] = a4.z;
+  } else {
+    const V4 a1 = ld4(w.in[1] + src), a2 = ld4(w.in[2] + src), a3 = ld4(w.in[3] + src);
+    const V4 a5 = ld4(w.in[5] + src), a6 = ld4(w.in[6] + src);
+    T F[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
+    T C[9] = {a4.w, a5.x, a5.y, a5.z, a5.w, a6.x, a6.y, a6.z, a6.w};
+    T J = a3.y;
+    const MatDev& md = mat_of(w, sc, Bits<T>::unpack(a3.z) & 0xffffu);
+    if (MODE == AE_MPM_MODE_PHYSICS) {
+      T tau[9];
+      phys_tau(md, F, J, tau);
+      T kst = T(4) * sc.dt * (p.m / T(md.rho)) * sc.inv_dx * sc.inv_dx;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) p.A[k] = p.m * C[k] - kst * tau[k];
+      p.v[0] = p.m * a4.x;
+      p.v[1] = p.m * a4.y;
+      p.v[2] = p.m * a4.z;
+    } else {
+      T st[9];
+      ref_stress(md, F, J, st);
+      T vol = p.m / T(md.rho);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        p.sv[k] = sc.dt * (vol * st[k]);
+        p.A[k] = C[k];
+      }
+      p.v[0] = a4.x;
+      p.v[1] = a4.y;
+      p.v[2] = a4.z;
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    T X = (x[a] - sc.origin[a]) * sc.inv_dx;
+    if (MODE == AE_MPM_MODE_PHYSICS) {
+      int b = floor_to_int(X - T(0.5));
+      T fx = X - T(b);
+      p.g[a] = b;
+      T t0 = T(1.5) - fx, t1 = fx - T(1), t2 = fx - T(0.5);
+      p.w[a][0] = T(0.5) * t0 * t0;
+      p.w[a][1] = T(0.75) - t1 * t1;
+      p.w[a][2] = T(0.5) * t2 * t2;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) p.o[a][k] = (T(k) - fx) * sc.dx;
+    } else {
+      int gu = floor_to_int(X - T(0.5));
+      T fx = X - T(0.5) - T(gu);
+      int g = max(gu, 0);
+      p.g[a] = g;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        p.w[a][k] = b_spline(T(k) - fx);
+        if (MODE == AE_MPM_MODE_REFERENCE) {
+          p.dw[a][k] = b_spline_deriv(T(k) - fx) * sc.inv_dx;
+          p.o[a][k] = (T(g + k) + T(0.5)) * sc.dx + sc.origin[a] - x[a];
+        }
+      }
+    }
+  }
+}
+
+// Contribution of a particle to stencil node (a,b,c); returns false when the node is skipped.
+template <class T, int MODE>
+__device__ __forceinline__ bool p2g_contrib(const SceneDev<T>& sc, const P2GPart<T>& p, int a, int b, int c, T& cm,
+                                            T& cx, T& cy, T& cz) {
+  int X = p.g[0] + a, Y = p.g[1] + b, Z = p.g[2] + c;
+  if (X < 0 || Y < 0 || Z < 0 || X >= sc.n[0] || Y >= sc.n[1] || Z >= sc.n[2]) return false;
+  T wx = sel3(p.w[0], a), wy = sel3(p.w[1], b), wz = sel3(p.w[2], c);
+  if (MODE == AE_MPM_MODE_PHYSICS) {
+    T w = wx * wy * wz;
+    T d0 = sel3(p.o[0], a), d1 = sel3(p.o[1], b), d2 = sel3(p.o[2], c);
+    cm = w * p.m;
+    cx = w * (p.v[0] + p.A[0] * d0 + p.A[1] * d1 + p.A[2] * d2);
+    cy = w * (p.v[1] + p.A[3] * d0 + p.A[4] * d1 + p.A[5] * d2);
+    cz = w * (p.v[2] + p.A[6] * d0 + p.A[7] * d1 + p.A[8] * d2);
+    return true;
+  } else if (MODE == AE_MPM_MODE_REFERENCE) {
+    T w = wx * wy * wz;
+    if (w < T(1e-10)) return false;
+    T d0 = sel3(p.o[0], a), d1 = sel3(p.o[1], b), d2 = sel3(p.o[2], c);
+    T vx = p.v[0] + p.A[0] * d0 + p.A[1] * d1 + p.A[2] * d2;
+    T vy = p.v[1] + p.A[3] * d0 + p.A[4] * d1 + p.A[5] * d2;
+    T vz = p.v[2] + p.A[6] * d0 + p.A[7] * d1 + p.A[8] * d2;
+    T e0 = sel3(p.dw[0], a), e1 = sel3(p.dw[1], b), e2 = sel3(p.dw[2], c);
+    T wm = w * p.m;
+    cm = wm;
+    cx = wm * vx + (p.sv[0] * e0 + p.sv[1] * e1 + p.sv[2] * e2);
+    cy = wm * vy + (p.sv[3] * e0 + p.sv[4] * e1 + p.sv[5] * e2);
+    cz = wm * vz + (p.sv[6] * e0 + p.sv[7] * e1 + p.sv[8] * e2);
+    return true;
+  } else {
+    if (wz < T(1e-10) || wy < T(1e-10)) return false;
+    T w = wx * (wy * wz);
+    if (w < T(1e-10)) return false;
+    T wm = w * p.m;
+    cm = wm;
+    cx = wm * p.v[0];
+    cy = wm * p.v[1];
+    cz = wm * p.v[2];
+    return true;
+  }
+}
+
+// ============================================================================================
+// P2G
+// ============================================================================================
+enum { kVarTile = 1, kVarWarpAgg = 2, kVarGlobal = 3 };
+
+template <class T>
+__device__ __forceinline__ void shared_add4(typename V4T<T>::type* t, T a, T b, T c, T d) {
+  T* q = reinterpret_cast<T*>(t);
+  atomicAdd(q + 0, a);
+  atomicAdd(q + 1, b);
+  atomicAdd(q + 2, c);
+  atomicAdd(q + 3, d);
+}
+
+template <class T, int MODE, int VAR>
+__global__ void __launch_bounds__(512) p2g_kernel(WorldDev<T> w) {
+  using V4 = typename V4T<T>::type;
+  extern __shared__ __align__(16) unsigned char smem[];
+  V4* tile = reinterpret_cast<V4*>(smem);
+  __shared__ int s_lo[3], s_hi[3];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int4 ch = w.chunks[blockIdx.x];
+  const SceneDev<T>& sc = w.scenes[ch.x];
+  if (tid < 3) {
+    s_lo[tid] = INT_MAX;
+    s_hi[tid] = INT_MIN;
+  }
+  __syncthreads();
+  const int j = ch.y + tid;
+  const bool live = j < ch.z;
+  P2GPart<T> p;
+  int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+  bool has = false;
+  if (live) {
+    const uint32_t src = w.perm ? w.perm[j] : uint32_t(j);
+    p2g_setup<T, MODE>(w, sc, src, p);
+    has = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = max(p.g[a], 0);
+      hi[a] = min(p.g[a] + 2, sc.n[a] - 1);
+      if (lo[a] > hi[a]) has = false;
+    }
+  }
+  // block bounding box of all in-grid stencil nodes
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    int l = __reduce_min_sync(0xffffffffu, has ? lo[a] : INT_MAX);
+    int h = __reduce_max_sync(0xffffffffu, has ? hi[a] : INT_MIN);
+    if (lane == 0 && l != INT_MAX) {
+      atomicMin(&s_lo[a], l);
+      atomicMax(&s_hi[a], h);
+    }
+  }
+  __syncthreads();
+  const int L0 = s_lo[0], L1 = s_lo[1], L2 = s_lo[2];
+  const bool any = L0 != INT_MAX;
+  const int D0 = any ? s_hi[0] - L0 + 1 : 0, D1 = any ? s_hi[1] - L1 + 1 : 0, D2 = any ? s_hi[2] - L2 + 1 : 0;
+  const int vol = D0 * D1 * D2;
+  const bool use_tile = VAR != kVarGlobal && any && vol <= w.max_tile_nodes;
+  if (!any) return;
+  if (use_tile) {
+    for (int t = tid; t < vol; t += blockDim.x) tile[t] = mk4(T(0), T(0), T(0), T(0));
+    __syncthreads();
+    if (VAR == kVarWarpAgg) {
+      // lanes of one cell are one run in sorted order: reduce each run with shuffles and let its
+      // first lane add the run's sum to the tile
+      uint32_t key = has ? uint32_t(((p.g[2] - L2 + 2) * (D1 + 4) + (p.g[1] - L1 + 2)) * (D0 + 4) + (p.g[0] - L0 + 2))
+                         : (0x80000000u | uint32_t(lane));
+      uint32_t peers = __match_any_sync(0xffffffffu, key);
+      int first = __ffs(peers) - 1;
+      int cnt = __popc(peers);
+      uint32_t run = (cnt == 32) ? 0xffffffffu : (((1u << cnt) - 1u) << first);
+      bool contiguous = peers == run;
+      int last = first + cnt - 1;
+      int gmax = __reduce_max_sync(0xffffffffu, cnt);
+      if (__all_sync(0xffffffffu, contiguous)) {
+#pragma unroll 1
+        for (int o = 0; o < 27; ++o) {
+          const int a = o % 3, b = (o / 3) % 3, c = o / 9;
+          T cm = T(0), cx = T(0), cy = T(0), cz = T(0);
+          bool ok = has && p2g_contrib<T, MODE>(sc, p, a, b, c, cm, cx, cy, cz);
+          if (!ok) cm = cx = cy = cz = T(0);
+          for (int off = 1; off < gmax; off <<= 1) {
+            T tm = __shfl_down_sync(0xffffffffu, cm, off);
+            T tx = __shfl_down_sync(0xffffffffu, cx, off);
+            T ty = __shfl_down_sync(0xffffffffu, cy, off);
+            T tz = __shfl_down_sync(0xffffffffu, cz, off);
+            if (lane + off <= last) {
+              cm += tm;
+              cx += tx;
+              cy += ty;
+              cz += tz;
+            }
+          }
+          if (has && lane == first) {
+            int X = p.g[0] + a, Y = p.g[1] + b, Z = p.g[2] + c;
+            if (X >= 0 && Y >= 0 && Z >= 0 && X < sc.n[0] && Y < sc.n[1] && Z < sc.n[2] && cm != T(0))
+              shared_add4<T>(tile + ((Z - L2) * D1 + (Y - L1)) * D0 + (X - L0), cm, cx, cy, cz);
+          }
+        }
+      } else if (has) {
+        for (int o = 0; o < 27; ++o) {
+          const int a = o % 3, b = (o / 3) % 3, c = o / 9;
+          T cm, cx, cy, cz;
+          if (p2g_contrib<T, MODE>(sc, p, a, b, c, cm, cx, cy, cz))
+            shared_add4<T>(tile + ((p.g[2] + c - L2) * D1 + (p.g[1] + b - L1)) * D0 + (p.g[0] + a - L0), cm, cx, cy, cz);
+        }
+      }
+    } else if (has) {
+      // lanes of one cell start at different stencil nodes so their shared atomics do not collide
+      const int rot = lane % 27;
+#pragma unroll 3
+      for (int k = 0; k < 27; ++k) {
+        int o = k + rot;
+        o = (o >= 27) ? o - 27 : o;
+        const int a = o % 3, b = (o / 3) % 3, c = o / 9;
+        T cm, cx, cy, cz;
+        if (p2g_contrib<T, MODE>(sc, p, a, b, c, cm, cx, cy, cz))
+          shared_add4<T>(tile + ((p.g[2] + c - L2) * D1 + (p.g[1] + b - L1)) * D0 + (p.g[0] + a - L0), cm, cx, cy, cz);
+      }
+    }
+    __syncthreads();
+    for (int t = tid; t < vol; t += blockDim.x) {
+      V4 v = tile[t];
+      if (v.x != T(0)) {
+        int X = L0 + t % D0, Y = L1 + (t / D0) % D1, Z = L2 + t / (D0 * D1);
+        atomic_add4(w.acc + node_index(sc, X, Y, Z), v.x, v.y, v.z, v.w);
+      }
+    }
+    const int B0 = L0 >> 2, B1 = L1 >> 2, B2 = L2 >> 2;
+    const int E0 = (L0 + D0 - 1) >> 2, E1 = (L1 + D1 - 1) >> 2, E2 = (L2 + D2 - 1) >> 2;
+    const int nbx = E0 - B0 + 1, nby = E1 - B1 + 1, nbz = E2 - B2 + 1;
+    for (int t = tid; t < nbx * nby * nbz; t += blockDim.x) {
+      int bx = B0 + t % nbx, by = B1 + (t / nbx) % nby, bz = B2 + t / (nbx * nby);
+      mark_block(w, sc.blk_off + (uint32_t(bz) * sc.nb[1] + by) * sc.nb[0] + bx);
+    }
+  } else {
+    if (VAR != kVarGlobal && tid == 0) atomicAdd(w.err + 4 * ch.x + 3, 1u);
+    if (has) {
+#pragma unroll 1
+      for (int o = 0; o < 27; ++o) {
+        const int a = o % 3, b = (o / 3) % 3, c = o / 9;
+        T cm, cx, cy, cz;
+        if (p2g_contrib<T, MODE>(sc, p, a, b, c, cm, cx, cy, cz))
+          atomic_add4(w.acc + node_index(sc, p.g[0] + a, p.g[1] + b, p.g[2] + c), cm, cx, cy, cz);
+      }
+      for (int t = 0; t < 8; ++t) {
+        int bx = (t & 1) ? (hi[0] >> 2) : (lo[0] >> 2);
+        int by = (t & 2) ? (hi[1] >> 2) : (lo[1] >> 2);
+        int bz = (t & 4) ? (hi[2] >> 2) : (lo[2] >> 2);
+        mark_block(w, sc.blk_off + (uint32_t(bz) * sc.nb[1] + by) * sc.nb[0] + bx);
+      }
+    }
+  }
+}
+
+// ============================================================================================
+// grid update (momentum -> velocity, gravity, walls); clears accumulator and touched flags
+// ============================================================================================
+template <class T, int MODE>
+__device__ __forceinline__ void grid_velocity(const SceneDev<T>& sc, int i, int j, int k, T m, T px, T py, T pz,
+                                              T& vx, T& vy, T& vz) {
+  vx = vy = vz = T(0);
+  if (MODE == AE_MPM_MODE_PHYSICS) {
+    if (!(m > T(0))) return;
+    vx = px / m + sc.dt * sc.grav[0];
+    vy = py / m + sc.dt * sc.grav[1];
+    vz = pz / m + sc.dt * sc.grav[2];
+    const int mg = sc.wall_margin;
+    const int id[3] = {i, j, k};
+    if (sc.wall_mode == AE_MPM_WALL_STICKY) {
+      bool wall = false;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) wall = wall || id[a] < mg || id[a] >= sc.n[a] - mg;
+      if (wall) vx = vy = vz = T(0);
+    } else {
+      T v[3] = {vx, vy, vz};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        if (id[a] < mg && v[a] < T(0)) v[a] = -v[a] * sc.restitution;
+        if (id[a] >= sc.n[a] - mg && v[a] > T(0)) v[a] = -v[a] * sc.restitution;
+      }
+      vx = v[0];
+      vy = v[1];
+      vz = v[2];
+    }
+  } else {  // Grid::update_parallel (mpm_solver.rs:112-139), force folded into momentum
+    if (!(m > T(1e-12))) return;
+    vx = px / m + sc.grav[0] * sc.dt;
+    vy = py / m + sc.grav[1] * sc.dt;
+    vz = pz / m + sc.grav[2] * sc.dt;
+    if (j == 0) {
+      vy = t_max(vy, T(0));
+      vx *= T(0.9);
+      vz *= T(0.9);
+    }
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void block_coords(const SceneDev<T>& sc, uint32_t gb, int l, int& i, int& j, int& k) {
+  uint32_t lb = gb - sc.blk_off;
+  int bx = int(lb % uint32_t(sc.nb[0]));
+  int by = int((lb / uint32_t(sc.nb[0])) % uint32_t(sc.nb[1]));
+  int bz = int(lb / (uint32_t(sc.nb[0]) * uint32_t(sc.nb[1])));
+  i = bx * 4 + (l & 3);
+  j = by * 4 + ((l >> 2) & 3);
+  k = bz * 4 + (l >> 4);
+}
+
+template <class T, int MODE>
+__global__ void __launch_bounds__(256) grid_update_kernel(WorldDev<T> w, uint32_t* blk_epoch, const uint32_t* epoch) {
+  using V4 = typename V4T<T>::type;
+  const uint32_t count = *reinterpret_cast<volatile uint32_t*>(w.touched_count);
+  const uint32_t ep = *epoch;
+  const int sub = threadIdx.x >> 6, l = threadIdx.x & 63;
+  for (uint32_t t = blockIdx.x * 4 + sub; t < count; t += gridDim.x * 4) {
+    const uint32_t gb = w.touched[t];
+    const SceneDev<T>& sc = w.scenes[w.blk_scene[gb]];
+    int i, j, k;
+    block_coords(sc, gb, l, i, j, k);
+    const uint64_t gi = uint64_t(gb) * 64u + l;
+    V4 a = w.acc[gi];
+    w.acc[gi] = mk4(T(0), T(0), T(0), T(0));
+    T vx, vy, vz;
+    grid_velocity<T, MODE>(sc, i, j, k, a.x, a.y, a.z, a.w, vx, vy, vz);
+    w.vel[gi] = mk4(vx, vy, vz, a.x);
+    if (l == 0) {
+      w.blk_flag[gb] = 0u;
+      blk_epoch[gb] = ep;
+    }
+  }
+}
+
+// ============================================================================================
+// G2P
+// ============================================================================================
+template <class T>
+struct G2POut {
+  T x[3], v[3], C[9], F[9], J;
+  uint32_t err;    // kErr* bits
+  bool fallback;   // FP64 SVD used
+  bool clamped;
+};
+
+template <class T>
+__device__ __forceinline__ void g2p_physics(const WorldDev<T>& w, const SceneDev<T>& sc, const MatDev& md, const T* x0,
+                                            const T* F, T J, G2POut<T>& o) {
+  using V4 = typename V4T<T>::type;
+  int b[3];
+  T wt[3][3], dp[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    T X = (x0[a] - sc.origin[a]) * sc.inv_dx;
+    int bb = floor_to_int(X - T(0.5));
+    T fx = X - T(bb);
+    b[a] = bb;
+    T t0 = T(1.5) - fx, t1 = fx - T(1), t2 = fx - T(0.5);
+    wt[a][0] = T(0.5) * t0 * t0;
+    wt[a][1] = T(0.75) - t1 * t1;
+    wt[a][2] = T(0.5) * t2 * t2;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) dp[a][k] = (T(k) - fx) * sc.dx;
+  }
+  T v[3] = {0, 0, 0}, B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        int X = b[0] + a, Y = b[1] + bb, Z = b[2] + c;
+        if (X < 0 || Y < 0 || Z < 0 || X >= sc.n[0] || Y >= sc.n[1] || Z >= sc.n[2]) continue;
+        T ww = wt[0][a] * wt[1][bb] * wt[2][c];
+        V4 gv = ld4(w.vel + node_index(sc, X, Y, Z));
+        T g3[3] = {gv.x, gv.y, gv.z};
+        T d[3] = {dp[0][a], dp[1][bb], dp[2][c]};
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          v[r] += ww * g3[r];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) B[r * 3 + k] += ww * g3[r] * d[k];
+        }
+      }
+  const T cs = T(4) * sc.inv_dx * sc.inv_dx;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) o.C[k] = cs * B[k];
+  bool nan = false, clamped = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    T nx = x0[a] + sc.dt * v[a];
+    if (!t_finite(nx)) nan = true;
+    T lo = sc.origin[a] + sc.dx, hi = sc.origin[a] + T(sc.n[a] - 2) * sc.dx;
+    T cx = t_fclamp(nx, lo, hi);
+    if (cx != nx) clamped = true;
+    o.x[a] = cx;
+    o.v[a] = v[a];
+  }
+  o.err = (nan ? kErrNaN : 0u) | (clamped ? kErrDomain : 0u);
+  o.clamped = clamped;
+  o.fallback = false;
+  if (md.model == kPhysFluid) {
+    T Jn = J * (T(1) + sc.dt * (o.C[0] + o.C[4] + o.C[8]));
+    o.J = t_max(Jn, T(0.01));
+#pragma unroll
+    for (int k = 0; k < 9; ++k) o.F[k] = F[k];
+    return;
+  }
+  T G[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) G[k] = ((k % 4 == 0) ? T(1) : T(0)) + sc.dt * o.C[k];
+  T nF[9];
+  mm3(G, F, nF);
+  if (md.model == kPhysSnow) {
+    T U[9], sg[3], V[9];
+    o.fallback = svd3_fallback(nF, U, sg, V, w.svd_fallback != 0);
+    T lo = T(1) - T(md.theta_c), hi = T(1) + T(md.theta_s);
+    T scl[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) scl[k] = t_min(t_max(sg[k], lo), hi);
+    o.J = J * ((sg[0] * sg[1] * sg[2]) / (scl[0] * scl[1] * scl[2]));
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        o.F[r * 3 + c] = U[r * 3 + 0] * scl[0] * V[c * 3 + 0] + U[r * 3 + 1] * scl[1] * V[c * 3 + 1] + U[r * 3 + 2] * scl[2] * V[c * 3 + 2];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) o.F[k] = nF[k];
+    o.J = det3(nF);
+  }
+}
+
+// mpm_substep_serial_active / parallel_with_indices G2P (mpm_solver.rs:914-1053, 1206-1325)
+template <class T>
+__device__ __forceinline__ void g2p_reference(const WorldDev<T>& w, const SceneDev<T>& sc, const T* pos, const T* f,
+                                              G2POut<T>& o) {
+  using V4 = typename V4T<T>::type;
+  int g[3];
+  T fx[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    T q = (pos[a] - sc.origin[a]) * sc.inv_dx - T(0.5);
+    int gu = floor_to_int(q);
+    fx[a] = q - T(gu);
+    g[a] = max(gu, 0);
+  }
+  T nv[3] = {0, 0, 0}, nc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, gvm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+  for (int dk = 0; dk < 3; ++dk)
+#pragma unroll 1
+    for (int dj = 0; dj < 3; ++dj)
+#pragma unroll
+      for (int di = 0; di < 3; ++di) {
+        T wx = b_spline(T(di) - fx[0]), wy = b_spline(T(dj) - fx[1]), wz = b_spline(T(dk) - fx[2]);
+        T ww = wx * wy * wz;
+        if (ww < T(1e-10)) continue;
+        int X = g[0] + di, Y = g[1] + dj, Z = g[2] + dk;
+        if (X >= sc.n[0] || Y >= sc.n[1] || Z >= sc.n[2]) continue;
+        V4 gv = ld4(w.vel + node_index(sc, X, Y, Z));
+        if (gv.w < T(1e-12)) continue;
+        T g3[3] = {gv.x, gv.y, gv.z};
+        nv[0] += ww * g3[0];
+        nv[1] += ww * g3[1];
+        nv[2] += ww * g3[2];
+        T d3[3] = {(T(X) + T(0.5)) * sc.dx + sc.origin[0] - pos[0], (T(Y) + T(0.5)) * sc.dx + sc.origin[1] - pos[1],
+                   (T(Z) + T(0.5)) * sc.dx + sc.origin[2] - pos[2]};
+        T scale = T(4) * sc.inv_dx * sc.inv_dx * ww;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) nc[r * 3 + c] += scale * g3[r] * d3[c];
+        T dw[3] = {b_spline_deriv(T(di) - fx[0]) * sc.inv_dx, b_spline_deriv(T(dj) - fx[1]) * sc.inv_dx,
+                   b_spline_deriv(T(dk) - fx[2]) * sc.inv_dx};
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) gvm[r * 3 + c] -= ww * g3[r] * dw[c];
+      }
+  if (!t_finite(nv[0]) || !t_finite(nv[1]) || !t_finite(nv[2])) {
+    nv[0] = nv[1] = nv[2] = T(0);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) nc[k] = T(0);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) nv[a] = t_clamp(nv[a], T(-50), T(50));
+  T np[3] = {pos[0] + nv[0] * sc.dt, pos[1] + nv[1] * sc.dt, pos[2] + nv[2] * sc.dt};
+  if (!t_finite(np[0]) || !t_finite(np[1]) || !t_finite(np[2])) {
+    np[0] = T(6);
+    np[1] = T(5);
+    np[2] = T(6);
+    nv[0] = nv[1] = nv[2] = T(0);
+  }
+  if (np[1] < T(0)) {
+    np[1] = T(0);
+    nv[1] = t_max(nv[1], T(0)) * T(0.5);
+  }
+  const T gmx = T(sc.n[0] - 1) * sc.dx, gmz = T(sc.n[2] - 1) * sc.dx;
+  const T lox = sc.wall_origin ? sc.origin[0] : T(0), loz = sc.wall_origin ? sc.origin[2] : T(0);
+  if (np[0] < lox) {
+    np[0] = lox;
+    nv[0] = t_max(nv[0], T(0)) * T(0.5);
+  } else if (np[0] > gmx + lox) {
+    np[0] = gmx + lox;
+    nv[0] = t_min(nv[0], T(0)) * T(0.5);
+  }
+  if (np[2] < loz) {
+    np[2] = loz;
+    nv[2] = t_max(nv[2], T(0)) * T(0.5);
+  } else if (np[2] > gmz + loz) {
+    np[2] = gmz + loz;
+    nv[2] = t_min(nv[2], T(0)) * T(0.5);
+  }
+  T nf[9];
+  bool valid = true;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      T sum = T(0);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) sum += (((r == k) ? T(1) : T(0)) + gvm[r * 3 + k] * sc.dt) * f[k * 3 + c];
+      nf[r * 3 + c] = sum;
+      if (!t_finite(sum) || t_abs(sum) > T(1e3)) valid = false;
+    }
+  if (valid) {
+    o.J = t_clamp(det3(nf), T(0.1), T(10));
+  } else {
+    ident3(nf);
+    o.J = T(1);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    o.v[a] = nv[a] * sc.damping;
+    o.x[a] = np[a];
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    o.C[k] = nc[k];
+    o.F[k] = nf[k];
+  }
+  o.err = 0;
+  o.fallback = o.clamped = false;
+}
+
+// mpm_substep_velocity_only G2P (mpm_solver.rs:1465-1571); C, F and J are carried unchanged
+template <class T>
+__device__ __forceinline__ void g2p_velonly(const WorldDev<T>& w, const SceneDev<T>& sc, const T* pos, G2POut<T>& o) {
+  using V4 = typename V4T<T>::type;
+  int g[3];
+  T wx[3], wy[3], wz[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    T q = (pos[a] - sc.origin[a]) * sc.inv_dx - T(0.5);
+    int gu = floor_to_int(q);
+    T fx = q - T(gu);
+    g[a] = max(gu, 0);
+    T* wa = a == 0 ? wx : (a == 1 ? wy : wz);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) wa[k] = b_spline(T(k) - fx);
+  }
+  T nv[3] = {0, 0, 0};
+#pragma unroll
+  for (int dk = 0; dk < 3; ++dk) {
+    if (wz[dk] < T(1e-10)) continue;
+    int Z = g[2] + dk;
+    if (Z >= sc.n[2]) continue;
+#pragma unroll
+    for (int dj = 0; dj < 3; ++dj) {
+      if (wy[dj] < T(1e-10)) continue;
+      int Y = g[1] + dj;
+      if (Y >= sc.n[1]) continue;
+      T wyz = wy[dj] * wz[dk];
+#pragma unroll
+      for (int di = 0; di < 3; ++di) {
+        T ww = wx[di] * wyz;
+        if (ww < T(1e-10)) continue;
+        int X = g[0] + di;
+        if (X >= sc.n[0]) continue;
+        V4 gv = ld4(w.vel + node_index(sc, X, Y, Z));
+        if (gv.w < T(1e-12)) continue;
+        nv[0] += ww * gv.x;
+        nv[1] += ww * gv.y;
+        nv[2] += ww * gv.z;
+      }
+    }
+  }
+  if (!t_finite(nv[0]) || !t_finite(nv[1]) || !t_finite(nv[2])) nv[0] = nv[1] = nv[2] = T(0);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) nv[a] = t_clamp(nv[a], T(-50), T(50));
+  T np[3] = {pos[0] + nv[0] * sc.dt, pos[1] + nv[1] * sc.dt, pos[2] + nv[2] * sc.dt};
+  if (!t_finite(np[0]) || !t_finite(np[1]) || !t_finite(np[2])) {
+    np[0] = pos[0];
+    np[1] = pos[1];
+    np[2] = pos[2];
+    nv[0] = nv[1] = nv[2] = T(0);
+  }
+  if (np[1] < T(0)) {
+    np[1] = T(0);
+    nv[1] = t_max(nv[1], T(0)) * T(0.5);
+  }
+  const T gmx = T(sc.n[0] - 1) * sc.dx, gmz = T(sc.n[2] - 1) * sc.dx;
+  if (np[0] < T(0)) {
+    np[0] = T(0);
+    nv[0] = t_max(nv[0], T(0)) * T(0.5);
+  } else if (np[0] > gmx + sc.origin[0]) {
+    np[0] = gmx + sc.origin[0];
+    nv[0] = t_min(nv[0], T(0)) * T(0.5);
+  }
+  if (np[2] < T(0)) {
+    np[2] = T(0);
+    nv[2] = t_max(nv[2], T(0)) * T(0.5);
+  } else if (np[2] > gmz + sc.origin[2]) {
+    np[2] = gmz + sc.origin[2];
+    nv[2] = t_min(nv[2], T(0)) * T(0.5);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    o.v[a] = nv[a] * sc.damping;
+    o.x[a] = np[a];
+  }
+  o.err = 0;
+  o.fallback = o.clamped = false;
+}
+
+template <class T, int MODE>
+__global__ void __launch_bounds__(256) g2p_kernel(WorldDev<T> w, uint32_t* epoch) {
+  using V4 = typename V4T<T>::type;
+  const int4 ch = w.chunks[blockIdx.x];
+  const SceneDev<T>& sc = w.scenes[ch.x];
+  const int j = ch.y + threadIdx.x;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *w.touched_count = 0u;
+    if (w.cell_count) *w.cell_count = 0u;
+    *epoch += 1u;
+  }
+  uint32_t err = 0;
+  bool fb = false, cl = false;
+  if (j < ch.z) {
+    const uint32_t src = w.perm ? w.perm[j] : uint32_t(j);
+    const V4 a0 = ld4(w.in[0] + src), a1 = ld4(w.in[1] + src), a2 = ld4(w.in[2] + src), a3 = ld4(w.in[3] + src);
+    const T x0[3] = {a0.x, a0.y, a0.z};
+    const T F[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
+    G2POut<T> o;
+    if (MODE == AE_MPM_MODE_PHYSICS) {
+      const MatDev& md = mat_of(w, sc, Bits<T>::unpack(a3.z) & 0xffffu);
+      g2p_physics<T>(w, sc, md, x0, F, a3.y, o);
+    } else if (MODE == AE_MPM_MODE_REFERENCE) {
+      g2p_reference<T>(w, sc, x0, F, o);
+    } else {
+      const V4 a4 = ld4(w.in[4] + src), a5 = ld4(w.in[5] + src), a6 = ld4(w.in[6] + src);
+      g2p_velonly<T>(w, sc, x0, o);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) o.F[k] = F[k];
+      o.J = a3.y;
+      o.C[0] = a4.w;
+      o.C[1] = a5.x;
+      o.C[2] = a5.y;
+      o.C[3] = a5.z;
+      o.C[4] = a5.w;
+      o.C[5] = a6.x;
+      o.C[6] = a6.y;
+      o.C[7] = a6.z;
+      o.C[8] = a6.w;
+    }
+    w.out[0][j] = mk4(o.x[0], o.x[1], o.x[2], a0.w);
+    w.out[1][j] = mk4(o.F[0], o.F[1], o.F[2], o.F[3]);
+    w.out[2][j] = mk4(o.F[4], o.F[5], o.F[6], o.F[7]);
+    w.out[3][j] = mk4(o.F[8], o.J, a3.z, a3.w);
+    w.out[4][j] = mk4(o.v[0], o.v[1], o.v[2], o.C[0]);
+    w.out[5][j] = mk4(o.C[1], o.C[2], o.C[3], o.C[4]);
+    w.out[6][j] = mk4(o.C[5], o.C[6], o.C[7], o.C[8]);
+    w.keys[j] = cell_key(sc, MODE, o.x[0], o.x[1], o.x[2]);
+    err = o.err;
+    fb = o.fallback;
+    cl = o.clamped;
+  } else if (j < ch.w) {
+    w.keys[j] = sc.dead_key;
+  }
+  // warp-aggregated error words and counters
+  const uint32_t e = __reduce_or_sync(0xffffffffu, err);
+  const uint32_t nfb = __popc(__ballot_sync(0xffffffffu, fb));
+  const uint32_t ncl = __popc(__ballot_sync(0xffffffffu, cl));
+  if ((threadIdx.x & 31) == 0) {
+    if (e) atomicOr(w.err + 4 * ch.x, e);
+    if (nfb) atomicAdd(w.err + 4 * ch.x + 1, nfb);
+    if (ncl) atomicAdd(w.err + 4 * ch.x + 2, ncl);
+  }
+}
+
+// ============================================================================================
+// deterministic mode: per-cell fixed-order sums, per-node fixed-order gather
+// ============================================================================================
+__global__ void det_heads_kernel(const uint32_t* __restrict__ skeys, uint64_t n, const uint32_t* __restrict__ dead_flag,
+                                 uint32_t* cell_slot, uint32_t* seg_start, uint32_t* cell_count) {
+  uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t k = skeys[i];
+  if (dead_flag[k >> 6]) return;  // spare blocks hold dead and off-grid particles
+  if (i > 0 && skeys[i - 1] == k) return;
+  uint32_t s = atomicAdd(cell_count, 1u);
+  cell_slot[k] = s;
+  seg_start[s] = uint32_t(i);
+}
+
+template <class T, int MODE>
+__global__ void __launch_bounds__(128) det_cellsum_kernel(WorldDev<T> w, uint64_t n_sorted) {
+  using V4 = typename V4T<T>::type;
+  const uint32_t count = *reinterpret_cast<volatile uint32_t*>(w.cell_count);
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < count; s += gridDim.x * blockDim.x) {
+    const uint32_t start = w.seg_start[s];
+    const uint32_t key = w.sorted_keys[start];
+    const SceneDev<T>& sc = w.scenes[w.blk_scene[key >> 6]];
+    T acc[27][4];
+#pragma unroll
+    for (int o = 0; o < 27; ++o) acc[o][0] = acc[o][1] = acc[o][2] = acc[o][3] = T(0);
+    int g0 = 0, g1 = 0, g2 = 0;
+    for (uint64_t i = start; i < n_sorted && w.sorted_keys[i] == key; ++i) {
+      P2GPart<T> p;
+      p2g_setup<T, MODE>(w, sc, w.perm[i], p);
+      g0 = p.g[0];
+      g1 = p.g[1];
+      g2 = p.g[2];
+#pragma unroll
+      for (int o = 0; o < 27; ++o) {
+        T cm, cx, cy, cz;
+        if (p2g_contrib<T, MODE>(sc, p, o % 3, (o / 3) % 3, o / 9, cm, cx, cy, cz)) {
+          acc[o][0] += cm;
+          acc[o][1] += cx;
+          acc[o][2] += cy;
+          acc[o][3] += cz;
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 0; o < 27; ++o) w.cell_rec[uint64_t(s) * 27 + o] = mk4(acc[o][0], acc[o][1], acc[o][2], acc[o][3]);
+    // the cell's stencil spans at most two blocks per axis
+    for (int t = 0; t < 8; ++t) {
+      int X = (t & 1) ? min(g0 + 2, sc.n[0] - 1) : max(g0, 0);
+      int Y = (t & 2) ? min(g1 + 2, sc.n[1] - 1) : max(g1, 0);
+      int Z = (t & 4) ? min(g2 + 2, sc.n[2] - 1) : max(g2, 0);
+      mark_block(w, sc.blk_off + (uint32_t(Z >> 2) * sc.nb[1] + (Y >> 2)) * sc.nb[0] + (X >> 2));
+    }
+  }
+}
+
+template <class T, int MODE>
+__global__ void __launch_bounds__(256) det_gather_kernel(WorldDev<T> w, uint32_t* blk_epoch, const uint32_t* epoch) {
+  using V4 = typename V4T<T>::type;
+  const uint32_t count = *reinterpret_cast<volatile uint32_t*>(w.touched_count);
+  const uint32_t ep = *epoch;
+  const int sub = threadIdx.x >> 6, l = threadIdx.x & 63;
+  for (uint32_t t = blockIdx.x * 4 + sub; t < count; t += gridDim.x * 4) {
+    const uint32_t gb = w.touched[t];
+    const SceneDev<T>& sc = w.scenes[w.blk_scene[gb]];
+    int i, j, k;
+    block_coords(sc, gb, l, i, j, k);
+    T m = 0, px = 0, py = 0, pz = 0;
+    if (i < sc.n[0] && j < sc.n[1] && k < sc.n[2]) {
+      // node (i,j,k) receives offset (a,b,c) of the cell based at (i-a, j-b, k-c), in fixed order
+#pragma unroll 1
+      for (int o = 0; o < 27; ++o) {
+        const int a = o % 3, b = (o / 3) % 3, c = o / 9;
+        int X = i - a, Y = j - b, Z = k - c;
+        if (X < 0 || Y < 0 || Z < 0) continue;
+        uint32_t s = w.cell_slot[node_index(sc, X, Y, Z)];
+        if (s == 0xffffffffu) continue;
+        V4 r = w.cell_rec[uint64_t(s) * 27 + o];
+        m += r.x;
+        px += r.y;
+        py += r.z;
+        pz += r.w;
+      }
+    }
+    T vx, vy, vz;
+    grid_velocity<T, MODE>(sc, i, j, k, m, px, py, pz, vx, vy, vz);
+    w.vel[uint64_t(gb) * 64u + l] = mk4(vx, vy, vz, m);
+    if (l == 0) {
+      w.blk_flag[gb] = 0u;
+      blk_epoch[gb] = ep;
+    }
+  }
+}
+
+__global__ void det_reset_kernel(const uint32_t* __restrict__ seg_start, const uint32_t* __restrict__ skeys,
+                                 const uint32_t* cell_count, uint32_t* cell_slot) {
+  const uint32_t count = *reinterpret_cast<const volatile uint32_t*>(cell_count);
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < count; s += gridDim.x * blockDim.x)
+    cell_slot[skeys[seg_start[s]]] = 0xffffffffu;
+}
+
+// ============================================================================================
+// keys, pack/unpack, totals, grid export
+// ============================================================================================
+template <class T, int MODE>
+__global__ void init_keys_kernel(WorldDev<T> w) {
+  const int4 ch = w.chunks[blockIdx.x];
+  const SceneDev<T>& sc = w.scenes[ch.x];
+  const int j = ch.y + threadIdx.x;
+  if (j < ch.z) {
+    auto a0 = ld4(w.in[0] + j);
+    w.keys[j] = cell_key(sc, MODE, a0.x, a0.y, a0.z);
+  } else if (j < ch.w) {
+    w.keys[j] = sc.dead_key;
+  }
+}
+
+// staging layout (elements of T): pos 3n | vel 3n | F 9n | J n | C 9n | mass n | then u16 mat n
+template <class T>
+__global__ void pack_kernel(typename V4T<T>::type* const* dst, const T* __restrict__ st, uint64_t n, uint32_t p_off) {
+  uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const T* pos = st;
+  const T* vel = st + 3 * n;
+  const T* F = st + 6 * n;
+  const T* J = st + 15 * n;
+  const T* C = st + 16 * n;
+  const T* mass = st + 25 * n;
+  const uint16_t* mat = reinterpret_cast<const uint16_t*>(st + 26 * n);
+  uint64_t s = p_off + i;
+  dst[0][s] = mk4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], mass[i]);
+  dst[1][s] = mk4(F[9 * i], F[9 * i + 1], F[9 * i + 2], F[9 * i + 3]);
+  dst[2][s] = mk4(F[9 * i + 4], F[9 * i + 5], F[9 * i + 6], F[9 * i + 7]);
+  dst[3][s] = mk4(F[9 * i + 8], J[i], Bits<T>::pack(uint32_t(mat[i])), Bits<T>::pack(uint32_t(i)));
+  dst[4][s] = mk4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], C[9 * i]);
+  dst[5][s] = mk4(C[9 * i + 1], C[9 * i + 2], C[9 * i + 3], C[9 * i + 4]);
+  dst[6][s] = mk4(C[9 * i + 5], C[9 * i + 6], C[9 * i + 7], C[9 * i + 8]);
+}
+
+template <class T>
+__global__ void unpack_kernel(const typename V4T<T>::type* const* src, T* __restrict__ st, uint64_t n, uint32_t p_off) {
+  using V4 = typename V4T<T>::type;
+  uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t s = p_off + i;
+  V4 a0 = src[0][s], a1 = src[1][s], a2 = src[2][s], a3 = src[3][s], a4 = src[4][s], a5 = src[5][s], a6 = src[6][s];
+  uint64_t o = Bits<T>::unpack(a3.w);
+  if (o >= n) return;
+  T* pos = st;
+  T* vel = st + 3 * n;
+  T* F = st + 6 * n;
+  T* J = st + 15 * n;
+  T* C = st + 16 * n;
+  T* mass = st + 25 * n;
+  uint16_t* mat = reinterpret_cast<uint16_t*>(st + 26 * n);
+  pos[3 * o] = a0.x;
+  pos[3 * o + 1] = a0.y;
+  pos[3 * o + 2] = a0.z;
+  mass[o] = a0.w;
+  const T f[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
+  const T c[9] = {a4.w, a5.x, a5.y, a5.z, a5.w, a6.x, a6.y, a6.z, a6.w};
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    F[9 * o + k] = f[k];
+    C[9 * o + k] = c[k];
+  }
+  J[o] = a3.y;
+  vel[3 * o] = a4.x;
+  vel[3 * o + 1] = a4.y;
+  vel[3 * o + 2] = a4.z;
+  mat[o] = uint16_t(Bits<T>::unpack(a3.z) & 0xffffu);
+}
+
+// per-chunk FP64 partial sums [mass, px, py, pz, ke]; fixed reduction order (deterministic)
+template <class T>
+__global__ void __launch_bounds__(256) totals_kernel(WorldDev<T> w, double* partial) {
+  __shared__ double sm[8][5];
+  const int4 ch = w.chunks[blockIdx.x];
+  const int j = ch.y + threadIdx.x;
+  double v[5] = {0, 0, 0, 0, 0};
+  if (j < ch.z) {
+    auto a0 = ld4(w.in[0] + j);
+    auto a4 = ld4(w.in[4] + j);
+    double m = double(a0.w), vx = double(a4.x), vy = double(a4.y), vz = double(a4.z);
+    v[0] = m;
+    v[1] = m * vx;
+    v[2] = m * vy;
+    v[3] = m * vz;
+    v[4] = 0.5 * m * (vx * vx + vy * vy + vz * vz);
+  }
+#pragma unroll
+  for (int k = 0; k < 5; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int k = 0; k < 5; ++k) sm[wi][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) / 32;
+    for (int k = 0; k < 5; ++k) {
+      double s = 0;
+      for (int q = 0; q < nw; ++q) s += sm[q][k];
+      partial[uint64_t(blockIdx.x) * 5 + k] = s;
+    }
+  }
+}
+
+// dense reference-order grid export of scene 0's last substep (mass, velocity)
+template <class T>
+__global__ void grid_export_kernel(const typename V4T<T>::type* vel, const SceneDev<T>* scp, const uint32_t* blk_epoch,
+                                   const uint32_t* epoch, float* mass_out, float* vel_out) {
+  const SceneDev<T>& sc = *scp;
+  uint64_t idx = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  uint64_t nn = uint64_t(sc.n[0]) * sc.n[1] * sc.n[2];
+  if (idx >= nn) return;
+  int i = int(idx % sc.n[0]), j = int((idx / sc.n[0]) % sc.n[1]), k = int(idx / (uint64_t(sc.n[0]) * sc.n[1]));
+  uint32_t gi = node_index(sc, i, j, k);
+  bool fresh = blk_epoch[gi >> 6] + 1u == *epoch;
+  auto v = vel[gi];
+  mass_out[idx] = fresh ? float(v.w) : 0.0f;
+  vel_out[3 * idx] = fresh ? float(v.x) : 0.0f;
+  vel_out[3 * idx + 1] = fresh ? float(v.y) : 0.0f;
+  vel_out[3 * idx + 2] = fresh ? float(v.z) : 0.0f;
+}
+
+// ============================================================================================
+// host side
+// ============================================================================================
+int device_sm_count() {
+  static int cached[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    cached[dev] = v > 0 ? v : 148;
+  }
+  return cached[dev];
+}
+
+static MatDev mat_dev(const ae_mpm_material& m, int model) {
+  MatDev d{};
+  float nu = std::min(std::max(m.poisson_ratio, -0.999f), 0.4999f);
+  d.model = model;
+  d.lambda = m.young_modulus * nu / ((1.0f + nu) * (1.0f - 2.0f * nu));
+  d.mu = m.young_modulus / (2.0f * (1.0f + nu));
+  d.bulk = m.young_modulus / (3.0f * (1.0f - 2.0f * nu));
+  if (model >= kPhysJelly && m.bulk_modulus > 0.0f) d.bulk = m.bulk_modulus;
+  d.rho = m.density;
+  d.yield_stress = m.yield_stress;
+  d.friction_angle = m.friction_angle;
+  d.cohesion = m.cohesion;
+  d.theta_c = m.theta_c;
+  d.theta_s = m.theta_s;
+  d.xi = m.hardening_xi;
+  return d;
+}
+
+static uint64_t blocks_of(const ae_mpm_scene_desc& d) {
+  return uint64_t((d.n[0] + 3) / 4) * ((d.n[1] + 3) / 4) * ((d.n[2] + 3) / 4) + 1;  // + spare block
+}
+
+uint64_t scene_device_bytes(const ae_mpm_scene_desc& d, int precision) {
+  uint64_t es = precision == 64 ? 8 : 4;
+  uint64_t parts = d.max_particles * (2 * 7 * 4 * es + 5 * 4 + 26 * es + 2);
+  uint64_t grid = blocks_of(d) * 64 * (2 * 4 * es) + blocks_of(d) * 16;
+  return parts + grid;
+}
+
+#define AE_TRY(call)                                                                           \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) {                                                                   \
+      err = std::string(#call) + ": " + cudaGetErrorString(e_);                                \
+      return (e_ == cudaErrorMemoryAllocation) ? AE_MPM_ENOMEM : AE_MPM_ECUDA;                 \
+    }                                                                                          \
+  } while (0)
+
+// the caller's arrays, from an ae_mpm_particles (f32) or ae_mpm_particles_f64 (f64) view
+template <class T>
+struct HostView {
+  T* f[6];  // pos, vel, strain, jacobian, c, mass
+  uint16_t* mat;
+};
+template <class T>
+HostView<T> host_view(const void* host);
+template <>
+HostView<float> host_view<float>(const void* host) {
+  const auto* h = static_cast<const ae_mpm_particles*>(host);
+  return HostView<float>{{h->pos, h->vel, h->strain, h->jacobian, h->c, h->mass}, h->material_idx};
+}
+template <>
+HostView<double> host_view<double>(const void* host) {
+  const auto* h = static_cast<const ae_mpm_particles_f64*>(host);
+  return HostView<double>{{h->pos, h->vel, h->strain, h->jacobian, h->c, h->mass}, h->material_idx};
+}
+
+template <class T>
+class World final : public WorldBase {
+ public:
+  using V4 = typename V4T<T>::type;
+
+  ~World() override { release(); }
+
+  int init(const ae_mpm_scene_desc* sc, uint32_t n, const ae_mpm_exec_opts& o) {
+    opts_ = o;
+    if (n == 0) {
+      err = "a world needs at least one scene";
+      return AE_MPM_EINVAL;
+    }
+    mode_ = sc[0].mode;
+    if (mode_ < AE_MPM_MODE_PHYSICS || mode_ > AE_MPM_MODE_VELOCITY_ONLY) {
+      err = "unknown substep mode";
+      return AE_MPM_EINVAL;
+    }
+    uint64_t blk = 0, cap = 0;
+    for (uint32_t s = 0; s < n; ++s) {
+      const ae_mpm_scene_desc& d = sc[s];
+      if (d.mode != mode_) {
+        err = "all scenes of a world must use the same substep mode";
+        return AE_MPM_EINVAL;
+      }
+      const uint32_t nmin = mode_ == AE_MPM_MODE_PHYSICS ? 4u : 1u;
+      if (d.n[0] < nmin || d.n[1] < nmin || d.n[2] < nmin || !(d.dx > 0.0f) || !(d.dt >= 0.0f)) {
+        err = "scene " + std::to_string(s) + ": grid needs >= " + std::to_string(nmin) +
+              " nodes per axis, dx > 0 and dt >= 0";
+        return AE_MPM_EINVAL;
+      }
+      if (d.n_materials == 0 || !d.materials) {
+        err = "scene " + std::to_string(s) + ": material table is empty";
+        return AE_MPM_EINVAL;
+      }
+      if (mode_ == AE_MPM_MODE_PHYSICS && d.wall_margin < 1) {
+        err = "physics mode needs wall_margin >= 1";
+        return AE_MPM_EINVAL;
+      }
+      descs_.push_back(d);
+      mats_.emplace_back(d.materials, d.materials + d.n_materials);
+      blk += blocks_of(d);
+      cap += d.max_particles;
+    }
+    if (blk * 64 >= (1ull << 31) || cap >= (1ull << 31)) {
+      err = "world too large for 32-bit keys";
+      return AE_MPM_EINVAL;
+    }
+    total_blocks_ = blk;
+    total_cap_ = cap;
+    key_bits_ = 1;
+    while ((1ull << key_bits_) < blk * 64) ++key_bits_;
+    if (opts_.precision != 32 && opts_.precision != 64) opts_.precision = sizeof(T) == 8 ? 64 : 32;
+    if (opts_.sort_interval < 1) opts_.sort_interval = 1;
+    if (opts_.block_threads != 128 && opts_.block_threads != 256) opts_.block_threads = 256;
+    if (opts_.p2g_variant < kVarTile || opts_.p2g_variant > kVarGlobal) opts_.p2g_variant = kVarTile;
+    AE_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    // scene table and materials
+    uint64_t mat_off = 0, boff = 0, poff = 0;
+    std::vector<uint32_t> blk_scene(blk), dead(blk, 0u);
+    for (uint32_t s = 0; s < n; ++s) {
+      const ae_mpm_scene_desc& d = descs_[s];
+      SceneDev<T> h{};
+      h.mode = d.mode;
+      h.wall_mode = d.wall_mode;
+      h.wall_margin = d.wall_margin;
+      h.wall_origin = d.wall_origin;
+      for (int a = 0; a < 3; ++a) {
+        h.n[a] = int(d.n[a]);
+        h.nb[a] = int((d.n[a] + 3) / 4);
+      }
+      h.blk_off = uint32_t(boff);
+      uint64_t nbk = blocks_of(d);
+      h.dead_key = uint32_t((boff + nbk - 1) * 64);
+      for (uint64_t b = 0; b < nbk; ++b) blk_scene[boff + b] = s;
+      dead[boff + nbk - 1] = 1u;
+      boff += nbk;
+      h.mat_off = uint32_t(mat_off);
+      h.n_mat = d.n_materials;
+      for (uint32_t k = 0; k < d.n_materials; ++k) h_mats_.push_back(mat_dev(d.materials[k], d.materials[k].model));
+      // out-of-range material index: materials[0]'s parameters; the reference pairs them with
+      // the neo-Hookean model (mpm_solver.rs:840-841)
+      h_mats_.push_back(mat_dev(d.materials[0], mode_ == AE_MPM_MODE_PHYSICS ? d.materials[0].model : kNeoHookean));
+      mat_off += d.n_materials + 1;
+      h.p_off = uint32_t(poff);
+      h.p_cap = uint32_t(d.max_particles);
+      h.p_count = 0;
+      poff += d.max_particles;
+      fill_scene_params(h, d);
+      h_scenes_.push_back(h);
+    }
+    AE_TRY(dmalloc(&d_scenes_, sizeof(SceneDev<T>) * n));
+    AE_TRY(dmalloc(&d_mats_, sizeof(MatDev) * h_mats_.size()));
+    AE_TRY(cudaMemcpy(d_mats_, h_mats_.data(), sizeof(MatDev) * h_mats_.size(), cudaMemcpyHostToDevice));
+    AE_TRY(dmalloc(&blk_scene_, sizeof(uint32_t) * blk));
+    AE_TRY(cudaMemcpy(blk_scene_, blk_scene.data(), sizeof(uint32_t) * blk, cudaMemcpyHostToDevice));
+    AE_TRY(dmalloc(&dead_blk_, sizeof(uint32_t) * blk));
+    AE_TRY(cudaMemcpy(dead_blk_, dead.data(), sizeof(uint32_t) * blk, cudaMemcpyHostToDevice));
+    // particles
+    const uint64_t pc = std::max<uint64_t>(cap, 1);
+    for (int k = 0; k < 7; ++k) {
+      AE_TRY(dmalloc(&bufA_[k], sizeof(V4) * pc));
+      AE_TRY(dmalloc(&bufB_[k], sizeof(V4) * pc));
+      AE_TRY(cudaMemset(bufA_[k], 0, sizeof(V4) * pc));
+      AE_TRY(cudaMemset(bufB_[k], 0, sizeof(V4) * pc));
+    }
+    AE_TRY(dmalloc(&d_ptrA_, sizeof(V4*) * 7));
+    AE_TRY(dmalloc(&d_ptrB_, sizeof(V4*) * 7));
+    AE_TRY(cudaMemcpy(d_ptrA_, bufA_, sizeof(V4*) * 7, cudaMemcpyHostToDevice));
+    AE_TRY(cudaMemcpy(d_ptrB_, bufB_, sizeof(V4*) * 7, cudaMemcpyHostToDevice));
+    AE_TRY(dmalloc(&keys_, sizeof(uint32_t) * pc));
+    AE_TRY(sort_scratch_alloc(sort_, pc, alloc_ ? &World::sort_alloc : nullptr, alloc_));
+    // grid
+    const uint64_t nodes = blk * 64;
+    AE_TRY(dmalloc(&acc_, sizeof(V4) * nodes));
+    AE_TRY(cudaMemset(acc_, 0, sizeof(V4) * nodes));
+    AE_TRY(dmalloc(&vel_, sizeof(V4) * nodes));
+    AE_TRY(cudaMemset(vel_, 0, sizeof(V4) * nodes));
+    AE_TRY(dmalloc(&blk_flag_, sizeof(uint32_t) * blk));
+    AE_TRY(cudaMemset(blk_flag_, 0, sizeof(uint32_t) * blk));
+    AE_TRY(dmalloc(&blk_epoch_, sizeof(uint32_t) * blk));
+    AE_TRY(cudaMemset(blk_epoch_, 0xff, sizeof(uint32_t) * blk));
+    AE_TRY(dmalloc(&touched_, sizeof(uint32_t) * blk));
+    AE_TRY(dmalloc(&counters_, sizeof(uint32_t) * 4));
+    AE_TRY(cudaMemset(counters_, 0, sizeof(uint32_t) * 4));
+    AE_TRY(dmalloc(&err_, sizeof(uint32_t) * 4 * n));
+    AE_TRY(cudaMemset(err_, 0, sizeof(uint32_t) * 4 * n));
+    if (opts_.deterministic) {
+      AE_TRY(dmalloc(&cell_slot_, sizeof(uint32_t) * nodes));
+      AE_TRY(cudaMemset(cell_slot_, 0xff, sizeof(uint32_t) * nodes));
+      AE_TRY(dmalloc(&seg_start_, sizeof(uint32_t) * pc));
+      AE_TRY(dmalloc(&cell_rec_, sizeof(V4) * 27 * pc));
+    }
+    return AE_MPM_OK;
+  }
+
+  void fill_scene_params(SceneDev<T>& h, const ae_mpm_scene_desc& d) {
+    h.dx = T(d.dx);
+    h.inv_dx = T(1) / T(d.dx);
+    h.dt = T(d.dt);
+    h.restitution = T(d.restitution);
+    h.damping = T(d.damping);
+    h.wall_mode = d.wall_mode;
+    h.wall_margin = d.wall_margin;
+    h.wall_origin = d.wall_origin;
+    for (int a = 0; a < 3; ++a) {
+      h.origin[a] = T(d.origin[a]);
+      h.grav[a] = T(d.gravity[a]);
+    }
+    if (sizeof(T) == 4) h.inv_dx = T(1.0f / d.dx);  // f32: the reference's `1.0 / dx` in f32
+  }
+
+  int set_scene_params(uint32_t s, const ae_mpm_scene_desc& d) override {
+    if (s >= h_scenes_.size()) {
+      err = "unknown scene";
+      return AE_MPM_ENOTFOUND;
+    }
+    if (d.n[0] != uint32_t(h_scenes_[s].n[0]) || d.n[1] != uint32_t(h_scenes_[s].n[1]) || d.n[2] != uint32_t(h_scenes_[s].n[2])) {
+      err = "grid size of a resident scene cannot change";
+      return AE_MPM_EINVAL;
+    }
+    if (d.n_materials != h_scenes_[s].n_mat || !d.materials) {
+      err = "material count of a resident scene cannot change";
+      return AE_MPM_EINVAL;
+    }
+    fill_scene_params(h_scenes_[s], d);
+    for (uint32_t k = 0; k < d.n_materials; ++k) h_mats_[h_scenes_[s].mat_off + k] = mat_dev(d.materials[k], d.materials[k].model);
+    h_mats_[h_scenes_[s].mat_off + d.n_materials] =
+        mat_dev(d.materials[0], mode_ == AE_MPM_MODE_PHYSICS ? d.materials[0].model : kNeoHookean);
+    scenes_dirty_ = true;
+    mats_dirty_ = true;
+    return AE_MPM_OK;
+  }
+
+  int upload(uint32_t s, const void* host, uint64_t n, bool f64) override {
+    if (s >= h_scenes_.size()) {
+      err = "unknown scene";
+      return AE_MPM_ENOTFOUND;
+    }
+    if ((sizeof(T) == 8) != f64) {
+      err = "particle view precision does not match the world precision";
+      return AE_MPM_EINVAL;
+    }
+    if (n > h_scenes_[s].p_cap) {
+      err = "scene " + std::to_string(s) + ": " + std::to_string(n) + " particles exceed max_particles " +
+            std::to_string(h_scenes_[s].p_cap);
+      return AE_MPM_EINVAL;
+    }
+    HostView<T> hv = host_view<T>(host);
+    const T* const* f = hv.f;
+    if (n > 0 && (!f[0] || !f[1] || !f[2] || !f[3] || !f[4] || !f[5] || !hv.mat)) {
+      err = "particle view has a null array";
+      return AE_MPM_EINVAL;
+    }
+    int rc = ensure_stage(n);
+    if (rc) return rc;
+    if (n > 0) {
+      AE_TRY(cudaMemcpyAsync(stage_, f[0], sizeof(T) * 3 * n, cudaMemcpyHostToDevice, stream_));
+      AE_TRY(cudaMemcpyAsync(stage_ + 3 * n, f[1], sizeof(T) * 3 * n, cudaMemcpyHostToDevice, stream_));
+      AE_TRY(cudaMemcpyAsync(stage_ + 6 * n, f[2], sizeof(T) * 9 * n, cudaMemcpyHostToDevice, stream_));
+      AE_TRY(cudaMemcpyAsync(stage_ + 15 * n, f[3], sizeof(T) * n, cudaMemcpyHostToDevice, stream_));
+      AE_TRY(cudaMemcpyAsync(stage_ + 16 * n, f[4], sizeof(T) * 9 * n, cudaMemcpyHostToDevice, stream_));
+      AE_TRY(cudaMemcpyAsync(stage_ + 25 * n, f[5], sizeof(T) * n, cudaMemcpyHostToDevice, stream_));
+      AE_TRY(cudaMemcpyAsync(stage_ + 26 * n, hv.mat, sizeof(uint16_t) * n, cudaMemcpyHostToDevice, stream_));
+      pack_kernel<T><<<unsigned((n + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), stage_, n, h_scenes_[s].p_off);
+      AE_TRY(cudaGetLastError());
+    }
+    h_scenes_[s].p_count = uint32_t(n);
+    scenes_dirty_ = chunks_dirty_ = keys_stale_ = true;
+    return AE_MPM_OK;
+  }
+
+  int download(uint32_t s, void* host, bool f64) override {
+    if (s >= h_scenes_.size()) {
+      err = "unknown scene";
+      return AE_MPM_ENOTFOUND;
+    }
+    if ((sizeof(T) == 8) != f64) {
+      err = "particle view precision does not match the world precision";
+      return AE_MPM_EINVAL;
+    }
+    const uint64_t n = h_scenes_[s].p_count;
+    HostView<T> hv = host_view<T>(host);
+    T* const* f = hv.f;
+    if (n == 0) return AE_MPM_OK;
+    if (!f[0] || !f[1] || !f[2] || !f[3] || !f[4] || !f[5] || !hv.mat) {
+      err = "particle view has a null array";
+      return AE_MPM_EINVAL;
+    }
+    int rc = ensure_stage(n);
+    if (rc) return rc;
+    unpack_kernel<T><<<unsigned((n + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), stage_, n, h_scenes_[s].p_off);
+    AE_TRY(cudaGetLastError());
+    AE_TRY(cudaMemcpyAsync(f[0], stage_, sizeof(T) * 3 * n, cudaMemcpyDeviceToHost, stream_));
+    AE_TRY(cudaMemcpyAsync(f[1], stage_ + 3 * n, sizeof(T) * 3 * n, cudaMemcpyDeviceToHost, stream_));
+    AE_TRY(cudaMemcpyAsync(f[2], stage_ + 6 * n, sizeof(T) * 9 * n, cudaMemcpyDeviceToHost, stream_));
+    AE_TRY(cudaMemcpyAsync(f[3], stage_ + 15 * n, sizeof(T) * n, cudaMemcpyDeviceToHost, stream_));
+    AE_TRY(cudaMemcpyAsync(f[4], stage_ + 16 * n, sizeof(T) * 9 * n, cudaMemcpyDeviceToHost, stream_));
+    AE_TRY(cudaMemcpyAsync(f[5], stage_ + 25 * n, sizeof(T) * n, cudaMemcpyDeviceToHost, stream_));
+    AE_TRY(cudaMemcpyAsync(hv.mat, stage_ + 26 * n, sizeof(uint16_t) * n, cudaMemcpyDeviceToHost, stream_));
+    AE_TRY(cudaStreamSynchronize(stream_));
+    return AE_MPM_OK;
+  }
+
+  int step(uint32_t n) override {
+    launches_ = 0;
+    int rc = prepare();
+    if (rc) return rc;
+    if (n == 0) return AE_MPM_OK;
+    if (keys_stale_) {
+      WorldDev<T> w = dev(false);
+      launch_init_keys(w);
+      keys_stale_ = false;
+    }
+    const int interval = opts_.deterministic ? 1 : opts_.sort_interval;
+    const uint64_t period = (interval % 2 == 0) ? uint64_t(interval) : uint64_t(2 * interval);
+    uint32_t left = n;
+    if (opts_.use_graph) {
+      while (left > 0 && substep_ % period != 0) {
+        substep_eager();
+        --left;
+      }
+      if (left >= period) {
+        rc = ensure_graph(period);
+        if (rc) return rc;
+        while (left >= period) {
+          AE_TRY(cudaGraphLaunch(graph_, stream_));
+          launches_ += graph_launches_;
+          substep_ += period;
+          left -= uint32_t(period);
+        }
+      }
+    }
+    while (left > 0) {
+      substep_eager();
+      --left;
+    }
+    AE_TRY(cudaGetLastError());
+    return AE_MPM_OK;
+  }
+
+  int sync() override {
+    AE_TRY(cudaStreamSynchronize(stream_));
+    std::vector<uint32_t> e(4 * h_scenes_.size());
+    AE_TRY(cudaMemcpy(e.data(), err_, sizeof(uint32_t) * e.size(), cudaMemcpyDeviceToHost));
+    uint32_t any = 0;
+    for (size_t s = 0; s < h_scenes_.size(); ++s) any |= e[4 * s];
+    if (any & kErrNaN) {
+      err = "a particle position became non-finite";
+      return AE_MPM_ENAN;
+    }
+    if (any & kErrDomain) {
+      err = "particles reached the grid's outer ring and were clamped back";
+      return AE_MPM_EDOMAIN;
+    }
+    return AE_MPM_OK;
+  }
+
+  int totals(uint32_t s, double out[5]) override {
+    if (s >= h_scenes_.size()) {
+      err = "unknown scene";
+      return AE_MPM_ENOTFOUND;
+    }
+    int rc = prepare();
+    if (rc) return rc;
+    if (n_chunks_ == 0) {
+      for (int k = 0; k < 5; ++k) out[k] = 0;
+      return AE_MPM_OK;
+    }
+    if (!partial_) AE_TRY(dmalloc(&partial_, sizeof(double) * 5 * n_chunks_alloc_));
+    WorldDev<T> w = dev(false);
+    totals_kernel<T><<<n_chunks_, chunk_threads_, 0, stream_>>>(w, partial_);
+    AE_TRY(cudaGetLastError());
+    std::vector<double> h(5 * size_t(n_chunks_));
+    AE_TRY(cudaMemcpyAsync(h.data(), partial_, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream_));
+    AE_TRY(cudaStreamSynchronize(stream_));
+    for (int k = 0; k < 5; ++k) out[k] = 0;
+    for (int c = 0; c < n_chunks_; ++c)
+      if (uint32_t(h_chunks_[c].x) == s)
+        for (int k = 0; k < 5; ++k) out[k] += h[5 * size_t(c) + k];
+    return AE_MPM_OK;
+  }
+
+  int errors(uint32_t s, uint32_t* word, uint64_t counters[3]) override {
+    if (s >= h_scenes_.size()) {
+      err = "unknown scene";
+      return AE_MPM_ENOTFOUND;
+    }
+    uint32_t e[4];
+    AE_TRY(cudaStreamSynchronize(stream_));
+    AE_TRY(cudaMemcpy(e, err_ + 4 * s, sizeof(e), cudaMemcpyDeviceToHost));
+    AE_TRY(cudaMemset(err_ + 4 * s, 0, sizeof(e)));
+    if (word) *word = e[0];
+    if (counters) {
+      counters[0] = e[1];
+      counters[1] = e[2];
+      counters[2] = e[3];
+    }
+    return AE_MPM_OK;
+  }
+
+  int grid_download(uint32_t s, float* mass, float* vel, uint64_t n_nodes) override {
+    if (s >= h_scenes_.size()) {
+      err = "unknown scene";
+      return AE_MPM_ENOTFOUND;
+    }
+    const SceneDev<T>& h = h_scenes_[s];
+    uint64_t nn = uint64_t(h.n[0]) * h.n[1] * h.n[2];
+    if (n_nodes != nn || !mass || !vel) {
+      err = "grid download needs nx*ny*nz nodes";
+      return AE_MPM_EINVAL;
+    }
+    float *dm = nullptr, *dv = nullptr;
+    AE_TRY(dmalloc(&dm, sizeof(float) * nn));
+    AE_TRY(dmalloc(&dv, sizeof(float) * 3 * nn));
+    grid_export_kernel<T><<<unsigned((nn + 255) / 256), 256, 0, stream_>>>(vel_, d_scenes_ + s, blk_epoch_, counters_ + 2,
+                                                                           dm, dv);
+    cudaError_t e1 = cudaMemcpyAsync(mass, dm, sizeof(float) * nn, cudaMemcpyDeviceToHost, stream_);
+    cudaError_t e2 = cudaMemcpyAsync(vel, dv, sizeof(float) * 3 * nn, cudaMemcpyDeviceToHost, stream_);
+    cudaError_t e3 = cudaStreamSynchronize(stream_);
+    dfree(dm);
+    dfree(dv);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+      err = "grid download failed";
+      return AE_MPM_ECUDA;
+    }
+    return AE_MPM_OK;
+  }
+
+  int snapshot(bool restore) override {
+    const uint64_t pc = std::max<uint64_t>(total_cap_, 1);
+    if (!restore) {
+      for (int k = 0; k < 7; ++k) {
+        if (!snap_[k]) AE_TRY(dmalloc(&snap_[k], sizeof(V4) * pc));
+        AE_TRY(cudaMemcpyAsync(snap_[k], in_buf()[k], sizeof(V4) * pc, cudaMemcpyDeviceToDevice, stream_));
+      }
+      snap_substep_ = substep_;
+    } else {
+      if (!snap_[0]) {
+        err = "no snapshot";
+        return AE_MPM_EINVAL;
+      }
+      for (int k = 0; k < 7; ++k)
+        AE_TRY(cudaMemcpyAsync(in_buf()[k], snap_[k], sizeof(V4) * pc, cudaMemcpyDeviceToDevice, stream_));
+      keys_stale_ = true;
+      AE_TRY(cudaMemsetAsync(err_, 0, sizeof(uint32_t) * 4 * h_scenes_.size(), stream_));
+    }
+    AE_TRY(cudaStreamSynchronize(stream_));
+    return AE_MPM_OK;
+  }
+
+  uint64_t last_launches() const override { return launches_; }
+  uint64_t particles() const override {
+    uint64_t s = 0;
+    for (auto& h : h_scenes_) s += h.p_count;
+    return s;
+  }
+  cudaStream_t stream() const override { return stream_; }
+  ae_mpm_exec_opts& opts() override { return opts_; }
+  void invalidate_graph() override {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+    chunks_dirty_ = true;
+  }
+  uint64_t device_bytes() const override { return device_bytes_; }
+
+  int copy_scene_from(uint32_t dst, WorldBase* srcb, uint32_t s) override {
+    auto* src = dynamic_cast<World<T>*>(srcb);
+    if (!src || dst >= h_scenes_.size() || s >= src->h_scenes_.size()) {
+      err = "scene copy between incompatible worlds";
+      return AE_MPM_EINVAL;
+    }
+    const SceneDev<T>& a = src->h_scenes_[s];
+    SceneDev<T>& b = h_scenes_[dst];
+    if (a.n[0] != b.n[0] || a.n[1] != b.n[1] || a.n[2] != b.n[2] || a.p_count > b.p_cap) {
+      err = "scene copy needs the same grid and enough particle capacity";
+      return AE_MPM_EINVAL;
+    }
+    for (int k = 0; k < 7; ++k)
+      if (a.p_count)
+        AE_TRY(cudaMemcpyAsync(in_buf()[k] + b.p_off, src->in_buf()[k] + a.p_off, sizeof(V4) * a.p_count,
+                               cudaMemcpyDeviceToDevice, stream_));
+    b.p_count = a.p_count;
+    scenes_dirty_ = chunks_dirty_ = keys_stale_ = true;
+    return AE_MPM_OK;
+  }
+  uint32_t scene_count(uint32_t s) const override { return s < h_scenes_.size() ? h_scenes_[s].p_count : 0; }
+  int precision() const override { return sizeof(T) == 8 ? 64 : 32; }
+
+  int stage_times(uint32_t n, double out_us[5]) override {
+    for (int k = 0; k < 5; ++k) out_us[k] = 0;
+    int rc = prepare();
+    if (rc) return rc;
+    if (n == 0 || n_chunks_ == 0) return AE_MPM_OK;
+    if (keys_stale_) {
+      WorldDev<T> w = dev(false);
+      launch_init_keys(w);
+      keys_stale_ = false;
+    }
+    cudaEvent_t ev[5];
+    for (auto& e : ev) AE_TRY(cudaEventCreate(&e));
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (uint32_t i = 0; i < n; ++i) {
+      stage_events_ = ev;
+      substep_eager();
+      stage_events_ = nullptr;
+      AE_TRY(cudaEventSynchronize(ev[4]));
+      float ms;
+      for (int k = 0; k < 4; ++k) {
+        cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+        acc[k] += ms;
+      }
+      cudaEventElapsedTime(&ms, ev[0], ev[4]);
+      acc[4] += ms;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < 5; ++k) out_us[k] = 1000.0 * acc[k] / n;
+    return AE_MPM_OK;
+  }
+
+ private:
+  template <class P>
+  cudaError_t dmalloc(P** p, size_t bytes) {
+    void* q = nullptr;
+    cudaError_t e = alloc_ ? alloc_->alloc(&q, bytes) : cudaMalloc(&q, bytes);
+    *p = static_cast<P*>(q);
+    return e;
+  }
+  void dfree(const void* p) {
+    if (!p) return;
+    if (alloc_)
+      alloc_->release(const_cast<void*>(p));
+    else
+      cudaFree(const_cast<void*>(p));
+  }
+  static cudaError_t sort_alloc(void* user, void** p, size_t bytes) { return static_cast<DevAlloc*>(user)->alloc(p, bytes); }
+  static void sort_free(void* user, void* p) { static_cast<DevAlloc*>(user)->release(p); }
+
+  V4** in_buf() { return a_in_ ? bufA_ : bufB_; }
+  V4** out_buf() { return a_in_ ? bufB_ : bufA_; }
+  V4* const* in_ptrs_dev() { return a_in_ ? d_ptrA_ : d_ptrB_; }
+
+  int ensure_stage(uint64_t n) {
+    size_t need = sizeof(T) * 26 * n + sizeof(uint16_t) * n + 64;
+    if (need <= stage_bytes_) return AE_MPM_OK;
+    dfree(stage_);
+    stage_ = nullptr;
+    stage_bytes_ = 0;
+    AE_TRY(dmalloc(&stage_, need));
+    stage_bytes_ = need;
+    return AE_MPM_OK;
+  }
+
+  int prepare() {
+    if (opts_.block_threads != 128 && opts_.block_threads != 256) opts_.block_threads = 256;
+    if (opts_.sort_interval < 1) opts_.sort_interval = 1;
+    if (opts_.p2g_variant < kVarTile || opts_.p2g_variant > kVarGlobal) opts_.p2g_variant = kVarTile;
+    if (opts_.block_threads != chunk_threads_) chunks_dirty_ = true;
+    if (chunks_dirty_) {
+      chunk_threads_ = opts_.block_threads;
+      h_chunks_.clear();
+      for (size_t s = 0; s < h_scenes_.size(); ++s) {
+        const SceneDev<T>& h = h_scenes_[s];
+        for (uint64_t lo = h.p_off; lo < uint64_t(h.p_off) + h.p_cap; lo += chunk_threads_) {
+          uint64_t hl = std::min<uint64_t>(lo + chunk_threads_, uint64_t(h.p_off) + h.p_count);
+          uint64_t hc = std::min<uint64_t>(lo + chunk_threads_, uint64_t(h.p_off) + h.p_cap);
+          h_chunks_.push_back(make_int4(int(s), int(lo), int(std::max(hl, lo)), int(hc)));
+        }
+      }
+      n_chunks_ = int(h_chunks_.size());
+      if (n_chunks_ > n_chunks_alloc_) {
+        dfree(d_chunks_);
+        d_chunks_ = nullptr;
+        dfree(partial_);
+        partial_ = nullptr;
+        AE_TRY(dmalloc(&d_chunks_, sizeof(int4) * n_chunks_));
+        n_chunks_alloc_ = n_chunks_;
+      }
+      if (n_chunks_ > 0)
+        AE_TRY(cudaMemcpyAsync(d_chunks_, h_chunks_.data(), sizeof(int4) * n_chunks_, cudaMemcpyHostToDevice, stream_));
+      if (graph_) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+      }
+      chunks_dirty_ = false;
+    }
+    if (scenes_dirty_) {
+      AE_TRY(cudaMemcpyAsync(d_scenes_, h_scenes_.data(), sizeof(SceneDev<T>) * h_scenes_.size(), cudaMemcpyHostToDevice,
+                             stream_));
+      scenes_dirty_ = false;
+    }
+    if (mats_dirty_) {
+      AE_TRY(cudaMemcpyAsync(d_mats_, h_mats_.data(), sizeof(MatDev) * h_mats_.size(), cudaMemcpyHostToDevice, stream_));
+      mats_dirty_ = false;
+    }
+    // the tables are copied from pageable host memory, which the copy stages before returning
+    return AE_MPM_OK;
+  }
+
+  WorldDev<T> dev(bool sorted) {
+    WorldDev<T> w{};
+    w.scenes = d_scenes_;
+    w.mats = d_mats_;
+    w.chunks = d_chunks_;
+    for (int k = 0; k < 7; ++k) {
+      w.in[k] = in_buf()[k];
+      w.out[k] = out_buf()[k];
+    }
+    w.perm = sorted ? perm_ : nullptr;
+    w.keys = keys_;
+    w.acc = acc_;
+    w.vel = vel_;
+    w.blk_flag = blk_flag_;
+    w.touched = touched_;
+    w.touched_count = counters_;
+    w.blk_scene = blk_scene_;
+    w.err = err_;
+    w.svd_fallback = opts_.svd_fp64_fallback;
+    w.max_tile_nodes = max_tile_nodes();
+    w.sorted_keys = sorted ? sorted_keys_ : nullptr;
+    w.cell_slot = cell_slot_;
+    w.cell_rec = cell_rec_;
+    w.cell_count = opts_.deterministic ? counters_ + 1 : nullptr;
+    w.seg_start = seg_start_;
+    return w;
+  }
+
+  int max_tile_nodes() const { return sizeof(T) == 4 ? 1024 : 512; }
+
+  void launch_init_keys(WorldDev<T>& w) {
+    if (n_chunks_ == 0) return;
+    switch (mode_) {
+      case AE_MPM_MODE_PHYSICS: init_keys_kernel<T, AE_MPM_MODE_PHYSICS><<<n_chunks_, chunk_threads_, 0, stream_>>>(w); break;
+      case AE_MPM_MODE_REFERENCE: init_keys_kernel<T, AE_MPM_MODE_REFERENCE><<<n_chunks_, chunk_threads_, 0, stream_>>>(w); break;
+      default: init_keys_kernel<T, AE_MPM_MODE_VELOCITY_ONLY><<<n_chunks_, chunk_threads_, 0, stream_>>>(w); break;
+    }
+    ++launches_;
+  }
+
+  template <int MODE>
+  void launch_p2g(WorldDev<T>& w) {
+    const size_t sm = sizeof(V4) * max_tile_nodes();
+    switch (opts_.p2g_variant) {
+      case kVarWarpAgg: p2g_kernel<T, MODE, kVarWarpAgg><<<n_chunks_, chunk_threads_, sm, stream_>>>(w); break;
+      case kVarGlobal: p2g_kernel<T, MODE, kVarGlobal><<<n_chunks_, chunk_threads_, 0, stream_>>>(w); break;
+      default: p2g_kernel<T, MODE, kVarTile><<<n_chunks_, chunk_threads_, sm, stream_>>>(w); break;
+    }
+  }
+
+  template <int MODE>
+  void substep_mode(WorldDev<T>& w) {
+    const int sms = device_sm_count();
+    if (opts_.deterministic) {
+      det_heads_kernel<<<unsigned((total_cap_ + 255) / 256), 256, 0, stream_>>>(w.sorted_keys, total_cap_, dead_blk_,
+                                                                                 cell_slot_, seg_start_, counters_ + 1);
+      det_cellsum_kernel<T, MODE><<<sms * 8, 128, 0, stream_>>>(w, total_cap_);
+      det_gather_kernel<T, MODE><<<sms * 8, 256, 0, stream_>>>(w, blk_epoch_, counters_ + 2);
+      mark(2);
+      det_reset_kernel<<<sms * 4, 256, 0, stream_>>>(seg_start_, w.sorted_keys, counters_ + 1, cell_slot_);
+      launches_ += 4;
+    } else {
+      launch_p2g<MODE>(w);
+      mark(2);
+      grid_update_kernel<T, MODE><<<sms * 8, 256, 0, stream_>>>(w, blk_epoch_, counters_ + 2);
+      launches_ += 2;
+    }
+    mark(3);
+    g2p_kernel<T, MODE><<<n_chunks_, chunk_threads_, 0, stream_>>>(w, counters_ + 2);
+    ++launches_;
+    mark(4);
+  }
+
+  void mark(int k) {
+    if (stage_events_) cudaEventRecord(stage_events_[k], stream_);
+  }
+
+  void substep_eager() {
+    const int interval = opts_.deterministic ? 1 : opts_.sort_interval;
+    const bool do_sort = (substep_ % uint64_t(interval)) == 0;
+    if (n_chunks_ > 0) {
+      mark(0);
+      if (do_sort) launches_ += radix_sort_pairs(keys_, total_cap_, key_bits_, sort_, stream_, &sorted_keys_, &perm_);
+      mark(1);
+      WorldDev<T> w = dev(do_sort);
+      switch (mode_) {
+        case AE_MPM_MODE_PHYSICS: substep_mode<AE_MPM_MODE_PHYSICS>(w); break;
+        case AE_MPM_MODE_REFERENCE: substep_mode<AE_MPM_MODE_REFERENCE>(w); break;
+        default: substep_mode<AE_MPM_MODE_VELOCITY_ONLY>(w); break;
+      }
+      a_in_ = !a_in_;
+    }
+    ++substep_;
+  }
+
+  int ensure_graph(uint64_t period) {
+    if (graph_ && graph_period_ == period && graph_variant_ == opts_.p2g_variant) return AE_MPM_OK;
+    if (graph_) {
+      cudaGraphExecDestroy(graph_);
+      graph_ = nullptr;
+    }
+    const bool a_in0 = a_in_;
+    const uint64_t sub0 = substep_, l0 = launches_;
+    AE_TRY(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    for (uint64_t k = 0; k < period; ++k) substep_eager();
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(stream_, &g);
+    a_in_ = a_in0;
+    substep_ = sub0;
+    graph_launches_ = launches_ - l0;
+    launches_ = l0;
+    if (e != cudaSuccess) {
+      err = std::string("stream capture failed: ") + cudaGetErrorString(e);
+      return AE_MPM_ECUDA;
+    }
+    e = cudaGraphInstantiate(&graph_, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      err = std::string("graph instantiation failed: ") + cudaGetErrorString(e);
+      graph_ = nullptr;
+      return AE_MPM_ECUDA;
+    }
+    graph_period_ = period;
+    graph_variant_ = opts_.p2g_variant;
+    return AE_MPM_OK;
+  }
+
+  void release() {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (int k = 0; k < 7; ++k) {
+      dfree(bufA_[k]);
+      dfree(bufB_[k]);
+      dfree(snap_[k]);
+    }
+    dfree(d_ptrA_);
+    dfree(d_ptrB_);
+    dfree(keys_);
+    sort_scratch_free(sort_, alloc_ ? &World::sort_free : nullptr, alloc_);
+    dfree(acc_);
+    dfree(vel_);
+    dfree(blk_flag_);
+    dfree(blk_epoch_);
+    dfree(touched_);
+    dfree(counters_);
+    dfree(err_);
+    dfree(cell_slot_);
+    dfree(seg_start_);
+    dfree(cell_rec_);
+    dfree(d_scenes_);
+    dfree(d_mats_);
+    dfree(blk_scene_);
+    dfree(dead_blk_);
+    dfree(d_chunks_);
+    dfree(partial_);
+    dfree(stage_);
+    if (stream_) cudaStreamDestroy(stream_);
+  }
+
+ public:
+  DevAlloc* alloc_ = nullptr;
+  int mode_ = 0;
+  ae_mpm_exec_opts opts_{};
+  std::vector<ae_mpm_scene_desc> descs_;
+  std::vector<std::vector<ae_mpm_material>> mats_;
+  std::vector<SceneDev<T>> h_scenes_;
+  std::vector<MatDev> h_mats_;
+  std::vector<int4> h_chunks_;
+  SceneDev<T>* d_scenes_ = nullptr;
+  MatDev* d_mats_ = nullptr;
+  int4* d_chunks_ = nullptr;
+  int n_chunks_ = 0, n_chunks_alloc_ = 0, chunk_threads_ = 0;
+  V4* bufA_[7] = {};
+  V4* bufB_[7] = {};
+  V4* snap_[7] = {};
+  V4** d_ptrA_ = nullptr;
+  V4** d_ptrB_ = nullptr;
+  bool a_in_ = true;
+  uint32_t* keys_ = nullptr;
+  SortScratch sort_;
+  const uint32_t* perm_ = nullptr;
+  const uint32_t* sorted_keys_ = nullptr;
+  V4* acc_ = nullptr;
+  V4* vel_ = nullptr;
+  uint32_t *blk_flag_ = nullptr, *blk_epoch_ = nullptr, *touched_ = nullptr, *blk_scene_ = nullptr, *dead_blk_ = nullptr;
+  uint32_t* counters_ = nullptr;  // [touched count, cell count, epoch, spare]
+  uint32_t* err_ = nullptr;
+  uint32_t *cell_slot_ = nullptr, *seg_start_ = nullptr;
+  V4* cell_rec_ = nullptr;
+  T* stage_ = nullptr;
+  size_t stage_bytes_ = 0;
+  double* partial_ = nullptr;
+  cudaStream_t stream_ = nullptr;
+  cudaGraphExec_t graph_ = nullptr;
+  uint64_t graph_period_ = 0, graph_launches_ = 0;
+  int graph_variant_ = -1;
+  uint64_t substep_ = 0, snap_substep_ = 0, launches_ = 0;
+  cudaEvent_t* stage_events_ = nullptr;
+  uint64_t total_cap_ = 0, total_blocks_ = 0, device_bytes_ = 0;
+  int key_bits_ = 1;
+  bool keys_stale_ = true, chunks_dirty_ = true, scenes_dirty_ = true, mats_dirty_ = false;
+};
+
+WorldBase* make_world(const ae_mpm_scene_desc* scenes, uint32_t n_scenes, const ae_mpm_exec_opts& opts, std::string& why,
+                      int* status, DevAlloc* alloc) {
+  size_t free0 = 0, total = 0;
+  cudaMemGetInfo(&free0, &total);
+  WorldBase* w = nullptr;
+  int rc;
+  if (opts.precision == 64) {
+    auto* x = new World<double>();
+    x->alloc_ = alloc;
+    rc = x->init(scenes, n_scenes, opts);
+    w = x;
+  } else {
+    auto* x = new World<float>();
+    x->alloc_ = alloc;
+    rc = x->init(scenes, n_scenes, opts);
+    w = x;
+  }
+  if (rc != AE_MPM_OK) {
+    why = w->err;
+    delete w;
+    if (status) *status = rc;
+    return nullptr;
+  }
+  size_t free1 = 0;
+  cudaMemGetInfo(&free1, &total);
+  if (opts.precision == 64)
+    static_cast<World<double>*>(w)->device_bytes_ = free0 > free1 ? free0 - free1 : 0;
+  else
+    static_cast<World<float>*>(w)->device_bytes_ = free0 > free1 ? free0 - free1 : 0;
+  if (status) *status = AE_MPM_OK;
+  return w;
+}
+
+}  // namespace aemp

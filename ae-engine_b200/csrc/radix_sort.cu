@@ -1,0 +1,230 @@
+// radix_sort.cu -- stable LSD radix sort of cell keys (see radix_sort.cuh for the design).
+#include "radix_sort.cuh"
+
+namespace aemp {
+
+namespace {
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  return x;
+}
+
+__global__ void __launch_bounds__(kSortThreads) sort_hist(const uint32_t* __restrict__ keys, uint64_t n, int shift,
+                                                          uint32_t mask, uint32_t* __restrict__ hist,
+                                                          uint32_t* __restrict__ totals, uint32_t tiles) {
+  __shared__ uint32_t cnt[kMaxRadix];
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int i = tid; i < kMaxRadix; i += kSortThreads) cnt[i] = 0;
+  __syncthreads();
+  const uint64_t base = uint64_t(blockIdx.x) * kSortTile;
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k) {
+    uint64_t idx = base + uint64_t(k) * kSortThreads + tid;
+    bool valid = idx < n;
+    uint32_t d = valid ? (__ldg(keys + idx) >> shift) & mask : 0xffffffffu;
+    uint32_t peers = __match_any_sync(0xffffffffu, d);
+    if (valid && lane == __ffs(peers) - 1) atomicAdd(&cnt[d], uint32_t(__popc(peers)));
+  }
+  __syncthreads();
+  for (uint32_t d = tid; d <= mask; d += kSortThreads) {
+    uint32_t c = cnt[d];
+    hist[uint64_t(d) * tiles + blockIdx.x] = c;
+    if (c) atomicAdd(&totals[d], c);
+  }
+}
+
+constexpr int kScanThreads = 1024;
+
+__global__ void __launch_bounds__(kScanThreads) sort_scan(const uint32_t* __restrict__ hist,
+                                                          const uint32_t* __restrict__ totals,
+                                                          uint32_t* __restrict__ offsets, uint32_t tiles) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t carry;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const uint32_t d = blockIdx.x;
+  if (w == 0) {
+    uint32_t s = 0;
+    for (uint32_t i = lane; i < d; i += 32) s += totals[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) carry = s;
+  }
+  __syncthreads();
+  const uint32_t* row = hist + uint64_t(d) * tiles;
+  uint32_t* orow = offsets + uint64_t(d) * tiles;
+  for (uint32_t start = 0; start < tiles; start += kScanThreads) {
+    uint32_t i = start + tid;
+    uint32_t x = (i < tiles) ? row[i] : 0u;
+    uint32_t incl = warp_incl_scan(x, lane);
+    if (lane == 31) warp_sums[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      uint32_t ws = warp_sums[lane];
+      uint32_t wi = warp_incl_scan(ws, lane);
+      warp_sums[lane] = wi - ws;
+    }
+    __syncthreads();
+    uint32_t c = carry;
+    if (i < tiles) orow[i] = c + warp_sums[w] + incl - x;
+    __syncthreads();
+    if (tid == kScanThreads - 1) carry = c + warp_sums[w] + incl;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kSortThreads) sort_scatter(const uint32_t* __restrict__ keys_in,
+                                                             const uint32_t* __restrict__ vals_in,
+                                                             uint32_t* __restrict__ keys_out,
+                                                             uint32_t* __restrict__ vals_out, uint64_t n, int shift,
+                                                             uint32_t mask, const uint32_t* __restrict__ offsets,
+                                                             uint32_t tiles) {
+  __shared__ uint32_t wcnt[kSortWarps][kMaxRadix];
+  __shared__ uint32_t tstart[kMaxRadix];
+  __shared__ uint32_t goff[kMaxRadix];
+  __shared__ uint32_t wsum[kSortWarps];
+  __shared__ uint32_t skeys[kSortTile];
+  __shared__ uint32_t svals[kSortTile];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  for (int i = tid; i < kSortWarps * kMaxRadix; i += kSortThreads) (&wcnt[0][0])[i] = 0;
+  __syncthreads();
+  const uint64_t base = uint64_t(blockIdx.x) * kSortTile;
+  uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    uint64_t idx = base + uint64_t(w) * (32 * kSortItems) + uint64_t(r) * 32 + lane;
+    bool valid = idx < n;
+    key[r] = valid ? __ldg(keys_in + idx) : 0xffffffffu;
+    val[r] = valid ? (vals_in ? __ldg(vals_in + idx) : uint32_t(idx)) : 0u;
+    uint32_t d = valid ? (key[r] >> shift) & mask : 0xffffffffu;
+    uint32_t peers = __match_any_sync(0xffffffffu, d);
+    uint32_t cur = valid ? wcnt[w][d] : 0u;
+    rank[r] = cur + __popc(peers & lt);
+    __syncwarp();
+    if (valid && lane == __ffs(peers) - 1) wcnt[w][d] = cur + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // per digit: exclusive prefix over warps and the tile total
+  uint32_t total = 0;
+  if (uint32_t(tid) <= mask) {
+#pragma unroll
+    for (int ww = 0; ww < kSortWarps; ++ww) {
+      uint32_t c = wcnt[ww][tid];
+      wcnt[ww][tid] = total;
+      total += c;
+    }
+    goff[tid] = offsets[uint64_t(tid) * tiles + blockIdx.x];
+  }
+  // exclusive scan of the tile totals over digits (one digit per thread, kMaxRadix == threads)
+  uint32_t incl = warp_incl_scan(total, lane);
+  if (lane == 31) wsum[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t ws = (lane < kSortWarps) ? wsum[lane] : 0u;
+    uint32_t wi = warp_incl_scan(ws, lane);
+    if (lane < kSortWarps) wsum[lane] = wi - ws;
+  }
+  __syncthreads();
+  tstart[tid] = wsum[w] + incl - total;
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    uint64_t idx = base + uint64_t(w) * (32 * kSortItems) + uint64_t(r) * 32 + lane;
+    if (idx < n) {
+      uint32_t d = (key[r] >> shift) & mask;
+      uint32_t pos = tstart[d] + wcnt[w][d] + rank[r];
+      skeys[pos] = key[r];
+      svals[pos] = val[r];
+    }
+  }
+  __syncthreads();
+  const uint32_t tile_n = uint32_t((n - base) < uint64_t(kSortTile) ? (n - base) : uint64_t(kSortTile));
+  for (uint32_t i = tid; i < tile_n; i += kSortThreads) {
+    uint32_t k = skeys[i];
+    uint32_t d = (k >> shift) & mask;
+    uint32_t o = goff[d] + (i - tstart[d]);
+    keys_out[o] = k;
+    vals_out[o] = svals[i];
+  }
+}
+
+}  // namespace
+
+cudaError_t sort_scratch_alloc(SortScratch& s, uint64_t n, SortAllocFn alloc, void* user) {
+  sort_scratch_free(s);
+  auto A = [&](uint32_t** p, size_t bytes) -> cudaError_t {
+    void* q = nullptr;
+    cudaError_t e = alloc ? alloc(user, &q, bytes) : cudaMalloc(&q, bytes);
+    *p = static_cast<uint32_t*>(q);
+    return e;
+  };
+  const uint64_t tiles = sort_tiles(n > 0 ? n : 1), m = n > 0 ? n : 1;
+  cudaError_t e;
+  if ((e = A(&s.hist, sizeof(uint32_t) * kMaxRadix * tiles)) != cudaSuccess) return e;
+  if ((e = A(&s.offsets, sizeof(uint32_t) * kMaxRadix * tiles)) != cudaSuccess) return e;
+  if ((e = A(&s.totals, sizeof(uint32_t) * 4 * kMaxRadix)) != cudaSuccess) return e;
+  if ((e = A(&s.keys_alt, sizeof(uint32_t) * m)) != cudaSuccess) return e;
+  if ((e = A(&s.vals_a, sizeof(uint32_t) * m)) != cudaSuccess) return e;
+  if ((e = A(&s.vals_b, sizeof(uint32_t) * m)) != cudaSuccess) return e;
+  s.n_cap = n;
+  return cudaSuccess;
+}
+
+void sort_scratch_free(SortScratch& s, SortFreeFn release, void* user) {
+  uint32_t* ps[6] = {s.hist, s.offsets, s.totals, s.keys_alt, s.vals_a, s.vals_b};
+  for (uint32_t* p : ps)
+    if (p) {
+      if (release)
+        release(user, p);
+      else
+        cudaFree(p);
+    }
+  s = SortScratch{};
+}
+
+int radix_sort_pairs(uint32_t* keys, uint64_t n, int key_bits, SortScratch& s, cudaStream_t stream,
+                     const uint32_t** sorted_keys_out, const uint32_t** perm_out) {
+  if (n == 0) {
+    *sorted_keys_out = keys;
+    *perm_out = s.vals_a;
+    return 0;
+  }
+  const SortPlan p = make_sort_plan(key_bits);
+  const uint32_t tiles = uint32_t(sort_tiles(n));
+  cudaMemsetAsync(s.totals, 0, sizeof(uint32_t) * 4 * kMaxRadix, stream);
+  uint32_t* kin = keys;
+  uint32_t* kout = s.keys_alt;
+  const uint32_t* vin = nullptr;
+  uint32_t* vout = s.vals_a;
+  int launches = 0;
+  for (int ps = 0; ps < p.passes; ++ps) {
+    const uint32_t mask = (p.bits[ps] >= 32) ? 0xffffffffu : ((1u << p.bits[ps]) - 1u);
+    uint32_t* tot = s.totals + ps * kMaxRadix;
+    sort_hist<<<tiles, kSortThreads, 0, stream>>>(kin, n, p.shift[ps], mask, s.hist, tot, tiles);
+    sort_scan<<<mask + 1, kScanThreads, 0, stream>>>(s.hist, tot, s.offsets, tiles);
+    sort_scatter<<<tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, p.shift[ps], mask, s.offsets, tiles);
+    launches += 3;
+    uint32_t* nk = (kout == s.keys_alt) ? keys : s.keys_alt;
+    kin = kout;
+    kout = nk;
+    vin = vout;
+    vout = (vout == s.vals_a) ? s.vals_b : s.vals_a;
+  }
+  *sorted_keys_out = kin;
+  *perm_out = vin;
+  return launches;
+}
+
+}  // namespace aemp

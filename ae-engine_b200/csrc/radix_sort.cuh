@@ -1,0 +1,77 @@
+// radix_sort.cuh -- stable LSD radix sort of 32-bit cell keys with a 32-bit payload, sm_100a.
+//
+// The reference has no sort on its MPM path (its P2G walks particle_indices in buffer order,
+// ae_particle/src/mpm_solver.rs:831, 1108); the sort is what lets P2G aggregate same-cell
+// contributions.  It must be bit-exact against a stable CPU sort of the same keys: equal keys
+// keep their input order.
+//
+// One pass per digit (<= 8 bits), three kernels per pass:
+//   1. sort_hist:    per-tile digit counts (warp-aggregated with __match_any_sync), written
+//                    digit-major, plus the global digit totals (one atomic per tile and digit).
+//   2. sort_scan:    one block per digit: exclusive scan of that digit's per-tile counts,
+//                    offset by the totals of all smaller digits.
+//   3. sort_scatter: each warp ranks its 256 keys in input order (match + popc), the block
+//                    turns warp counts into tile-local positions, stages keys in shared memory
+//                    in sorted order and writes runs of equal digits contiguously to HBM.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace aemp {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per block
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kMaxRadix = 256;
+
+struct SortPlan {
+  int passes;
+  int shift[4];
+  int bits[4];
+};
+
+inline SortPlan make_sort_plan(int key_bits) {
+  SortPlan p{};
+  if (key_bits < 1) key_bits = 1;
+  if (key_bits > 32) key_bits = 32;
+  p.passes = (key_bits + 7) / 8;
+  int per = (key_bits + p.passes - 1) / p.passes;
+  int s = 0;
+  for (int i = 0; i < p.passes; ++i) {
+    int b = (key_bits - s < per) ? key_bits - s : per;
+    p.shift[i] = s;
+    p.bits[i] = b;
+    s += b;
+  }
+  return p;
+}
+
+// Scratch for one sort of up to n keys (device pointers owned by the caller).
+struct SortScratch {
+  uint32_t* hist = nullptr;     // [kMaxRadix * tiles]
+  uint32_t* offsets = nullptr;  // [kMaxRadix * tiles]
+  uint32_t* totals = nullptr;   // [4 * kMaxRadix]
+  uint32_t* keys_alt = nullptr; // [n]
+  uint32_t* vals_a = nullptr;   // [n]
+  uint32_t* vals_b = nullptr;   // [n]
+  uint64_t n_cap = 0;
+};
+
+inline uint64_t sort_tiles(uint64_t n) { return (n + kSortTile - 1) / kSortTile; }
+
+// Allocates scratch for n keys; returns cudaSuccess or the failing call's status.
+// `alloc(p, bytes)` / `release(p)` default to cudaMalloc / cudaFree.
+typedef cudaError_t (*SortAllocFn)(void* user, void** p, size_t bytes);
+typedef void (*SortFreeFn)(void* user, void* p);
+cudaError_t sort_scratch_alloc(SortScratch& s, uint64_t n, SortAllocFn alloc = nullptr, void* user = nullptr);
+void sort_scratch_free(SortScratch& s, SortFreeFn release = nullptr, void* user = nullptr);
+
+// Sorts keys[0..n) (only bits [0, key_bits) compared).  On return *perm_out points to the
+// permutation (perm[i] = input index of the i-th smallest key) and *sorted_keys_out to the sorted
+// keys; both live in `keys` / scratch buffers and are valid until the next sort.  `keys` is
+// clobbered.  Queues 3 kernels per pass plus one memset on `stream`; returns the launch count.
+int radix_sort_pairs(uint32_t* keys, uint64_t n, int key_bits, SortScratch& s, cudaStream_t stream,
+                     const uint32_t** sorted_keys_out, const uint32_t** perm_out);
+
+}  // namespace aemp

@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""MPM particle-updates/s on B200.
+
+Default workload: 3D snow collision, 128^3 grid, 1 048 576 Stomakhin-snow particles in two
+0.2^3 boxes at +-2 m/s, dt 5e-5 (f32).  One bench step = one MPM substep of the whole scene
+(radix sort by cell key, P2G, grid update, G2P).  Particle state (2 x 112 B x 1M = 235 MB) plus
+the grid exceeds the 126 MB L2, so no flush is needed between steps.
+
+  value      particle-updates/s with the scene resident in HBM (CUDA events on the world's
+             stream around K substeps; max over ranks)
+  e2e        the same metric through the public C ABI with host buffers: upload from pinned
+             host memory, 500 substeps (the config's run length), download, per call
+  roofline   the dominant kernel (P2G or G2P): algorithmic bytes / its mean event-timed duration
+  cpu_baseline  the CPU restatement of the reference substep (oracle/) on this host's cores
+
+--impl reference times that CPU restatement alone (the reference is Rust and cannot be built
+here).  --gpus N runs N independent replicas (one scene per GPU; the substep does
+not shard within a scene).  Other workloads: --workload jelly|dam|batched|served.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ae-engine_b200"))
+
+import numpy as np  # noqa: E402
+
+# algorithmic bytes per particle-substep of each kernel (f32 layout of mpm_world.cuh):
+# P2G reads 7 x 16 B of particle state; G2P reads 4 x 16 B, writes 7 x 16 B and a 4 B key.
+P2G_BYTES_PER_PARTICLE = 112
+G2P_BYTES_PER_PARTICLE = 64 + 112 + 4
+# per active grid node: P2G accumulator write 16, grid update read 16 + write 16 + clear 16, G2P read 16
+P2G_BYTES_PER_NODE = 16
+G2P_BYTES_PER_NODE = 16
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="snow", choices=["snow", "jelly", "dam", "batched", "served"])
+    ap.add_argument("--e2e-reps", type=int, default=3)
+    ap.add_argument("--e2e-substeps", type=int, default=500)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--scenes", type=int, default=512, help="batched/served: number of scenes")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.tmp = None
+
+    def start(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.tmp.flush()
+        self.tmp.seek(0)
+        rows = [r.split(",") for r in self.tmp.read().strip().splitlines() if r.strip()]
+        os.unlink(self.tmp.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def dist_setup(args):
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world_size > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return rank, local, world_size, pg
+
+
+def max_over_ranks(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def workload(name: str, rank: int, n_scenes: int):
+    import ae_mpm_scenes as S
+
+    if name == "snow":
+        sc, p = S.config2_snow(0xAE02 + 1000 * rank)
+        return [sc], [p], {"workload": "snow collision 128^3, 1048576 Stomakhin snow particles, dt 5e-5",
+                           "grid": 128, "particles": p.n}
+    if name == "jelly":
+        sc, p = S.config1_jelly(0xAE01 + 1000 * rank)
+        return [sc], [p], {"workload": "jelly 64^3, 32768 neo-Hookean particles, dt 1e-4", "grid": 64,
+                           "particles": p.n}
+    if name == "dam":
+        sc, p = S.config3_dam(0xAE03 + 1000 * rank)
+        return [sc], [p], {"workload": "mixed dam break 256^3, 8388608 particles (60% fluid, 25% jelly, 15% snow)",
+                           "grid": 256, "particles": p.n}
+    pairs = S.config4_batched(n_scenes, 0xAE04 + 1000 * rank)
+    return [a for a, _ in pairs], [b for _, b in pairs], {
+        "workload": "%d independent scenes, grids {32,48,64}^3, 2k-64k particles, jelly/snow/water" % n_scenes,
+        "scenes": n_scenes, "particles": int(sum(b.n for _, b in pairs))}
+
+
+def active_nodes(scene, p) -> int:
+    """Distinct grid nodes covered by particle stencils (3x3x3 from the base node)."""
+    X = (p.pos.astype(np.float64) - np.asarray(scene.origin)) / scene.dx
+    base = np.floor(X - 0.5).astype(np.int64)
+    n = np.asarray(scene.n, np.int64)
+    cells = np.unique((base[:, 2] * n[1] + base[:, 1]) * n[0] + base[:, 0])
+    bz, r = np.divmod(cells, n[0] * n[1])
+    by, bx = np.divmod(r, n[0])
+    nodes = set()
+    out = []
+    for dz in range(3):
+        for dy in range(3):
+            for dxx in range(3):
+                out.append(((bz + dz) * n[1] + (by + dy)) * n[0] + (bx + dxx))
+    nodes = np.unique(np.concatenate(out))
+    return int(nodes.size)
+
+
+def cpu_rate(scene, p, substeps: int, threads: int) -> tuple[float, float]:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    q = p.copy()
+    t0 = time.perf_counter()
+    O.run(scene, q, substeps, threads=threads)
+    dt = time.perf_counter() - t0
+    return p.n * substeps / dt, dt
+
+
+def run_reference(args, rank, pg):
+    """CPU restatement of the reference substep on this host's cores, same workload and metric."""
+    if rank != 0:
+        return
+    scenes, parts, cfg = workload(args.workload, 0, args.scenes)
+    scene, p = scenes[0], parts[0]
+    threads = os.cpu_count() or 1
+    # size each step to a bounded sample so the whole run stays within a few minutes
+    probe_n = min(p.n, 65536)
+    probe = p.subset(np.arange(probe_n))
+    rate, _ = cpu_rate(scene, probe, 1, threads)
+    budget_s = max(0.2, 120.0 / max(1, args.steps + args.warmup))
+    n_sample = int(min(p.n, max(probe_n, rate * budget_s)))
+    sample = p.subset(np.arange(n_sample)) if n_sample < p.n else p
+    for _ in range(args.warmup):
+        cpu_rate(scene, sample, 1, threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cpu_rate(scene, sample, 1, threads)
+    dt = time.perf_counter() - t0
+    value = sample.n * args.steps / dt
+    desc = "%d of %d particles (first in scene order), 1 substep per step" % (sample.n, p.n)
+    line = {"impl": "reference", "metric": "MPM particle-updates/s", "value": value, "unit": "particle-updates/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64)", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": "particle-updates/s", "cores": threads, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": value, "unit": "particle-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, local, world_size, pg):
+    import torch
+
+    import ae_mpm as M
+
+    ctx = M.Context(local)
+    scenes, parts, cfg = workload(args.workload, rank, args.scenes)
+    if args.workload == "served":
+        return run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg)
+    opts = M.exec_opts()
+    world = M.World(ctx, scenes, opts)
+    for i, p in enumerate(parts):
+        world.upload(i, p)
+    n_total = sum(p.n for p in parts)
+    tune = None
+    if not args.no_autotune:
+        r = world.autotune(8)
+        tune = {"p2g_variant": {1: "tile", 2: "warp_agg", 3: "global"}.get(r.p2g_variant, r.p2g_variant),
+                "block_threads": r.block_threads, "sort_interval": r.sort_interval,
+                "us_per_substep": round(r.us_per_substep, 2)}
+    world.step(max(args.warmup, 3))
+    world.sync()
+    stages = world.stage_times(20)
+    stream = torch.cuda.ExternalStream(world.stream(), device=local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(local)
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0.record(stream)
+    world.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(local)
+    clk = clocks.stop()
+    world.sync(raise_on_error=False)
+    launches = world.launches()
+    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(pg, ms)
+    value = n_total * world_size * args.steps / (ms / 1e3)
+
+    # roofline of the dominant kernel (P2G or G2P), from its event-timed mean duration
+    A = sum(active_nodes(s, world.download(i, p.n)) for i, (s, p) in enumerate(zip(scenes[:64], parts[:64])))
+    if len(scenes) > 64:
+        A = int(A * len(scenes) / 64)
+    kern = "g2p" if stages["g2p"] >= stages["p2g"] else "p2g"
+    per_p = G2P_BYTES_PER_PARTICLE if kern == "g2p" else P2G_BYTES_PER_PARTICLE
+    per_n = G2P_BYTES_PER_NODE if kern == "g2p" else P2G_BYTES_PER_NODE
+    alg_bytes = per_p * n_total + per_n * A
+    achieved = alg_bytes / (stages[kern] * 1e-6) / 1e9
+    peak, peak_kind = peaks()
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tr = json.load(f)
+        if args.workload in tr and kern in tr[args.workload]:
+            traffic = tr[args.workload][kern]
+    except Exception:
+        pass
+
+    # end to end through the public API with pinned host buffers
+    e2e = None
+    if args.e2e_reps > 0 and len(scenes) == 1:
+        def pinned_like(a):
+            t = torch.empty(a.shape, dtype={np.float32: torch.float32, np.uint16: torch.int16}[a.dtype.type],
+                            pin_memory=True)
+            v = t.numpy().view(a.dtype)
+            v[...] = a
+            return t, v
+
+        keep = []
+        arrays = {}
+        for f in ("pos", "vel", "F", "J", "C", "mass", "mat"):
+            t, v = pinned_like(getattr(parts[0], f))
+            keep.append(t)
+            arrays[f] = v
+        hin = M.Particles(**arrays)
+        outs = {}
+        for f in ("pos", "vel", "F", "J", "C", "mass", "mat"):
+            t, v = pinned_like(getattr(parts[0], f))
+            keep.append(t)
+            outs[f] = v
+        hout = M.Particles(**outs)
+        h2d = sum(getattr(hin, f).nbytes for f in arrays)
+        d2h = h2d
+        world.upload(0, hin)
+        world.step(args.e2e_substeps)
+        world.download_into(0, hout)
+        times = []
+        for _ in range(args.e2e_reps):
+            barrier(pg)
+            torch.cuda.synchronize(local)
+            a0 = torch.cuda.Event(enable_timing=True)
+            a1 = torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            world.upload(0, hin)
+            world.step(args.e2e_substeps)
+            world.download_into(0, hout)
+            a1.record(stream)
+            a1.synchronize()
+            times.append(max_over_ranks(pg, a0.elapsed_time(a1)))
+        t = statistics.median(times)
+        e2e = {"value": n_total * world_size * args.e2e_substeps / (t / 1e3), "unit": "particle-updates/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "substeps_per_step": args.e2e_substeps, "ms_per_step": t}
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        scene, p = scenes[0], parts[0]
+        sub = 2
+        rate, dt = cpu_rate(scene, p, sub, threads)
+        cpu = {"value": rate, "unit": "particle-updates/s", "cores": threads, "kind": "port",
+               "sample": "%d particles (whole scene), %d substeps, %.1f s" % (p.n, sub, dt)}
+
+    if rank == 0:
+        line = {
+            "metric": "MPM particle-updates/s", "value": value, "unit": "particle-updates/s",
+            "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64 scenes)",
+            "config": dict(cfg, parallelism="replicas" if world_size > 1 else "single GPU",
+                           l2="inputs larger than L2 (235 MB particle state), no flush"),
+            "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg_bytes, "active_nodes": A, "kernel_us": stages[kern]},
+            "stages_us": {k: round(v, 2) for k, v in stages.items()},
+            "autotune": tune,
+            "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    world.close()
+
+
+def run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
+    raise SystemExit("served workload: see bench_served in a later revision")
+
+
+def main():
+    args = parse()
+    rank, local, world_size, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, pg)
+        else:
+            run_ours(args, rank, local, world_size, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,334 @@
+/*
+ * ae_mpm.h -- C ABI of the B200 (sm_100a) MPM substep library `libae_mpm.so`.
+ *
+ * This is the drop-in boundary for AE-ENGINE's engine-driven MPM substep.  The engine calls
+ *   ae_particle::mpm_solver::mpm_step_parallel_with_grid   (ae_particle/src/mpm_solver.rs:1063-1084)
+ * from SimulationManager::update_fields_and_particles      (ae_engine/src/managers/simulation.rs:573-581)
+ * and the mid-field LOD tier calls
+ *   ae_particle::mpm_solver::mpm_step_velocity_only_parallel (ae_particle/src/mpm_solver.rs:1337-1351).
+ * A Rust FFI crate binds these entry points exactly as ae_cpp_kernel binds its C++ kernel
+ * (ae_cpp_kernel/src/lib.rs:21-32): raw pointers into the caller's SoA `Vec`s plus counts,
+ * no Rust or torch types.  Unlike that template every call returns a status code.
+ *
+ * Besides the drop-in calls the library keeps scenes resident in HBM ("worlds": one or more
+ * independent scenes stepped in lockstep by the same kernels), and runs a continuous-batching
+ * server on top of worlds.  Nothing here allocates on the caller's behalf except through the
+ * create functions, and every pointer argument is borrowed for the duration of the call only.
+ *
+ * Threading: an ae_mpm_ctx, and every world or server made from it, must be used from one host
+ * thread at a time.  Work is queued on library-owned CUDA streams.
+ */
+#ifndef AE_MPM_H
+#define AE_MPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AE_MPM_ABI_VERSION 1
+
+/* ---- status codes (every function returns one; the message is in ae_mpm_last_error) ---- */
+enum {
+  AE_MPM_OK = 0,
+  AE_MPM_EINVAL = 1,    /* bad argument (the reference panics or misbehaves instead)        */
+  AE_MPM_ENOMEM = 2,    /* device or pinned host allocation failed                          */
+  AE_MPM_ENAN = 3,      /* a particle position became non-finite on the device              */
+  AE_MPM_ETIMEOUT = 4,  /* a bounded wait ran out (server wait, world sync with a deadline)  */
+  AE_MPM_EBUDGET = 5,   /* admission refused: the scene does not fit the HBM budget          */
+  AE_MPM_ECUDA = 6,     /* a CUDA runtime call failed                                       */
+  AE_MPM_EDOMAIN = 7,   /* particles reached the grid's outer ring and were clamped back    */
+  AE_MPM_ENOTFOUND = 8, /* unknown scene or request id                                      */
+  AE_MPM_EAGAIN = 9     /* nothing ready yet (server poll)                                  */
+};
+
+/* ---- constitutive models ----
+ * 0..6 are ae_particle::constitutive::ConstitutiveModel in declaration order
+ * (ae_particle/src/constitutive.rs:12-27); they give Cauchy stress in the reference substep.
+ * 16..18 are the physics-mode materials of the MLS-MPM substep:
+ *   16 neo-Hookean jelly   tau = mu (F F^T - I) + lambda ln(J) I     (ae_physics/src/mpm.rs:429-454)
+ *   17 Stomakhin snow      neo-Hookean on F_E, singular values of F_E clamped to
+ *                          [1-theta_c, 1+theta_s] (ae_physics/src/mpm.rs:565-606), mu and lambda
+ *                          scaled by exp(xi (1 - J_p)) (Stomakhin et al. 2013)
+ *   18 J-only fluid        tau = K (J - 1) I, J <- J (1 + dt tr C)   (ae_compute/src/mpm_compute.rs:287-291,453-457)
+ */
+enum {
+  AE_MPM_NEO_HOOKEAN = 0,
+  AE_MPM_DRUCKER_PRAGER = 1,
+  AE_MPM_VON_MISES = 2,
+  AE_MPM_NEWTONIAN_FLUID = 3,
+  AE_MPM_COROTATED = 4,
+  AE_MPM_FIXED_COROTATED = 5,
+  AE_MPM_RIGID = 6,
+  AE_MPM_PHYS_JELLY = 16,
+  AE_MPM_PHYS_SNOW = 17,
+  AE_MPM_PHYS_FLUID = 18
+};
+
+/* ---- substep flavours ---- */
+enum {
+  /* MLS-MPM (Hu et al. 2018) with nodes at integer i*dx, base = floor(x/dx - 0.5), full F,
+   * physics-mode materials and 3-cell walls (ae_compute/src/mpm_compute.rs:128-459 stencil). */
+  AE_MPM_MODE_PHYSICS = 0,
+  /* Bug-for-bug restatement of ae_particle::mpm_solver::mpm_substep_serial_active /
+   * mpm_substep_parallel_with_indices (ae_particle/src/mpm_solver.rs:812-1054, 1088-1326):
+   * nodes at (g+0.5)*dx, stencil g..g+2, reference Cauchy-stress models, floor-only grid rule,
+   * particle wall clamps with x0.5 restitution, |v|<=50 clamp, NaN guards, damping. */
+  AE_MPM_MODE_REFERENCE = 1,
+  /* ae_particle::mpm_solver::mpm_substep_velocity_only (ae_particle/src/mpm_solver.rs:1353-1572). */
+  AE_MPM_MODE_VELOCITY_ONLY = 2
+};
+
+/* ---- grid wall handling in physics mode ---- */
+enum {
+  AE_MPM_WALL_STICKY = 0, /* every velocity component zeroed on nodes within `wall_margin` of a face */
+  AE_MPM_WALL_SLIP = 1    /* ae_compute rule (mpm_compute.rs:364-383): the outward normal component
+                             is reflected with `restitution` */
+};
+
+/* Material parameters.  The first seven fields are ae_particle::constitutive::MaterialParams
+ * (ae_particle/src/constitutive.rs:31-40) in order; mu/lambda/K derive from them exactly as
+ * MaterialParams::{mu,lambda,bulk_modulus} (constitutive.rs:55-82, poisson_ratio clamped to
+ * [-0.999, 0.4999]).  The trailing fields are used by the physics-mode materials only. */
+typedef struct ae_mpm_material {
+  float young_modulus;  /* E (Pa)                                  */
+  float poisson_ratio;  /* nu                                      */
+  float yield_stress;   /* sigma_y (Pa)                            */
+  float hardening;      /* isotropic hardening coefficient         */
+  float density;        /* rho (kg/m^3); particle volume = m / rho */
+  float friction_angle; /* phi (degrees), Drucker-Prager           */
+  float cohesion;       /* c (Pa), Drucker-Prager                  */
+  int32_t model;        /* one of the AE_MPM_* model values above  */
+  float theta_c;        /* snow critical compression (2.5e-2)      */
+  float theta_s;        /* snow critical stretch (7.5e-3)          */
+  float hardening_xi;   /* snow hardening exponent xi (10)         */
+  float bulk_modulus;   /* fluid K; <= 0 means E / (3 (1 - 2 nu))  */
+} ae_mpm_material;
+
+/* ae_particle::mpm_solver::MpmConfig (ae_particle/src/mpm_solver.rs:46-55), field for field. */
+typedef struct ae_mpm_config {
+  float grid_dx;
+  uint64_t grid_size[3];
+  uint64_t substeps;
+  float gravity[3];
+  float damping;
+  uint8_t enable_plasticity;
+  uint8_t enable_contact;
+  uint8_t use_sparse_grid;
+} ae_mpm_config;
+
+/* The parts of ae_particle::mpm_solver::Grid (mpm_solver.rs:73-86) that a substep reads:
+ * node counts, spacing and the moving-window origin.  The node arrays themselves live on the
+ * device; ae_mpm_grid_download copies mass and velocity back when a caller wants them. */
+typedef struct ae_mpm_grid {
+  uint64_t nx, ny, nz;
+  float dx;
+  float origin[3];
+} ae_mpm_grid;
+
+/* Borrowed views of the MPM fields of ae_particle::mpss::MpssBuffer (ae_particle/src/mpss.rs:105-157),
+ * in its strides: pos/vel are [f32;3] per particle, strain (F) and c (APIC C) are row-major [f32;9].
+ * In physics mode `jacobian` carries det F for jelly, J for fluid and the plastic J_p for snow. */
+typedef struct ae_mpm_particles {
+  float* pos;
+  float* vel;
+  float* strain;
+  float* jacobian;
+  float* c;
+  float* mass;
+  uint16_t* material_idx;
+} ae_mpm_particles;
+
+/* Same view in double precision, for FP64 worlds (error reference runs of the same kernels). */
+typedef struct ae_mpm_particles_f64 {
+  double* pos;
+  double* vel;
+  double* strain;
+  double* jacobian;
+  double* c;
+  double* mass;
+  uint16_t* material_idx;
+} ae_mpm_particles_f64;
+
+/* One scene of a world. */
+typedef struct ae_mpm_scene_desc {
+  int32_t mode;          /* AE_MPM_MODE_*                                         */
+  uint32_t n[3];         /* grid nodes per axis (each >= 4)                        */
+  float dx;              /* node spacing                                          */
+  float origin[3];       /* world position of node (0,0,0) (ref: minus 0.5 dx)     */
+  float gravity[3];
+  float dt;              /* substep length                                        */
+  int32_t wall_mode;     /* physics mode: AE_MPM_WALL_*                            */
+  int32_t wall_margin;   /* physics mode: cells of wall at each face (3)           */
+  float restitution;     /* physics mode, slip walls                              */
+  float damping;         /* reference modes: velocity damping (0.995)             */
+  int32_t wall_origin;   /* reference modes: 1 = particle walls offset by origin
+                            (parallel path, mpm_solver.rs:1290-1297), 0 = walls at 0
+                            (serial path, mpm_solver.rs:998-1015)                  */
+  uint32_t n_materials;
+  const ae_mpm_material* materials; /* indexed by particle material_idx; an index past the end
+                                       uses materials[0] (mpm_solver.rs:840-841)          */
+  uint64_t max_particles;
+} ae_mpm_scene_desc;
+
+/* Execution options of a world. */
+enum { AE_MPM_P2G_AUTO = 0, AE_MPM_P2G_TILE = 1, AE_MPM_P2G_WARP_AGG = 2, AE_MPM_P2G_GLOBAL = 3 };
+typedef struct ae_mpm_exec_opts {
+  int32_t precision;      /* 32 or 64                                                        */
+  int32_t deterministic;  /* 1: fixed-order segmented sums, no float atomics (bitwise replay) */
+  int32_t sort_interval;  /* radix sort every k substeps (>=1; deterministic mode forces 1)   */
+  int32_t p2g_variant;    /* AE_MPM_P2G_*; AUTO takes the autotuned choice                    */
+  int32_t block_threads;  /* particles per P2G/G2P block (128 or 256); 0 = autotuned          */
+  int32_t use_graph;      /* 1: replay substeps from a captured CUDA graph                    */
+  int32_t track_totals;   /* 1: accumulate FP64 mass/momentum totals every substep            */
+  int32_t svd_fp64_fallback; /* 1 (default): snow SVD redone in FP64 near degenerate sigma    */
+} ae_mpm_exec_opts;
+
+typedef struct ae_mpm_ctx ae_mpm_ctx;
+typedef struct ae_mpm_world ae_mpm_world;
+typedef struct ae_mpm_server ae_mpm_server;
+
+/* ---------------------------------------------------------------------------------------------
+ * Context
+ * ------------------------------------------------------------------------------------------- */
+int ae_mpm_ctx_create(int device, ae_mpm_ctx** out);
+void ae_mpm_ctx_destroy(ae_mpm_ctx* ctx);
+/* Text of the last failure on this context (never NULL). */
+const char* ae_mpm_last_error(const ae_mpm_ctx* ctx);
+/* Fills the default execution options (autotuned fields left at 0). */
+void ae_mpm_exec_opts_default(ae_mpm_exec_opts* opts);
+int ae_mpm_abi_version(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Drop-in entry points (host buffers in the reference's layout; state copied in, stepped on the
+ * device, copied back).  `capacity` is the length of the MpssBuffer arrays; `particle_indices`
+ * select the particles to step, as in the reference.  The reference's trailing
+ * buffer.update_lifetimes(total_dt) (mpm_solver.rs:1083) manipulates the MpssBuffer free list and
+ * stays with the host wrapper.  An empty index list returns AE_MPM_OK without touching anything
+ * (mpm_solver.rs:1072-1074).  An empty material table is AE_MPM_EINVAL (the reference panics at
+ * material_table[0], mpm_solver.rs:840).
+ * ------------------------------------------------------------------------------------------- */
+
+/* Replaces mpm_step_parallel_with_grid (ae_particle/src/mpm_solver.rs:1063-1084): config.substeps
+ * substeps of total_dt/config.substeps, each the serial-path rules below 50 000 particles and the
+ * parallel-path rules at or above (mpm_solver.rs:1077). */
+int ae_mpm_step_parallel_with_grid(ae_mpm_ctx* ctx, const ae_mpm_particles* buffer,
+                                   uint64_t capacity, const ae_mpm_grid* grid,
+                                   const ae_mpm_config* config,
+                                   const ae_mpm_material* material_table, uint32_t n_materials,
+                                   const int32_t* model_table, uint32_t n_models,
+                                   float total_dt, const uint64_t* particle_indices,
+                                   uint64_t n_indices);
+
+/* Replaces mpm_step_velocity_only_parallel (ae_particle/src/mpm_solver.rs:1337-1351). */
+int ae_mpm_step_velocity_only_parallel(ae_mpm_ctx* ctx, const ae_mpm_particles* buffer,
+                                       uint64_t capacity, const ae_mpm_grid* grid,
+                                       const ae_mpm_config* config, float total_dt,
+                                       const uint64_t* particle_indices, uint64_t n_indices);
+
+/* Grid mass and velocity (after the grid update of the last substep of the last drop-in call),
+ * dense in the reference's index order i + j*nx + k*nx*ny (mpm_solver.rs:157-159).
+ * mass: nx*ny*nz floats; vel: nx*ny*nz*3 floats. */
+int ae_mpm_grid_download(ae_mpm_ctx* ctx, float* mass, float* vel, uint64_t n_nodes);
+
+/* ---------------------------------------------------------------------------------------------
+ * Device-resident worlds: one or more independent scenes stepped in lockstep by one set of
+ * launches (the batched path).  A world with one scene is the plain path.
+ * ------------------------------------------------------------------------------------------- */
+int ae_mpm_world_create(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32_t n_scenes,
+                        const ae_mpm_exec_opts* opts, ae_mpm_world** out);
+int ae_mpm_world_destroy(ae_mpm_world* world);
+/* Copy n particles (indices 0..n-1 of the view) into scene `scene`; n <= max_particles.
+ * The _f64 variants are for precision-64 worlds. */
+int ae_mpm_world_upload(ae_mpm_world* world, uint32_t scene, const ae_mpm_particles* host, uint64_t n);
+int ae_mpm_world_upload_f64(ae_mpm_world* world, uint32_t scene, const ae_mpm_particles_f64* host, uint64_t n);
+/* Queue n substeps of every scene (asynchronous; returns after queueing). */
+int ae_mpm_world_step(ae_mpm_world* world, uint32_t n_substeps);
+/* Wait for queued work; returns AE_MPM_ENAN / AE_MPM_EDOMAIN if a scene raised its error word. */
+int ae_mpm_world_sync(ae_mpm_world* world);
+/* Copy scene particles back in their upload order. */
+int ae_mpm_world_download(ae_mpm_world* world, uint32_t scene, ae_mpm_particles* host);
+int ae_mpm_world_download_f64(ae_mpm_world* world, uint32_t scene, ae_mpm_particles_f64* host);
+/* FP64 totals of a scene: [mass, px, py, pz, kinetic energy] of its particles, now. */
+int ae_mpm_world_totals(ae_mpm_world* world, uint32_t scene, double out[5]);
+/* Per-scene error word (bit 0 NaN, bit 1 domain clamp) and counters
+ * [svd_fp64_fallbacks, domain_clamps, tile_overflow_blocks]; clears them. */
+int ae_mpm_world_errors(ae_mpm_world* world, uint32_t scene, uint32_t* error_word, uint64_t counters[3]);
+/* Number of kernels the last ae_mpm_world_step queued (graph nodes count as launches). */
+int ae_mpm_world_launch_count(const ae_mpm_world* world, uint64_t* launches);
+/* Runs n substeps eagerly with CUDA events between the stages on the world's stream and returns
+ * the mean device time per substep of each stage in microseconds:
+ * out_us = [sort, P2G (deterministic: cell sums + gather), grid update, G2P, whole substep]. */
+int ae_mpm_world_stage_times(ae_mpm_world* world, uint32_t n_substeps, double out_us[5]);
+/* CUDA stream the world queues on (cudaStream_t), so callers can time it with events. */
+void* ae_mpm_world_stream(ae_mpm_world* world);
+/* Particle count of every scene summed. */
+uint64_t ae_mpm_world_particles(const ae_mpm_world* world);
+
+/* ---------------------------------------------------------------------------------------------
+ * Radix sort by cell key, exposed for parity testing: stable ascending sort of n 32-bit keys
+ * (only the low `key_bits` bits are compared).  Host buffers.  perm_out[i] = index of the i-th
+ * smallest key; equal keys keep their input order.
+ * ------------------------------------------------------------------------------------------- */
+int ae_mpm_radix_sort_keys(ae_mpm_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t key_bits,
+                           uint32_t* sorted_keys_out, uint32_t* perm_out);
+
+/* ---------------------------------------------------------------------------------------------
+ * Autotuner: times the P2G variants, block sizes and sort intervals on a world and writes the
+ * fastest choice back into the world's options.  Choices are cached per workload signature.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ae_mpm_tune_result {
+  int32_t p2g_variant;
+  int32_t block_threads;
+  int32_t sort_interval;
+  float us_per_substep;
+} ae_mpm_tune_result;
+int ae_mpm_world_autotune(ae_mpm_world* world, uint32_t substeps_per_trial, ae_mpm_tune_result* out);
+
+/* ---------------------------------------------------------------------------------------------
+ * Continuous-batching server.  Requests (a scene plus its particles and a substep count) are
+ * admitted while their device state fits the HBM budget, kept resident, and stepped together
+ * with every other admitted scene; a finished scene is copied back and its memory freed, which
+ * lets waiting requests in.  One host thread per server drives the device.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ae_mpm_server_opts {
+  uint64_t hbm_budget_bytes;   /* admission budget for resident scene state                 */
+  uint32_t substeps_per_tick;  /* substeps run between admission checks (default 10)         */
+  uint32_t max_scenes;         /* cap on resident scenes (default 4096)                      */
+  ae_mpm_exec_opts exec;
+} ae_mpm_server_opts;
+
+typedef struct ae_mpm_request_result {
+  uint64_t request_id;
+  int32_t status;          /* AE_MPM_OK or the scene's error                          */
+  double submit_s;         /* host steady-clock seconds at submit                      */
+  double admit_s;          /* ... when admitted to the device                          */
+  double done_s;           /* ... when its results were in the caller's buffers         */
+} ae_mpm_request_result;
+
+int ae_mpm_server_create(ae_mpm_ctx* ctx, const ae_mpm_server_opts* opts, ae_mpm_server** out);
+/* Submit: the particles are copied at submit time; results are written into `out` (which must
+ * stay valid until the request's result has been polled).  Requests larger than the budget are
+ * refused with AE_MPM_EBUDGET. */
+int ae_mpm_server_submit(ae_mpm_server* server, const ae_mpm_scene_desc* scene,
+                         const ae_mpm_particles* in, uint64_t n, uint32_t substeps,
+                         ae_mpm_particles* out, uint64_t* request_id);
+/* Cancel a request that has not finished; its result reports AE_MPM_ENOTFOUND-free status
+ * AE_MPM_EINVAL ("cancelled") and its buffers are left untouched. */
+int ae_mpm_server_cancel(ae_mpm_server* server, uint64_t request_id);
+/* Collect finished results (up to max); returns AE_MPM_EAGAIN when none are ready. */
+int ae_mpm_server_poll(ae_mpm_server* server, ae_mpm_request_result* results, uint32_t max,
+                       uint32_t* n_out);
+/* Wait until every submitted request has finished, at most timeout_s seconds. */
+int ae_mpm_server_drain(ae_mpm_server* server, double timeout_s);
+/* Resident bytes and scenes right now; total substeps run (batched ticks). */
+int ae_mpm_server_stats(ae_mpm_server* server, uint64_t* resident_bytes, uint32_t* resident_scenes,
+                        uint64_t* ticks, uint64_t* particle_substeps);
+int ae_mpm_server_destroy(ae_mpm_server* server);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AE_MPM_H */

@@ -1,0 +1,163 @@
+"""ctypes binding of the CPU oracle (oracle/mpm_oracle.cpp).  TEST INFRASTRUCTURE ONLY.
+
+Imported by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg to check or time
+the CUDA library against a CPU restatement of the reference's MPM substep.  The product path
+(ae-engine_b200/) never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(ROOT, "ae-engine_b200"))
+import ae_mpm as M  # noqa: E402  (struct definitions shared with the C ABI)
+
+LIB_PATH = os.path.join(HERE, "_build", "libae_mpm_oracle.so")
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("oracle library not built (%s)" % LIB_PATH)
+    lib = C.CDLL(LIB_PATH)
+    f = C.c_float
+    for name in ("oracle_b_spline", "oracle_b_spline_deriv", "oracle_quadratic_weight",
+                 "oracle_quadratic_weight_grad"):
+        getattr(lib, name).restype = f
+        getattr(lib, name).argtypes = [f]
+    lib.oracle_material_lame.argtypes = [C.POINTER(M.Material), C.POINTER(f)]
+    lib.oracle_compute_stress.restype = C.c_int
+    lib.oracle_compute_stress.argtypes = [C.c_int32, C.POINTER(M.Material), C.POINTER(f), f, C.POINTER(f),
+                                          C.POINTER(f)]
+    lib.oracle_polar_decomp.argtypes = [C.POINTER(f)] * 3
+    lib.oracle_svd3_f32.restype = C.c_int
+    lib.oracle_svd3_f32.argtypes = [C.POINTER(f)] * 4 + [C.c_int32]
+    d = C.c_double
+    lib.oracle_svd3_f64.argtypes = [C.POINTER(d)] * 4
+    lib.oracle_phys_tau_f64.argtypes = [C.POINTER(M.Material), C.POINTER(d), d, C.POINTER(d)]
+    for name in ("oracle_run_f32", "oracle_run_f64"):
+        g = getattr(lib, name)
+        g.restype = C.c_int
+        g.argtypes = [C.POINTER(M.SceneDesc), C.POINTER(M.ParticlesView), C.c_uint64, C.c_uint32, C.c_int32,
+                      C.c_int32, C.POINTER(C.c_uint64)]
+    lib.oracle_totals_f32.argtypes = [C.POINTER(M.ParticlesView), C.c_uint64, C.POINTER(d)]
+    lib.oracle_totals_f64.argtypes = [C.POINTER(M.ParticlesView), C.c_uint64, C.POINTER(d)]
+    lib.oracle_mpm_step_parallel_with_grid.restype = C.c_int
+    lib.oracle_mpm_step_parallel_with_grid.argtypes = [
+        C.POINTER(M.ParticlesView), C.c_uint64, C.POINTER(M.Grid), C.POINTER(M.Config), C.POINTER(M.Material),
+        C.c_uint32, C.POINTER(C.c_int32), C.c_uint32, f, C.POINTER(C.c_uint64), C.c_uint64, C.c_int32]
+    lib.oracle_mpm_step_velocity_only_parallel.restype = C.c_int
+    lib.oracle_mpm_step_velocity_only_parallel.argtypes = [
+        C.POINTER(M.ParticlesView), C.c_uint64, C.POINTER(M.Grid), C.POINTER(M.Config), f,
+        C.POINTER(C.c_uint64), C.c_uint64, C.c_int32]
+    _lib = lib
+    return lib
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def run(scene: M.Scene, p: M.Particles, substeps: int, threads: int = 1, svd_fallback: bool = True):
+    """Steps `p` in place; returns [svd fallbacks, domain clamps, NaN positions]."""
+    lib = load()
+    d = scene.desc()
+    v = p.view()
+    cnt = (C.c_uint64 * 3)()
+    fn = lib.oracle_run_f64 if p.dtype == np.float64 else lib.oracle_run_f32
+    rc = fn(C.byref(d), C.byref(v), p.n, substeps, threads, 1 if svd_fallback else 0, cnt)
+    if rc != 0:
+        raise RuntimeError("oracle run failed: %d" % rc)
+    return [int(x) for x in cnt]
+
+
+def totals(p: M.Particles) -> np.ndarray:
+    lib = load()
+    out = (C.c_double * 5)()
+    v = p.view()
+    (lib.oracle_totals_f64 if p.dtype == np.float64 else lib.oracle_totals_f32)(C.byref(v), p.n, out)
+    return np.array(out[:])
+
+
+def step_parallel_with_grid(p: M.Particles, grid: M.Grid, config: M.Config, materials, models, total_dt, indices,
+                            threads: int = 1) -> int:
+    lib = load()
+    mats = (M.Material * max(len(materials), 1))(*materials)
+    mods = (C.c_int32 * max(len(models), 1))(*models)
+    idx = np.ascontiguousarray(np.asarray(indices, np.uint64))
+    v = p.view()
+    return lib.oracle_mpm_step_parallel_with_grid(C.byref(v), p.n, C.byref(grid), C.byref(config), mats,
+                                                  len(materials), mods, len(models), total_dt,
+                                                  idx.ctypes.data_as(C.POINTER(C.c_uint64)), idx.size, threads)
+
+
+def step_velocity_only_parallel(p: M.Particles, grid: M.Grid, config: M.Config, total_dt, indices,
+                                threads: int = 1) -> int:
+    lib = load()
+    idx = np.ascontiguousarray(np.asarray(indices, np.uint64))
+    v = p.view()
+    return lib.oracle_mpm_step_velocity_only_parallel(C.byref(v), p.n, C.byref(grid), C.byref(config), total_dt,
+                                                      idx.ctypes.data_as(C.POINTER(C.c_uint64)), idx.size,
+                                                      threads)
+
+
+def b_spline(x):
+    return load().oracle_b_spline(x)
+
+
+def b_spline_deriv(x):
+    return load().oracle_b_spline_deriv(x)
+
+
+def quadratic_weight(x):
+    return load().oracle_quadratic_weight(x)
+
+
+def quadratic_weight_grad(x):
+    return load().oracle_quadratic_weight_grad(x)
+
+
+def compute_stress(model: int, params: M.Material, F, J: float):
+    F = np.ascontiguousarray(np.asarray(F, np.float32).reshape(9))
+    st = np.zeros(9, np.float32)
+    nf = np.zeros(9, np.float32)
+    plastic = load().oracle_compute_stress(model, C.byref(params), _fp(F), J, _fp(st), _fp(nf))
+    return st, nf, bool(plastic)
+
+
+def lame(params: M.Material):
+    out = (C.c_float * 3)()
+    load().oracle_material_lame(C.byref(params), out)
+    return tuple(out[:])
+
+
+def polar_decomp(F):
+    F = np.ascontiguousarray(np.asarray(F, np.float32).reshape(9))
+    R = np.zeros(9, np.float32)
+    S = np.zeros(9, np.float32)
+    load().oracle_polar_decomp(_fp(F), _fp(R), _fp(S))
+    return R, S
+
+
+def svd3(F, f64: bool = False, allow_fallback: bool = True):
+    if f64:
+        F = np.ascontiguousarray(np.asarray(F, np.float64).reshape(9))
+        U, s, V = np.zeros(9), np.zeros(3), np.zeros(9)
+        load().oracle_svd3_f64(_dp(F), _dp(U), _dp(s), _dp(V))
+        return U.reshape(3, 3), s, V.reshape(3, 3), False
+    F = np.ascontiguousarray(np.asarray(F, np.float32).reshape(9))
+    U, s, V = np.zeros(9, np.float32), np.zeros(3, np.float32), np.zeros(9, np.float32)
+    fb = load().oracle_svd3_f32(_fp(F), _fp(U), _fp(s), _fp(V), 1 if allow_fallback else 0)
+    return U.reshape(3, 3), s, V.reshape(3, 3), bool(fb)

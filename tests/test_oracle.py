@@ -1,0 +1,279 @@
+"""CPU tests of the oracle (oracle/mpm_oracle.cpp) against the reference's own known answers and
+property tests.  These pin the oracle before it is trusted as the checker of the CUDA library.
+
+Sources of every check (reference project paths):
+  tests/golden/known_answers.json    b_spline / quadratic_weight values (mpm_solver.rs:1595-1609,
+                                     mpm_compute.rs:1103-1132), extracted from the Rust tests
+  partition of unity                 mpm_compute.rs:1134-1151
+  constitutive known answers         constitutive.rs:619-665
+  sandpile / water / steel           mpm_solver.rs:1611-1745
+  mass conservation, fall, floor     mpm_compute.rs:1223-1301
+  conservation harness thresholds    game/src/bin/conservation_test.rs:141,209
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import ae_mpm as M
+import ae_mpm_scenes as S
+import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def known_answers():
+    with open(os.path.join(HERE, "golden", "known_answers.json")) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("row", known_answers(), ids=lambda r: "%s(%g)@%s" % (r["function"], r["arg"], r["source"]))
+def test_kernel_known_answers(row):
+    f = getattr(O, row["function"])
+    assert abs(f(row["arg"]) - row["expected"]) < row["tol"]
+
+
+def test_known_answer_fixture_is_complete():
+    rows = known_answers()
+    assert len(rows) == 19
+    assert {r["function"] for r in rows} == {"b_spline", "b_spline_deriv", "quadratic_weight", "quadratic_weight_grad"}
+
+
+def test_partition_of_unity():
+    # mpm_compute.rs:1134-1151: weights of the 3-node stencil sum to 1 for fx in [0.5, 1.5]
+    for i in range(101):
+        fx = 0.5 + i / 100.0
+        s = O.quadratic_weight(fx) + O.quadratic_weight(fx - 1.0) + O.quadratic_weight(fx - 2.0)
+        assert abs(s - 1.0) < 1e-5
+
+
+def test_reference_stencil_partition_defect():
+    # the ae_particle stencil (nodes g..g+2 with fx in [0,1)) sums to 0.875 at fx = 0: the
+    # documented reference inconsistency that reference mode reproduces
+    s = O.b_spline(0.0) + O.b_spline(1.0) + O.b_spline(2.0)
+    assert abs(s - 0.875) < 1e-7
+
+
+def test_lame_constants_match_material_params():
+    m = M.material(young_modulus=1e6, poisson_ratio=0.3)
+    mu, lam, k = O.lame(m)
+    assert math.isclose(mu, 1e6 / 2.6, rel_tol=1e-6)
+    assert math.isclose(lam, 1e6 * 0.3 / (1.3 * 0.4), rel_tol=1e-6)
+    assert math.isclose(k, 1e6 / (3 * 0.4), rel_tol=1e-6)
+    # poisson_ratio clamped to 0.4999 (constitutive.rs:61-63): finite at nu = 0.5
+    assert all(math.isfinite(x) for x in O.lame(M.material(poisson_ratio=0.5)))
+
+
+I3 = np.eye(3, dtype=np.float32).reshape(9)
+
+
+def test_neo_hookean_identity_is_stress_free():  # constitutive.rs:623-631
+    st, _, _ = O.compute_stress(M.NEO_HOOKEAN, M.material(), I3, 1.0)
+    assert np.abs(st).max() < 1e-4
+
+
+def test_newtonian_fluid_signs():  # constitutive.rs:633-648
+    st, _, _ = O.compute_stress(M.NEWTONIAN_FLUID, M.material(), I3, 1.0)
+    assert np.abs(st[[0, 4, 8]]).max() < 1e-4
+    st, _, _ = O.compute_stress(M.NEWTONIAN_FLUID, M.material(), I3, 0.9)
+    assert st[0] < 0
+
+
+def test_sand_yields_under_shear():  # constitutive.rs:650-658
+    F = I3.copy()
+    F[1] = 0.5
+    sand = M.material(young_modulus=5e7, poisson_ratio=0.2, yield_stress=1e4, hardening=0.005, density=1600,
+                      friction_angle=35.0, cohesion=0.0)
+    _, _, plastic = O.compute_stress(M.DRUCKER_PRAGER, sand, F, 1.0)
+    assert plastic
+
+
+def test_steel_elastic_at_identity():  # constitutive.rs:660-665
+    steel = M.material(young_modulus=2e11, poisson_ratio=0.3, yield_stress=2.5e8, hardening=0.01, density=7850,
+                       friction_angle=0.0)
+    _, _, plastic = O.compute_stress(M.VON_MISES, steel, I3, 1.0)
+    assert not plastic
+
+
+def test_rigid_returns_identity_stress():  # constitutive.rs:370-373
+    st, _, _ = O.compute_stress(M.RIGID, M.material(), I3 * 1.1, 1.0)
+    assert np.allclose(st, I3)
+
+
+def test_polar_decomposition_reproduces_reference_sign_iteration():
+    # The reference's inv_transpose (constitutive.rs:306-324) returns the inverse, not the inverse
+    # transpose, so its "Newton polar" iteration R <- (R + R^-1)/2 (:284-304) is the matrix sign
+    # iteration: R -> I whenever F's eigenvalues have positive real part, and S = R^T F = F.
+    th = 0.3
+    R = np.array([[math.cos(th), -math.sin(th), 0], [math.sin(th), math.cos(th), 0], [0, 0, 1]])
+    F = R @ np.diag([1.1, 0.95, 1.02])
+    Rg, Sg = O.polar_decomp(F.reshape(9))
+    assert np.allclose(Rg.reshape(3, 3), np.eye(3), atol=1e-5)
+    assert np.allclose(Sg.reshape(3, 3), F, atol=1e-5)
+    # a rotation past 90 degrees has eigenvalues with negative real part: sign(F) != I there
+    th = 2.5
+    R2 = np.array([[math.cos(th), -math.sin(th), 0], [math.sin(th), math.cos(th), 0], [0, 0, 1]])
+    Rg2, _ = O.polar_decomp(R2.reshape(9))
+    assert not np.allclose(Rg2.reshape(3, 3), np.eye(3), atol=1e-2)
+
+
+@pytest.mark.parametrize("seed", range(20))
+def test_svd3_reconstructs_and_is_proper(seed):
+    rng = np.random.default_rng(seed)
+    F = np.eye(3) + rng.normal(0, 0.3 if seed % 2 else 0.01, (3, 3))
+    for f64 in (False, True):
+        U, s, V, _ = O.svd3(F, f64=f64)
+        tol = 1e-12 if f64 else 2e-6
+        assert np.abs(U @ np.diag(s) @ V.T - F).max() <= tol * max(1.0, np.abs(F).max()) * 10
+        assert abs(np.linalg.det(U) - 1) < 1e-5 and abs(np.linalg.det(V) - 1) < 1e-5
+        assert np.allclose(np.abs(s), np.linalg.svd(F)[1], rtol=1e-5, atol=1e-6)
+        assert s[0] >= s[1] >= abs(s[2]) - 1e-6
+
+
+def test_svd3_near_degenerate_uses_fp64_fallback():
+    F = np.diag([1.0, 1.0 + 1e-6, 0.999]).astype(np.float32)
+    _, _, _, fb = O.svd3(F, f64=False, allow_fallback=True)
+    assert fb
+    F2 = np.diag([1.2, 1.0, 0.8]).astype(np.float32)
+    _, _, _, fb2 = O.svd3(F2, f64=False, allow_fallback=True)
+    assert not fb2
+
+
+def test_svd3_reflection_gives_negative_last_singular_value():
+    F = np.diag([1.1, 0.9, -1.0])
+    U, s, V, _ = O.svd3(F, f64=True)
+    assert s[2] < 0 and np.abs(U @ np.diag(s) @ V.T - F).max() < 1e-12
+
+
+# ---------------------------------------------------------------- reference-mode property tests
+def _ref_buffer(positions, mass, material=0, J=1.0):
+    p = M.Particles.empty(len(positions))
+    p.pos[:] = np.asarray(positions, np.float32)
+    p.mass[:] = mass
+    p.mat[:] = material
+    p.J[:] = J
+    return p
+
+
+def test_oracle_sandpile_static_angle():  # mpm_solver.rs:1611-1657
+    pos = [(x * 0.05, y * 0.05 + 0.5, z * 0.05) for x in range(10) for y in range(10) for z in range(10)]
+    p = _ref_buffer(pos, 0.001)
+    cfg = M.Config(grid_dx=1.6, grid_size=(16, 16, 16), substeps=8, gravity=(0, -9.81, 0), damping=0.995)
+    g = M.Grid(16, 16, 16, 1.6, (0, 0, 0))
+    mats = [M.material(young_modulus=1e4, poisson_ratio=0.2, yield_stress=1e3, hardening=0.005, density=1600,
+                       friction_angle=35.0, cohesion=0.0)]
+    idx = np.arange(p.n, dtype=np.uint64)
+    for _ in range(60):
+        assert O.step_parallel_with_grid(p, g, cfg, mats, [M.DRUCKER_PRAGER], 0.016, idx) == 0
+    assert (p.pos[:, 1] >= 0).all()
+
+
+def test_oracle_water_pressure():  # mpm_solver.rs:1659-1711
+    pos = [(x * 0.05, y * 0.05 + 0.1, z * 0.05) for y in range(10) for x in range(5) for z in range(5)]
+    p = _ref_buffer(pos, 0.001, J=0.95)
+    cfg = M.Config(grid_dx=0.05, grid_size=(32, 32, 32), substeps=8, gravity=(0, -9.81, 0), damping=0.995)
+    g = M.Grid(32, 32, 32, 0.05, (0, 0, 0))
+    mats = [M.material(young_modulus=1e3, poisson_ratio=0.499, yield_stress=0, hardening=0, density=1000,
+                       friction_angle=0, cohesion=0)]
+    assert O.step_parallel_with_grid(p, g, cfg, mats, [M.NEWTONIAN_FLUID], 0.016, np.arange(p.n)) == 0
+    assert np.isfinite(p.J).all() and (p.J > 0).all() and (p.J < 100).all()
+
+
+def test_oracle_steel_rigid_fall():  # mpm_solver.rs:1713-1745
+    p = _ref_buffer([(0.2, 0.5, 0.2)], 0.01)
+    cfg = M.Config(grid_dx=0.02, grid_size=(32, 32, 32), substeps=8, gravity=(0, -9.81, 0), damping=0.995)
+    g = M.Grid(32, 32, 32, 0.02, (0, 0, 0))
+    mats = [M.material(young_modulus=1e5, poisson_ratio=0.3, yield_stress=1e4, hardening=0.01, density=7850,
+                       friction_angle=0, cohesion=0)]
+    for _ in range(30):
+        assert O.step_parallel_with_grid(p, g, cfg, mats, [M.VON_MISES], 0.016, [0]) == 0
+    assert 0.0 <= p.pos[0, 1] < 0.5
+
+
+def test_oracle_parallel_path_matches_serial_fold_order():
+    # thread-local grids merged in order (rayon fold/reduce shape) agree with the serial path
+    rng = np.random.default_rng(3)
+    p = _ref_buffer(rng.random((4000, 3)) * 0.6 + 0.2, 0.001)
+    p.vel[:] = rng.normal(0, 0.2, (4000, 3))
+    sc = M.Scene(n=(32, 32, 32), dx=1.0 / 32, dt=1e-3, materials=[M.material(young_modulus=1e4, density=1000)],
+                 mode=M.MODE_REFERENCE, wall_origin=1)
+    a, b = p.copy(), p.copy()
+    O.run(sc, a, 5, threads=1)
+    O.run(sc, b, 5, threads=4)
+    assert np.abs(a.pos - b.pos).max() <= 1e-6
+
+
+# ---------------------------------------------------------------- physics-mode property tests
+def test_physics_mass_conserved_and_falls():  # mpm_compute.rs:1223-1274
+    sc, p = S.tiny_scene(1000, 32, S.jelly())
+    sc.wall_mode = M.WALL_SLIP
+    m0 = O.totals(p)[0]
+    y0 = p.pos[:, 1].mean()
+    q = p.copy()
+    O.run(sc, q, 10)
+    assert abs(O.totals(q)[0] - m0) < 1e-5 * max(m0, 1)
+    assert q.pos[:, 1].mean() < y0
+
+
+def test_physics_floor_not_penetrated():  # mpm_compute.rs:1276-1301
+    sc, p = S.tiny_scene(64, 32, S.jelly(), box=(0.45, 0.55))
+    sc.wall_mode = M.WALL_SLIP
+    sc.gravity = (0.0, -20.0, 0.0)
+    sc.dt = 1e-3
+    O.run(sc, p, 200)
+    assert (p.pos[:, 1] >= 0).all() and p.pos[:, 1].max() < 0.5
+
+
+def test_physics_compressed_block_expands():
+    # force sign: a compressed elastic block pushes outward (the reference's ae_compute force is
+    # sign-flipped, mpm_compute.rs:328-335; physics mode uses the physically correct sign)
+    sc, p = S.tiny_scene(4096, 32, S.jelly(E=1e3), box=(0.4, 0.6))
+    sc.gravity = (0.0, 0.0, 0.0)
+    p.F[:, [0, 4, 8]] = 0.95
+    c0 = p.pos.mean(0)
+    spread0 = np.abs(p.pos - c0).mean()
+    O.run(sc, p, 30)
+    assert np.abs(p.pos - p.pos.mean(0)).mean() > spread0
+
+
+def test_physics_momentum_conserved_without_gravity():
+    # conservation_test.rs:209 style: free-flight momentum of a colliding pair is conserved
+    sc, p = S.tiny_scene(2048, 32, S.jelly(E=500.0))
+    sc.gravity = (0.0, 0.0, 0.0)
+    half = p.n // 2
+    p.vel[:half] = (0.5, 0.0, 0.0)
+    p.vel[half:] = (-0.5, 0.0, 0.0)
+    t0 = O.totals(p)
+    O.run(sc, p, 50)
+    t1 = O.totals(p)
+    assert abs(t1[1] - t0[1]) < 1e-6 and abs(t1[3] - t0[3]) < 1e-6
+
+
+def test_physics_fp32_oracle_tracks_fp64():
+    sc, p = S.config1_jelly()
+    sub = p.subset(np.arange(0, p.n, 8))
+    a = sub.copy()
+    b = sub.astype(np.float64)
+    O.run(sc, a, 40)
+    O.run(sc, b, 40)
+    assert np.abs(a.pos - b.pos).max() / np.abs(b.pos).max() < 1e-6
+
+
+def test_physics_snow_clamps_singular_values():
+    sc, p = S.tiny_scene(2048, 32, S.snow())
+    p.F[:, [0, 4, 8]] = (1.1, 0.9, 1.0)  # beyond theta_s / theta_c
+    O.run(sc, p, 1)
+    for k in range(0, p.n, 97):
+        s = np.linalg.svd(p.F[k].reshape(3, 3).astype(np.float64))[1]
+        assert s.max() <= 1 + 7.5e-3 + 1e-4 and s.min() >= 1 - 2.5e-2 - 1e-4
+    assert (p.J != 1.0).all()  # plastic J_p absorbed the clamped part
+
+
+def test_physics_threads_agree():
+    sc, p = S.tiny_scene(4096, 32, S.water(), v=(1, 0, 0))
+    a, b = p.copy(), p.copy()
+    O.run(sc, a, 10, threads=1)
+    O.run(sc, b, 10, threads=3)
+    assert np.abs(a.pos - b.pos).max() <= 1e-6
