@@ -27,7 +27,7 @@ NEO_HOOKEAN, DRUCKER_PRAGER, VON_MISES, NEWTONIAN_FLUID, COROTATED, FIXED_COROTA
 PHYS_JELLY, PHYS_SNOW, PHYS_FLUID = 16, 17, 18
 MODE_PHYSICS, MODE_REFERENCE, MODE_VELOCITY_ONLY = 0, 1, 2
 WALL_STICKY, WALL_SLIP = 0, 1
-P2G_AUTO, P2G_TILE, P2G_WARP_AGG, P2G_GLOBAL = 0, 1, 2, 3
+P2G_AUTO, P2G_TILE, P2G_WARP_AGG, P2G_GLOBAL, P2G_LANES = 0, 1, 2, 3, 4
 
 
 class MpmError(RuntimeError):

@@ -1,0 +1,210 @@
+//! ae_mpm_cuda -- Rust binding of include/ae_mpm.h (the B200 MPM substep library).
+//!
+//! The raw `extern "C"` block mirrors the header one to one.  The safe layer keeps the
+//! reference's argument shapes: `mpm_step_parallel_with_grid` takes the MpssBuffer field slices
+//! (`pos`, `vel`, `strain`, `jacobian`, `c`, `mass`, `material_idx`), the grid's node counts,
+//! spacing and origin, `MpmConfig`, the material and model tables, `total_dt` and the particle
+//! indices, exactly like ae_particle::mpm_solver::mpm_step_parallel_with_grid
+//! (ae_particle/src/mpm_solver.rs:1063-1084).  Errors come back as `Result`; the reference panics
+//! instead, and ae_particle's wrapper keeps that by unwrapping.
+
+#![allow(non_camel_case_types)]
+use std::ffi::CStr;
+use std::os::raw::{c_char, c_int, c_void};
+use std::sync::OnceLock;
+
+#[repr(C)]
+#[derive(Clone, Copy, Debug, Default)]
+pub struct ae_mpm_material {
+    pub young_modulus: f32,
+    pub poisson_ratio: f32,
+    pub yield_stress: f32,
+    pub hardening: f32,
+    pub density: f32,
+    pub friction_angle: f32,
+    pub cohesion: f32,
+    pub model: i32,
+    pub theta_c: f32,
+    pub theta_s: f32,
+    pub hardening_xi: f32,
+    pub bulk_modulus: f32,
+}
+
+#[repr(C)]
+#[derive(Clone, Copy, Debug, Default)]
+pub struct ae_mpm_config {
+    pub grid_dx: f32,
+    pub grid_size: [u64; 3],
+    pub substeps: u64,
+    pub gravity: [f32; 3],
+    pub damping: f32,
+    pub enable_plasticity: u8,
+    pub enable_contact: u8,
+    pub use_sparse_grid: u8,
+}
+
+#[repr(C)]
+#[derive(Clone, Copy, Debug, Default)]
+pub struct ae_mpm_grid {
+    pub nx: u64,
+    pub ny: u64,
+    pub nz: u64,
+    pub dx: f32,
+    pub origin: [f32; 3],
+}
+
+#[repr(C)]
+pub struct ae_mpm_particles {
+    pub pos: *mut f32,
+    pub vel: *mut f32,
+    pub strain: *mut f32,
+    pub jacobian: *mut f32,
+    pub c: *mut f32,
+    pub mass: *mut f32,
+    pub material_idx: *mut u16,
+}
+
+#[repr(C)]
+pub struct ae_mpm_ctx {
+    _private: [u8; 0],
+}
+
+pub const AE_MPM_OK: c_int = 0;
+
+extern "C" {
+    pub fn ae_mpm_ctx_create(device: c_int, out: *mut *mut ae_mpm_ctx) -> c_int;
+    pub fn ae_mpm_ctx_destroy(ctx: *mut ae_mpm_ctx);
+    pub fn ae_mpm_last_error(ctx: *const ae_mpm_ctx) -> *const c_char;
+    pub fn ae_mpm_step_parallel_with_grid(
+        ctx: *mut ae_mpm_ctx,
+        buffer: *const ae_mpm_particles,
+        capacity: u64,
+        grid: *const ae_mpm_grid,
+        config: *const ae_mpm_config,
+        material_table: *const ae_mpm_material,
+        n_materials: u32,
+        model_table: *const i32,
+        n_models: u32,
+        total_dt: f32,
+        particle_indices: *const u64,
+        n_indices: u64,
+    ) -> c_int;
+    pub fn ae_mpm_step_velocity_only_parallel(
+        ctx: *mut ae_mpm_ctx,
+        buffer: *const ae_mpm_particles,
+        capacity: u64,
+        grid: *const ae_mpm_grid,
+        config: *const ae_mpm_config,
+        total_dt: f32,
+        particle_indices: *const u64,
+        n_indices: u64,
+    ) -> c_int;
+    pub fn ae_mpm_grid_download(ctx: *mut ae_mpm_ctx, mass: *mut f32, vel: *mut f32, n_nodes: u64) -> c_int;
+}
+
+/// Library context on device 0, created on first use (one per process, like the rayon pool).
+struct Ctx(*mut ae_mpm_ctx);
+unsafe impl Send for Ctx {}
+unsafe impl Sync for Ctx {}
+
+fn ctx() -> *mut ae_mpm_ctx {
+    static CTX: OnceLock<Ctx> = OnceLock::new();
+    CTX.get_or_init(|| {
+        let mut p = std::ptr::null_mut();
+        let rc = unsafe { ae_mpm_ctx_create(0, &mut p) };
+        assert_eq!(rc, AE_MPM_OK, "ae_mpm: no usable CUDA device");
+        Ctx(p)
+    })
+    .0
+}
+
+fn check(rc: c_int) -> Result<(), String> {
+    if rc == AE_MPM_OK {
+        Ok(())
+    } else {
+        Err(unsafe { CStr::from_ptr(ae_mpm_last_error(ctx())) }.to_string_lossy().into_owned())
+    }
+}
+
+/// The MpssBuffer fields one substep reads and writes.
+pub struct ParticleSlices<'a> {
+    pub pos: &'a mut [[f32; 3]],
+    pub vel: &'a mut [[f32; 3]],
+    pub strain: &'a mut [[f32; 9]],
+    pub jacobian: &'a mut [f32],
+    pub c: &'a mut [[f32; 9]],
+    pub mass: &'a mut [f32],
+    pub material_idx: &'a mut [u16],
+}
+
+impl<'a> ParticleSlices<'a> {
+    fn raw(&mut self) -> ae_mpm_particles {
+        ae_mpm_particles {
+            pos: self.pos.as_mut_ptr() as *mut f32,
+            vel: self.vel.as_mut_ptr() as *mut f32,
+            strain: self.strain.as_mut_ptr() as *mut f32,
+            jacobian: self.jacobian.as_mut_ptr(),
+            c: self.c.as_mut_ptr() as *mut f32,
+            mass: self.mass.as_mut_ptr(),
+            material_idx: self.material_idx.as_mut_ptr(),
+        }
+    }
+    fn capacity(&self) -> u64 {
+        self.pos.len() as u64
+    }
+}
+
+/// Same semantics as ae_particle::mpm_solver::mpm_step_parallel_with_grid minus the trailing
+/// `buffer.update_lifetimes(total_dt)`, which stays with the caller (it edits the free list).
+pub fn mpm_step_parallel_with_grid(
+    p: &mut ParticleSlices,
+    grid: &ae_mpm_grid,
+    config: &ae_mpm_config,
+    material_table: &[ae_mpm_material],
+    model_table: &[i32],
+    total_dt: f32,
+    particle_indices: &[usize],
+) -> Result<(), String> {
+    let idx: Vec<u64> = particle_indices.iter().map(|&i| i as u64).collect();
+    let raw = p.raw();
+    check(unsafe {
+        ae_mpm_step_parallel_with_grid(
+            ctx(),
+            &raw,
+            p.capacity(),
+            grid,
+            config,
+            material_table.as_ptr(),
+            material_table.len() as u32,
+            model_table.as_ptr(),
+            model_table.len() as u32,
+            total_dt,
+            idx.as_ptr(),
+            idx.len() as u64,
+        )
+    })
+}
+
+/// Same semantics as ae_particle::mpm_solver::mpm_step_velocity_only_parallel.
+pub fn mpm_step_velocity_only_parallel(
+    p: &mut ParticleSlices,
+    grid: &ae_mpm_grid,
+    config: &ae_mpm_config,
+    total_dt: f32,
+    particle_indices: &[usize],
+) -> Result<(), String> {
+    let idx: Vec<u64> = particle_indices.iter().map(|&i| i as u64).collect();
+    let raw = p.raw();
+    check(unsafe {
+        ae_mpm_step_velocity_only_parallel(ctx(), &raw, p.capacity(), grid, config, total_dt, idx.as_ptr(), idx.len() as u64)
+    })
+}
+
+/// Grid mass and velocity after the last drop-in step (reference node order i + j nx + k nx ny).
+pub fn grid_download(mass: &mut [f32], vel: &mut [[f32; 3]]) -> Result<(), String> {
+    assert_eq!(mass.len(), vel.len());
+    check(unsafe { ae_mpm_grid_download(ctx(), mass.as_mut_ptr(), vel.as_mut_ptr() as *mut f32, mass.len() as u64) })
+}
+
+#[allow(dead_code)]
+fn _assert_ffi_safe(_: *const c_void) {}

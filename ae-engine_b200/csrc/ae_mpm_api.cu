@@ -309,7 +309,7 @@ int ae_mpm_world_create(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32
     if (o.block_threads == 0) o.block_threads = it->second.block_threads;
     if (opts == nullptr || opts->p2g_variant == AE_MPM_P2G_AUTO) o.sort_interval = it->second.sort_interval;
   }
-  if (o.p2g_variant == AE_MPM_P2G_AUTO) o.p2g_variant = AE_MPM_P2G_TILE;
+  if (o.p2g_variant == AE_MPM_P2G_AUTO) o.p2g_variant = AE_MPM_P2G_LANES;
   if (o.block_threads == 0) o.block_threads = 256;
   std::string why;
   int st = 0;
@@ -420,7 +420,7 @@ int ae_mpm_world_autotune(ae_mpm_world* world, uint32_t substeps_per_trial, ae_m
   if (substeps_per_trial == 0) substeps_per_trial = 8;
   const ae_mpm_exec_opts saved = w->opts();
   if ((rc = w->snapshot(false))) return fail(ctx, rc, w->err);
-  std::vector<int> variants = {AE_MPM_P2G_TILE, AE_MPM_P2G_WARP_AGG, AE_MPM_P2G_GLOBAL};
+  std::vector<int> variants = {AE_MPM_P2G_LANES, AE_MPM_P2G_TILE, AE_MPM_P2G_WARP_AGG, AE_MPM_P2G_GLOBAL};
   std::vector<int> threads = {128, 256};
   std::vector<int> intervals = {1, 2, 4, 8};
   if (saved.deterministic) {

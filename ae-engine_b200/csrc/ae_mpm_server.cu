@@ -316,7 +316,7 @@ int ae_mpm_server_create(ae_mpm_ctx* ctx, const ae_mpm_server_opts* opts, ae_mpm
   if (s->opts.substeps_per_tick == 0) s->opts.substeps_per_tick = 10;
   if (s->opts.max_scenes == 0) s->opts.max_scenes = 4096;
   if (s->opts.exec.precision != 64) s->opts.exec.precision = 32;
-  if (s->opts.exec.p2g_variant == AE_MPM_P2G_AUTO) s->opts.exec.p2g_variant = AE_MPM_P2G_TILE;
+  if (s->opts.exec.p2g_variant == AE_MPM_P2G_AUTO) s->opts.exec.p2g_variant = AE_MPM_P2G_LANES;
   if (s->opts.exec.block_threads == 0) s->opts.exec.block_threads = 256;
   if (s->opts.exec.sort_interval < 1) s->opts.exec.sort_interval = 1;
   if (s->opts.hbm_budget_bytes == 0) {

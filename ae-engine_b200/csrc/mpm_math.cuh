@@ -388,16 +388,45 @@ AE_HD void svd3(const T* F, T* U, T* s, T* V) {
   for (int i = 0; i < 9; ++i) V[i] = v[i];
 }
 
-// relative singular-value gap below which an FP32 SVD is redone in FP64 (sqrt(eps_f32))
+// relative gap below which two FP32 singular values count as near-degenerate (sqrt(eps_f32))
 constexpr double kSvdGapTol = 3.5e-4;
 
+// every singular value of F provably in [lo, hi] and det F > 0 (Gershgorin discs of F^T F inside
+// [lo^2, hi^2]): the snow clamp is then the identity map and needs no SVD
 template <class T>
-AE_HD bool svd3_fallback(const T* F, T* U, T* s, T* V, bool allow) {
+AE_HD bool clamp_is_identity(const T* F, T lo, T hi) {
+  T a[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) a[i * 3 + j] = F[0 * 3 + i] * F[0 * 3 + j] + F[1 * 3 + i] * F[1 * 3 + j] + F[2 * 3 + i] * F[2 * 3 + j];
+  const T lo2 = lo * lo, hi2 = hi * hi;
+  bool ok = true;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    T r = T(0);
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      if (j != i) r += t_abs(a[i * 3 + j]);
+    ok = ok && !(a[i * 4] - r < lo2) && !(a[i * 4] + r > hi2);
+  }
+  return ok && det3(F) > T(0);
+}
+
+// FP32 SVD, redone in FP64 when a near-degenerate pair straddles a clamp threshold
+template <class T>
+AE_HD bool svd3_fallback(const T* F, T* U, T* s, T* V, bool allow, T lo, T hi) {
   svd3(F, U, s, V);
   if (!allow || sizeof(T) == sizeof(double)) return false;
   T smax = t_max(t_abs(s[0]), T(1e-30));
-  T gap = t_min(t_abs(s[0] - s[1]), t_min(t_abs(s[1] - s[2]), t_abs(s[0] - s[2]))) / smax;
-  if (gap >= T(kSvdGapTol)) return false;
+  bool need = false;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = i + 1; j < 3; ++j)
+      if (t_abs(s[i] - s[j]) < T(kSvdGapTol) * smax && ((s[i] < lo) != (s[j] < lo) || (s[i] > hi) != (s[j] > hi)))
+        need = true;
+  if (!need) return false;
   double Fd[9], Ud[9], sd[3], Vd[9];
 #pragma unroll
   for (int i = 0; i < 9; ++i) Fd[i] = double(F[i]);

@@ -58,6 +58,20 @@ __device__ __forceinline__ void atomic_add4(double4* p, double a, double b, doub
   atomicAdd(&p->w, d);
 }
 
+// asynchronous 16-byte global -> shared copies (cp.async, no registers held while in flight)
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+template <class V4>
+__device__ __forceinline__ void cp_async_v4(V4* sdst, const V4* gsrc) {
+#pragma unroll
+  for (int k = 0; k < int(sizeof(V4) / 16); ++k)
+    cp_async16(reinterpret_cast<char*>(sdst) + 16 * k, reinterpret_cast<const char*>(gsrc) + 16 * k);
+}
+
 template <class T>
 __device__ __forceinline__ int floor_to_int(T v) {
   if (v != v) return 0;  // NaN -> 0, as Rust's `as isize`
@@ -118,6 +132,7 @@ struct P2GPart {
   int g[3];     // stencil base node per axis (nodes g..g+2)
   T w[3][3];    // per-axis weights
   T o[3][3];    // physics: (k - fx) dx;  reference: node position - particle position
+  T fx[3];      // physics: position relative to the base node, in cells (in [0.5, 1.5))
   T dw[3][3];   // reference: N'(k - fx) / dx
   T m;
   T v[3];       // physics: m v;  reference/velonly: v
@@ -173,6 +188,7 @@ __device__ __forceinline__ void p2g_setup(const WorldDev<T>& w, const SceneDev<T
       int b = floor_to_int(X - T(0.5));
       T fx = X - T(b);
       p.g[a] = b;
+      p.fx[a] = fx;
       T t0 = T(1.5) - fx, t1 = fx - T(1), t2 = fx - T(0.5);
       p.w[a][0] = T(0.5) * t0 * t0;
       p.w[a][1] = T(0.75) - t1 * t1;
@@ -241,7 +257,7 @@ __device__ __forceinline__ bool p2g_contrib(const SceneDev<T>& sc, const P2GPart
 // ============================================================================================
 // P2G
 // ============================================================================================
-enum { kVarTile = 1, kVarWarpAgg = 2, kVarGlobal = 3 };
+enum { kVarTile = 1, kVarWarpAgg = 2, kVarGlobal = 3, kVarLanes = 4 };
 
 template <class T>
 __device__ __forceinline__ void shared_add4(typename V4T<T>::type* t, T a, T b, T c, T d) {
@@ -395,6 +411,139 @@ __global__ void __launch_bounds__(512) p2g_kernel(WorldDev<T> w) {
   }
 }
 
+// --------------------------------------------------------------------------------------------
+// P2G, physics mode, lanes as stencil nodes.  Particles are sorted by cell, so a warp's 32
+// particles form a few runs of equal cells.  The warp finds the runs with one ballot, then walks
+// each run particle by particle: lane l < 27 owns node (l%3, l/3%3, l/9) of the run's cell and
+// keeps that node's sum in registers; at the end of the run the 27 lanes add their sums to the
+// shared tile (27 distinct addresses).  Each particle's record (fx, m, m v, affine matrix) is
+// staged field-major in shared memory by its own thread and read by the warp as broadcasts.
+// --------------------------------------------------------------------------------------------
+constexpr int kRecVecs = 4;  // per-particle record: (fx fy fz m) (mvx mvy mvz A00) (A01..A11) (A12..A22)
+
+template <class T>
+__global__ void __launch_bounds__(256) p2g_lanes_kernel(WorldDev<T> w) {
+  using V4 = typename V4T<T>::type;
+  extern __shared__ __align__(16) unsigned char smem[];
+  V4* tile = reinterpret_cast<V4*>(smem);
+  V4* rec = tile + w.max_tile_nodes;  // rec[k * blockDim.x + q]
+  __shared__ int s_lo[3], s_hi[3];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
+  const int4 ch = w.chunks[blockIdx.x];
+  const SceneDev<T>& sc = w.scenes[ch.x];
+  if (tid < 3) {
+    s_lo[tid] = INT_MAX;
+    s_hi[tid] = INT_MIN;
+  }
+  __syncthreads();
+  const int j = ch.y + tid;
+  bool has = false;
+  int g[3] = {0, 0, 0};
+  int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+  if (j < ch.z) {
+    const uint32_t src = w.perm ? w.perm[j] : uint32_t(j);
+    P2GPart<T> p;
+    p2g_setup<T, AE_MPM_MODE_PHYSICS>(w, sc, src, p);
+    has = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      g[a] = p.g[a];
+      lo[a] = max(p.g[a], 0);
+      hi[a] = min(p.g[a] + 2, sc.n[a] - 1);
+      if (lo[a] > hi[a]) has = false;
+    }
+    rec[0 * nt + tid] = mk4(p.fx[0], p.fx[1], p.fx[2], p.m);
+    rec[1 * nt + tid] = mk4(p.v[0], p.v[1], p.v[2], p.A[0]);
+    rec[2 * nt + tid] = mk4(p.A[1], p.A[2], p.A[3], p.A[4]);
+    rec[3 * nt + tid] = mk4(p.A[5], p.A[6], p.A[7], p.A[8]);
+  }
+  // run key: unique per cell (a stencil with any node in the grid has g in [-2, n-1] per axis)
+  const uint32_t key = has ? uint32_t(g[0] + 2) + uint32_t(sc.n[0] + 2) * (uint32_t(g[1] + 2) + uint32_t(sc.n[1] + 2) * uint32_t(g[2] + 2))
+                           : 0xffffffffu;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    int l = __reduce_min_sync(0xffffffffu, has ? lo[a] : INT_MAX);
+    int h = __reduce_max_sync(0xffffffffu, has ? hi[a] : INT_MIN);
+    if (lane == 0 && l != INT_MAX) {
+      atomicMin(&s_lo[a], l);
+      atomicMax(&s_hi[a], h);
+    }
+  }
+  __syncthreads();
+  const int L0 = s_lo[0], L1 = s_lo[1], L2 = s_lo[2];
+  if (L0 == INT_MAX) return;
+  const int D0 = s_hi[0] - L0 + 1, D1 = s_hi[1] - L1 + 1, D2 = s_hi[2] - L2 + 1;
+  const int vol = D0 * D1 * D2;
+  const bool use_tile = vol <= w.max_tile_nodes;
+  if (use_tile) {
+    for (int t = tid; t < vol; t += nt) tile[t] = mk4(T(0), T(0), T(0), T(0));
+  } else if (tid == 0) {
+    atomicAdd(w.err + 4 * ch.x + 3, 1u);
+  }
+  __syncthreads();
+  // runs of equal keys among this warp's particles (particles without nodes form their own runs)
+  const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+  uint32_t starts = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
+  // this lane's stencil node and its weights: with t = fx - off_k, w_0 = t^2/2 (off 1.5),
+  // w_1 = 3/4 - t^2 (off 1), w_2 = t^2/2 (off 0.5): the quadratic B-spline at fx, fx-1, fx-2,
+  // evaluated branch-free from per-lane constants
+  const int na = lane % 3, nb = (lane / 3) % 3, nc = lane / 9;
+  const T offa = T(1.5) - T(0.5) * T(na), offb = T(1.5) - T(0.5) * T(nb), offc = T(1.5) - T(0.5) * T(nc);
+  const T sa = na == 1 ? T(-1) : T(0.5), sb = nb == 1 ? T(-1) : T(0.5), sc2 = nc == 1 ? T(-1) : T(0.5);
+  const T ka = na == 1 ? T(0.75) : T(0), kb = nb == 1 ? T(0.75) : T(0), kc = nc == 1 ? T(0.75) : T(0);
+  const T fa = T(na), fb = T(nb), fc = T(nc);
+  const T dx = sc.dx;
+  const V4* r0p = rec + warp * 32;
+  const V4* r1p = rec + nt + warp * 32;
+  const V4* r2p = rec + 2 * nt + warp * 32;
+  const V4* r3p = rec + 3 * nt + warp * 32;
+  while (starts) {
+    const int s0 = __ffs(starts) - 1;
+    starts &= starts - 1u;
+    const int e0 = starts ? __ffs(starts) - 1 : 32;
+    const uint32_t rk = __shfl_sync(0xffffffffu, key, s0);
+    const int X = __shfl_sync(0xffffffffu, g[0], s0) + na;
+    const int Y = __shfl_sync(0xffffffffu, g[1], s0) + nb;
+    const int Z = __shfl_sync(0xffffffffu, g[2], s0) + nc;
+    if (rk == 0xffffffffu) continue;
+    T am = 0, ax = 0, ay = 0, az = 0;
+    for (int i = s0; i < e0; ++i) {
+      const V4 r0 = r0p[i], r1 = r1p[i], r2 = r2p[i], r3 = r3p[i];
+      const T tx = r0.x - offa, ty = r0.y - offb, tz = r0.z - offc;
+      const T ww = (sa * tx * tx + ka) * (sb * ty * ty + kb) * (sc2 * tz * tz + kc);
+      const T d0 = (fa - r0.x) * dx, d1 = (fb - r0.y) * dx, d2 = (fc - r0.z) * dx;
+      am += ww * r0.w;
+      ax += ww * (r1.x + r1.w * d0 + r2.x * d1 + r2.y * d2);
+      ay += ww * (r1.y + r2.z * d0 + r2.w * d1 + r3.x * d2);
+      az += ww * (r1.z + r3.y * d0 + r3.z * d1 + r3.w * d2);
+    }
+    if (lane < 27 && am != T(0) && X >= 0 && Y >= 0 && Z >= 0 && X < sc.n[0] && Y < sc.n[1] && Z < sc.n[2]) {
+      if (use_tile) {
+        shared_add4<T>(tile + ((Z - L2) * D1 + (Y - L1)) * D0 + (X - L0), am, ax, ay, az);
+      } else {
+        atomic_add4(w.acc + node_index(sc, X, Y, Z), am, ax, ay, az);
+        mark_block(w, sc.blk_off + (uint32_t(Z >> 2) * sc.nb[1] + (Y >> 2)) * sc.nb[0] + (X >> 2));
+      }
+    }
+  }
+  if (!use_tile) return;
+  __syncthreads();
+  for (int t = tid; t < vol; t += nt) {
+    V4 v = tile[t];
+    if (v.x != T(0)) {
+      int X = L0 + t % D0, Y = L1 + (t / D0) % D1, Z = L2 + t / (D0 * D1);
+      atomic_add4(w.acc + node_index(sc, X, Y, Z), v.x, v.y, v.z, v.w);
+    }
+  }
+  const int B0 = L0 >> 2, B1 = L1 >> 2, B2 = L2 >> 2;
+  const int E0 = (L0 + D0 - 1) >> 2, E1 = (L1 + D1 - 1) >> 2, E2 = (L2 + D2 - 1) >> 2;
+  const int nbx = E0 - B0 + 1, nby = E1 - B1 + 1, nbz = E2 - B2 + 1;
+  for (int t = tid; t < nbx * nby * nbz; t += nt) {
+    int bx = B0 + t % nbx, by = B1 + (t / nbx) % nby, bz = B2 + t / (nbx * nby);
+    mark_block(w, sc.blk_off + (uint32_t(bz) * sc.nb[1] + by) * sc.nb[0] + bx);
+  }
+}
+
 // ============================================================================================
 // grid update (momentum -> velocity, gravity, walls); clears accumulator and touched flags
 // ============================================================================================
@@ -454,6 +603,7 @@ __global__ void __launch_bounds__(256) grid_update_kernel(WorldDev<T> w, uint32_
   using V4 = typename V4T<T>::type;
   const uint32_t count = *reinterpret_cast<volatile uint32_t*>(w.touched_count);
   const uint32_t ep = *epoch;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *w.clamp_count = 0u;  // G2P of this substep refills it
   const int sub = threadIdx.x >> 6, l = threadIdx.x & 63;
   for (uint32_t t = blockIdx.x * 4 + sub; t < count; t += gridDim.x * 4) {
     const uint32_t gb = w.touched[t];
@@ -479,14 +629,29 @@ __global__ void __launch_bounds__(256) grid_update_kernel(WorldDev<T> w, uint32_
 template <class T>
 struct G2POut {
   T x[3], v[3], C[9], F[9], J;
-  uint32_t err;    // kErr* bits
-  bool fallback;   // FP64 SVD used
+  uint32_t err;       // kErr* bits
+  bool needs_clamp;   // snow: F left the elastic region; the clamp kernel finishes the update
   bool clamped;
 };
 
+// Node velocities for one block of particles: the block's bounding-box tile in shared memory
+// (filled with coalesced loads before the gather), or the global array when the box is too big.
 template <class T>
-__device__ __forceinline__ void g2p_physics(const WorldDev<T>& w, const SceneDev<T>& sc, const MatDev& md, const T* x0,
-                                            const T* F, T J, G2POut<T>& o) {
+struct VelTile {
+  using V4 = typename V4T<T>::type;
+  const V4* tile;
+  const V4* vel;
+  int L0, L1, L2, D0, D1;
+  __device__ __forceinline__ V4 operator()(const SceneDev<T>& sc, int X, int Y, int Z) const {
+    if (tile) return tile[((Z - L2) * D1 + (Y - L1)) * D0 + (X - L0)];
+    return ld4(vel + node_index(sc, X, Y, Z));
+  }
+};
+
+// gather half of the physics G2P: grid velocity and APIC C at the particle
+template <class T>
+__device__ __forceinline__ void g2p_physics_gather(const VelTile<T>& vt, const SceneDev<T>& sc, const T* x0, T* v,
+                                                   T* C) {
   using V4 = typename V4T<T>::type;
   int b[3];
   T wt[3][3], dp[3][3];
@@ -503,7 +668,8 @@ __device__ __forceinline__ void g2p_physics(const WorldDev<T>& w, const SceneDev
 #pragma unroll
     for (int k = 0; k < 3; ++k) dp[a][k] = (T(k) - fx) * sc.dx;
   }
-  T v[3] = {0, 0, 0}, B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  T B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  v[0] = v[1] = v[2] = T(0);
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -513,7 +679,7 @@ __device__ __forceinline__ void g2p_physics(const WorldDev<T>& w, const SceneDev
         int X = b[0] + a, Y = b[1] + bb, Z = b[2] + c;
         if (X < 0 || Y < 0 || Z < 0 || X >= sc.n[0] || Y >= sc.n[1] || Z >= sc.n[2]) continue;
         T ww = wt[0][a] * wt[1][bb] * wt[2][c];
-        V4 gv = ld4(w.vel + node_index(sc, X, Y, Z));
+        V4 gv = vt(sc, X, Y, Z);
         T g3[3] = {gv.x, gv.y, gv.z};
         T d[3] = {dp[0][a], dp[1][bb], dp[2][c]};
 #pragma unroll
@@ -525,7 +691,13 @@ __device__ __forceinline__ void g2p_physics(const WorldDev<T>& w, const SceneDev
       }
   const T cs = T(4) * sc.inv_dx * sc.inv_dx;
 #pragma unroll
-  for (int k = 0; k < 9; ++k) o.C[k] = cs * B[k];
+  for (int k = 0; k < 9; ++k) C[k] = cs * B[k];
+}
+
+// update half of the physics G2P: advection, F update and the material's return mapping
+template <class T>
+__device__ __forceinline__ void g2p_physics_update(const SceneDev<T>& sc, const MatDev& md, const T* x0, const T* v,
+                                                   const T* F, T J, G2POut<T>& o) {
   bool nan = false, clamped = false;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -539,7 +711,7 @@ __device__ __forceinline__ void g2p_physics(const WorldDev<T>& w, const SceneDev
   }
   o.err = (nan ? kErrNaN : 0u) | (clamped ? kErrDomain : 0u);
   o.clamped = clamped;
-  o.fallback = false;
+  o.needs_clamp = false;
   if (md.model == kPhysFluid) {
     T Jn = J * (T(1) + sc.dt * (o.C[0] + o.C[4] + o.C[8]));
     o.J = t_max(Jn, T(0.01));
@@ -550,31 +722,20 @@ __device__ __forceinline__ void g2p_physics(const WorldDev<T>& w, const SceneDev
   T G[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) G[k] = ((k % 4 == 0) ? T(1) : T(0)) + sc.dt * o.C[k];
-  T nF[9];
-  mm3(G, F, nF);
+  mm3(G, F, o.F);
   if (md.model == kPhysSnow) {
-    T U[9], sg[3], V[9];
-    o.fallback = svd3_fallback(nF, U, sg, V, w.svd_fallback != 0);
-    T lo = T(1) - T(md.theta_c), hi = T(1) + T(md.theta_s);
-    T scl[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) scl[k] = t_min(t_max(sg[k], lo), hi);
-    o.J = J * ((sg[0] * sg[1] * sg[2]) / (scl[0] * scl[1] * scl[2]));
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-        o.F[r * 3 + c] = U[r * 3 + 0] * scl[0] * V[c * 3 + 0] + U[r * 3 + 1] * scl[1] * V[c * 3 + 1] + U[r * 3 + 2] * scl[2] * V[c * 3 + 2];
+    // elastic region (every singular value provably inside the clamp interval): F_E and J_p
+    // are final; otherwise the clamp kernel does the SVD and the return mapping
+    o.J = J;
+    o.needs_clamp = !clamp_is_identity(o.F, T(1) - T(md.theta_c), T(1) + T(md.theta_s));
   } else {
-#pragma unroll
-    for (int k = 0; k < 9; ++k) o.F[k] = nF[k];
-    o.J = det3(nF);
+    o.J = det3(o.F);
   }
 }
 
 // mpm_substep_serial_active / parallel_with_indices G2P (mpm_solver.rs:914-1053, 1206-1325)
 template <class T>
-__device__ __forceinline__ void g2p_reference(const WorldDev<T>& w, const SceneDev<T>& sc, const T* pos, const T* f,
+__device__ __forceinline__ void g2p_reference(const VelTile<T>& vt, const SceneDev<T>& sc, const T* pos, const T* f,
                                               G2POut<T>& o) {
   using V4 = typename V4T<T>::type;
   int g[3];
@@ -598,7 +759,7 @@ __device__ __forceinline__ void g2p_reference(const WorldDev<T>& w, const SceneD
         if (ww < T(1e-10)) continue;
         int X = g[0] + di, Y = g[1] + dj, Z = g[2] + dk;
         if (X >= sc.n[0] || Y >= sc.n[1] || Z >= sc.n[2]) continue;
-        V4 gv = ld4(w.vel + node_index(sc, X, Y, Z));
+        V4 gv = vt(sc, X, Y, Z);
         if (gv.w < T(1e-12)) continue;
         T g3[3] = {gv.x, gv.y, gv.z};
         nv[0] += ww * g3[0];
@@ -681,12 +842,12 @@ __device__ __forceinline__ void g2p_reference(const WorldDev<T>& w, const SceneD
     o.F[k] = nf[k];
   }
   o.err = 0;
-  o.fallback = o.clamped = false;
+  o.needs_clamp = o.clamped = false;
 }
 
 // mpm_substep_velocity_only G2P (mpm_solver.rs:1465-1571); C, F and J are carried unchanged
 template <class T>
-__device__ __forceinline__ void g2p_velonly(const WorldDev<T>& w, const SceneDev<T>& sc, const T* pos, G2POut<T>& o) {
+__device__ __forceinline__ void g2p_velonly(const VelTile<T>& vt, const SceneDev<T>& sc, const T* pos, G2POut<T>& o) {
   using V4 = typename V4T<T>::type;
   int g[3];
   T wx[3], wy[3], wz[3];
@@ -718,7 +879,7 @@ __device__ __forceinline__ void g2p_velonly(const WorldDev<T>& w, const SceneDev
         if (ww < T(1e-10)) continue;
         int X = g[0] + di;
         if (X >= sc.n[0]) continue;
-        V4 gv = ld4(w.vel + node_index(sc, X, Y, Z));
+        V4 gv = vt(sc, X, Y, Z);
         if (gv.w < T(1e-12)) continue;
         nv[0] += ww * gv.x;
         nv[1] += ww * gv.y;
@@ -761,36 +922,105 @@ __device__ __forceinline__ void g2p_velonly(const WorldDev<T>& w, const SceneDev
     o.x[a] = np[a];
   }
   o.err = 0;
-  o.fallback = o.clamped = false;
+  o.needs_clamp = o.clamped = false;
+}
+
+// in-grid stencil node range of a position along one axis (empty when lo > hi)
+template <class T, int MODE>
+__device__ __forceinline__ void stencil_range(const SceneDev<T>& sc, T x, int a, int& lo, int& hi) {
+  int g = floor_to_int((x - sc.origin[a]) * sc.inv_dx - T(0.5));
+  if (MODE != AE_MPM_MODE_PHYSICS) g = max(g, 0);
+  lo = max(g, 0);
+  hi = min(g + 2, sc.n[a] - 1);
 }
 
 template <class T, int MODE>
 __global__ void __launch_bounds__(256) g2p_kernel(WorldDev<T> w, uint32_t* epoch) {
   using V4 = typename V4T<T>::type;
+  extern __shared__ __align__(16) unsigned char smem[];
+  V4* tile = reinterpret_cast<V4*>(smem);
+  V4* stage = tile + w.max_tile_nodes;  // a1..a3 of this block's particles: stage[k * blockDim.x + tid]
+  __shared__ int s_lo[3], s_hi[3];
   const int4 ch = w.chunks[blockIdx.x];
   const SceneDev<T>& sc = w.scenes[ch.x];
-  const int j = ch.y + threadIdx.x;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  const int tid = threadIdx.x, lane = tid & 31, nt = blockDim.x;
+  const int j = ch.y + tid;
+  const bool live = j < ch.z;
+  if (blockIdx.x == 0 && tid == 0) {
     *w.touched_count = 0u;
     if (w.cell_count) *w.cell_count = 0u;
     *epoch += 1u;
   }
+  if (tid < 3) {
+    s_lo[tid] = INT_MAX;
+    s_hi[tid] = INT_MIN;
+  }
+  __syncthreads();
+  uint32_t src = 0;
+  V4 a0 = mk4(T(0), T(0), T(0), T(0));
+  int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+  bool has = false;
+  if (live) {
+    src = w.perm ? w.perm[j] : uint32_t(j);
+    // F, J and the material arrive in shared memory while the velocity tile is gathered
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cp_async_v4(stage + k * nt + tid, w.in[1 + k] + src);
+    cp_async_commit();
+    a0 = ld4(w.in[0] + src);
+    const T x3[3] = {a0.x, a0.y, a0.z};
+    has = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      stencil_range<T, MODE>(sc, x3[a], a, lo[a], hi[a]);
+      if (lo[a] > hi[a]) has = false;
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    int l = __reduce_min_sync(0xffffffffu, has ? lo[a] : INT_MAX);
+    int h = __reduce_max_sync(0xffffffffu, has ? hi[a] : INT_MIN);
+    if (lane == 0 && l != INT_MAX) {
+      atomicMin(&s_lo[a], l);
+      atomicMax(&s_hi[a], h);
+    }
+  }
+  __syncthreads();
+  VelTile<T> vt;
+  vt.tile = nullptr;
+  vt.vel = w.vel;
+  vt.L0 = s_lo[0];
+  vt.L1 = s_lo[1];
+  vt.L2 = s_lo[2];
+  vt.D0 = s_hi[0] - vt.L0 + 1;
+  vt.D1 = s_hi[1] - vt.L1 + 1;
+  const int D2 = s_hi[2] - vt.L2 + 1;
+  if (vt.L0 != INT_MAX && vt.D0 * vt.D1 * D2 <= w.max_tile_nodes) {
+    const int vol = vt.D0 * vt.D1 * D2;
+    for (int t = tid; t < vol; t += blockDim.x) {
+      int X = vt.L0 + t % vt.D0, Y = vt.L1 + (t / vt.D0) % vt.D1, Z = vt.L2 + t / (vt.D0 * vt.D1);
+      tile[t] = ld4(w.vel + node_index(sc, X, Y, Z));
+    }
+    vt.tile = tile;
+  }
+  __syncthreads();
   uint32_t err = 0;
-  bool fb = false, cl = false;
-  if (j < ch.z) {
-    const uint32_t src = w.perm ? w.perm[j] : uint32_t(j);
-    const V4 a0 = ld4(w.in[0] + src), a1 = ld4(w.in[1] + src), a2 = ld4(w.in[2] + src), a3 = ld4(w.in[3] + src);
+  bool cl = false, need = false;
+  if (live) {
     const T x0[3] = {a0.x, a0.y, a0.z};
-    const T F[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
     G2POut<T> o;
+    T pv[3] = {0, 0, 0};
+    if (MODE == AE_MPM_MODE_PHYSICS) g2p_physics_gather<T>(vt, sc, x0, pv, o.C);
+    cp_async_wait_all();
+    const V4 a1 = stage[tid], a2 = stage[nt + tid], a3 = stage[2 * nt + tid];
+    const T F[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
     if (MODE == AE_MPM_MODE_PHYSICS) {
       const MatDev& md = mat_of(w, sc, Bits<T>::unpack(a3.z) & 0xffffu);
-      g2p_physics<T>(w, sc, md, x0, F, a3.y, o);
+      g2p_physics_update<T>(sc, md, x0, pv, F, a3.y, o);
     } else if (MODE == AE_MPM_MODE_REFERENCE) {
-      g2p_reference<T>(w, sc, x0, F, o);
+      g2p_reference<T>(vt, sc, x0, F, o);
     } else {
       const V4 a4 = ld4(w.in[4] + src), a5 = ld4(w.in[5] + src), a6 = ld4(w.in[6] + src);
-      g2p_velonly<T>(w, sc, x0, o);
+      g2p_velonly<T>(vt, sc, x0, o);
 #pragma unroll
       for (int k = 0; k < 9; ++k) o.F[k] = F[k];
       o.J = a3.y;
@@ -813,19 +1043,55 @@ __global__ void __launch_bounds__(256) g2p_kernel(WorldDev<T> w, uint32_t* epoch
     w.out[6][j] = mk4(o.C[5], o.C[6], o.C[7], o.C[8]);
     w.keys[j] = cell_key(sc, MODE, o.x[0], o.x[1], o.x[2]);
     err = o.err;
-    fb = o.fallback;
     cl = o.clamped;
+    need = o.needs_clamp;
   } else if (j < ch.w) {
     w.keys[j] = sc.dead_key;
   }
-  // warp-aggregated error words and counters
+  // warp-aggregated error words, counters and clamp-queue appends
   const uint32_t e = __reduce_or_sync(0xffffffffu, err);
-  const uint32_t nfb = __popc(__ballot_sync(0xffffffffu, fb));
   const uint32_t ncl = __popc(__ballot_sync(0xffffffffu, cl));
-  if ((threadIdx.x & 31) == 0) {
+  const uint32_t qmask = __ballot_sync(0xffffffffu, need);
+  uint32_t qbase = 0;
+  if (lane == 0) {
     if (e) atomicOr(w.err + 4 * ch.x, e);
-    if (nfb) atomicAdd(w.err + 4 * ch.x + 1, nfb);
     if (ncl) atomicAdd(w.err + 4 * ch.x + 2, ncl);
+    if (qmask) qbase = atomicAdd(w.clamp_count, uint32_t(__popc(qmask)));
+  }
+  qbase = __shfl_sync(0xffffffffu, qbase, 0);
+  if (need) w.clamp_queue[qbase + __popc(qmask & ((1u << lane) - 1u))] = make_uint2(uint32_t(j), uint32_t(ch.x));
+}
+
+// Snow return mapping for the particles G2P queued: F = U S V^T, singular values clamped to
+// [1-theta_c, 1+theta_s], J_p *= prod(S)/prod(S_clamped) (ae_physics/src/mpm.rs:565-606 plus
+// Stomakhin's J_p), with the FP64 SVD redo where a near-degenerate pair straddles a threshold.
+template <class T>
+__global__ void __launch_bounds__(128) snow_clamp_kernel(WorldDev<T> w) {
+  using V4 = typename V4T<T>::type;
+  const uint32_t count = *reinterpret_cast<volatile uint32_t*>(w.clamp_count);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint2 q = w.clamp_queue[i];
+    const SceneDev<T>& sc = w.scenes[q.y];
+    V4 a1 = w.out[1][q.x], a2 = w.out[2][q.x], a3 = w.out[3][q.x];
+    const MatDev& md = mat_of(w, sc, Bits<T>::unpack(a3.z) & 0xffffu);
+    const T F[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
+    const T lo = T(1) - T(md.theta_c), hi = T(1) + T(md.theta_s);
+    T U[9], sg[3], V[9];
+    const bool fb = svd3_fallback(F, U, sg, V, w.svd_fallback != 0, lo, hi);
+    T scl[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) scl[k] = t_min(t_max(sg[k], lo), hi);
+    const T J = a3.y * ((sg[0] * sg[1] * sg[2]) / (scl[0] * scl[1] * scl[2]));
+    T nF[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        nF[r * 3 + c] = U[r * 3 + 0] * scl[0] * V[c * 3 + 0] + U[r * 3 + 1] * scl[1] * V[c * 3 + 1] + U[r * 3 + 2] * scl[2] * V[c * 3 + 2];
+    w.out[1][q.x] = mk4(nF[0], nF[1], nF[2], nF[3]);
+    w.out[2][q.x] = mk4(nF[4], nF[5], nF[6], nF[7]);
+    w.out[3][q.x] = mk4(nF[8], J, a3.z, a3.w);
+    if (fb) atomicAdd(w.err + 4 * q.y + 1, 1u);
   }
 }
 
@@ -890,6 +1156,7 @@ __global__ void __launch_bounds__(256) det_gather_kernel(WorldDev<T> w, uint32_t
   using V4 = typename V4T<T>::type;
   const uint32_t count = *reinterpret_cast<volatile uint32_t*>(w.touched_count);
   const uint32_t ep = *epoch;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *w.clamp_count = 0u;
   const int sub = threadIdx.x >> 6, l = threadIdx.x & 63;
   for (uint32_t t = blockIdx.x * 4 + sub; t < count; t += gridDim.x * 4) {
     const uint32_t gb = w.touched[t];
@@ -1167,6 +1434,10 @@ class World final : public WorldBase {
         err = "physics mode needs wall_margin >= 1";
         return AE_MPM_EINVAL;
       }
+      if (mode_ == AE_MPM_MODE_PHYSICS && (d.n[0] > 1024 || d.n[1] > 1024 || d.n[2] > 1024)) {
+        err = "physics-mode grids are limited to 1024 nodes per axis";
+        return AE_MPM_EINVAL;
+      }
       descs_.push_back(d);
       mats_.emplace_back(d.materials, d.materials + d.n_materials);
       blk += blocks_of(d);
@@ -1183,7 +1454,7 @@ class World final : public WorldBase {
     if (opts_.precision != 32 && opts_.precision != 64) opts_.precision = sizeof(T) == 8 ? 64 : 32;
     if (opts_.sort_interval < 1) opts_.sort_interval = 1;
     if (opts_.block_threads != 128 && opts_.block_threads != 256) opts_.block_threads = 256;
-    if (opts_.p2g_variant < kVarTile || opts_.p2g_variant > kVarGlobal) opts_.p2g_variant = kVarTile;
+    if (opts_.p2g_variant < kVarTile || opts_.p2g_variant > kVarLanes) opts_.p2g_variant = kVarLanes;
     AE_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     // scene table and materials
     uint64_t mat_off = 0, boff = 0, poff = 0;
@@ -1207,7 +1478,10 @@ class World final : public WorldBase {
       boff += nbk;
       h.mat_off = uint32_t(mat_off);
       h.n_mat = d.n_materials;
-      for (uint32_t k = 0; k < d.n_materials; ++k) h_mats_.push_back(mat_dev(d.materials[k], d.materials[k].model));
+      for (uint32_t k = 0; k < d.n_materials; ++k) {
+        h_mats_.push_back(mat_dev(d.materials[k], d.materials[k].model));
+        if (d.materials[k].model == kPhysSnow) has_snow_ = true;
+      }
       // out-of-range material index: materials[0]'s parameters; the reference pairs them with
       // the neo-Hookean model (mpm_solver.rs:840-841)
       h_mats_.push_back(mat_dev(d.materials[0], mode_ == AE_MPM_MODE_PHYSICS ? d.materials[0].model : kNeoHookean));
@@ -1253,6 +1527,7 @@ class World final : public WorldBase {
     AE_TRY(dmalloc(&touched_, sizeof(uint32_t) * blk));
     AE_TRY(dmalloc(&counters_, sizeof(uint32_t) * 4));
     AE_TRY(cudaMemset(counters_, 0, sizeof(uint32_t) * 4));
+    AE_TRY(dmalloc(&clamp_queue_, sizeof(uint2) * pc));
     AE_TRY(dmalloc(&err_, sizeof(uint32_t) * 4 * n));
     AE_TRY(cudaMemset(err_, 0, sizeof(uint32_t) * 4 * n));
     if (opts_.deterministic) {
@@ -1294,7 +1569,13 @@ class World final : public WorldBase {
       return AE_MPM_EINVAL;
     }
     fill_scene_params(h_scenes_[s], d);
-    for (uint32_t k = 0; k < d.n_materials; ++k) h_mats_[h_scenes_[s].mat_off + k] = mat_dev(d.materials[k], d.materials[k].model);
+    for (uint32_t k = 0; k < d.n_materials; ++k) {
+      h_mats_[h_scenes_[s].mat_off + k] = mat_dev(d.materials[k], d.materials[k].model);
+      if (d.materials[k].model == kPhysSnow && !has_snow_) {
+        has_snow_ = true;  // the substep gains the clamp kernel: recapture
+        invalidate_graph();
+      }
+    }
     h_mats_[h_scenes_[s].mat_off + d.n_materials] =
         mat_dev(d.materials[0], mode_ == AE_MPM_MODE_PHYSICS ? d.materials[0].model : kNeoHookean);
     scenes_dirty_ = true;
@@ -1624,7 +1905,7 @@ class World final : public WorldBase {
   int prepare() {
     if (opts_.block_threads != 128 && opts_.block_threads != 256) opts_.block_threads = 256;
     if (opts_.sort_interval < 1) opts_.sort_interval = 1;
-    if (opts_.p2g_variant < kVarTile || opts_.p2g_variant > kVarGlobal) opts_.p2g_variant = kVarTile;
+    if (opts_.p2g_variant < kVarTile || opts_.p2g_variant > kVarLanes) opts_.p2g_variant = kVarLanes;
     if (opts_.block_threads != chunk_threads_) chunks_dirty_ = true;
     if (chunks_dirty_) {
       chunk_threads_ = opts_.block_threads;
@@ -1692,6 +1973,8 @@ class World final : public WorldBase {
     w.cell_rec = cell_rec_;
     w.cell_count = opts_.deterministic ? counters_ + 1 : nullptr;
     w.seg_start = seg_start_;
+    w.clamp_queue = clamp_queue_;
+    w.clamp_count = counters_ + 3;
     return w;
   }
 
@@ -1710,6 +1993,15 @@ class World final : public WorldBase {
   template <int MODE>
   void launch_p2g(WorldDev<T>& w) {
     const size_t sm = sizeof(V4) * max_tile_nodes();
+    if (MODE == AE_MPM_MODE_PHYSICS && opts_.p2g_variant == kVarLanes) {
+      const size_t sm2 = sm + sizeof(V4) * kRecVecs * chunk_threads_;
+      if (!lanes_smem_set_) {
+        cudaFuncSetAttribute(p2g_lanes_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm2 + 1024));
+        lanes_smem_set_ = true;
+      }
+      p2g_lanes_kernel<T><<<n_chunks_, chunk_threads_, sm2, stream_>>>(w);
+      return;
+    }
     switch (opts_.p2g_variant) {
       case kVarWarpAgg: p2g_kernel<T, MODE, kVarWarpAgg><<<n_chunks_, chunk_threads_, sm, stream_>>>(w); break;
       case kVarGlobal: p2g_kernel<T, MODE, kVarGlobal><<<n_chunks_, chunk_threads_, 0, stream_>>>(w); break;
@@ -1731,12 +2023,17 @@ class World final : public WorldBase {
     } else {
       launch_p2g<MODE>(w);
       mark(2);
-      grid_update_kernel<T, MODE><<<sms * 8, 256, 0, stream_>>>(w, blk_epoch_, counters_ + 2);
+      grid_update_kernel<T, MODE><<<sms * 2, 256, 0, stream_>>>(w, blk_epoch_, counters_ + 2);
       launches_ += 2;
     }
     mark(3);
-    g2p_kernel<T, MODE><<<n_chunks_, chunk_threads_, 0, stream_>>>(w, counters_ + 2);
+    g2p_kernel<T, MODE><<<n_chunks_, chunk_threads_, sizeof(V4) * (max_tile_nodes() + 3 * chunk_threads_), stream_>>>(
+        w, counters_ + 2);
     ++launches_;
+    if (MODE == AE_MPM_MODE_PHYSICS && has_snow_) {
+      snow_clamp_kernel<T><<<sms * 4, 128, 0, stream_>>>(w);
+      ++launches_;
+    }
     mark(4);
   }
 
@@ -1816,6 +2113,7 @@ class World final : public WorldBase {
     dfree(cell_slot_);
     dfree(seg_start_);
     dfree(cell_rec_);
+    dfree(clamp_queue_);
     dfree(d_scenes_);
     dfree(d_mats_);
     dfree(blk_scene_);
@@ -1852,10 +2150,12 @@ class World final : public WorldBase {
   V4* acc_ = nullptr;
   V4* vel_ = nullptr;
   uint32_t *blk_flag_ = nullptr, *blk_epoch_ = nullptr, *touched_ = nullptr, *blk_scene_ = nullptr, *dead_blk_ = nullptr;
-  uint32_t* counters_ = nullptr;  // [touched count, cell count, epoch, spare]
+  uint32_t* counters_ = nullptr;  // [touched count, cell count, epoch, snow clamp queue count]
   uint32_t* err_ = nullptr;
   uint32_t *cell_slot_ = nullptr, *seg_start_ = nullptr;
   V4* cell_rec_ = nullptr;
+  uint2* clamp_queue_ = nullptr;
+  bool has_snow_ = false;
   T* stage_ = nullptr;
   size_t stage_bytes_ = 0;
   double* partial_ = nullptr;
@@ -1863,6 +2163,7 @@ class World final : public WorldBase {
   cudaGraphExec_t graph_ = nullptr;
   uint64_t graph_period_ = 0, graph_launches_ = 0;
   int graph_variant_ = -1;
+  bool lanes_smem_set_ = false;
   uint64_t substep_ = 0, snap_substep_ = 0, launches_ = 0;
   cudaEvent_t* stage_events_ = nullptr;
   uint64_t total_cap_ = 0, total_blocks_ = 0, device_bytes_ = 0;

@@ -71,6 +71,9 @@ struct WorldDev {
   uint32_t* err;  // per scene: [error bits, svd fallbacks, domain clamps, tile overflows]
   int32_t svd_fallback;
   int32_t max_tile_nodes;
+  // snow particles whose F left the elastic region: {slot, scene}, filled by G2P
+  uint2* clamp_queue;
+  uint32_t* clamp_count;
   // deterministic mode
   const uint32_t* sorted_keys;
   uint32_t* cell_slot;  // per node: index of the occupied cell record, or 0xffffffff

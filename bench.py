@@ -251,7 +251,7 @@ def run_ours(args, rank, local, world_size, pg):
     tune = None
     if not args.no_autotune:
         r = world.autotune(8)
-        tune = {"p2g_variant": {1: "tile", 2: "warp_agg", 3: "global"}.get(r.p2g_variant, r.p2g_variant),
+        tune = {"p2g_variant": {1: "tile", 2: "warp_agg", 3: "global", 4: "lanes"}.get(r.p2g_variant, r.p2g_variant),
                 "block_threads": r.block_threads, "sort_interval": r.sort_interval,
                 "us_per_substep": round(r.us_per_substep, 2)}
     world.step(max(args.warmup, 3))

@@ -174,7 +174,10 @@ typedef struct ae_mpm_scene_desc {
 } ae_mpm_scene_desc;
 
 /* Execution options of a world. */
-enum { AE_MPM_P2G_AUTO = 0, AE_MPM_P2G_TILE = 1, AE_MPM_P2G_WARP_AGG = 2, AE_MPM_P2G_GLOBAL = 3 };
+/* P2G variants: TILE = per-particle shared-tile atomics; WARP_AGG = same-cell runs reduced with
+ * __match_any_sync + shuffles first; GLOBAL = vector atomics straight to HBM; LANES = warp walks
+ * its sorted particles with one lane per stencil node (physics mode; others use TILE). */
+enum { AE_MPM_P2G_AUTO = 0, AE_MPM_P2G_TILE = 1, AE_MPM_P2G_WARP_AGG = 2, AE_MPM_P2G_GLOBAL = 3, AE_MPM_P2G_LANES = 4 };
 typedef struct ae_mpm_exec_opts {
   int32_t precision;      /* 32 or 64                                                        */
   int32_t deterministic;  /* 1: fixed-order segmented sums, no float atomics (bitwise replay) */

@@ -349,18 +349,40 @@ void svd3(const T* F, T* U, T* s, T* V) {
   std::memcpy(V, v, sizeof(v));
 }
 
-// Relative gap below which the FP32 SVD is recomputed in FP64: sqrt(eps_f32), the gap at which
-// FP32 singular vectors keep only half their digits.
+// Relative gap below which two FP32 singular values count as near-degenerate: sqrt(eps_f32),
+// the gap at which FP32 singular vectors keep only half their digits.
 constexpr double kSvdGapTol = 3.5e-4;
 
+// True when every singular value of F provably lies in [lo, hi] and det F > 0, so the snow clamp
+// is the identity map: Gershgorin discs of F^T F inside [lo^2, hi^2].
 template <class T>
-bool svd3_with_fallback(const T* F, T* U, T* s, T* V, bool allow_fallback) {
+bool clamp_is_identity(const T* F, T lo, T hi) {
+  T a[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) a[i * 3 + j] = F[0 * 3 + i] * F[0 * 3 + j] + F[1 * 3 + i] * F[1 * 3 + j] + F[2 * 3 + i] * F[2 * 3 + j];
+  T lo2 = lo * lo, hi2 = hi * hi;
+  for (int i = 0; i < 3; ++i) {
+    T r = T(0);
+    for (int j = 0; j < 3; ++j)
+      if (j != i) r += std::fabs(a[i * 3 + j]);
+    if (a[i * 4] - r < lo2 || a[i * 4] + r > hi2) return false;
+  }
+  return det3(F) > T(0);
+}
+
+// FP32 SVD, redone in FP64 when a near-degenerate pair of singular values straddles a clamp
+// threshold (the one case where the clamped result depends on the individual singular vectors).
+template <class T>
+bool svd3_with_fallback(const T* F, T* U, T* s, T* V, bool allow_fallback, T lo, T hi) {
   svd3(F, U, s, V);
   if (!allow_fallback || sizeof(T) == sizeof(double)) return false;
   T smax = std::max(std::fabs(s[0]), T(1e-30));
-  T g01 = std::fabs(s[0] - s[1]), g12 = std::fabs(s[1] - s[2]), g02 = std::fabs(s[0] - s[2]);
-  T gap = std::min(g01, std::min(g12, g02)) / smax;
-  if (gap >= T(kSvdGapTol)) return false;
+  bool need = false;
+  for (int i = 0; i < 3; ++i)
+    for (int j = i + 1; j < 3; ++j)
+      if (std::fabs(s[i] - s[j]) < T(kSvdGapTol) * smax && ((s[i] < lo) != (s[j] < lo) || (s[i] > hi) != (s[j] > hi)))
+        need = true;
+  if (!need) return false;
   double Fd[9], Ud[9], sd[3], Vd[9];
   for (int i = 0; i < 9; ++i) Fd[i] = double(F[i]);
   svd3(Fd, Ud, sd, Vd);
@@ -956,9 +978,13 @@ void phys_g2p_particle(const PhysGrid<T>& g, const Buf<T>& b, const std::vector<
   T nF[9];
   mat_mul(G, F, nF);
   if (pm.model == AE_MPM_PHYS_SNOW) {  // ae_physics/src/mpm.rs:565-606 with J_p bookkeeping
-    T U[9], sg[3], V[9];
-    if (svd3_with_fallback(nF, U, sg, V, fallback)) st.fallbacks++;
     T lo = T(1) - T(pm.theta_c), hi = T(1) + T(pm.theta_s);
+    if (clamp_is_identity(nF, lo, hi)) {  // elastic: F_E and J_p unchanged
+      std::memcpy(F, nF, sizeof(nF));
+      return;
+    }
+    T U[9], sg[3], V[9];
+    if (svd3_with_fallback(nF, U, sg, V, fallback, lo, hi)) st.fallbacks++;
     T sc[3];
     for (int k = 0; k < 3; ++k) sc[k] = std::min(std::max(sg[k], lo), hi);
     b.J[i] = b.J[i] * ((sg[0] * sg[1] * sg[2]) / (sc[0] * sc[1] * sc[2]));
@@ -1107,9 +1133,11 @@ int oracle_compute_stress(int32_t model, const ae_mpm_material* params, const fl
 
 void oracle_polar_decomp(const float F[9], float R[9], float S[9]) { polar_decomp<float>(F, R, S); }
 
-int oracle_svd3_f32(const float F[9], float U[9], float s[3], float V[9], int32_t allow_fallback) {
-  return svd3_with_fallback<float>(F, U, s, V, allow_fallback != 0) ? 1 : 0;
+// lo/hi: the clamp interval deciding whether a near-degenerate pair needs the FP64 redo
+int oracle_svd3_f32(const float F[9], float U[9], float s[3], float V[9], int32_t allow_fallback, float lo, float hi) {
+  return svd3_with_fallback<float>(F, U, s, V, allow_fallback != 0, lo, hi) ? 1 : 0;
 }
+int oracle_clamp_is_identity_f32(const float F[9], float lo, float hi) { return clamp_is_identity<float>(F, lo, hi) ? 1 : 0; }
 void oracle_svd3_f64(const double F[9], double U[9], double s[3], double V[9]) { svd3<double>(F, U, s, V); }
 
 void oracle_phys_tau_f64(const ae_mpm_material* m, const double F[9], double jslot, double tau[9]) {

@@ -39,7 +39,9 @@ def load():
                                           C.POINTER(f)]
     lib.oracle_polar_decomp.argtypes = [C.POINTER(f)] * 3
     lib.oracle_svd3_f32.restype = C.c_int
-    lib.oracle_svd3_f32.argtypes = [C.POINTER(f)] * 4 + [C.c_int32]
+    lib.oracle_svd3_f32.argtypes = [C.POINTER(f)] * 4 + [C.c_int32, f, f]
+    lib.oracle_clamp_is_identity_f32.restype = C.c_int
+    lib.oracle_clamp_is_identity_f32.argtypes = [C.POINTER(f), f, f]
     d = C.c_double
     lib.oracle_svd3_f64.argtypes = [C.POINTER(d)] * 4
     lib.oracle_phys_tau_f64.argtypes = [C.POINTER(M.Material), C.POINTER(d), d, C.POINTER(d)]
@@ -151,7 +153,12 @@ def polar_decomp(F):
     return R, S
 
 
-def svd3(F, f64: bool = False, allow_fallback: bool = True):
+def clamp_is_identity(F, lo: float, hi: float) -> bool:
+    F = np.ascontiguousarray(np.asarray(F, np.float32).reshape(9))
+    return bool(load().oracle_clamp_is_identity_f32(_fp(F), lo, hi))
+
+
+def svd3(F, f64: bool = False, allow_fallback: bool = True, lo: float = 1 - 2.5e-2, hi: float = 1 + 7.5e-3):
     if f64:
         F = np.ascontiguousarray(np.asarray(F, np.float64).reshape(9))
         U, s, V = np.zeros(9), np.zeros(3), np.zeros(9)
@@ -159,5 +166,5 @@ def svd3(F, f64: bool = False, allow_fallback: bool = True):
         return U.reshape(3, 3), s, V.reshape(3, 3), False
     F = np.ascontiguousarray(np.asarray(F, np.float32).reshape(9))
     U, s, V = np.zeros(9, np.float32), np.zeros(3, np.float32), np.zeros(9, np.float32)
-    fb = load().oracle_svd3_f32(_fp(F), _fp(U), _fp(s), _fp(V), 1 if allow_fallback else 0)
+    fb = load().oracle_svd3_f32(_fp(F), _fp(U), _fp(s), _fp(V), 1 if allow_fallback else 0, lo, hi)
     return U.reshape(3, 3), s, V.reshape(3, 3), bool(fb)

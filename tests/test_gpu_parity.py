@@ -64,7 +64,7 @@ def test_radix_sort_empty(ctx):
 
 
 # ------------------------------------------------------------------ physics mode parity
-@pytest.mark.parametrize("variant", [M.P2G_TILE, M.P2G_WARP_AGG, M.P2G_GLOBAL])
+@pytest.mark.parametrize("variant", [M.P2G_TILE, M.P2G_WARP_AGG, M.P2G_GLOBAL, M.P2G_LANES])
 def test_physics_jelly_matches_fp64_oracle(ctx, variant):
     sc, p = S.tiny_scene(4096, 32, S.jelly(), v=(0.7, -0.2, 0.3))
     ref = p.astype(np.float64)

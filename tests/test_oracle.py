@@ -132,13 +132,31 @@ def test_svd3_reconstructs_and_is_proper(seed):
         assert s[0] >= s[1] >= abs(s[2]) - 1e-6
 
 
-def test_svd3_near_degenerate_uses_fp64_fallback():
-    F = np.diag([1.0, 1.0 + 1e-6, 0.999]).astype(np.float32)
-    _, _, _, fb = O.svd3(F, f64=False, allow_fallback=True)
-    assert fb
-    F2 = np.diag([1.2, 1.0, 0.8]).astype(np.float32)
-    _, _, _, fb2 = O.svd3(F2, f64=False, allow_fallback=True)
-    assert not fb2
+def test_svd3_fp64_fallback_only_where_a_degenerate_pair_straddles_a_threshold():
+    lo, hi = 1 - 2.5e-2, 1 + 7.5e-3
+    # sigma_0 ~ sigma_1 on both sides of the stretch threshold hi: their clamped values differ
+    F = np.diag([hi + 5e-5, hi - 5e-5, 0.999]).astype(np.float32)
+    assert O.svd3(F, allow_fallback=True, lo=lo, hi=hi)[3]
+    # near-degenerate but on the same side (both clamped to hi): FP32 suffices
+    F = np.diag([1.02, 1.02 + 1e-6, 0.999]).astype(np.float32)
+    assert not O.svd3(F, allow_fallback=True, lo=lo, hi=hi)[3]
+    # well separated
+    assert not O.svd3(np.diag([1.2, 1.0, 0.8]).astype(np.float32), allow_fallback=True, lo=lo, hi=hi)[3]
+
+
+def test_clamp_identity_fast_path_is_exact():
+    lo, hi = 1 - 2.5e-2, 1 + 7.5e-3
+    rng = np.random.default_rng(7)
+    for _ in range(200):
+        F = np.eye(3) + rng.normal(0, 4e-3, (3, 3))
+        s = np.linalg.svd(F)[1]
+        inside = s.min() >= lo and s.max() <= hi and np.linalg.det(F) > 0
+        if O.clamp_is_identity(F, lo, hi):
+            assert inside  # the bound never claims a clamp-free F that would be clamped
+    th = 0.4
+    R = np.array([[math.cos(th), -math.sin(th), 0], [math.sin(th), math.cos(th), 0], [0, 0, 1]])
+    assert O.clamp_is_identity(R, lo, hi)  # pure rotations need no SVD
+    assert not O.clamp_is_identity(np.diag([1.0, 1.0, -1.0]), lo, hi)  # inverted
 
 
 def test_svd3_reflection_gives_negative_last_singular_value():
