@@ -119,6 +119,7 @@ SIGNATURES = {
     "ae_mpm_world_stream": (_P, [_P]),
     "ae_mpm_world_particles": (C.c_uint64, [_P]),
     "ae_mpm_radix_sort_keys": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, _P, _P]),
+    "ae_mpm_radix_sort_keys_noalloc": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, _P, _P, _P]),
     "ae_mpm_world_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(TuneResult)]),
     "ae_mpm_server_create": (C.c_int, [_P, C.POINTER(ServerOpts), C.POINTER(_P)]),
     "ae_mpm_server_submit": (C.c_int, [_P, C.POINTER(SceneDesc), C.POINTER(ParticlesView), C.c_uint64, C.c_uint32,

@@ -8,7 +8,7 @@ fn main() {
     let csrc = PathBuf::from(env::var("CARGO_MANIFEST_DIR").unwrap()).join("../csrc");
     let out = PathBuf::from(env::var("OUT_DIR").unwrap());
     let nvcc = env::var("NVCC").unwrap_or_else(|_| "nvcc".to_string());
-    let sources = ["radix_sort.cu", "mpm_world.cu", "ae_mpm_api.cu", "ae_mpm_server.cu"];
+    let sources = ["radix_sort.cu", "mpm_world.cu", "ae_mpm_api.cu", "ae_mpm_server.cu", "ae_mpm_noalloc.cu"];
     let mut objects = Vec::new();
     for src in sources.iter() {
         let obj = out.join(src.replace(".cu", ".o"));

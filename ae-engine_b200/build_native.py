@@ -26,7 +26,7 @@ LIB = os.path.join(BUILD, "libae_mpm.so")
 HOST_TEST = os.path.join(BUILD, "test_host_mirror")
 ORACLE_LIB = os.path.join(ORACLE_BUILD, "libae_mpm_oracle.so")
 
-CU_SOURCES = ["radix_sort.cu", "mpm_world.cu", "ae_mpm_api.cu", "ae_mpm_server.cu"]
+CU_SOURCES = ["radix_sort.cu", "mpm_world.cu", "ae_mpm_api.cu", "ae_mpm_server.cu", "ae_mpm_noalloc.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",

@@ -47,6 +47,9 @@ struct ae_mpm_world {
 
 namespace aemp {
 int ctx_device(const ae_mpm_ctx* ctx) { return ctx ? ctx->device : 0; }
+void ctx_set_error(ae_mpm_ctx* ctx, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+}
 }  // namespace aemp
 
 namespace {

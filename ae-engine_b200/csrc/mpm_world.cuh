@@ -128,7 +128,8 @@ uint64_t scene_device_bytes(const ae_mpm_scene_desc& d, int precision);
 // Device SM count (cached per device).
 int device_sm_count();
 
-// CUDA device of a context (defined with the C ABI).
+// CUDA device of a context and its error text (defined with the C ABI).
 int ctx_device(const ae_mpm_ctx* ctx);
+void ctx_set_error(ae_mpm_ctx* ctx, const std::string& msg);
 
 }  // namespace aemp

@@ -228,3 +228,34 @@ int radix_sort_pairs(uint32_t* keys, uint64_t n, int key_bits, SortScratch& s, c
 }
 
 }  // namespace aemp
+
+namespace aemp {
+
+int radix_sort_pairs_into(const uint32_t* keys_in, uint64_t n, int key_bits, uint32_t* keys_out, uint32_t* vals_out,
+                          uint32_t* keys_alt, uint32_t* vals_alt, uint32_t* hist, uint32_t* offsets, uint32_t* totals,
+                          cudaStream_t stream) {
+  if (n == 0) return 0;
+  const SortPlan p = make_sort_plan(key_bits);
+  const uint32_t tiles = uint32_t(sort_tiles(n));
+  cudaMemsetAsync(totals, 0, sizeof(uint32_t) * 4 * kMaxRadix, stream);
+  const uint32_t* kin = keys_in;
+  const uint32_t* vin = nullptr;
+  int launches = 0;
+  for (int ps = 0; ps < p.passes; ++ps) {
+    // the last pass writes the caller's output; earlier passes alternate so that holds
+    const bool to_out = ((p.passes - 1 - ps) % 2) == 0;
+    uint32_t* kout = to_out ? keys_out : keys_alt;
+    uint32_t* vout = to_out ? vals_out : vals_alt;
+    const uint32_t mask = (1u << p.bits[ps]) - 1u;
+    uint32_t* tot = totals + ps * kMaxRadix;
+    sort_hist<<<tiles, kSortThreads, 0, stream>>>(kin, n, p.shift[ps], mask, hist, tot, tiles);
+    sort_scan<<<mask + 1, kScanThreads, 0, stream>>>(hist, tot, offsets, tiles);
+    sort_scatter<<<tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, p.shift[ps], mask, offsets, tiles);
+    launches += 3;
+    kin = kout;
+    vin = vout;
+  }
+  return launches;
+}
+
+}  // namespace aemp

@@ -74,4 +74,12 @@ void sort_scratch_free(SortScratch& s, SortFreeFn release = nullptr, void* user 
 int radix_sort_pairs(uint32_t* keys, uint64_t n, int key_bits, SortScratch& s, cudaStream_t stream,
                      const uint32_t** sorted_keys_out, const uint32_t** perm_out);
 
+// Same sort with every buffer supplied by the caller: keys_in is only read; the result lands in
+// keys_out / vals_out; keys_alt / vals_alt (n entries each), hist and offsets (kMaxRadix *
+// sort_tiles(n) entries each) and totals (4 * kMaxRadix entries) are scratch.  Clears the
+// totals itself; allocates nothing.  Returns the kernel launch count.
+int radix_sort_pairs_into(const uint32_t* keys_in, uint64_t n, int key_bits, uint32_t* keys_out, uint32_t* vals_out,
+                          uint32_t* keys_alt, uint32_t* vals_alt, uint32_t* hist, uint32_t* offsets, uint32_t* totals,
+                          cudaStream_t stream);
+
 }  // namespace aemp

@@ -278,6 +278,20 @@ uint64_t ae_mpm_world_particles(const ae_mpm_world* world);
 int ae_mpm_radix_sort_keys(ae_mpm_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t key_bits,
                            uint32_t* sorted_keys_out, uint32_t* perm_out);
 
+/* The same sort for callers that cannot allocate GPU memory: an engine frame loop living on
+ * memory it reserved up front, work queued during CUDA stream capture, a host whose own pool owns
+ * all of HBM.  This entry point has no counterpart in the reference.  keys_dev, sorted_keys_dev
+ * and perm_dev are device buffers the caller owns; the scratch is a fixed array compiled into the
+ * library (about 9 MB per GPU that loads it, held until exit), so at most
+ * AE_MPM_NOALLOC_MAX_KEYS keys are accepted and larger n is AE_MPM_EINVAL.  Nothing is allocated
+ * or freed.  The work is queued on `stream` (a cudaStream_t; NULL = default stream).  ctx may be
+ * NULL; when given, its device is made current and failures leave their text in it.  The first
+ * call on a device looks up the array's device address, so make that first call before any stream
+ * capture.  All calls on a device share the scratch: calls whose work overlaps on the GPU race. */
+#define AE_MPM_NOALLOC_MAX_KEYS (1u << 20)
+int ae_mpm_radix_sort_keys_noalloc(ae_mpm_ctx* ctx, const uint32_t* keys_dev, uint64_t n, uint32_t key_bits,
+                                   uint32_t* sorted_keys_dev, uint32_t* perm_dev, void* stream);
+
 /* ---------------------------------------------------------------------------------------------
  * Autotuner: times the P2G variants, block sizes and sort intervals on a world and writes the
  * fastest choice back into the world's options.  Choices are cached per workload signature.
