@@ -109,6 +109,7 @@ SIGNATURES = {
     "ae_mpm_world_upload": (C.c_int, [_P, C.c_uint32, C.POINTER(ParticlesView), C.c_uint64]),
     "ae_mpm_world_upload_f64": (C.c_int, [_P, C.c_uint32, C.POINTER(ParticlesView), C.c_uint64]),
     "ae_mpm_world_step": (C.c_int, [_P, C.c_uint32]),
+    "ae_mpm_world_set_scene": (C.c_int, [_P, C.c_uint32, C.POINTER(SceneDesc)]),
     "ae_mpm_world_sync": (C.c_int, [_P]),
     "ae_mpm_world_download": (C.c_int, [_P, C.c_uint32, C.POINTER(ParticlesView)]),
     "ae_mpm_world_download_f64": (C.c_int, [_P, C.c_uint32, C.POINTER(ParticlesView)]),
@@ -350,6 +351,11 @@ class World:
 
     def step(self, n: int) -> None:
         self.ctx.check(self.ctx.lib.ae_mpm_world_step(self.h, n))
+
+    def set_scene(self, index: int, scene: "Scene") -> None:
+        d = scene.desc()
+        self.ctx.check(self.ctx.lib.ae_mpm_world_set_scene(self.h, index, C.byref(d)))
+        self.scenes[index] = scene
 
     def sync(self, raise_on_error: bool = True) -> int:
         rc = self.ctx.lib.ae_mpm_world_sync(self.h)

@@ -348,6 +348,10 @@ int ae_mpm_world_upload_f64(ae_mpm_world* world, uint32_t scene, const ae_mpm_pa
   if (world && !host) return fail(world->ctx, AE_MPM_EINVAL, "null particle view");
   AE_WORLD_CALL(world->w->upload(scene, host, n, true));
 }
+int ae_mpm_world_set_scene(ae_mpm_world* world, uint32_t scene, const ae_mpm_scene_desc* desc) {
+  if (world && !desc) return fail(world->ctx, AE_MPM_EINVAL, "null scene description");
+  AE_WORLD_CALL(world->w->set_scene_params(scene, *desc));
+}
 int ae_mpm_world_step(ae_mpm_world* world, uint32_t n_substeps) { AE_WORLD_CALL(world->w->step(n_substeps)); }
 int ae_mpm_world_sync(ae_mpm_world* world) { AE_WORLD_CALL(world->w->sync()); }
 int ae_mpm_world_download(ae_mpm_world* world, uint32_t scene, ae_mpm_particles* host) {

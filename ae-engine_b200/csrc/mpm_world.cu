@@ -124,6 +124,24 @@ __device__ __forceinline__ const MatDev& mat_of(const WorldDev<T>& w, const Scen
   return w.mats[sc.mat_off + (m < sc.n_mat ? m : sc.n_mat)];
 }
 
+// MLS-MPM affine momentum matrix (Hu et al. 2018): A = m C - k tau(F, J) with
+// k = 4 dt V0 / dx^2, V0 = m / rho.  Physics mode stores A in the particle's C slot between
+// substeps (G2P computes it while F is in registers), so P2G needs neither F nor the stress;
+// pack/unpack convert to and from the caller's C at the boundary.
+template <class T>
+__device__ __forceinline__ T affine_k(const SceneDev<T>& sc, const MatDev& md, T m) {
+  return T(4) * sc.dt * (m / T(md.rho)) * sc.inv_dx * sc.inv_dx;
+}
+template <class T>
+__device__ __forceinline__ void affine_from_c(const SceneDev<T>& sc, const MatDev& md, T m, const T* C, const T* F, T J,
+                                              T* A) {
+  T tau[9];
+  phys_tau(md, F, J, tau);
+  const T k = affine_k(sc, md, m);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) A[i] = m * C[i] - k * tau[i];
+}
+
 // ============================================================================================
 // per-particle P2G setup
 // ============================================================================================
@@ -151,6 +169,14 @@ __device__ __forceinline__ void p2g_setup(const WorldDev<T>& w, const SceneDev<T
     p.v[0] = a4.x;
     p.v[1] = a4.y;
     p.v[2] = a4.z;
+  } else if (MODE == AE_MPM_MODE_PHYSICS) {
+    const V4 a5 = ld4(w.in[5] + src), a6 = ld4(w.in[6] + src);
+    const T A[9] = {a4.w, a5.x, a5.y, a5.z, a5.w, a6.x, a6.y, a6.z, a6.w};
+#pragma unroll
+    for (int k = 0; k < 9; ++k) p.A[k] = A[k];
+    p.v[0] = p.m * a4.x;
+    p.v[1] = p.m * a4.y;
+    p.v[2] = p.m * a4.z;
   } else {
     const V4 a1 = ld4(w.in[1] + src), a2 = ld4(w.in[2] + src), a3 = ld4(w.in[3] + src);
     const V4 a5 = ld4(w.in[5] + src), a6 = ld4(w.in[6] + src);
@@ -158,16 +184,7 @@ __device__ __forceinline__ void p2g_setup(const WorldDev<T>& w, const SceneDev<T
     T C[9] = {a4.w, a5.x, a5.y, a5.z, a5.w, a6.x, a6.y, a6.z, a6.w};
     T J = a3.y;
     const MatDev& md = mat_of(w, sc, Bits<T>::unpack(a3.z) & 0xffffu);
-    if (MODE == AE_MPM_MODE_PHYSICS) {
-      T tau[9];
-      phys_tau(md, F, J, tau);
-      T kst = T(4) * sc.dt * (p.m / T(md.rho)) * sc.inv_dx * sc.inv_dx;
-#pragma unroll
-      for (int k = 0; k < 9; ++k) p.A[k] = p.m * C[k] - kst * tau[k];
-      p.v[0] = p.m * a4.x;
-      p.v[1] = p.m * a4.y;
-      p.v[2] = p.m * a4.z;
-    } else {
+    {
       T st[9];
       ref_stress(md, F, J, st);
       T vol = p.m / T(md.rho);
@@ -697,7 +714,7 @@ __device__ __forceinline__ void g2p_physics_gather(const VelTile<T>& vt, const S
 // update half of the physics G2P: advection, F update and the material's return mapping
 template <class T>
 __device__ __forceinline__ void g2p_physics_update(const SceneDev<T>& sc, const MatDev& md, const T* x0, const T* v,
-                                                   const T* F, T J, G2POut<T>& o) {
+                                                   const T* F, T J, T m, G2POut<T>& o) {
   bool nan = false, clamped = false;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -717,6 +734,10 @@ __device__ __forceinline__ void g2p_physics_update(const SceneDev<T>& sc, const 
     o.J = t_max(Jn, T(0.01));
 #pragma unroll
     for (int k = 0; k < 9; ++k) o.F[k] = F[k];
+    T A[9];
+    affine_from_c(sc, md, m, o.C, o.F, o.J, A);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) o.C[k] = A[k];
     return;
   }
   T G[9];
@@ -725,11 +746,17 @@ __device__ __forceinline__ void g2p_physics_update(const SceneDev<T>& sc, const 
   mm3(G, F, o.F);
   if (md.model == kPhysSnow) {
     // elastic region (every singular value provably inside the clamp interval): F_E and J_p
-    // are final; otherwise the clamp kernel does the SVD and the return mapping
+    // are final; otherwise the clamp kernel does the SVD, the return mapping and A
     o.J = J;
     o.needs_clamp = !clamp_is_identity(o.F, T(1) - T(md.theta_c), T(1) + T(md.theta_s));
   } else {
     o.J = det3(o.F);
+  }
+  if (!o.needs_clamp) {  // the C slot carries A from here on
+    T A[9];
+    affine_from_c(sc, md, m, o.C, o.F, o.J, A);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) o.C[k] = A[k];
   }
 }
 
@@ -1015,7 +1042,7 @@ __global__ void __launch_bounds__(256) g2p_kernel(WorldDev<T> w, uint32_t* epoch
     const T F[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
     if (MODE == AE_MPM_MODE_PHYSICS) {
       const MatDev& md = mat_of(w, sc, Bits<T>::unpack(a3.z) & 0xffffu);
-      g2p_physics_update<T>(sc, md, x0, pv, F, a3.y, o);
+      g2p_physics_update<T>(sc, md, x0, pv, F, a3.y, a0.w, o);
     } else if (MODE == AE_MPM_MODE_REFERENCE) {
       g2p_reference<T>(vt, sc, x0, F, o);
     } else {
@@ -1091,6 +1118,14 @@ __global__ void __launch_bounds__(128) snow_clamp_kernel(WorldDev<T> w) {
     w.out[1][q.x] = mk4(nF[0], nF[1], nF[2], nF[3]);
     w.out[2][q.x] = mk4(nF[4], nF[5], nF[6], nF[7]);
     w.out[3][q.x] = mk4(nF[8], J, a3.z, a3.w);
+    // G2P left C in the C slot of queued particles: turn it into A with the returned F and J_p
+    const V4 a0 = w.out[0][q.x], a4 = w.out[4][q.x], a5 = w.out[5][q.x], a6 = w.out[6][q.x];
+    const T C[9] = {a4.w, a5.x, a5.y, a5.z, a5.w, a6.x, a6.y, a6.z, a6.w};
+    T A[9];
+    affine_from_c(sc, md, a0.w, C, nF, J, A);
+    w.out[4][q.x] = mk4(a4.x, a4.y, a4.z, A[0]);
+    w.out[5][q.x] = mk4(A[1], A[2], A[3], A[4]);
+    w.out[6][q.x] = mk4(A[5], A[6], A[7], A[8]);
     if (fb) atomicAdd(w.err + 4 * q.y + 1, 1u);
   }
 }
@@ -1215,7 +1250,8 @@ __global__ void init_keys_kernel(WorldDev<T> w) {
 
 // staging layout (elements of T): pos 3n | vel 3n | F 9n | J n | C 9n | mass n | then u16 mat n
 template <class T>
-__global__ void pack_kernel(typename V4T<T>::type* const* dst, const T* __restrict__ st, uint64_t n, uint32_t p_off) {
+__global__ void pack_kernel(typename V4T<T>::type* const* dst, const T* __restrict__ st, uint64_t n, uint32_t p_off,
+                            const SceneDev<T>* scp, const MatDev* mats) {
   uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const T* pos = st;
@@ -1230,13 +1266,28 @@ __global__ void pack_kernel(typename V4T<T>::type* const* dst, const T* __restri
   dst[1][s] = mk4(F[9 * i], F[9 * i + 1], F[9 * i + 2], F[9 * i + 3]);
   dst[2][s] = mk4(F[9 * i + 4], F[9 * i + 5], F[9 * i + 6], F[9 * i + 7]);
   dst[3][s] = mk4(F[9 * i + 8], J[i], Bits<T>::pack(uint32_t(mat[i])), Bits<T>::pack(uint32_t(i)));
-  dst[4][s] = mk4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], C[9 * i]);
-  dst[5][s] = mk4(C[9 * i + 1], C[9 * i + 2], C[9 * i + 3], C[9 * i + 4]);
-  dst[6][s] = mk4(C[9 * i + 5], C[9 * i + 6], C[9 * i + 7], C[9 * i + 8]);
+  T c[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) c[k] = C[9 * i + k];
+  const SceneDev<T>& sc = *scp;
+  if (sc.mode == AE_MPM_MODE_PHYSICS) {  // the C slot holds A = m C - k tau on the device
+    const uint32_t mi = mat[i];
+    const MatDev& md = mats[sc.mat_off + (mi < sc.n_mat ? mi : sc.n_mat)];
+    T f[9], a[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = F[9 * i + k];
+    affine_from_c(sc, md, mass[i], c, f, J[i], a);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) c[k] = a[k];
+  }
+  dst[4][s] = mk4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], c[0]);
+  dst[5][s] = mk4(c[1], c[2], c[3], c[4]);
+  dst[6][s] = mk4(c[5], c[6], c[7], c[8]);
 }
 
 template <class T>
-__global__ void unpack_kernel(const typename V4T<T>::type* const* src, T* __restrict__ st, uint64_t n, uint32_t p_off) {
+__global__ void unpack_kernel(const typename V4T<T>::type* const* src, T* __restrict__ st, uint64_t n, uint32_t p_off,
+                              const SceneDev<T>* scp, const MatDev* mats) {
   using V4 = typename V4T<T>::type;
   uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -1256,7 +1307,17 @@ __global__ void unpack_kernel(const typename V4T<T>::type* const* src, T* __rest
   pos[3 * o + 2] = a0.z;
   mass[o] = a0.w;
   const T f[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
-  const T c[9] = {a4.w, a5.x, a5.y, a5.z, a5.w, a6.x, a6.y, a6.z, a6.w};
+  T c[9] = {a4.w, a5.x, a5.y, a5.z, a5.w, a6.x, a6.y, a6.z, a6.w};
+  const SceneDev<T>& sc = *scp;
+  if (sc.mode == AE_MPM_MODE_PHYSICS) {  // C = (A + k tau) / m
+    const uint32_t mi = Bits<T>::unpack(a3.z) & 0xffffu;
+    const MatDev& md = mats[sc.mat_off + (mi < sc.n_mat ? mi : sc.n_mat)];
+    T tau[9];
+    phys_tau(md, f, a3.y, tau);
+    const T k = affine_k(sc, md, a0.w);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) c[q] = (c[q] + k * tau[q]) / a0.w;
+  }
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
     F[9 * o + k] = f[k];
@@ -1568,6 +1629,22 @@ class World final : public WorldBase {
       err = "material count of a resident scene cannot change";
       return AE_MPM_EINVAL;
     }
+    if (d.mode != mode_ || !(d.dx > 0.0f) || !(d.dt >= 0.0f) || (mode_ == AE_MPM_MODE_PHYSICS && d.wall_margin < 1)) {
+      err = "scene update needs the world's mode, dx > 0, dt >= 0 and (physics) wall_margin >= 1";
+      return AE_MPM_EINVAL;
+    }
+    // physics mode stores A = m C - k tau, which depends on dt and the materials: convert the
+    // resident particles back to C with the old tables and again to A with the new ones
+    const uint64_t cnt = h_scenes_[s].p_count;
+    const bool rebase = mode_ == AE_MPM_MODE_PHYSICS && cnt > 0;
+    if (rebase) {
+      int rc = ensure_stage(cnt);
+      if (rc) return rc;
+      if ((rc = sync_tables())) return rc;
+      unpack_kernel<T><<<unsigned((cnt + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), stage_, cnt, h_scenes_[s].p_off,
+                                                                          d_scenes_ + s, d_mats_);
+      AE_TRY(cudaGetLastError());
+    }
     fill_scene_params(h_scenes_[s], d);
     for (uint32_t k = 0; k < d.n_materials; ++k) {
       h_mats_[h_scenes_[s].mat_off + k] = mat_dev(d.materials[k], d.materials[k].model);
@@ -1580,6 +1657,15 @@ class World final : public WorldBase {
         mat_dev(d.materials[0], mode_ == AE_MPM_MODE_PHYSICS ? d.materials[0].model : kNeoHookean);
     scenes_dirty_ = true;
     mats_dirty_ = true;
+    keys_stale_ = true;  // dx or origin may have moved the cells
+    if (rebase) {
+      int rc = sync_tables();
+      if (rc) return rc;
+      pack_kernel<T><<<unsigned((cnt + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), stage_, cnt, h_scenes_[s].p_off,
+                                                                        d_scenes_ + s, d_mats_);
+      AE_TRY(cudaGetLastError());
+      keys_stale_ = true;
+    }
     return AE_MPM_OK;
   }
 
@@ -1613,7 +1699,10 @@ class World final : public WorldBase {
       AE_TRY(cudaMemcpyAsync(stage_ + 16 * n, f[4], sizeof(T) * 9 * n, cudaMemcpyHostToDevice, stream_));
       AE_TRY(cudaMemcpyAsync(stage_ + 25 * n, f[5], sizeof(T) * n, cudaMemcpyHostToDevice, stream_));
       AE_TRY(cudaMemcpyAsync(stage_ + 26 * n, hv.mat, sizeof(uint16_t) * n, cudaMemcpyHostToDevice, stream_));
-      pack_kernel<T><<<unsigned((n + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), stage_, n, h_scenes_[s].p_off);
+      rc = sync_tables();
+      if (rc) return rc;
+      pack_kernel<T><<<unsigned((n + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), stage_, n, h_scenes_[s].p_off,
+                                                                      d_scenes_ + s, d_mats_);
       AE_TRY(cudaGetLastError());
     }
     h_scenes_[s].p_count = uint32_t(n);
@@ -1640,7 +1729,10 @@ class World final : public WorldBase {
     }
     int rc = ensure_stage(n);
     if (rc) return rc;
-    unpack_kernel<T><<<unsigned((n + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), stage_, n, h_scenes_[s].p_off);
+    rc = sync_tables();
+    if (rc) return rc;
+    unpack_kernel<T><<<unsigned((n + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), stage_, n, h_scenes_[s].p_off,
+                                                                      d_scenes_ + s, d_mats_);
     AE_TRY(cudaGetLastError());
     AE_TRY(cudaMemcpyAsync(f[0], stage_, sizeof(T) * 3 * n, cudaMemcpyDeviceToHost, stream_));
     AE_TRY(cudaMemcpyAsync(f[1], stage_ + 3 * n, sizeof(T) * 3 * n, cudaMemcpyDeviceToHost, stream_));
@@ -1935,6 +2027,14 @@ class World final : public WorldBase {
       }
       chunks_dirty_ = false;
     }
+    int rc = sync_tables();
+    if (rc) return rc;
+    // the tables are copied from pageable host memory, which the copy stages before returning
+    return AE_MPM_OK;
+  }
+
+  // scene and material tables to the device (copied from pageable memory, staged at the call)
+  int sync_tables() {
     if (scenes_dirty_) {
       AE_TRY(cudaMemcpyAsync(d_scenes_, h_scenes_.data(), sizeof(SceneDev<T>) * h_scenes_.size(), cudaMemcpyHostToDevice,
                              stream_));
@@ -1944,7 +2044,6 @@ class World final : public WorldBase {
       AE_TRY(cudaMemcpyAsync(d_mats_, h_mats_.data(), sizeof(MatDev) * h_mats_.size(), cudaMemcpyHostToDevice, stream_));
       mats_dirty_ = false;
     }
-    // the tables are copied from pageable host memory, which the copy stages before returning
     return AE_MPM_OK;
   }
 

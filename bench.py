@@ -152,6 +152,11 @@ def barrier(pg):
         pg.barrier()
 
 
+def shard(items, rank: int, world_size: int):
+    """Scenes of a batched workload dealt round-robin to ranks (scenes are independent)."""
+    return list(items[rank::world_size])
+
+
 def workload(name: str, rank: int, n_scenes: int):
     import ae_mpm_scenes as S
 

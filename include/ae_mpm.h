@@ -247,6 +247,9 @@ int ae_mpm_world_destroy(ae_mpm_world* world);
  * The _f64 variants are for precision-64 worlds. */
 int ae_mpm_world_upload(ae_mpm_world* world, uint32_t scene, const ae_mpm_particles* host, uint64_t n);
 int ae_mpm_world_upload_f64(ae_mpm_world* world, uint32_t scene, const ae_mpm_particles_f64* host, uint64_t n);
+/* Change a resident scene's dt, gravity, walls, damping, origin or material parameters (grid size
+ * and material count stay), e.g. a CFL-adapted dt per frame as the reference's total_dt per call. */
+int ae_mpm_world_set_scene(ae_mpm_world* world, uint32_t scene, const ae_mpm_scene_desc* desc);
 /* Queue n substeps of every scene (asynchronous; returns after queueing). */
 int ae_mpm_world_step(ae_mpm_world* world, uint32_t n_substeps);
 /* Wait for queued work; returns AE_MPM_ENAN / AE_MPM_EDOMAIN if a scene raised its error word. */

@@ -1,0 +1,222 @@
+"""GPU tests of the features around the substep: scene updates, error words and host-side fault
+injection, FP64 totals and conservation, the autotuner, the continuous-batching server, and the
+BASELINE configurations at (or near) full size.
+
+Tolerances are stated per check.  Faults are injected on the host only (NaN and out-of-domain
+inputs, oversize requests, cancellation); nothing here faults, traps or hangs the GPU.
+"""
+import time
+
+import numpy as np
+import pytest
+
+import ae_mpm as M
+import ae_mpm_scenes as S
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b, floor=1e-12):
+    return float(np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64)).max() /
+                 max(float(np.abs(np.asarray(b, np.float64)).max()), floor))
+
+
+def world_of(ctx, scenes, parts, **opts):
+    f64 = parts[0].dtype == np.float64
+    w = M.World(ctx, scenes, M.exec_opts(precision=64 if f64 else 32, **opts))
+    for i, p in enumerate(parts):
+        w.upload(i, p)
+    return w
+
+
+# ------------------------------------------------------------------ scene updates
+def test_set_scene_changes_dt_mid_run_like_the_oracle(ctx):
+    sc, p = S.tiny_scene(4096, 32, S.snow(), v=(1.0, -0.5, 0.0))
+    ref = p.astype(np.float64)
+    w = world_of(ctx, [sc], [p.astype(np.float64)])
+    O.run(sc, ref, 10)
+    w.step(10)
+    sc2 = S.tiny_scene(4096, 32, S.snow(E=2.0e5))[0]
+    sc2.dt = 5e-5
+    sc2.gravity = (0.0, -5.0, 0.0)
+    w.set_scene(0, sc2)
+    O.run(sc2, ref, 10)
+    w.step(10)
+    got = w.download(0, p.n)
+    assert rel(got.pos, ref.pos) <= 1e-10
+    assert rel(got.F, ref.F) <= 1e-10
+    assert np.abs(got.C - ref.C).max() <= 1e-8 * np.abs(ref.vel).max() / sc.dx
+
+
+def test_set_scene_rejects_grid_or_mode_changes(ctx):
+    sc, p = S.tiny_scene(512, 16)
+    w = world_of(ctx, [sc], [p])
+    bad = S.tiny_scene(512, 32)[0]
+    with pytest.raises(M.MpmError):
+        w.set_scene(0, bad)
+    bad2 = S.tiny_scene(512, 16)[0]
+    bad2.mode = M.MODE_REFERENCE
+    with pytest.raises(M.MpmError):
+        w.set_scene(0, bad2)
+
+
+# ------------------------------------------------------------------ error words (host-side injection)
+def test_nan_position_raises_enan(ctx):
+    sc, p = S.tiny_scene(512, 16)
+    p.pos[7] = (np.nan, 0.5, 0.5)
+    w = world_of(ctx, [sc], [p])
+    w.step(2)
+    assert w.sync(raise_on_error=False) == M.ENAN
+    word, _ = w.errors(0)
+    assert word & 1
+
+
+def test_out_of_domain_particles_are_clamped_and_reported(ctx):
+    # 40 m/s for 100 substeps of 1e-4 s carries the block 0.4 m, past the domain edge (14/16)
+    sc, p = S.tiny_scene(512, 16, v=(40.0, 0.0, 0.0))
+    sc.wall_mode = M.WALL_SLIP
+    sc.wall_margin = 1
+    sc.restitution = 1.0
+    w = world_of(ctx, [sc], [p])
+    w.step(100)
+    assert w.sync(raise_on_error=False) == M.EDOMAIN
+    got = w.download(0, p.n)
+    assert (got.pos <= (sc.n[0] - 2) * sc.dx + 1e-6).all() and (got.pos >= sc.dx - 1e-6).all()
+    word, counters = w.errors(0)
+    assert word & 2 and counters[1] > 0
+
+
+def test_upload_rejects_bad_requests(ctx):
+    sc, p = S.tiny_scene(512, 16)
+    w = world_of(ctx, [sc], [p])
+    with pytest.raises(M.MpmError) as e:
+        w.upload(0, S.tiny_scene(600, 16)[1])
+    assert e.value.code == M.EINVAL
+    with pytest.raises(TypeError):
+        w.upload(0, p.astype(np.float64))
+    with pytest.raises(M.MpmError):
+        M.World(ctx, [S.tiny_scene(64, 2)[0]])  # physics grids need >= 4 nodes per axis
+
+
+# ------------------------------------------------------------------ totals and conservation
+def test_totals_and_momentum_conservation(ctx):
+    # conservation_test.rs:141 (mass) and :209 (x/z momentum without gravity on those axes)
+    sc, p = S.tiny_scene(8192, 32, S.jelly(E=500.0))
+    sc.gravity = (0.0, 0.0, 0.0)
+    half = p.n // 2
+    p.vel[:half] = (0.6, 0.0, 0.1)
+    p.vel[half:] = (-0.6, 0.0, -0.1)
+    w = world_of(ctx, [sc], [p])
+    t0 = w.totals(0)
+    w.step(60)
+    t1 = w.totals(0)
+    # particle masses are carried, not recomputed; the FP64 sum only changes order with the sort
+    assert abs(t1[0] - t0[0]) <= 1e-12 * t0[0]
+    assert abs(t1[1] - t0[1]) < 1e-5 * t0[0] and abs(t1[3] - t0[3]) < 1e-5 * t0[0]
+    ref = O.totals(w.download(0, p.n))
+    assert np.allclose(ref, t1, rtol=1e-12, atol=1e-15)
+
+
+# ------------------------------------------------------------------ autotuner
+def test_autotune_picks_a_valid_choice_and_restores_state(ctx):
+    sc, p = S.tiny_scene(8192, 32, S.water(), v=(0.5, 0.0, 0.0))
+    w = world_of(ctx, [sc], [p], deterministic=0)
+    before = w.download(0, p.n)
+    r = w.autotune(4)
+    assert r.p2g_variant in (M.P2G_TILE, M.P2G_WARP_AGG, M.P2G_GLOBAL, M.P2G_LANES)
+    assert r.block_threads in (128, 256) and r.sort_interval in (1, 2, 4, 8) and r.us_per_substep > 0
+    after = w.download(0, p.n)
+    assert np.array_equal(before.pos, after.pos) and np.array_equal(before.F, after.F)
+
+
+# ------------------------------------------------------------------ server
+def test_server_results_equal_running_alone(ctx):
+    rng = S.Rng(0x5E4E)
+    reqs = [S.batched_scene(rng) for _ in range(5)]
+    substeps = [20, 35, 10, 50, 25]
+    srv = M.Server(ctx, hbm_budget_bytes=4 << 30, substeps_per_tick=7, exec_options=M.exec_opts(deterministic=1))
+    ids = []
+    for (sc, p), k in zip(reqs, substeps):
+        ids.append(srv.submit(sc, p, k))
+        time.sleep(0.002)  # arrivals while earlier requests are on the device
+    assert srv.drain(120.0) == M.OK
+    done = {}
+    for _ in range(100):
+        for rid, st, t0, ta, td, out in srv.poll():
+            done[rid] = (st, out, t0, ta, td)
+        if len(done) == len(ids):
+            break
+        time.sleep(0.01)
+    assert len(done) == len(ids)
+    stats = srv.stats()
+    srv.close()
+    for rid, (sc, p), k in zip(ids, reqs, substeps):
+        st, out, t0, ta, td = done[rid]
+        assert st == M.OK and t0 <= ta <= td
+        w = world_of(ctx, [sc], [p], deterministic=1)
+        w.step(k)
+        alone = w.download(0, p.n)
+        w.close()
+        for f in ("pos", "vel", "F", "J", "C"):
+            assert np.array_equal(getattr(out, f), getattr(alone, f)), (rid, f)
+    assert stats["particle_substeps"] >= sum(p.n * k for (_, p), k in zip(reqs, substeps))
+
+
+def test_server_budget_and_cancel(ctx):
+    sc, p = S.batched_scene(S.Rng(7))
+    srv = M.Server(ctx, hbm_budget_bytes=1 << 20, substeps_per_tick=5)
+    with pytest.raises(M.MpmError) as e:
+        srv.submit(sc, p, 10)
+    assert e.value.code == M.EBUDGET
+    srv.close()
+    srv = M.Server(ctx, hbm_budget_bytes=4 << 30, substeps_per_tick=5)
+    rid = srv.submit(sc, p, 100000)
+    time.sleep(0.05)
+    assert srv.cancel(rid) == M.OK
+    assert srv.drain(60.0) == M.OK
+    res = srv.poll()
+    assert len(res) == 1 and res[0][1] == M.EINVAL
+    srv.close()
+
+
+# ------------------------------------------------------------------ BASELINE configurations
+def test_config1_fp32_vs_fp64_after_200_substeps(ctx):
+    # north-star target: <= 1e-4 relative position error vs FP64 after 200 substeps
+    sc, p = S.config1_jelly()
+    w32 = world_of(ctx, [sc], [p])
+    w64 = world_of(ctx, [sc], [p.astype(np.float64)])
+    w32.step(200)
+    w64.step(200)
+    a, b = w32.download(0, p.n), w64.download(0, p.n)
+    err = rel(a.pos, b.pos)
+    assert err <= 1e-4, err
+    ref = p.astype(np.float64)
+    O.run(sc, ref, 200, threads=8)
+    assert rel(b.pos, ref.pos) <= 1e-9
+
+
+def test_config2_full_size_properties(ctx):
+    sc, p = S.config2_snow()
+    w32 = world_of(ctx, [sc], [p])
+    w64 = world_of(ctx, [sc], [p.astype(np.float64)])
+    t0 = w64.totals(0)
+    w32.step(100)
+    w64.step(100)
+    assert w32.sync(raise_on_error=False) == M.OK
+    a, b = w32.download(0, p.n), w64.download(0, p.n)
+    assert rel(a.pos, b.pos) <= 1e-4
+    t1 = w64.totals(0)
+    assert abs(t1[1] - t0[1]) < 1e-6 * t0[0] and abs(t1[3] - t0[3]) < 1e-6 * t0[0]  # symmetric x collision
+
+
+def test_config3_deterministic_runs_are_bitwise_equal(ctx):
+    sc, p = S.config3_dam(scale=0.125)
+    outs = []
+    for _ in range(2):
+        w = world_of(ctx, [sc], [p], deterministic=1)
+        w.step(20)
+        outs.append(w.download(0, p.n))
+        w.close()
+    for f in ("pos", "vel", "F", "J", "C"):
+        assert np.array_equal(getattr(outs[0], f), getattr(outs[1], f)), f

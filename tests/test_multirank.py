@@ -1,0 +1,52 @@
+"""Multi-rank host logic of bench.py on CPU (gloo, world_size 2): the max-over-ranks timing and the
+round-robin scene sharding used when --gpus N > 1.  The substep itself does not shard within a
+scene (replicas only), so there is no data-path collective to test."""
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, out):
+    import datetime
+    import sys
+
+    import torch.distributed as dist
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench
+
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        got = bench.max_over_ranks(dist, 10.0 + 5.0 * rank)
+        mine = bench.shard(list(range(11)), rank, world)
+        out.put((rank, got, mine))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_and_scene_sharding_with_two_gloo_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    assert [r[1] for r in res] == [15.0, 15.0]
+    assert res[0][2] == [0, 2, 4, 6, 8, 10] and res[1][2] == [1, 3, 5, 7, 9]
+    assert sorted(res[0][2] + res[1][2]) == list(range(11))
