@@ -316,7 +316,14 @@ int ae_mpm_server_create(ae_mpm_ctx* ctx, const ae_mpm_server_opts* opts, ae_mpm
   if (s->opts.substeps_per_tick == 0) s->opts.substeps_per_tick = 10;
   if (s->opts.max_scenes == 0) s->opts.max_scenes = 4096;
   if (s->opts.exec.precision != 64) s->opts.exec.precision = 32;
-  if (s->opts.exec.p2g_variant == AE_MPM_P2G_AUTO) s->opts.exec.p2g_variant = AE_MPM_P2G_LANES;
+  if (s->opts.exec.p2g_variant == AE_MPM_P2G_AUTO) {
+    // options left to the library: batches are rebuilt whenever membership changes, so graphs
+    // (captured per world) would be re-captured every few ticks; sort every 4th substep as the
+    // autotuner usually picks for batched worlds
+    s->opts.exec.p2g_variant = AE_MPM_P2G_LANES;
+    s->opts.exec.use_graph = 0;
+    if (s->opts.exec.sort_interval <= 1) s->opts.exec.sort_interval = 4;
+  }
   if (s->opts.exec.block_threads == 0) s->opts.exec.block_threads = 256;
   if (s->opts.exec.sort_interval < 1) s->opts.exec.sort_interval = 1;
   if (s->opts.hbm_budget_bytes == 0) {

@@ -621,21 +621,33 @@ __global__ void __launch_bounds__(256) grid_update_kernel(WorldDev<T> w, uint32_
   const uint32_t count = *reinterpret_cast<volatile uint32_t*>(w.touched_count);
   const uint32_t ep = *epoch;
   if (blockIdx.x == 0 && threadIdx.x == 0) *w.clamp_count = 0u;  // G2P of this substep refills it
+  // each 64-thread group takes 4 touched blocks per iteration and issues their 4 accumulator loads
+  // before using any, so a long touched list is not one latency-bound load after another
+  constexpr int kU = 4;
   const int sub = threadIdx.x >> 6, l = threadIdx.x & 63;
-  for (uint32_t t = blockIdx.x * 4 + sub; t < count; t += gridDim.x * 4) {
-    const uint32_t gb = w.touched[t];
-    const SceneDev<T>& sc = w.scenes[w.blk_scene[gb]];
-    int i, j, k;
-    block_coords(sc, gb, l, i, j, k);
-    const uint64_t gi = uint64_t(gb) * 64u + l;
-    V4 a = w.acc[gi];
-    w.acc[gi] = mk4(T(0), T(0), T(0), T(0));
-    T vx, vy, vz;
-    grid_velocity<T, MODE>(sc, i, j, k, a.x, a.y, a.z, a.w, vx, vy, vz);
-    w.vel[gi] = mk4(vx, vy, vz, a.x);
-    if (l == 0) {
-      w.blk_flag[gb] = 0u;
-      blk_epoch[gb] = ep;
+  for (uint32_t t0 = (blockIdx.x * 4 + sub) * kU; t0 < count; t0 += gridDim.x * 4 * kU) {
+    uint32_t gb[kU];
+    V4 a[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) gb[u] = (t0 + u < count) ? w.touched[t0 + u] : 0xffffffffu;
+#pragma unroll
+    for (int u = 0; u < kU; ++u)
+      if (gb[u] != 0xffffffffu) a[u] = w.acc[uint64_t(gb[u]) * 64u + l];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      if (gb[u] == 0xffffffffu) continue;
+      const SceneDev<T>& sc = w.scenes[w.blk_scene[gb[u]]];
+      int i, j, k;
+      block_coords(sc, gb[u], l, i, j, k);
+      const uint64_t gi = uint64_t(gb[u]) * 64u + l;
+      w.acc[gi] = mk4(T(0), T(0), T(0), T(0));
+      T vx, vy, vz;
+      grid_velocity<T, MODE>(sc, i, j, k, a[u].x, a[u].y, a[u].z, a[u].w, vx, vy, vz);
+      w.vel[gi] = mk4(vx, vy, vz, a[u].x);
+      if (l == 0) {
+        w.blk_flag[gb[u]] = 0u;
+        blk_epoch[gb[u]] = ep;
+      }
     }
   }
 }
@@ -2122,7 +2134,7 @@ class World final : public WorldBase {
     } else {
       launch_p2g<MODE>(w);
       mark(2);
-      grid_update_kernel<T, MODE><<<sms * 2, 256, 0, stream_>>>(w, blk_epoch_, counters_ + 2);
+      grid_update_kernel<T, MODE><<<sms * 4, 256, 0, stream_>>>(w, blk_epoch_, counters_ + 2);
       launches_ += 2;
     }
     mark(3);

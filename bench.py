@@ -35,9 +35,10 @@ sys.path.insert(0, os.path.join(ROOT, "ae-engine_b200"))
 
 import numpy as np  # noqa: E402
 
-# algorithmic bytes per particle-substep of each kernel (f32 layout of mpm_world.cuh):
-# P2G reads 7 x 16 B of particle state; G2P reads 4 x 16 B, writes 7 x 16 B and a 4 B key.
-P2G_BYTES_PER_PARTICLE = 112
+# algorithmic bytes per particle-substep of each kernel (f32 layout of mpm_world.cuh, physics mode):
+# P2G reads 4 x 16 B (position+mass, velocity and the affine matrix); G2P reads 4 x 16 B
+# (position+mass, F, J, material) and writes 7 x 16 B plus a 4 B cell key.
+P2G_BYTES_PER_PARTICLE = 64
 G2P_BYTES_PER_PARTICLE = 64 + 112 + 4
 # per active grid node: P2G accumulator write 16, grid update read 16 + write 16 + clear 16, G2P read 16
 P2G_BYTES_PER_NODE = 16
@@ -55,7 +56,11 @@ def parse():
     ap.add_argument("--e2e-substeps", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--scenes", type=int, default=512, help="batched/served: number of scenes")
+    ap.add_argument("--scenes", type=int, default=512, help="batched: number of scenes")
+    ap.add_argument("--plain-sample", type=int, default=48, help="batched: scenes timed one at a time")
+    ap.add_argument("--rates", default="50,200,1000", help="served: Poisson arrival rates (scenes/s)")
+    ap.add_argument("--served-seconds", type=float, default=1.5, help="served: arrival window per rate")
+    ap.add_argument("--served-max", type=int, default=300, help="served: cap on requests per rate")
     return ap.parse_args()
 
 
@@ -160,6 +165,8 @@ def shard(items, rank: int, world_size: int):
 def workload(name: str, rank: int, n_scenes: int):
     import ae_mpm_scenes as S
 
+    if name == "served":
+        return [], [], {"workload": "served"}
     if name == "snow":
         sc, p = S.config2_snow(0xAE02 + 1000 * rank)
         return [sc], [p], {"workload": "snow collision 128^3, 1048576 Stomakhin snow particles, dt 5e-5",
@@ -248,6 +255,8 @@ def run_ours(args, rank, local, world_size, pg):
     scenes, parts, cfg = workload(args.workload, rank, args.scenes)
     if args.workload == "served":
         return run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg)
+    if args.workload == "batched":
+        return run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg)
     opts = M.exec_opts()
     world = M.World(ctx, scenes, opts)
     for i, p in enumerate(parts):
@@ -375,8 +384,150 @@ def run_ours(args, rank, local, world_size, pg):
     world.close()
 
 
+def percentile(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = (len(xs) - 1) * q / 100.0
+    lo, hi = int(math.floor(k)), int(math.ceil(k))
+    return xs[lo] + (xs[hi] - xs[lo]) * (k - lo)
+
+
+def time_world(torch, world, local, steps, warmup):
+    """CUDA-event time (ms) of `steps` substeps on the world's stream after `warmup` untimed ones."""
+    world.step(warmup)
+    world.sync()
+    stream = torch.cuda.ExternalStream(world.stream(), device=local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    world.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
+    """Config 4: all scenes in one world (one launch per kernel per substep) against the plain
+    path, the same kernels stepping one scene at a time."""
+    import torch
+
+    import ae_mpm as M
+
+    n_total = sum(p.n for p in parts)
+    world = M.World(ctx, scenes, M.exec_opts())
+    for i, p in enumerate(parts):
+        world.upload(i, p)
+    tune = None
+    if not args.no_autotune:
+        r = world.autotune(8)
+        tune = {"p2g_variant": r.p2g_variant, "block_threads": r.block_threads, "sort_interval": r.sort_interval}
+    clocks = Clocks(local)
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    clocks.start()
+    ms = time_world(torch, world, local, args.steps, max(args.warmup, 3))
+    clk = clocks.stop()
+    launches = world.launches()
+    world.sync(raise_on_error=False)
+    ms = max_over_ranks(pg, ms)
+    value = n_total * world_size * args.steps / (ms / 1e3)
+    stages = world.stage_times(10)
+    world.close()
+    # plain path: a sample of the scenes, each its own world, stepped one after another
+    k = min(args.plain_sample, len(scenes))
+    idx = list(range(0, len(scenes), max(1, len(scenes) // k)))[:k]
+    t_plain, n_plain, per_scene_ms = 0.0, 0, []
+    for i in idx:
+        w1 = M.World(ctx, [scenes[i]], M.exec_opts())
+        w1.upload(0, parts[i])
+        t = time_world(torch, w1, local, args.steps, 3)
+        w1.close()
+        t_plain += t
+        n_plain += parts[i].n
+        per_scene_ms.append(t)
+    plain_rate = n_plain * args.steps / (t_plain / 1e3)
+    # scene completion latency for the whole set (each scene runs `steps` substeps): batched
+    # scenes all finish with the batch; plain scenes finish one after another
+    scale = len(scenes) / len(idx)
+    plain_done = []
+    acc = 0.0
+    for t in per_scene_ms * int(round(scale)):
+        acc += t
+        plain_done.append(acc)
+    if rank == 0:
+        line = {
+            "metric": "MPM particle-updates/s", "value": value, "unit": "particle-updates/s", "n_gpus": world_size,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64 scenes)",
+            "config": dict(cfg, parallelism="replicas" if world_size > 1 else "single GPU",
+                           l2="inputs larger than L2, no flush"),
+            "batched_vs_plain": {"plain_value": plain_rate, "ratio": value / plain_rate,
+                                 "plain_sample_scenes": len(idx), "plain_kind": "one world per scene, same kernels"},
+            "scene_latency_s": {"batched_p50": ms / 1e3, "batched_p99": ms / 1e3,
+                                "plain_p50": percentile(plain_done, 50) / 1e3,
+                                "plain_p99": percentile(plain_done, 99) / 1e3},
+            "stages_us": {a: round(b, 2) for a, b in stages.items()}, "autotune": tune, "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
-    raise SystemExit("served workload: see bench_served in a later revision")
+    """Config 5: Poisson arrivals of config-4 scenes plus 5% large 1M-particle snow scenes, each
+    with 100..2000 substeps, into the continuous-batching server; per rate the throughput and the
+    p50/p99 completion latency (submit -> results in the caller's buffers)."""
+    import ae_mpm as M
+    import ae_mpm_scenes as S
+
+    rates = [float(r) for r in args.rates.split(",") if r]
+    free = 0
+    try:
+        import torch
+
+        free = torch.cuda.mem_get_info(local)[0]
+    except Exception:
+        pass
+    budget = int(min(free * 0.6, 64 << 30)) if free else (32 << 30)
+    out = []
+    for ri, rate in enumerate(rates):
+        rng = S.Rng(0xAE05 + 100 * ri + 1000 * rank)
+        n_req = int(min(args.served_max, max(1, rate * args.served_seconds)))
+        reqs = [S.config5_request(rng) for _ in range(n_req)]
+        gaps = [-math.log(1.0 - rng.scalar()) / rate for _ in range(n_req)]
+        srv = M.Server(ctx, hbm_budget_bytes=budget, substeps_per_tick=20)
+        lat, work, t_first, t_last = [], 0, None, None
+        done = 0
+        t0 = time.perf_counter()
+        nxt = t0
+        for (sc, p, k), gap in zip(reqs, gaps):
+            nxt += gap
+            while time.perf_counter() < nxt:
+                for rid, st, ts, ta, td, res in srv.poll():
+                    done += 1
+                    lat.append(td - ts)
+                time.sleep(0.0005)
+            srv.submit(sc, p, k)
+            work += p.n * k
+        srv.drain(600.0)
+        for rid, st, ts, ta, td, res in srv.poll(4096):
+            done += 1
+            lat.append(td - ts)
+        wall = time.perf_counter() - t0
+        stats = srv.stats()
+        srv.close()
+        out.append({"rate_per_s": rate, "requests": n_req, "completed": done,
+                    "throughput": stats["particle_substeps"] / wall, "p50_s": percentile(lat, 50),
+                    "p99_s": percentile(lat, 99), "ticks": stats["ticks"], "wall_s": wall})
+    if rank == 0:
+        best = max(out, key=lambda r: r["throughput"])
+        line = {"metric": "MPM particle-updates/s", "value": best["throughput"], "unit": "particle-updates/s",
+                "n_gpus": world_size, "steps": None, "warmup": None, "ms_per_step": None, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64 scenes)",
+                "config": {"workload": "served: Poisson arrivals of config-4 scenes + 5% 128^3 1M-particle snow, "
+                                       "100-2000 substeps each", "hbm_budget_bytes": budget},
+                "served": out}
+        print(json.dumps(line), flush=True)
 
 
 def main():
