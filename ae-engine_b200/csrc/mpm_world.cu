@@ -429,30 +429,37 @@ __global__ void __launch_bounds__(512) p2g_kernel(WorldDev<T> w) {
 }
 
 // --------------------------------------------------------------------------------------------
-// P2G, physics mode, lanes as stencil nodes.  Particles are sorted by cell, so a warp's 32
-// particles form a few runs of equal cells.  The warp finds the runs with one ballot, then walks
-// each run particle by particle: lane l < 27 owns node (l%3, l/3%3, l/9) of the run's cell and
-// keeps that node's sum in registers; at the end of the run the 27 lanes add their sums to the
-// shared tile (27 distinct addresses).  Each particle's record (fx, m, m v, affine matrix) is
-// staged field-major in shared memory by its own thread and read by the warp as broadcasts.
+// P2G, physics mode, lanes as stencil columns.  Particles are sorted by cell, so a warp's 32
+// particles form a few runs of equal cells (about 30 particles per cell in a dense snow block).
+// Lanes 0..26 are 3 particle groups x 9 (y,z) columns of the 3x3x3 stencil: lane (G, b + 3c)
+// takes particles s0+G, s0+G+3, ... of a run and keeps the sums of nodes (0..2, b, c) of the
+// run's cell in 12 registers.  At the end of the run the three groups are summed with shuffles
+// and lanes 0..8 add the run's 27 node sums to the grid with 16-byte vector reductions, one per
+// node and run instead of one per node and particle.  Warps never wait for one another: each
+// stages its own particles and marks the grid blocks its own stencils touch.
+//
+// Everything that depends on one particle only is computed by the particle's own thread (in
+// parallel over particles) and staged particle-major in shared memory:
+//   col[q*9 + b + 3c] = (u, wy[b] wz[c])    u = m v + A d, d = node (0,b,c) - particle
+//   wxm[q]            = (wx[0], wx[1], wx[2], m)
+//   acol[q]           = (dx A[.][0], 0)      node (a+1,b,c) has u + dx A[.][0]
+// so a lane's work per particle is 3 shared loads (the 27 column loads are consecutive vectors,
+// conflict-free), 3 weight products, 12 FMAs and 6 adds.
 // --------------------------------------------------------------------------------------------
-constexpr int kRecVecs = 4;  // per-particle record: (fx fy fz m) (mvx mvy mvz A00) (A01..A11) (A12..A22)
+constexpr int kLaneVecs = 11;  // shared vectors per particle: 9 columns, x weights + mass, x column
 
 template <class T>
-__global__ void __launch_bounds__(256) p2g_lanes_kernel(WorldDev<T> w) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) p2g_lanes_kernel(WorldDev<T> w) {
   using V4 = typename V4T<T>::type;
   extern __shared__ __align__(16) unsigned char smem[];
-  V4* tile = reinterpret_cast<V4*>(smem);
-  V4* rec = tile + w.max_tile_nodes;  // rec[k * blockDim.x + q]
-  __shared__ int s_lo[3], s_hi[3];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
+  const int nt = blockDim.x;
+  V4* col = reinterpret_cast<V4*>(smem);  // col[q * 9 + j]
+  V4* wxm = col + 9 * nt;                 // wxm[q]
+  V4* acol = wxm + nt;                    // acol[q]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int4 ch = w.chunks[blockIdx.x];
   const SceneDev<T>& sc = w.scenes[ch.x];
-  if (tid < 3) {
-    s_lo[tid] = INT_MAX;
-    s_hi[tid] = INT_MIN;
-  }
-  __syncthreads();
+  const int n0 = sc.n[0], n1 = sc.n[1], n2 = sc.n[2];
   const int j = ch.y + tid;
   bool has = false;
   int g[3] = {0, 0, 0};
@@ -469,95 +476,103 @@ __global__ void __launch_bounds__(256) p2g_lanes_kernel(WorldDev<T> w) {
       hi[a] = min(p.g[a] + 2, sc.n[a] - 1);
       if (lo[a] > hi[a]) has = false;
     }
-    rec[0 * nt + tid] = mk4(p.fx[0], p.fx[1], p.fx[2], p.m);
-    rec[1 * nt + tid] = mk4(p.v[0], p.v[1], p.v[2], p.A[0]);
-    rec[2 * nt + tid] = mk4(p.A[1], p.A[2], p.A[3], p.A[4]);
-    rec[3 * nt + tid] = mk4(p.A[5], p.A[6], p.A[7], p.A[8]);
-  }
-  // run key: unique per cell (a stencil with any node in the grid has g in [-2, n-1] per axis)
-  const uint32_t key = has ? uint32_t(g[0] + 2) + uint32_t(sc.n[0] + 2) * (uint32_t(g[1] + 2) + uint32_t(sc.n[1] + 2) * uint32_t(g[2] + 2))
-                           : 0xffffffffu;
+    const T dx = sc.dx;
+    T c0[3], c1[3], c2[3], q[3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    int l = __reduce_min_sync(0xffffffffu, has ? lo[a] : INT_MAX);
-    int h = __reduce_max_sync(0xffffffffu, has ? hi[a] : INT_MIN);
-    if (lane == 0 && l != INT_MAX) {
-      atomicMin(&s_lo[a], l);
-      atomicMax(&s_hi[a], h);
+    for (int r = 0; r < 3; ++r) {
+      c0[r] = dx * p.A[3 * r + 0];
+      c1[r] = dx * p.A[3 * r + 1];
+      c2[r] = dx * p.A[3 * r + 2];
+      q[r] = p.v[r] - (c0[r] * p.fx[0] + c1[r] * p.fx[1] + c2[r] * p.fx[2]);
     }
+    V4* cq = col + tid * 9;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const T ux = q[0] + T(b) * c1[0] + T(c) * c2[0];
+        const T uy = q[1] + T(b) * c1[1] + T(c) * c2[1];
+        const T uz = q[2] + T(b) * c1[2] + T(c) * c2[2];
+        cq[b + 3 * c] = mk4(ux, uy, uz, p.w[1][b] * p.w[2][c]);
+      }
+    }
+    wxm[tid] = mk4(p.w[0][0], p.w[0][1], p.w[0][2], p.m);
+    acol[tid] = mk4(c0[0], c0[1], c0[2], T(0));
   }
-  __syncthreads();
-  const int L0 = s_lo[0], L1 = s_lo[1], L2 = s_lo[2];
-  if (L0 == INT_MAX) return;
-  const int D0 = s_hi[0] - L0 + 1, D1 = s_hi[1] - L1 + 1, D2 = s_hi[2] - L2 + 1;
-  const int vol = D0 * D1 * D2;
-  const bool use_tile = vol <= w.max_tile_nodes;
-  if (use_tile) {
-    for (int t = tid; t < vol; t += nt) tile[t] = mk4(T(0), T(0), T(0), T(0));
-  } else if (tid == 0) {
-    atomicAdd(w.err + 4 * ch.x + 3, 1u);
-  }
-  __syncthreads();
+  __syncwarp();
+  // run key: unique per cell (a stencil with any node in the grid has g in [-2, n-1] per axis)
+  const uint32_t key = has ? uint32_t(g[0] + 2) + uint32_t(n0 + 2) * (uint32_t(g[1] + 2) + uint32_t(n1 + 2) * uint32_t(g[2] + 2))
+                           : 0xffffffffu;
   // runs of equal keys among this warp's particles (particles without nodes form their own runs)
   const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
   uint32_t starts = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
-  // this lane's stencil node and its weights: with t = fx - off_k, w_0 = t^2/2 (off 1.5),
-  // w_1 = 3/4 - t^2 (off 1), w_2 = t^2/2 (off 0.5): the quadratic B-spline at fx, fx-1, fx-2,
-  // evaluated branch-free from per-lane constants
-  const int na = lane % 3, nb = (lane / 3) % 3, nc = lane / 9;
-  const T offa = T(1.5) - T(0.5) * T(na), offb = T(1.5) - T(0.5) * T(nb), offc = T(1.5) - T(0.5) * T(nc);
-  const T sa = na == 1 ? T(-1) : T(0.5), sb = nb == 1 ? T(-1) : T(0.5), sc2 = nc == 1 ? T(-1) : T(0.5);
-  const T ka = na == 1 ? T(0.75) : T(0), kb = nb == 1 ? T(0.75) : T(0), kc = nc == 1 ? T(0.75) : T(0);
-  const T fa = T(na), fb = T(nb), fc = T(nc);
-  const T dx = sc.dx;
-  const V4* r0p = rec + warp * 32;
-  const V4* r1p = rec + nt + warp * 32;
-  const V4* r2p = rec + 2 * nt + warp * 32;
-  const V4* r3p = rec + 3 * nt + warp * 32;
+  // lanes 27..31 mirror the columns of lanes 22..26 (in-bounds reads, results never used)
+  const int grp = lane < 27 ? lane / 9 : 2;
+  const int jc = lane < 27 ? lane - 9 * grp : lane - 23;
+  const int nb = jc % 3, nc = jc / 3;
+  const V4* colw = col + warp * 32 * 9 + jc;
+  const V4* wxw = wxm + warp * 32;
+  const V4* acw = acol + warp * 32;
   while (starts) {
     const int s0 = __ffs(starts) - 1;
     starts &= starts - 1u;
     const int e0 = starts ? __ffs(starts) - 1 : 32;
     const uint32_t rk = __shfl_sync(0xffffffffu, key, s0);
-    const int X = __shfl_sync(0xffffffffu, g[0], s0) + na;
+    const int X = __shfl_sync(0xffffffffu, g[0], s0);
     const int Y = __shfl_sync(0xffffffffu, g[1], s0) + nb;
     const int Z = __shfl_sync(0xffffffffu, g[2], s0) + nc;
     if (rk == 0xffffffffu) continue;
-    T am = 0, ax = 0, ay = 0, az = 0;
-    for (int i = s0; i < e0; ++i) {
-      const V4 r0 = r0p[i], r1 = r1p[i], r2 = r2p[i], r3 = r3p[i];
-      const T tx = r0.x - offa, ty = r0.y - offb, tz = r0.z - offc;
-      const T ww = (sa * tx * tx + ka) * (sb * ty * ty + kb) * (sc2 * tz * tz + kc);
-      const T d0 = (fa - r0.x) * dx, d1 = (fb - r0.y) * dx, d2 = (fc - r0.z) * dx;
-      am += ww * r0.w;
-      ax += ww * (r1.x + r1.w * d0 + r2.x * d1 + r2.y * d2);
-      ay += ww * (r1.y + r2.z * d0 + r2.w * d1 + r3.x * d2);
-      az += ww * (r1.z + r3.y * d0 + r3.z * d1 + r3.w * d2);
+    T m0 = 0, x0 = 0, y0 = 0, z0 = 0, m1 = 0, x1 = 0, y1 = 0, z1 = 0, m2 = 0, x2 = 0, y2 = 0, z2 = 0;
+    for (int i = s0 + grp; i < e0; i += 3) {
+      const V4 u = colw[i * 9];
+      const V4 r = wxw[i];
+      const V4 a = acw[i];
+      const T W0 = r.x * u.w, W1 = r.y * u.w, W2 = r.z * u.w;
+      m0 += W0 * r.w;
+      x0 += W0 * u.x;
+      y0 += W0 * u.y;
+      z0 += W0 * u.z;
+      const T ux = u.x + a.x, uy = u.y + a.y, uz = u.z + a.z;
+      m1 += W1 * r.w;
+      x1 += W1 * ux;
+      y1 += W1 * uy;
+      z1 += W1 * uz;
+      m2 += W2 * r.w;
+      x2 += W2 * (ux + a.x);
+      y2 += W2 * (uy + a.y);
+      z2 += W2 * (uz + a.z);
     }
-    if (lane < 27 && am != T(0) && X >= 0 && Y >= 0 && Z >= 0 && X < sc.n[0] && Y < sc.n[1] && Z < sc.n[2]) {
-      if (use_tile) {
-        shared_add4<T>(tile + ((Z - L2) * D1 + (Y - L1)) * D0 + (X - L0), am, ax, ay, az);
-      } else {
-        atomic_add4(w.acc + node_index(sc, X, Y, Z), am, ax, ay, az);
-        mark_block(w, sc.blk_off + (uint32_t(Z >> 2) * sc.nb[1] + (Y >> 2)) * sc.nb[0] + (X >> 2));
-      }
+    if (e0 - s0 > 1) {
+      auto groups = [](T v) { return v + __shfl_down_sync(0xffffffffu, v, 9) + __shfl_down_sync(0xffffffffu, v, 18); };
+      m0 = groups(m0), x0 = groups(x0), y0 = groups(y0), z0 = groups(z0);
+      m1 = groups(m1), x1 = groups(x1), y1 = groups(y1), z1 = groups(z1);
+      m2 = groups(m2), x2 = groups(x2), y2 = groups(y2), z2 = groups(z2);
+    }
+    if (lane < 9 && Y >= 0 && Z >= 0 && Y < n1 && Z < n2) {
+      if (m0 != T(0) && X >= 0 && X < n0) atomic_add4(w.acc + node_index(sc, X, Y, Z), m0, x0, y0, z0);
+      if (m1 != T(0) && X + 1 >= 0 && X + 1 < n0) atomic_add4(w.acc + node_index(sc, X + 1, Y, Z), m1, x1, y1, z1);
+      if (m2 != T(0) && X + 2 >= 0 && X + 2 < n0) atomic_add4(w.acc + node_index(sc, X + 2, Y, Z), m2, x2, y2, z2);
     }
   }
-  if (!use_tile) return;
-  __syncthreads();
-  for (int t = tid; t < vol; t += nt) {
-    V4 v = tile[t];
-    if (v.x != T(0)) {
-      int X = L0 + t % D0, Y = L1 + (t / D0) % D1, Z = L2 + t / (D0 * D1);
-      atomic_add4(w.acc + node_index(sc, X, Y, Z), v.x, v.y, v.z, v.w);
-    }
+  // grid blocks of this warp's stencil bounding box
+  int B[3], NB[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int l = __reduce_min_sync(0xffffffffu, has ? lo[a] : INT_MAX);
+    const int h = __reduce_max_sync(0xffffffffu, has ? hi[a] : INT_MIN);
+    B[a] = l >> 2;
+    NB[a] = l == INT_MAX ? 0 : (h >> 2) - (l >> 2) + 1;
   }
-  const int B0 = L0 >> 2, B1 = L1 >> 2, B2 = L2 >> 2;
-  const int E0 = (L0 + D0 - 1) >> 2, E1 = (L1 + D1 - 1) >> 2, E2 = (L2 + D2 - 1) >> 2;
-  const int nbx = E0 - B0 + 1, nby = E1 - B1 + 1, nbz = E2 - B2 + 1;
-  for (int t = tid; t < nbx * nby * nbz; t += nt) {
-    int bx = B0 + t % nbx, by = B1 + (t / nbx) % nby, bz = B2 + t / (nbx * nby);
-    mark_block(w, sc.blk_off + (uint32_t(bz) * sc.nb[1] + by) * sc.nb[0] + bx);
+  const int nblk = NB[0] * NB[1] * NB[2];
+  if (NB[0] <= 4 && NB[1] <= 4 && NB[2] <= 2) {
+    const int bx = lane & 3, by = (lane >> 2) & 3, bz = lane >> 4;
+    if (bx < NB[0] && by < NB[1] && bz < NB[2])
+      mark_block(w, sc.blk_off + (uint32_t(B[2] + bz) * sc.nb[1] + (B[1] + by)) * sc.nb[0] + (B[0] + bx));
+  } else {
+    for (int t = lane; t < nblk; t += 32) {
+      const int bx = B[0] + t % NB[0], by = B[1] + (t / NB[0]) % NB[1], bz = B[2] + t / (NB[0] * NB[1]);
+      mark_block(w, sc.blk_off + (uint32_t(bz) * sc.nb[1] + by) * sc.nb[0] + bx);
+    }
   }
 }
 
@@ -2105,9 +2120,10 @@ class World final : public WorldBase {
   void launch_p2g(WorldDev<T>& w) {
     const size_t sm = sizeof(V4) * max_tile_nodes();
     if (MODE == AE_MPM_MODE_PHYSICS && opts_.p2g_variant == kVarLanes) {
-      const size_t sm2 = sm + sizeof(V4) * kRecVecs * chunk_threads_;
-      if (!lanes_smem_set_) {
-        cudaFuncSetAttribute(p2g_lanes_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm2 + 1024));
+      const size_t sm2 = sizeof(V4) * kLaneVecs * chunk_threads_;
+      if (!lanes_smem_set_) {  // sized for the largest block (256 threads) the world accepts
+        cudaFuncSetAttribute(p2g_lanes_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(sizeof(V4) * kLaneVecs * 256));
         lanes_smem_set_ = true;
       }
       p2g_lanes_kernel<T><<<n_chunks_, chunk_threads_, sm2, stream_>>>(w);
