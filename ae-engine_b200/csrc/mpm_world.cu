@@ -680,17 +680,79 @@ struct G2POut {
 
 // Node velocities for one block of particles: the block's bounding-box tile in shared memory
 // (filled with coalesced loads before the gather), or the global array when the box is too big.
+// The tile's x and y pitches are powers of two (2^p0 >= D0, 2^(sp-p0) >= D1), so slot indexes
+// split into coordinates with shifts and masks.
 template <class T>
 struct VelTile {
   using V4 = typename V4T<T>::type;
   const V4* tile;
   const V4* vel;
-  int L0, L1, L2, D0, D1;
+  int L0, L1, L2, p0, sp;
   __device__ __forceinline__ V4 operator()(const SceneDev<T>& sc, int X, int Y, int Z) const {
-    if (tile) return tile[((Z - L2) * D1 + (Y - L1)) * D0 + (X - L0)];
+    if (tile) return tile[((Z - L2) << sp) + ((Y - L1) << p0) + (X - L0)];
     return ld4(vel + node_index(sc, X, Y, Z));
   }
 };
+
+// Physics gather from the tile for a particle whose 27 stencil nodes are all inside the grid
+// (every particle after its first substep: positions are clamped to [1, n-2] dx).  Separable:
+// each (y,z) column is summed over x first,
+//   S0 = sum_a wx[a] g(a,b,c),   S1 = sum_a wx[a] (a - fx) dx g(a,b,c),
+// then v += wy wz S0, B[.][0] += wy wz S1, B[.][1] += wy (b - fy) dx wz S0,
+// B[.][2] += wy wz (c - fz) dx S0: 36 instructions per column instead of 42 per node.
+// Returns false (nothing written) when the particle does not qualify.
+template <class T>
+__device__ __forceinline__ bool g2p_physics_gather_tile(const VelTile<T>& vt, const SceneDev<T>& sc, const T* x0, T* v,
+                                                        T* C) {
+  using V4 = typename V4T<T>::type;
+  if (!vt.tile) return false;
+  int b[3];
+  T w[3][3], e[3][3];
+  bool inside = true;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const T X = (x0[a] - sc.origin[a]) * sc.inv_dx;
+    const int bb = floor_to_int(X - T(0.5));
+    const T fx = X - T(bb);
+    b[a] = bb;
+    inside = inside && bb >= 0 && bb + 2 < sc.n[a];
+    const T t0 = T(1.5) - fx, t1 = fx - T(1), t2 = fx - T(0.5);
+    w[a][0] = T(0.5) * t0 * t0;
+    w[a][1] = T(0.75) - t1 * t1;
+    w[a][2] = T(0.5) * t2 * t2;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) e[a][k] = w[a][k] * ((T(k) - fx) * sc.dx);
+  }
+  if (!inside) return false;
+  const V4* t0 = vt.tile + ((b[2] - vt.L2) << vt.sp) + ((b[1] - vt.L1) << vt.p0) + (b[0] - vt.L0);
+  T vv[3] = {0, 0, 0}, B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+#pragma unroll
+    for (int bb = 0; bb < 3; ++bb) {
+      const V4* row = t0 + (c << vt.sp) + (bb << vt.p0);
+      const V4 g0 = row[0], g1 = row[1], g2 = row[2];
+      const T s0[3] = {w[0][0] * g0.x + w[0][1] * g1.x + w[0][2] * g2.x, w[0][0] * g0.y + w[0][1] * g1.y + w[0][2] * g2.y,
+                       w[0][0] * g0.z + w[0][1] * g1.z + w[0][2] * g2.z};
+      const T s1[3] = {e[0][0] * g0.x + e[0][1] * g1.x + e[0][2] * g2.x, e[0][0] * g0.y + e[0][1] * g1.y + e[0][2] * g2.y,
+                       e[0][0] * g0.z + e[0][1] * g1.z + e[0][2] * g2.z};
+      const T wbc = w[1][bb] * w[2][c], ebc = e[1][bb] * w[2][c], fbc = w[1][bb] * e[2][c];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        vv[r] += wbc * s0[r];
+        B[r * 3 + 0] += wbc * s1[r];
+        B[r * 3 + 1] += ebc * s0[r];
+        B[r * 3 + 2] += fbc * s0[r];
+      }
+    }
+  }
+  const T cs = T(4) * sc.inv_dx * sc.inv_dx;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) v[r] = vv[r];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) C[k] = cs * B[k];
+  return true;
+}
 
 // gather half of the physics G2P: grid velocity and APIC C at the particle
 template <class T>
@@ -1045,16 +1107,20 @@ __global__ void __launch_bounds__(256) g2p_kernel(WorldDev<T> w, uint32_t* epoch
   vt.L0 = s_lo[0];
   vt.L1 = s_lo[1];
   vt.L2 = s_lo[2];
-  vt.D0 = s_hi[0] - vt.L0 + 1;
-  vt.D1 = s_hi[1] - vt.L1 + 1;
-  const int D2 = s_hi[2] - vt.L2 + 1;
-  if (vt.L0 != INT_MAX && vt.D0 * vt.D1 * D2 <= w.max_tile_nodes) {
-    const int vol = vt.D0 * vt.D1 * D2;
-    for (int t = tid; t < vol; t += blockDim.x) {
-      int X = vt.L0 + t % vt.D0, Y = vt.L1 + (t / vt.D0) % vt.D1, Z = vt.L2 + t / (vt.D0 * vt.D1);
-      tile[t] = ld4(w.vel + node_index(sc, X, Y, Z));
+  if (vt.L0 != INT_MAX) {
+    const int D0 = s_hi[0] - vt.L0 + 1, D1 = s_hi[1] - vt.L1 + 1, D2 = s_hi[2] - vt.L2 + 1;
+    const int p0 = 32 - __clz(D0 - 1), p1 = 32 - __clz(D1 - 1);
+    vt.p0 = p0;
+    vt.sp = p0 + p1;
+    const int slots = D2 << vt.sp;
+    if (slots <= w.max_tile_nodes) {
+      const int mx = (1 << p0) - 1, my = (1 << p1) - 1;
+      for (int t = tid; t < slots; t += blockDim.x) {
+        const int X = t & mx, Y = (t >> p0) & my;
+        if (X < D0 && Y < D1) tile[t] = ld4(w.vel + node_index(sc, vt.L0 + X, vt.L1 + Y, vt.L2 + (t >> vt.sp)));
+      }
+      vt.tile = tile;
     }
-    vt.tile = tile;
   }
   __syncthreads();
   uint32_t err = 0;
@@ -1063,7 +1129,8 @@ __global__ void __launch_bounds__(256) g2p_kernel(WorldDev<T> w, uint32_t* epoch
     const T x0[3] = {a0.x, a0.y, a0.z};
     G2POut<T> o;
     T pv[3] = {0, 0, 0};
-    if (MODE == AE_MPM_MODE_PHYSICS) g2p_physics_gather<T>(vt, sc, x0, pv, o.C);
+    if (MODE == AE_MPM_MODE_PHYSICS && !g2p_physics_gather_tile<T>(vt, sc, x0, pv, o.C))
+      g2p_physics_gather<T>(vt, sc, x0, pv, o.C);
     cp_async_wait_all();
     const V4 a1 = stage[tid], a2 = stage[nt + tid], a3 = stage[2 * nt + tid];
     const T F[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
