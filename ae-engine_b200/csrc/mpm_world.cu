@@ -1051,7 +1051,7 @@ __device__ __forceinline__ void stencil_range(const SceneDev<T>& sc, T x, int a,
 }
 
 template <class T, int MODE>
-__global__ void __launch_bounds__(256) g2p_kernel(WorldDev<T> w, uint32_t* epoch) {
+__global__ void __launch_bounds__(256, (MODE == AE_MPM_MODE_PHYSICS && sizeof(T) == 4) ? 4 : 1) g2p_kernel(WorldDev<T> w, uint32_t* epoch) {
   using V4 = typename V4T<T>::type;
   extern __shared__ __align__(16) unsigned char smem[];
   V4* tile = reinterpret_cast<V4*>(smem);
