@@ -754,6 +754,68 @@ __device__ __forceinline__ bool g2p_physics_gather_tile(const VelTile<T>& vt, co
   return true;
 }
 
+// Physics gather straight from the grid's velocity array through the read-only cache, for a
+// particle whose 27 stencil nodes are all inside the grid.  Same separable sums as the tile
+// gather; node addresses are built per (y,z) column from the block-major layout.  The block
+// needs no bounding box, tile or barrier, so its warps never wait for one another.
+template <class T>
+__device__ __forceinline__ bool g2p_physics_gather_direct(const typename V4T<T>::type* __restrict__ vel,
+                                                          const SceneDev<T>& sc, const T* x0, T* v, T* C) {
+  using V4 = typename V4T<T>::type;
+  int b[3];
+  T w[3][3], e[3][3];
+  bool inside = true;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const T X = (x0[a] - sc.origin[a]) * sc.inv_dx;
+    const int bb = floor_to_int(X - T(0.5));
+    const T fx = X - T(bb);
+    b[a] = bb;
+    inside = inside && bb >= 0 && bb + 2 < sc.n[a];
+    const T t0 = T(1.5) - fx, t1 = fx - T(1), t2 = fx - T(0.5);
+    w[a][0] = T(0.5) * t0 * t0;
+    w[a][1] = T(0.75) - t1 * t1;
+    w[a][2] = T(0.5) * t2 * t2;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) e[a][k] = w[a][k] * ((T(k) - fx) * sc.dx);
+  }
+  if (!inside) return false;
+  uint32_t xo[3];  // x part of the node index: block column and lane within the block
+#pragma unroll
+  for (int a = 0; a < 3; ++a) xo[a] = (uint32_t((b[0] + a) >> 2) << 6) | uint32_t((b[0] + a) & 3);
+  const uint32_t nb0 = uint32_t(sc.nb[0]), nb1 = uint32_t(sc.nb[1]);
+  T vv[3] = {0, 0, 0}, B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const int Z = b[2] + c;
+#pragma unroll
+    for (int bb = 0; bb < 3; ++bb) {
+      const int Y = b[1] + bb;
+      const uint32_t row = ((sc.blk_off + (uint32_t(Z >> 2) * nb1 + uint32_t(Y >> 2)) * nb0) << 6) |
+                           (uint32_t(Z & 3) << 4) | (uint32_t(Y & 3) << 2);
+      const V4 g0 = ld4(vel + (row + xo[0])), g1 = ld4(vel + (row + xo[1])), g2 = ld4(vel + (row + xo[2]));
+      const T s0[3] = {w[0][0] * g0.x + w[0][1] * g1.x + w[0][2] * g2.x, w[0][0] * g0.y + w[0][1] * g1.y + w[0][2] * g2.y,
+                       w[0][0] * g0.z + w[0][1] * g1.z + w[0][2] * g2.z};
+      const T s1[3] = {e[0][0] * g0.x + e[0][1] * g1.x + e[0][2] * g2.x, e[0][0] * g0.y + e[0][1] * g1.y + e[0][2] * g2.y,
+                       e[0][0] * g0.z + e[0][1] * g1.z + e[0][2] * g2.z};
+      const T wbc = w[1][bb] * w[2][c], ebc = e[1][bb] * w[2][c], fbc = w[1][bb] * e[2][c];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        vv[r] += wbc * s0[r];
+        B[r * 3 + 0] += wbc * s1[r];
+        B[r * 3 + 1] += ebc * s0[r];
+        B[r * 3 + 2] += fbc * s0[r];
+      }
+    }
+  }
+  const T cs = T(4) * sc.inv_dx * sc.inv_dx;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) v[r] = vv[r];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) C[k] = cs * B[k];
+  return true;
+}
+
 // gather half of the physics G2P: grid velocity and APIC C at the particle
 template <class T>
 __device__ __forceinline__ void g2p_physics_gather(const VelTile<T>& vt, const SceneDev<T>& sc, const T* x0, T* v,
@@ -1055,7 +1117,9 @@ __global__ void __launch_bounds__(256, (MODE == AE_MPM_MODE_PHYSICS && sizeof(T)
   using V4 = typename V4T<T>::type;
   extern __shared__ __align__(16) unsigned char smem[];
   V4* tile = reinterpret_cast<V4*>(smem);
-  V4* stage = tile + w.max_tile_nodes;  // a1..a3 of this block's particles: stage[k * blockDim.x + tid]
+  // physics mode gathers straight from the grid (no block tile, no barriers)
+  constexpr bool kTile = MODE != AE_MPM_MODE_PHYSICS;
+  V4* stage = kTile ? tile + w.max_tile_nodes : tile;  // a1..a3 of this block's particles: stage[k * nt + tid]
   __shared__ int s_lo[3], s_hi[3];
   const int4 ch = w.chunks[blockIdx.x];
   const SceneDev<T>& sc = w.scenes[ch.x];
@@ -1067,47 +1131,53 @@ __global__ void __launch_bounds__(256, (MODE == AE_MPM_MODE_PHYSICS && sizeof(T)
     if (w.cell_count) *w.cell_count = 0u;
     *epoch += 1u;
   }
-  if (tid < 3) {
-    s_lo[tid] = INT_MAX;
-    s_hi[tid] = INT_MIN;
+  if (kTile) {
+    if (tid < 3) {
+      s_lo[tid] = INT_MAX;
+      s_hi[tid] = INT_MIN;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   uint32_t src = 0;
   V4 a0 = mk4(T(0), T(0), T(0), T(0));
   int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
   bool has = false;
   if (live) {
     src = w.perm ? w.perm[j] : uint32_t(j);
-    // F, J and the material arrive in shared memory while the velocity tile is gathered
+    // F, J and the material arrive in shared memory while the node velocities are gathered
 #pragma unroll
     for (int k = 0; k < 3; ++k) cp_async_v4(stage + k * nt + tid, w.in[1 + k] + src);
     cp_async_commit();
     a0 = ld4(w.in[0] + src);
     const T x3[3] = {a0.x, a0.y, a0.z};
     has = true;
+    if (kTile) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        stencil_range<T, MODE>(sc, x3[a], a, lo[a], hi[a]);
+        if (lo[a] > hi[a]) has = false;
+      }
+    }
+  }
+  if (kTile) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      stencil_range<T, MODE>(sc, x3[a], a, lo[a], hi[a]);
-      if (lo[a] > hi[a]) has = false;
+      int l = __reduce_min_sync(0xffffffffu, has ? lo[a] : INT_MAX);
+      int h = __reduce_max_sync(0xffffffffu, has ? hi[a] : INT_MIN);
+      if (lane == 0 && l != INT_MAX) {
+        atomicMin(&s_lo[a], l);
+        atomicMax(&s_hi[a], h);
+      }
     }
+    __syncthreads();
   }
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    int l = __reduce_min_sync(0xffffffffu, has ? lo[a] : INT_MAX);
-    int h = __reduce_max_sync(0xffffffffu, has ? hi[a] : INT_MIN);
-    if (lane == 0 && l != INT_MAX) {
-      atomicMin(&s_lo[a], l);
-      atomicMax(&s_hi[a], h);
-    }
-  }
-  __syncthreads();
   VelTile<T> vt;
   vt.tile = nullptr;
   vt.vel = w.vel;
-  vt.L0 = s_lo[0];
-  vt.L1 = s_lo[1];
-  vt.L2 = s_lo[2];
-  if (vt.L0 != INT_MAX) {
+  vt.L0 = kTile ? s_lo[0] : INT_MAX;
+  vt.L1 = kTile ? s_lo[1] : INT_MAX;
+  vt.L2 = kTile ? s_lo[2] : INT_MAX;
+  if (kTile && vt.L0 != INT_MAX) {
     const int D0 = s_hi[0] - vt.L0 + 1, D1 = s_hi[1] - vt.L1 + 1, D2 = s_hi[2] - vt.L2 + 1;
     const int p0 = 32 - __clz(D0 - 1), p1 = 32 - __clz(D1 - 1);
     vt.p0 = p0;
@@ -1122,14 +1192,14 @@ __global__ void __launch_bounds__(256, (MODE == AE_MPM_MODE_PHYSICS && sizeof(T)
       vt.tile = tile;
     }
   }
-  __syncthreads();
+  if (kTile) __syncthreads();
   uint32_t err = 0;
   bool cl = false, need = false;
   if (live) {
     const T x0[3] = {a0.x, a0.y, a0.z};
     G2POut<T> o;
     T pv[3] = {0, 0, 0};
-    if (MODE == AE_MPM_MODE_PHYSICS && !g2p_physics_gather_tile<T>(vt, sc, x0, pv, o.C))
+    if (MODE == AE_MPM_MODE_PHYSICS && !g2p_physics_gather_direct<T>(w.vel, sc, x0, pv, o.C))
       g2p_physics_gather<T>(vt, sc, x0, pv, o.C);
     cp_async_wait_all();
     const V4 a1 = stage[tid], a2 = stage[nt + tid], a3 = stage[2 * nt + tid];
@@ -2034,24 +2104,40 @@ class World final : public WorldBase {
       launch_init_keys(w);
       keys_stale_ = false;
     }
-    cudaEvent_t ev[5];
-    for (auto& e : ev) AE_TRY(cudaEventCreate(&e));
-    double acc[5] = {0, 0, 0, 0, 0};
-    for (uint32_t i = 0; i < n; ++i) {
-      stage_events_ = ev;
-      substep_eager();
+    // all substeps are queued before the one wait, so that (past the first) the stream is never
+    // idle waiting for the host and the events measure device time, not launch latency
+    std::vector<cudaEvent_t> ev(5 * size_t(n), nullptr);
+    int rc2 = AE_MPM_OK;
+    for (auto& e : ev)
+      if (cudaEventCreate(&e) != cudaSuccess) rc2 = AE_MPM_ECUDA;
+    if (rc2 == AE_MPM_OK) {
+      for (uint32_t i = 0; i < n; ++i) {
+        stage_events_ = ev.data() + 5 * size_t(i);
+        substep_eager();
+      }
       stage_events_ = nullptr;
-      AE_TRY(cudaEventSynchronize(ev[4]));
+      if (cudaEventSynchronize(ev.back()) != cudaSuccess) rc2 = AE_MPM_ECUDA;
+    }
+    double acc[5] = {0, 0, 0, 0, 0};
+    // the first substep starts on an idle stream: skip it when there is more than one
+    const uint32_t first = n > 1 ? 1u : 0u;
+    for (uint32_t i = first; i < n && rc2 == AE_MPM_OK; ++i) {
+      const cudaEvent_t* e = ev.data() + 5 * size_t(i);
       float ms;
       for (int k = 0; k < 4; ++k) {
-        cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+        cudaEventElapsedTime(&ms, e[k], e[k + 1]);
         acc[k] += ms;
       }
-      cudaEventElapsedTime(&ms, ev[0], ev[4]);
+      cudaEventElapsedTime(&ms, e[0], e[4]);
       acc[4] += ms;
     }
-    for (auto& e : ev) cudaEventDestroy(e);
-    for (int k = 0; k < 5; ++k) out_us[k] = 1000.0 * acc[k] / n;
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (rc2 != AE_MPM_OK) {
+      err = "stage timing events failed";
+      return rc2;
+    }
+    for (int k = 0; k < 5; ++k) out_us[k] = 1000.0 * acc[k] / (n - first);
     return AE_MPM_OK;
   }
 
@@ -2221,8 +2307,8 @@ class World final : public WorldBase {
       launches_ += 2;
     }
     mark(3);
-    g2p_kernel<T, MODE><<<n_chunks_, chunk_threads_, sizeof(V4) * (max_tile_nodes() + 3 * chunk_threads_), stream_>>>(
-        w, counters_ + 2);
+    const size_t g2p_smem = sizeof(V4) * ((MODE == AE_MPM_MODE_PHYSICS ? 0 : max_tile_nodes()) + 3 * chunk_threads_);
+    g2p_kernel<T, MODE><<<n_chunks_, chunk_threads_, g2p_smem, stream_>>>(w, counters_ + 2);
     ++launches_;
     if (MODE == AE_MPM_MODE_PHYSICS && has_snow_) {
       snow_clamp_kernel<T><<<sms * 4, 128, 0, stream_>>>(w);

@@ -41,6 +41,7 @@ def run_gpu(ctx, sc, p, substeps, **opts):
 @pytest.mark.parametrize("n,bits,kind", [
     (1, 8, "random"), (7, 3, "random"), (2048, 16, "random"), (2049, 21, "random"), (100000, 32, "random"),
     (300001, 24, "nearly_sorted"), (65536, 18, "equal"), (50000, 1, "random"), (1 << 21, 21, "nearly_sorted"),
+    (4095, 12, "random"), (4096, 22, "nearly_sorted"), (4097, 22, "random"), (3000001, 32, "random"),
 ])
 def test_radix_sort_matches_stable_cpu_sort(ctx, n, bits, kind):
     rng = np.random.default_rng(n + bits)
@@ -56,6 +57,18 @@ def test_radix_sort_matches_stable_cpu_sort(ctx, n, bits, kind):
     ref = np.argsort(keys, kind="stable").astype(np.uint32)
     assert np.array_equal(perm, ref)
     assert np.array_equal(sk, keys[ref])
+
+
+def test_radix_sort_repeated_sorts_of_changing_sizes(ctx):
+    # every sort reuses the context's look-back status array; entries left by earlier sorts (other
+    # sizes, other digit widths) must read as not yet written
+    rng = np.random.default_rng(77)
+    for n, bits in ((40000, 22), (9000, 8), (123457, 22), (4096, 32), (40000, 22), (250000, 14)):
+        keys = rng.integers(0, 1 << bits, n, dtype=np.uint64).astype(np.uint32)
+        sk, perm = ctx.radix_sort(keys, bits)
+        ref = np.argsort(keys, kind="stable").astype(np.uint32)
+        assert np.array_equal(perm, ref), (n, bits)
+        assert np.array_equal(sk, keys[ref]), (n, bits)
 
 
 def test_radix_sort_empty(ctx):
