@@ -429,7 +429,7 @@ int ae_mpm_world_autotune(ae_mpm_world* world, uint32_t substeps_per_trial, ae_m
   if ((rc = w->snapshot(false))) return fail(ctx, rc, w->err);
   std::vector<int> variants = {AE_MPM_P2G_LANES, AE_MPM_P2G_TILE, AE_MPM_P2G_WARP_AGG, AE_MPM_P2G_GLOBAL};
   std::vector<int> threads = {128, 256};
-  std::vector<int> intervals = {1, 2, 4, 8};
+  std::vector<int> intervals = {1, 2, 4, 8, 16, 32};
   if (saved.deterministic) {
     variants = {saved.p2g_variant};
     intervals = {1};

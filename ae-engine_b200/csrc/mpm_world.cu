@@ -453,63 +453,81 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) p2g_lanes_kernel(
   using V4 = typename V4T<T>::type;
   extern __shared__ __align__(16) unsigned char smem[];
   const int nt = blockDim.x;
-  V4* col = reinterpret_cast<V4*>(smem);  // col[q * 9 + j]
-  V4* wxm = col + 9 * nt;                 // wxm[q]
-  V4* acol = wxm + nt;                    // acol[q]
+  V4* col = reinterpret_cast<V4*>(smem);          // col[q * 9 + j]
+  V4* wxm = col + 9 * nt;                         // wxm[q]
+  V4* acol = wxm + nt;                            // acol[q]
+  int4* gk = reinterpret_cast<int4*>(acol + nt);  // gk[q] = (stencil base, cell key)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int4 ch = w.chunks[blockIdx.x];
   const SceneDev<T>& sc = w.scenes[ch.x];
   const int n0 = sc.n[0], n1 = sc.n[1], n2 = sc.n[2];
   const int j = ch.y + tid;
+  const bool live = j < ch.z;
   bool has = false;
-  int g[3] = {0, 0, 0};
   int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
-  if (j < ch.z) {
+  P2GPart<T> p;
+  p.g[0] = p.g[1] = p.g[2] = 0;
+  if (live) {
     const uint32_t src = w.perm ? w.perm[j] : uint32_t(j);
-    P2GPart<T> p;
     p2g_setup<T, AE_MPM_MODE_PHYSICS>(w, sc, src, p);
     has = true;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      g[a] = p.g[a];
       lo[a] = max(p.g[a], 0);
       hi[a] = min(p.g[a] + 2, sc.n[a] - 1);
       if (lo[a] > hi[a]) has = false;
     }
+  }
+  // cell key: unique per cell (a stencil with any node in the grid has g in [-2, n-1] per axis)
+  const uint32_t key = has ? uint32_t(p.g[0] + 2) + uint32_t(n0 + 2) * (uint32_t(p.g[1] + 2) + uint32_t(n1 + 2) * uint32_t(p.g[2] + 2))
+                           : 0xffffffffu;
+  // Group equal keys anywhere in the warp (not only adjacent ones: particles that crossed into a
+  // neighbouring cell since the last sort rejoin it): groups in order of their first lane, lanes
+  // within a group in lane order.  pos is this particle's slot in that grouped order.
+  const uint32_t peers = __match_any_sync(0xffffffffu, key);
+  const int leader = __ffs(peers) - 1;
+  const uint32_t lead_cnt = lane == leader ? uint32_t(__popc(peers)) : 0u;
+  uint32_t incl = lead_cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t lead_off = incl - lead_cnt;
+  const int pos = int(__shfl_sync(0xffffffffu, lead_off, leader)) + __popc(peers & ((1u << lane) - 1u));
+  uint32_t starts = __reduce_or_sync(0xffffffffu, lane == leader ? (1u << lead_off) : 0u);
+  const int q = warp * 32 + pos;
+  if (live) {
     const T dx = sc.dx;
-    T c0[3], c1[3], c2[3], q[3];
+    T c0[3], c1[3], c2[3], qv[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
       c0[r] = dx * p.A[3 * r + 0];
       c1[r] = dx * p.A[3 * r + 1];
       c2[r] = dx * p.A[3 * r + 2];
-      q[r] = p.v[r] - (c0[r] * p.fx[0] + c1[r] * p.fx[1] + c2[r] * p.fx[2]);
+      qv[r] = p.v[r] - (c0[r] * p.fx[0] + c1[r] * p.fx[1] + c2[r] * p.fx[2]);
     }
-    V4* cq = col + tid * 9;
+    V4* cq = col + q * 9;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
 #pragma unroll
       for (int b = 0; b < 3; ++b) {
-        const T ux = q[0] + T(b) * c1[0] + T(c) * c2[0];
-        const T uy = q[1] + T(b) * c1[1] + T(c) * c2[1];
-        const T uz = q[2] + T(b) * c1[2] + T(c) * c2[2];
+        const T ux = qv[0] + T(b) * c1[0] + T(c) * c2[0];
+        const T uy = qv[1] + T(b) * c1[1] + T(c) * c2[1];
+        const T uz = qv[2] + T(b) * c1[2] + T(c) * c2[2];
         cq[b + 3 * c] = mk4(ux, uy, uz, p.w[1][b] * p.w[2][c]);
       }
     }
-    wxm[tid] = mk4(p.w[0][0], p.w[0][1], p.w[0][2], p.m);
-    acol[tid] = mk4(c0[0], c0[1], c0[2], T(0));
+    wxm[q] = mk4(p.w[0][0], p.w[0][1], p.w[0][2], p.m);
+    acol[q] = mk4(c0[0], c0[1], c0[2], T(0));
   }
+  gk[q] = make_int4(p.g[0], p.g[1], p.g[2], int(key));
   __syncwarp();
-  // run key: unique per cell (a stencil with any node in the grid has g in [-2, n-1] per axis)
-  const uint32_t key = has ? uint32_t(g[0] + 2) + uint32_t(n0 + 2) * (uint32_t(g[1] + 2) + uint32_t(n1 + 2) * uint32_t(g[2] + 2))
-                           : 0xffffffffu;
-  // runs of equal keys among this warp's particles (particles without nodes form their own runs)
-  const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
-  uint32_t starts = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
   // lanes 27..31 mirror the columns of lanes 22..26 (in-bounds reads, results never used)
   const int grp = lane < 27 ? lane / 9 : 2;
   const int jc = lane < 27 ? lane - 9 * grp : lane - 23;
   const int nb = jc % 3, nc = jc / 3;
+  const uint32_t nb0u = uint32_t(sc.nb[0]), nb1u = uint32_t(sc.nb[1]);
   const V4* colw = col + warp * 32 * 9 + jc;
   const V4* wxw = wxm + warp * 32;
   const V4* acw = acol + warp * 32;
@@ -517,11 +535,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) p2g_lanes_kernel(
     const int s0 = __ffs(starts) - 1;
     starts &= starts - 1u;
     const int e0 = starts ? __ffs(starts) - 1 : 32;
-    const uint32_t rk = __shfl_sync(0xffffffffu, key, s0);
-    const int X = __shfl_sync(0xffffffffu, g[0], s0);
-    const int Y = __shfl_sync(0xffffffffu, g[1], s0) + nb;
-    const int Z = __shfl_sync(0xffffffffu, g[2], s0) + nc;
-    if (rk == 0xffffffffu) continue;
+    const int4 run = gk[warp * 32 + s0];
+    if (uint32_t(run.w) == 0xffffffffu) continue;
+    const int X = run.x, Y = run.y + nb, Z = run.z + nc;
     T m0 = 0, x0 = 0, y0 = 0, z0 = 0, m1 = 0, x1 = 0, y1 = 0, z1 = 0, m2 = 0, x2 = 0, y2 = 0, z2 = 0;
     for (int i = s0 + grp; i < e0; i += 3) {
       const V4 u = colw[i * 9];
@@ -549,9 +565,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) p2g_lanes_kernel(
       m2 = groups(m2), x2 = groups(x2), y2 = groups(y2), z2 = groups(z2);
     }
     if (lane < 9 && Y >= 0 && Z >= 0 && Y < n1 && Z < n2) {
-      if (m0 != T(0) && X >= 0 && X < n0) atomic_add4(w.acc + node_index(sc, X, Y, Z), m0, x0, y0, z0);
-      if (m1 != T(0) && X + 1 >= 0 && X + 1 < n0) atomic_add4(w.acc + node_index(sc, X + 1, Y, Z), m1, x1, y1, z1);
-      if (m2 != T(0) && X + 2 >= 0 && X + 2 < n0) atomic_add4(w.acc + node_index(sc, X + 2, Y, Z), m2, x2, y2, z2);
+      // block-major node index, the (y,z) part once: ((blk_off + (bz nb1 + by) nb0 + bx) << 6) | local
+      const uint32_t row = ((sc.blk_off + (uint32_t(Z >> 2) * nb1u + uint32_t(Y >> 2)) * nb0u) << 6) |
+                           (uint32_t(Z & 3) << 4) | (uint32_t(Y & 3) << 2);
+      auto node = [row](int xa) { return row + ((uint32_t(xa >> 2) << 6) | uint32_t(xa & 3)); };
+      if (m0 != T(0) && X >= 0 && X < n0) atomic_add4(w.acc + node(X), m0, x0, y0, z0);
+      if (m1 != T(0) && X + 1 >= 0 && X + 1 < n0) atomic_add4(w.acc + node(X + 1), m1, x1, y1, z1);
+      if (m2 != T(0) && X + 2 >= 0 && X + 2 < n0) atomic_add4(w.acc + node(X + 2), m2, x2, y2, z2);
     }
   }
   // grid blocks of this warp's stencil bounding box
@@ -2273,10 +2293,10 @@ class World final : public WorldBase {
   void launch_p2g(WorldDev<T>& w) {
     const size_t sm = sizeof(V4) * max_tile_nodes();
     if (MODE == AE_MPM_MODE_PHYSICS && opts_.p2g_variant == kVarLanes) {
-      const size_t sm2 = sizeof(V4) * kLaneVecs * chunk_threads_;
+      const size_t per = sizeof(V4) * kLaneVecs + sizeof(int4);
+      const size_t sm2 = per * chunk_threads_;
       if (!lanes_smem_set_) {  // sized for the largest block (256 threads) the world accepts
-        cudaFuncSetAttribute(p2g_lanes_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(sizeof(V4) * kLaneVecs * 256));
+        cudaFuncSetAttribute(p2g_lanes_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(per * 256));
         lanes_smem_set_ = true;
       }
       p2g_lanes_kernel<T><<<n_chunks_, chunk_threads_, sm2, stream_>>>(w);

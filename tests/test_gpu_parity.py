@@ -115,7 +115,7 @@ def test_physics_materials_match_fp64_oracle(ctx, mat):
     assert rel(g64.J, ref.J) <= 1e-9
 
 
-@pytest.mark.parametrize("interval", [2, 5])
+@pytest.mark.parametrize("interval", [2, 5, 32])
 def test_sort_interval_does_not_change_results(ctx, interval):
     sc, p = S.tiny_scene(4096, 32, S.jelly(), v=(0.5, 0.5, 0.0))
     a = run_gpu(ctx, sc, p, 25, sort_interval=1)
