@@ -1133,7 +1133,8 @@ __device__ __forceinline__ void stencil_range(const SceneDev<T>& sc, T x, int a,
 }
 
 template <class T, int MODE>
-__global__ void __launch_bounds__(256, (MODE == AE_MPM_MODE_PHYSICS && sizeof(T) == 4) ? 4 : 1) g2p_kernel(WorldDev<T> w, uint32_t* epoch) {
+__global__ void __launch_bounds__(256, (MODE == AE_MPM_MODE_PHYSICS && sizeof(T) == 4) ? 4 : 1) g2p_kernel(WorldDev<T> w, uint32_t* epoch,
+                                                                                                    int write_keys) {
   using V4 = typename V4T<T>::type;
   extern __shared__ __align__(16) unsigned char smem[];
   V4* tile = reinterpret_cast<V4*>(smem);
@@ -1252,11 +1253,12 @@ __global__ void __launch_bounds__(256, (MODE == AE_MPM_MODE_PHYSICS && sizeof(T)
     w.out[4][j] = mk4(o.v[0], o.v[1], o.v[2], o.C[0]);
     w.out[5][j] = mk4(o.C[1], o.C[2], o.C[3], o.C[4]);
     w.out[6][j] = mk4(o.C[5], o.C[6], o.C[7], o.C[8]);
-    w.keys[j] = cell_key(sc, MODE, o.x[0], o.x[1], o.x[2]);
+    // the next substep's cell key, only when the next substep sorts (the world tracks this)
+    if (write_keys) w.keys[j] = cell_key(sc, MODE, o.x[0], o.x[1], o.x[2]);
     err = o.err;
     cl = o.clamped;
     need = o.needs_clamp;
-  } else if (j < ch.w) {
+  } else if (j < ch.w && write_keys) {
     w.keys[j] = sc.dead_key;
   }
   // warp-aggregated error words, counters and clamp-queue appends
@@ -1938,6 +1940,7 @@ class World final : public WorldBase {
       WorldDev<T> w = dev(false);
       launch_init_keys(w);
       keys_stale_ = false;
+      keys_fresh_ = true;
     }
     const int interval = opts_.deterministic ? 1 : opts_.sort_interval;
     const uint64_t period = (interval % 2 == 0) ? uint64_t(interval) : uint64_t(2 * interval);
@@ -2123,6 +2126,7 @@ class World final : public WorldBase {
       WorldDev<T> w = dev(false);
       launch_init_keys(w);
       keys_stale_ = false;
+      keys_fresh_ = true;
     }
     // all substeps are queued before the one wait, so that (past the first) the stream is never
     // idle waiting for the host and the events measure device time, not launch latency
@@ -2310,7 +2314,7 @@ class World final : public WorldBase {
   }
 
   template <int MODE>
-  void substep_mode(WorldDev<T>& w) {
+  void substep_mode(WorldDev<T>& w, bool write_keys) {
     const int sms = device_sm_count();
     if (opts_.deterministic) {
       det_heads_kernel<<<unsigned((total_cap_ + 255) / 256), 256, 0, stream_>>>(w.sorted_keys, total_cap_, dead_blk_,
@@ -2328,7 +2332,7 @@ class World final : public WorldBase {
     }
     mark(3);
     const size_t g2p_smem = sizeof(V4) * ((MODE == AE_MPM_MODE_PHYSICS ? 0 : max_tile_nodes()) + 3 * chunk_threads_);
-    g2p_kernel<T, MODE><<<n_chunks_, chunk_threads_, g2p_smem, stream_>>>(w, counters_ + 2);
+    g2p_kernel<T, MODE><<<n_chunks_, chunk_threads_, g2p_smem, stream_>>>(w, counters_ + 2, write_keys ? 1 : 0);
     ++launches_;
     if (MODE == AE_MPM_MODE_PHYSICS && has_snow_) {
       snow_clamp_kernel<T><<<sms * 4, 128, 0, stream_>>>(w);
@@ -2344,16 +2348,26 @@ class World final : public WorldBase {
   void substep_eager() {
     const int interval = opts_.deterministic ? 1 : opts_.sort_interval;
     const bool do_sort = (substep_ % uint64_t(interval)) == 0;
+    // G2P writes the cell keys only for a substep that sorts next; a sort whose keys were not
+    // written by the G2P just before it (sort interval changed, first substep) computes them first
+    const bool next_sorts = ((substep_ + 1) % uint64_t(interval)) == 0;
     if (n_chunks_ > 0) {
       mark(0);
-      if (do_sort) launches_ += radix_sort_pairs(keys_, total_cap_, key_bits_, sort_, stream_, &sorted_keys_, &perm_);
+      if (do_sort) {
+        if (!keys_fresh_) {
+          WorldDev<T> wk = dev(false);
+          launch_init_keys(wk);
+        }
+        launches_ += radix_sort_pairs(keys_, total_cap_, key_bits_, sort_, stream_, &sorted_keys_, &perm_);
+      }
       mark(1);
       WorldDev<T> w = dev(do_sort);
       switch (mode_) {
-        case AE_MPM_MODE_PHYSICS: substep_mode<AE_MPM_MODE_PHYSICS>(w); break;
-        case AE_MPM_MODE_REFERENCE: substep_mode<AE_MPM_MODE_REFERENCE>(w); break;
-        default: substep_mode<AE_MPM_MODE_VELOCITY_ONLY>(w); break;
+        case AE_MPM_MODE_PHYSICS: substep_mode<AE_MPM_MODE_PHYSICS>(w, next_sorts); break;
+        case AE_MPM_MODE_REFERENCE: substep_mode<AE_MPM_MODE_REFERENCE>(w, next_sorts); break;
+        default: substep_mode<AE_MPM_MODE_VELOCITY_ONLY>(w, next_sorts); break;
       }
+      keys_fresh_ = next_sorts || opts_.deterministic;
       a_in_ = !a_in_;
     }
     ++substep_;
@@ -2469,6 +2483,7 @@ class World final : public WorldBase {
   uint64_t total_cap_ = 0, total_blocks_ = 0, device_bytes_ = 0;
   int key_bits_ = 1;
   bool keys_stale_ = true, chunks_dirty_ = true, scenes_dirty_ = true, mats_dirty_ = false;
+  bool keys_fresh_ = false;  // keys_ hold the cell keys of the current positions
 };
 
 WorldBase* make_world(const ae_mpm_scene_desc* scenes, uint32_t n_scenes, const ae_mpm_exec_opts& opts, std::string& why,
