@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--e2e-substeps", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--variant", choices=["lanes", "tile", "warp_agg", "global"],
+                    help="fixed P2G variant (with --block-threads and --sort-interval: no autotune)")
+    ap.add_argument("--block-threads", type=int, choices=[128, 256])
+    ap.add_argument("--sort-interval", type=int)
     ap.add_argument("--scenes", type=int, default=512, help="batched: number of scenes")
     ap.add_argument("--plain-sample", type=int, default=48, help="batched: scenes timed one at a time")
     ap.add_argument("--rates", default="50,200,1000", help="served: Poisson arrival rates (scenes/s)")
@@ -257,13 +261,21 @@ def run_ours(args, rank, local, world_size, pg):
         return run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg)
     if args.workload == "batched":
         return run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg)
-    opts = M.exec_opts()
+    fixed = {}
+    if args.variant:
+        fixed["p2g_variant"] = {"tile": M.P2G_TILE, "warp_agg": M.P2G_WARP_AGG, "global": M.P2G_GLOBAL,
+                                "lanes": M.P2G_LANES}[args.variant]
+    if args.block_threads:
+        fixed["block_threads"] = args.block_threads
+    if args.sort_interval:
+        fixed["sort_interval"] = args.sort_interval
+    opts = M.exec_opts(**fixed)
     world = M.World(ctx, scenes, opts)
     for i, p in enumerate(parts):
         world.upload(i, p)
     n_total = sum(p.n for p in parts)
-    tune = None
-    if not args.no_autotune:
+    tune = {"fixed": {k: int(v) for k, v in fixed.items()}} if fixed else None
+    if not args.no_autotune and not fixed:
         r = world.autotune(8)
         tune = {"p2g_variant": {1: "tile", 2: "warp_agg", 3: "global", 4: "lanes"}.get(r.p2g_variant, r.p2g_variant),
                 "block_threads": r.block_threads, "sort_interval": r.sort_interval,
