@@ -714,73 +714,32 @@ struct VelTile {
   }
 };
 
-// Physics gather from the tile for a particle whose 27 stencil nodes are all inside the grid
-// (every particle after its first substep: positions are clamped to [1, n-2] dx).  Separable:
-// each (y,z) column is summed over x first,
+// Node velocities of the block-major grid by (y,z) row, through the read-only cache: row(Y, Z)
+// once per stencil column, then at(row, X) for its three x nodes.  The block needs no bounding
+// box, tile or barrier, so its warps never wait for one another.
+template <class T>
+struct GridRows {
+  using V4 = typename V4T<T>::type;
+  const V4* __restrict__ vel;
+  uint32_t blk_off, nb0, nb1;
+  __device__ __forceinline__ uint32_t row(int Y, int Z) const {
+    return ((blk_off + (uint32_t(Z >> 2) * nb1 + uint32_t(Y >> 2)) * nb0) << 6) | (uint32_t(Z & 3) << 4) |
+           (uint32_t(Y & 3) << 2);
+  }
+  __device__ __forceinline__ V4 at(uint32_t r, int X) const {
+    return ld4(vel + (r + ((uint32_t(X >> 2) << 6) | uint32_t(X & 3))));
+  }
+};
+// Physics gather for a particle whose 27 stencil nodes are all inside the grid (every particle
+// after its first substep: positions are clamped to [1, n-2] dx).  Separable: each (y,z) column
+// is summed over x first,
 //   S0 = sum_a wx[a] g(a,b,c),   S1 = sum_a wx[a] (a - fx) dx g(a,b,c),
 // then v += wy wz S0, B[.][0] += wy wz S1, B[.][1] += wy (b - fy) dx wz S0,
 // B[.][2] += wy wz (c - fz) dx S0: 36 instructions per column instead of 42 per node.
 // Returns false (nothing written) when the particle does not qualify.
-template <class T>
-__device__ __forceinline__ bool g2p_physics_gather_tile(const VelTile<T>& vt, const SceneDev<T>& sc, const T* x0, T* v,
-                                                        T* C) {
-  using V4 = typename V4T<T>::type;
-  if (!vt.tile) return false;
-  int b[3];
-  T w[3][3], e[3][3];
-  bool inside = true;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const T X = (x0[a] - sc.origin[a]) * sc.inv_dx;
-    const int bb = floor_to_int(X - T(0.5));
-    const T fx = X - T(bb);
-    b[a] = bb;
-    inside = inside && bb >= 0 && bb + 2 < sc.n[a];
-    const T t0 = T(1.5) - fx, t1 = fx - T(1), t2 = fx - T(0.5);
-    w[a][0] = T(0.5) * t0 * t0;
-    w[a][1] = T(0.75) - t1 * t1;
-    w[a][2] = T(0.5) * t2 * t2;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) e[a][k] = w[a][k] * ((T(k) - fx) * sc.dx);
-  }
-  if (!inside) return false;
-  const V4* t0 = vt.tile + ((b[2] - vt.L2) << vt.sp) + ((b[1] - vt.L1) << vt.p0) + (b[0] - vt.L0);
-  T vv[3] = {0, 0, 0}, B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-#pragma unroll
-    for (int bb = 0; bb < 3; ++bb) {
-      const V4* row = t0 + (c << vt.sp) + (bb << vt.p0);
-      const V4 g0 = row[0], g1 = row[1], g2 = row[2];
-      const T s0[3] = {w[0][0] * g0.x + w[0][1] * g1.x + w[0][2] * g2.x, w[0][0] * g0.y + w[0][1] * g1.y + w[0][2] * g2.y,
-                       w[0][0] * g0.z + w[0][1] * g1.z + w[0][2] * g2.z};
-      const T s1[3] = {e[0][0] * g0.x + e[0][1] * g1.x + e[0][2] * g2.x, e[0][0] * g0.y + e[0][1] * g1.y + e[0][2] * g2.y,
-                       e[0][0] * g0.z + e[0][1] * g1.z + e[0][2] * g2.z};
-      const T wbc = w[1][bb] * w[2][c], ebc = e[1][bb] * w[2][c], fbc = w[1][bb] * e[2][c];
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        vv[r] += wbc * s0[r];
-        B[r * 3 + 0] += wbc * s1[r];
-        B[r * 3 + 1] += ebc * s0[r];
-        B[r * 3 + 2] += fbc * s0[r];
-      }
-    }
-  }
-  const T cs = T(4) * sc.inv_dx * sc.inv_dx;
-#pragma unroll
-  for (int r = 0; r < 3; ++r) v[r] = vv[r];
-#pragma unroll
-  for (int k = 0; k < 9; ++k) C[k] = cs * B[k];
-  return true;
-}
-
-// Physics gather straight from the grid's velocity array through the read-only cache, for a
-// particle whose 27 stencil nodes are all inside the grid.  Same separable sums as the tile
-// gather; node addresses are built per (y,z) column from the block-major layout.  The block
-// needs no bounding box, tile or barrier, so its warps never wait for one another.
-template <class T>
-__device__ __forceinline__ bool g2p_physics_gather_direct(const typename V4T<T>::type* __restrict__ vel,
-                                                          const SceneDev<T>& sc, const T* x0, T* v, T* C) {
+template <class T, class Rows>
+__device__ __forceinline__ bool g2p_physics_gather_sep(const Rows& rows, const SceneDev<T>& sc, const T* x0, T* v,
+                                                       T* C) {
   using V4 = typename V4T<T>::type;
   int b[3];
   T w[3][3], e[3][3];
@@ -800,37 +759,30 @@ __device__ __forceinline__ bool g2p_physics_gather_direct(const typename V4T<T>:
     for (int k = 0; k < 3; ++k) e[a][k] = w[a][k] * ((T(k) - fx) * sc.dx);
   }
   if (!inside) return false;
-  uint32_t xo[3];  // x part of the node index: block column and lane within the block
-#pragma unroll
-  for (int a = 0; a < 3; ++a) xo[a] = (uint32_t((b[0] + a) >> 2) << 6) | uint32_t((b[0] + a) & 3);
-  const uint32_t nb0 = uint32_t(sc.nb[0]), nb1 = uint32_t(sc.nb[1]);
   T vv[3] = {0, 0, 0}, B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const int Z = b[2] + c;
 #pragma unroll
     for (int bb = 0; bb < 3; ++bb) {
-      const int Y = b[1] + bb;
-      const uint32_t row = ((sc.blk_off + (uint32_t(Z >> 2) * nb1 + uint32_t(Y >> 2)) * nb0) << 6) |
-                           (uint32_t(Z & 3) << 4) | (uint32_t(Y & 3) << 2);
-      const V4 g0 = ld4(vel + (row + xo[0])), g1 = ld4(vel + (row + xo[1])), g2 = ld4(vel + (row + xo[2]));
+      const uint32_t r = rows.row(b[1] + bb, b[2] + c);
+      const V4 g0 = rows.at(r, b[0]), g1 = rows.at(r, b[0] + 1), g2 = rows.at(r, b[0] + 2);
       const T s0[3] = {w[0][0] * g0.x + w[0][1] * g1.x + w[0][2] * g2.x, w[0][0] * g0.y + w[0][1] * g1.y + w[0][2] * g2.y,
                        w[0][0] * g0.z + w[0][1] * g1.z + w[0][2] * g2.z};
       const T s1[3] = {e[0][0] * g0.x + e[0][1] * g1.x + e[0][2] * g2.x, e[0][0] * g0.y + e[0][1] * g1.y + e[0][2] * g2.y,
                        e[0][0] * g0.z + e[0][1] * g1.z + e[0][2] * g2.z};
       const T wbc = w[1][bb] * w[2][c], ebc = e[1][bb] * w[2][c], fbc = w[1][bb] * e[2][c];
 #pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        vv[r] += wbc * s0[r];
-        B[r * 3 + 0] += wbc * s1[r];
-        B[r * 3 + 1] += ebc * s0[r];
-        B[r * 3 + 2] += fbc * s0[r];
+      for (int k = 0; k < 3; ++k) {
+        vv[k] += wbc * s0[k];
+        B[k * 3 + 0] += wbc * s1[k];
+        B[k * 3 + 1] += ebc * s0[k];
+        B[k * 3 + 2] += fbc * s0[k];
       }
     }
   }
   const T cs = T(4) * sc.inv_dx * sc.inv_dx;
 #pragma unroll
-  for (int r = 0; r < 3; ++r) v[r] = vv[r];
+  for (int k = 0; k < 3; ++k) v[k] = vv[k];
 #pragma unroll
   for (int k = 0; k < 9; ++k) C[k] = cs * B[k];
   return true;
@@ -1220,8 +1172,11 @@ __global__ void __launch_bounds__(256, (MODE == AE_MPM_MODE_PHYSICS && sizeof(T)
     const T x0[3] = {a0.x, a0.y, a0.z};
     G2POut<T> o;
     T pv[3] = {0, 0, 0};
-    if (MODE == AE_MPM_MODE_PHYSICS && !g2p_physics_gather_direct<T>(w.vel, sc, x0, pv, o.C))
-      g2p_physics_gather<T>(vt, sc, x0, pv, o.C);
+    if (MODE == AE_MPM_MODE_PHYSICS) {
+      const bool done = g2p_physics_gather_sep<T>(
+          GridRows<T>{w.vel, sc.blk_off, uint32_t(sc.nb[0]), uint32_t(sc.nb[1])}, sc, x0, pv, o.C);
+      if (!done) g2p_physics_gather<T>(vt, sc, x0, pv, o.C);  // stencil partly outside the grid
+    }
     cp_async_wait_all();
     const V4 a1 = stage[tid], a2 = stage[nt + tid], a3 = stage[2 * nt + tid];
     const T F[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
