@@ -123,6 +123,33 @@ def test_sort_interval_does_not_change_results(ctx, interval):
     assert rel(b.pos, a.pos) <= 1e-6
 
 
+def test_split_steps_and_upload_mid_run_agree_with_one_run(ctx):
+    # World state carried between step() calls (buffer parity, sort phase, cell keys, graph
+    # replays) must give the same trajectory as one call, eager and graph alike; an upload
+    # mid-run must restart cleanly; the LANES and TILE P2G variants must agree.  Snow exercises the
+    # clamp kernel.  Tolerance: f32, only atomic summation order differs: 1e-6 relative in positions.
+    sc, p = S.tiny_scene(8192, 32, S.snow(), v=(1.0, -0.5, 0.25))
+    one = run_gpu(ctx, sc, p, 24, p2g_variant=M.P2G_LANES, use_graph=1)
+    for graph in (0, 1):
+        w = M.World(ctx, [sc], M.exec_opts(p2g_variant=M.P2G_LANES, use_graph=graph, sort_interval=4))
+        w.upload(0, p)
+        for k in (5, 11, 8):
+            w.step(k)
+        w.sync()
+        split = w.download(0, p.n)
+        w.upload(0, p)  # back to the start: the pending scatter of the stepped state must go
+        w.step(24)
+        w.sync()
+        again = w.download(0, p.n)
+        w.close()
+        assert rel(split.pos, one.pos) <= 1e-6, graph
+        assert rel(again.pos, one.pos) <= 1e-6, graph
+        assert rel(again.F, one.F) <= 1e-5, graph
+    unfused = run_gpu(ctx, sc, p, 24, p2g_variant=M.P2G_TILE)
+    assert rel(unfused.pos, one.pos) <= 1e-6
+    assert rel(unfused.F, one.F) <= 1e-5
+
+
 def test_graph_and_eager_paths_agree(ctx):
     sc, p = S.tiny_scene(4096, 32, S.snow(), v=(0.5, 0.5, 0.0))
     a = run_gpu(ctx, sc, p, 16, use_graph=0, deterministic=1)
