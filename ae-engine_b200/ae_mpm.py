@@ -121,6 +121,12 @@ SIGNATURES = {
     "ae_mpm_world_particles": (C.c_uint64, [_P]),
     "ae_mpm_radix_sort_keys": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, _P, _P]),
     "ae_mpm_radix_sort_keys_noalloc": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, _P, _P, _P]),
+    "ae_mpm_lod_classify": (C.c_int, [_P, _P, _P, C.c_uint64, _P, C.c_float, C.c_float, C.c_uint64, _P,
+                                      C.POINTER(C.c_uint64), _P, C.POINTER(C.c_uint64), _P, C.POINTER(C.c_uint64)]),
+    "ae_mpm_far_field_update": (C.c_int, [_P, _P, _P, _P, C.c_uint64, _P, C.c_uint64, _P, C.c_uint32, C.c_float, _P,
+                                          C.c_float]),
+    "ae_mpm_coarse_field_update": (C.c_int, [_P, _P, _P, _P, _P, C.c_uint64, _P, C.c_uint64, _P, C.c_uint32,
+                                             C.c_float, _P, C.c_float]),
     "ae_mpm_world_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(TuneResult)]),
     "ae_mpm_server_create": (C.c_int, [_P, C.POINTER(ServerOpts), C.POINTER(_P)]),
     "ae_mpm_server_submit": (C.c_int, [_P, C.POINTER(SceneDesc), C.POINTER(ParticlesView), C.c_uint64, C.c_uint32,
@@ -293,6 +299,45 @@ class Context:
         v = np.zeros((nx * ny * nz, 3), np.float32)
         self.check(self.lib.ae_mpm_grid_download(self.h, m.ctypes.data, v.ctypes.data, m.size))
         return m, v
+
+    # engine tick passes around the substep (simulation.rs): numpy arrays in MpssBuffer layout
+    # (pos, vel: (count, 3) f32; mass, temperature: (count,) f32; active: (count,) bool/u8 or None)
+    def lod_classify(self, pos, active, player, near_dist, mid_dist, max_near):
+        pos = np.ascontiguousarray(pos, np.float32)
+        n = pos.shape[0]
+        act = None if active is None else np.ascontiguousarray(active, np.uint8)
+        outs = [np.empty(max(n, 1), np.uint64) for _ in range(3)]
+        cnt = [C.c_uint64(0) for _ in range(3)]
+        pl = np.ascontiguousarray(player, np.float32)
+        self.check(self.lib.ae_mpm_lod_classify(self.h, pos.ctypes.data, None if act is None else act.ctypes.data, n,
+                                                pl.ctypes.data, near_dist, mid_dist, max_near,
+                                                outs[0].ctypes.data, C.byref(cnt[0]), outs[1].ctypes.data,
+                                                C.byref(cnt[1]), outs[2].ctypes.data, C.byref(cnt[2])))
+        return tuple(o[:c.value].copy() for o, c in zip(outs, cnt))
+
+    def far_field_update(self, pos, vel, temperature, far_idx, coarse, coarse_dx, origin, far_dt):
+        """Updates pos, vel and temperature (float32 arrays) in place."""
+        idx = np.ascontiguousarray(far_idx, np.uint64)
+        coarse = np.ascontiguousarray(coarse, np.float32)
+        cn = int(round(coarse.size ** (1.0 / 3.0)))
+        o = np.ascontiguousarray(origin, np.float32)
+        self.check(self.lib.ae_mpm_far_field_update(self.h, pos.ctypes.data, vel.ctypes.data, temperature.ctypes.data,
+                                                    pos.shape[0], idx.ctypes.data, idx.size, coarse.ctypes.data, cn,
+                                                    coarse_dx, o.ctypes.data, far_dt))
+
+    def coarse_field_update(self, pos, mass, temperature, active, near_idx, coarse, coarse_dx, origin, dt):
+        """Updates coarse (float32, n^3) in place."""
+        pos = np.ascontiguousarray(pos, np.float32)
+        mass = np.ascontiguousarray(mass, np.float32)
+        temperature = np.ascontiguousarray(temperature, np.float32)
+        act = None if active is None else np.ascontiguousarray(active, np.uint8)
+        idx = np.ascontiguousarray(near_idx, np.uint64)
+        cn = int(round(coarse.size ** (1.0 / 3.0)))
+        o = np.ascontiguousarray(origin, np.float32)
+        self.check(self.lib.ae_mpm_coarse_field_update(self.h, pos.ctypes.data, mass.ctypes.data, temperature.ctypes.data,
+                                                       None if act is None else act.ctypes.data, pos.shape[0],
+                                                       idx.ctypes.data, idx.size, coarse.ctypes.data, cn, coarse_dx,
+                                                       o.ctypes.data, dt))
 
     def radix_sort(self, keys: np.ndarray, key_bits: int):
         keys = np.ascontiguousarray(keys, np.uint32)

@@ -26,7 +26,7 @@ LIB = os.path.join(BUILD, "libae_mpm.so")
 HOST_TEST = os.path.join(BUILD, "test_host_mirror")
 ORACLE_LIB = os.path.join(ORACLE_BUILD, "libae_mpm_oracle.so")
 
-CU_SOURCES = ["radix_sort.cu", "mpm_world.cu", "ae_mpm_api.cu", "ae_mpm_server.cu", "ae_mpm_noalloc.cu"]
+CU_SOURCES = ["radix_sort.cu", "mpm_world.cu", "ae_mpm_api.cu", "ae_mpm_server.cu", "ae_mpm_noalloc.cu", "ae_mpm_lod.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
@@ -91,10 +91,11 @@ def build_host_test(force: bool = False) -> str:
 
 def build_oracle(force: bool = False) -> str:
     os.makedirs(ORACLE_BUILD, exist_ok=True)
-    src = os.path.join(ORACLE, "mpm_oracle.cpp")
-    if force or _stale(ORACLE_LIB, [src, os.path.join(ROOT, "include", "ae_mpm.h")]):
-        # x86-64-v3 (AVX2/FMA) so the binary also runs on the GPU hosts' CPUs
-        _run(["g++", "-O3", "-std=c++17", "-march=x86-64-v3", "-fPIC", "-shared", "-o", ORACLE_LIB, src, "-lpthread"])
+    srcs = [os.path.join(ORACLE, "mpm_oracle.cpp"), os.path.join(ORACLE, "lod_oracle.cpp")]
+    if force or _stale(ORACLE_LIB, srcs + [os.path.join(ROOT, "include", "ae_mpm.h")]):
+        # x86-64-v3 so the binary also runs on the GPU hosts' CPUs; no FMA contraction, as in Rust
+        _run(["g++", "-O3", "-std=c++17", "-march=x86-64-v3", "-ffp-contract=off", "-fPIC", "-shared", "-o", ORACLE_LIB]
+             + srcs + ["-lpthread"])
     return ORACLE_LIB
 
 

@@ -17,6 +17,7 @@
 
 #include "../../include/ae_mpm.h"
 #include "mpm_world.cuh"
+#include "ae_mpm_lod.cuh"
 #include "radix_sort.cuh"
 
 using aemp::WorldBase;
@@ -37,6 +38,10 @@ struct ae_mpm_ctx {
   uint64_t sort_keys_cap = 0;
   // autotune cache: workload signature -> choice
   std::map<std::string, ae_mpm_tune_result> tuned;
+  // engine tick passes (LOD, far field, coarse field) and their device staging for host arrays
+  aemp::LodWork* lod = nullptr;
+  void* dstage = nullptr;
+  size_t dstage_bytes = 0;
 };
 
 struct ae_mpm_world {
@@ -91,6 +96,33 @@ int ensure_pinned(ae_mpm_ctx* ctx, size_t bytes) {
   if (e != cudaSuccess) return fail(ctx, AE_MPM_ENOMEM, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
   ctx->pin_bytes = bytes;
   return AE_MPM_OK;
+}
+
+int ensure_dstage(ae_mpm_ctx* ctx, size_t bytes) {
+  if (bytes <= ctx->dstage_bytes) return AE_MPM_OK;
+  cudaFree(ctx->dstage);
+  ctx->dstage = nullptr;
+  ctx->dstage_bytes = 0;
+  cudaError_t e = cudaMalloc(&ctx->dstage, bytes);
+  if (e != cudaSuccess) return fail(ctx, AE_MPM_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  ctx->dstage_bytes = bytes;
+  return AE_MPM_OK;
+}
+
+// device (or managed) memory, as opposed to ordinary or pinned host memory
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+aemp::LodWork* lod_work(ae_mpm_ctx* ctx) {
+  if (!ctx->lod) ctx->lod = new aemp::LodWork();
+  return ctx->lod;
 }
 
 // reference-layout view over the pinned staging for n particles
@@ -236,6 +268,8 @@ void ae_mpm_ctx_destroy(ae_mpm_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   delete ctx->dropin;
+  delete ctx->lod;
+  cudaFree(ctx->dstage);
   if (ctx->pin) cudaFreeHost(ctx->pin);
   aemp::sort_scratch_free(ctx->sort);
   cudaFree(ctx->sort_keys);
@@ -413,6 +447,156 @@ int ae_mpm_radix_sort_keys(ae_mpm_ctx* ctx, const uint32_t* keys, uint64_t n, ui
   if (e == cudaSuccess) e = cudaMemcpy(sorted_keys_out, sk, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(perm_out, pm, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, cudaGetErrorString(e));
+  return AE_MPM_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// engine tick passes around the substep (simulation.rs:495-532, 612-679, 877-966)
+// ---------------------------------------------------------------------------------------------
+int ae_mpm_lod_classify(ae_mpm_ctx* ctx, const float* pos, const uint8_t* active, uint64_t count,
+                        const float player[3], float near_dist, float mid_dist, uint64_t max_near, uint64_t* near_out,
+                        uint64_t* n_near, uint64_t* mid_out, uint64_t* n_mid, uint64_t* far_out, uint64_t* n_far) {
+  if (!ctx) return AE_MPM_EINVAL;
+  if (!player || !n_near || !n_mid || !n_far || (count && (!pos || !near_out || !mid_out || !far_out)) ||
+      count >= (1ull << 32))
+    return fail(ctx, AE_MPM_EINVAL, "lod_classify: null array or more than 2^32 - 1 particles");
+  *n_near = *n_mid = *n_far = 0;
+  if (count == 0) return AE_MPM_OK;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  aemp::LodWork* lw = lod_work(ctx);
+  uint64_t counts[3] = {0, 0, 0};
+  cudaError_t e;
+  if (is_device_ptr(pos)) {
+    e = lw->classify(pos, active, count, player, near_dist, mid_dist, max_near, near_out, mid_out, far_out, counts, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  } else {
+    // device copies of pos and active, three output lists; each region starts on a 16-byte boundary
+    const size_t b_pos = (sizeof(float) * 3 * count + 15) & ~size_t(15), b_act = active ? ((count + 15) & ~size_t(15)) : 0;
+    rc = ensure_dstage(ctx, b_pos + b_act + 3 * sizeof(uint64_t) * count);
+    if (rc) return rc;
+    char* d = static_cast<char*>(ctx->dstage);
+    float* dpos = reinterpret_cast<float*>(d);
+    uint8_t* dact = active ? reinterpret_cast<uint8_t*>(d + b_pos) : nullptr;
+    uint64_t* dl = reinterpret_cast<uint64_t*>(d + b_pos + b_act);
+    e = cudaMemcpyAsync(dpos, pos, sizeof(float) * 3 * count, cudaMemcpyHostToDevice, 0);
+    if (e == cudaSuccess && active) e = cudaMemcpyAsync(dact, active, count, cudaMemcpyHostToDevice, 0);
+    if (e == cudaSuccess)
+      e = lw->classify(dpos, dact, count, player, near_dist, mid_dist, max_near, dl, dl + count, dl + 2 * count, counts, 0);
+    if (e == cudaSuccess && counts[0]) e = cudaMemcpyAsync(near_out, dl, sizeof(uint64_t) * counts[0], cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess && counts[1])
+      e = cudaMemcpyAsync(mid_out, dl + count, sizeof(uint64_t) * counts[1], cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess && counts[2])
+      e = cudaMemcpyAsync(far_out, dl + 2 * count, sizeof(uint64_t) * counts[2], cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  }
+  if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("lod_classify: ") + cudaGetErrorString(e));
+  *n_near = counts[0];
+  *n_mid = counts[1];
+  *n_far = counts[2];
+  return AE_MPM_OK;
+}
+
+int ae_mpm_far_field_update(ae_mpm_ctx* ctx, float* pos, float* vel, float* temperature, uint64_t count,
+                            const uint64_t* far_idx, uint64_t n_far, const float* coarse_temperature, uint32_t coarse_n,
+                            float coarse_dx, const float coarse_origin[3], float far_dt) {
+  if (!ctx) return AE_MPM_EINVAL;
+  if (!coarse_origin || (n_far && (!pos || !vel || !temperature || !far_idx || !coarse_temperature)) || coarse_n == 0 ||
+      uint64_t(coarse_n) * coarse_n * coarse_n >= (1ull << 31))
+    return fail(ctx, AE_MPM_EINVAL, "far_field_update: null array or coarse_n out of range");
+  if (n_far == 0) return AE_MPM_OK;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  aemp::LodWork* lw = lod_work(ctx);
+  const uint64_t cells = uint64_t(coarse_n) * coarse_n * coarse_n;
+  cudaError_t e;
+  if (is_device_ptr(pos)) {
+    e = lw->far_field(pos, vel, temperature, far_idx, n_far, coarse_temperature, coarse_n, coarse_dx, coarse_origin,
+                      far_dt, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  } else {
+    for (uint64_t k = 0; k < n_far; ++k)
+      if (far_idx[k] >= count) return fail(ctx, AE_MPM_EINVAL, "far_field_update: index out of range");
+    // gather the far particles (pos, vel, temperature: 7 floats each) and the field, one copy each way
+    const size_t bytes = sizeof(float) * (7 * n_far + cells);
+    rc = ensure_pinned(ctx, bytes);
+    if (rc) return rc;
+    rc = ensure_dstage(ctx, bytes);
+    if (rc) return rc;
+    float* h = ctx->pin;
+    for (uint64_t k = 0; k < n_far; ++k) {
+      const uint64_t i = far_idx[k];
+      std::memcpy(h + 3 * k, pos + 3 * i, sizeof(float) * 3);
+      std::memcpy(h + 3 * (n_far + k), vel + 3 * i, sizeof(float) * 3);
+      h[6 * n_far + k] = temperature[i];
+    }
+    std::memcpy(h + 7 * n_far, coarse_temperature, sizeof(float) * cells);
+    float* d = static_cast<float*>(ctx->dstage);
+    e = cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, 0);
+    if (e == cudaSuccess)
+      e = lw->far_field(d, d + 3 * n_far, d + 6 * n_far, nullptr, n_far, d + 7 * n_far, coarse_n, coarse_dx,
+                        coarse_origin, far_dt, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(float) * 7 * n_far, cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    if (e == cudaSuccess)
+      for (uint64_t k = 0; k < n_far; ++k) {
+        const uint64_t i = far_idx[k];
+        pos[3 * i + 1] = h[3 * k + 1];
+        vel[3 * i + 1] = h[3 * (n_far + k) + 1];
+        temperature[i] = h[6 * n_far + k];
+      }
+  }
+  if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("far_field_update: ") + cudaGetErrorString(e));
+  return AE_MPM_OK;
+}
+
+int ae_mpm_coarse_field_update(ae_mpm_ctx* ctx, const float* pos, const float* mass, const float* temperature,
+                               const uint8_t* active, uint64_t count, const uint64_t* near_idx, uint64_t n_near,
+                               float* coarse_temperature, uint32_t coarse_n, float coarse_dx,
+                               const float coarse_origin[3], float dt) {
+  if (!ctx) return AE_MPM_EINVAL;
+  if (!coarse_origin || !coarse_temperature || (n_near && (!pos || !mass || !temperature || !near_idx)) ||
+      coarse_n == 0 || uint64_t(coarse_n) * coarse_n * coarse_n >= (1ull << 31) || n_near >= (1ull << 32))
+    return fail(ctx, AE_MPM_EINVAL, "coarse_field_update: null array or size out of range");
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  aemp::LodWork* lw = lod_work(ctx);
+  const uint64_t cells = uint64_t(coarse_n) * coarse_n * coarse_n;
+  cudaError_t e;
+  if (is_device_ptr(coarse_temperature)) {
+    e = lw->coarse_field(pos, mass, temperature, active, near_idx, n_near, coarse_temperature, coarse_n, coarse_dx,
+                         coarse_origin, dt, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  } else {
+    for (uint64_t k = 0; k < n_near; ++k)
+      if (near_idx[k] >= count) return fail(ctx, AE_MPM_EINVAL, "coarse_field_update: index out of range");
+    // gather the near particles (pos, mass, temperature: 5 floats; active: 1 byte) and the field
+    const size_t b_f = sizeof(float) * (5 * n_near + cells), b_a = (n_near + 15) & ~uint64_t(15);
+    rc = ensure_pinned(ctx, b_f + b_a);
+    if (rc) return rc;
+    rc = ensure_dstage(ctx, b_f + b_a);
+    if (rc) return rc;
+    float* h = ctx->pin;
+    uint8_t* ha = reinterpret_cast<uint8_t*>(h + 5 * n_near + cells);
+    for (uint64_t k = 0; k < n_near; ++k) {
+      const uint64_t i = near_idx[k];
+      std::memcpy(h + 3 * k, pos + 3 * i, sizeof(float) * 3);
+      h[3 * n_near + k] = mass[i];
+      h[4 * n_near + k] = temperature[i];
+      ha[k] = active ? active[i] : uint8_t(1);
+    }
+    std::memcpy(h + 5 * n_near, coarse_temperature, sizeof(float) * cells);
+    float* d = static_cast<float*>(ctx->dstage);
+    uint8_t* da = reinterpret_cast<uint8_t*>(d + 5 * n_near + cells);
+    e = cudaMemcpyAsync(d, h, b_f + n_near, cudaMemcpyHostToDevice, 0);
+    if (e == cudaSuccess)
+      e = lw->coarse_field(d, d + 3 * n_near, d + 4 * n_near, da, nullptr, n_near, d + 5 * n_near, coarse_n, coarse_dx,
+                           coarse_origin, dt, 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(coarse_temperature, d + 5 * n_near, sizeof(float) * cells, cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  }
+  if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("coarse_field_update: ") + cudaGetErrorString(e));
   return AE_MPM_OK;
 }
 

@@ -296,6 +296,46 @@ int ae_mpm_radix_sort_keys_noalloc(ae_mpm_ctx* ctx, const uint32_t* keys_dev, ui
                                    uint32_t* sorted_keys_dev, uint32_t* perm_dev, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * The engine tick's particle passes around the substep (ae_engine/src/managers/simulation.rs,
+ * SimulationManager::update_fields_and_particles).  Arrays are MpssBuffer's: pos and vel are
+ * count x 3 floats, temperature and mass count floats, active count bytes (0/1; NULL = all
+ * active).  Index lists are usize (uint64).  The pointers of one call are either all host memory
+ * (staged through the context) or all device memory (used in place, no copies); which one is
+ * decided from `pos`.  Results equal the reference's f32 arithmetic bit for bit (the order of the
+ * near list aside, below).
+ * ------------------------------------------------------------------------------------------- */
+
+/* LOD classification, simulation.rs:495-532 (the reclassify branch; its Vec<(usize, f32)> /
+ * Vec<usize> lists become near_out / mid_out / far_out, each with room for count entries).
+ * near: active particles with |pos - player|^2 < near_dist^2, capped to the max_near closest, in
+ * ascending index order (the reference's select_nth_unstable_by leaves their order unspecified; on
+ * equal distances at the cap the lower index stays near).  mid: |pos - player|^2 < mid_dist^2, in
+ * ascending index order, followed by the near particles over the cap in ascending index order.
+ * far: the rest, ascending. */
+int ae_mpm_lod_classify(ae_mpm_ctx* ctx, const float* pos, const uint8_t* active, uint64_t count,
+                        const float player[3], float near_dist, float mid_dist, uint64_t max_near,
+                        uint64_t* near_out, uint64_t* n_near, uint64_t* mid_out, uint64_t* n_mid,
+                        uint64_t* far_out, uint64_t* n_far);
+
+/* Far-field update, simulation.rs:612-679: for each far particle v.y -= 9.81 far_dt,
+ * pos.y += v.y far_dt, and its temperature relaxes (rate 0.02 far_dt) toward the nearest cell
+ * ((pos - origin) / dx truncated toward zero) of the coarse_n^3 coarse temperature field (x
+ * fastest) when that cell exists.  Host indices are checked against count (AE_MPM_EINVAL). */
+int ae_mpm_far_field_update(ae_mpm_ctx* ctx, float* pos, float* vel, float* temperature, uint64_t count,
+                            const uint64_t* far_idx, uint64_t n_far, const float* coarse_temperature,
+                            uint32_t coarse_n, float coarse_dx, const float coarse_origin[3], float far_dt);
+
+/* Coarse temperature field update, SimulationManager::update_coarse_field (simulation.rs:877-966):
+ * mass-weighted temperature of the active near particles per cell, relaxation of the field toward
+ * it (rate min(0.1 dt, 1)), then one 6-neighbour FTCS diffusion step (coefficient
+ * min(10 dt / dx^2, 0.16)).  coarse_temperature (coarse_n^3 floats) is updated in place.  Host
+ * indices are checked against count (AE_MPM_EINVAL). */
+int ae_mpm_coarse_field_update(ae_mpm_ctx* ctx, const float* pos, const float* mass, const float* temperature,
+                               const uint8_t* active, uint64_t count, const uint64_t* near_idx, uint64_t n_near,
+                               float* coarse_temperature, uint32_t coarse_n, float coarse_dx,
+                               const float coarse_origin[3], float dt);
+
+/* ---------------------------------------------------------------------------------------------
  * Autotuner: times the P2G variants, block sizes and sort intervals on a world and writes the
  * fastest choice back into the world's options.  Choices are cached per workload signature.
  * ------------------------------------------------------------------------------------------- */

@@ -60,6 +60,11 @@ def load():
     lib.oracle_mpm_step_velocity_only_parallel.argtypes = [
         C.POINTER(M.ParticlesView), C.c_uint64, C.POINTER(M.Grid), C.POINTER(M.Config), f,
         C.POINTER(C.c_uint64), C.c_uint64, C.c_int32]
+    V = C.c_void_p
+    lib.oracle_lod_classify.argtypes = [V, V, C.c_uint64, V, f, f, C.c_uint64, V, C.POINTER(C.c_uint64), V,
+                                        C.POINTER(C.c_uint64), V, C.POINTER(C.c_uint64)]
+    lib.oracle_far_field_update.argtypes = [V, V, V, V, C.c_uint64, V, C.c_uint64, f, V, f]
+    lib.oracle_coarse_field_update.argtypes = [V, V, V, V, V, C.c_uint64, V, C.c_uint64, f, V, f]
     _lib = lib
     return lib
 
@@ -168,3 +173,41 @@ def svd3(F, f64: bool = False, allow_fallback: bool = True, lo: float = 1 - 2.5e
     U, s, V = np.zeros(9, np.float32), np.zeros(3, np.float32), np.zeros(9, np.float32)
     fb = load().oracle_svd3_f32(_fp(F), _fp(U), _fp(s), _fp(V), 1 if allow_fallback else 0, lo, hi)
     return U.reshape(3, 3), s, V.reshape(3, 3), bool(fb)
+
+
+# ---------------------------------------------------------------- engine tick passes (simulation.rs)
+def lod_classify(pos, active, player, near_dist, mid_dist, max_near):
+    """simulation.rs:495-532: (near, mid, far) index arrays; near in the order select_nth leaves it."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    n = pos.shape[0]
+    act = None if active is None else np.ascontiguousarray(active, np.uint8)
+    outs = [np.empty(max(n, 1), np.uint32) for _ in range(3)]
+    cnt = [C.c_uint64(0) for _ in range(3)]
+    pl = np.ascontiguousarray(player, np.float32)
+    load().oracle_lod_classify(pos.ctypes.data, None if act is None else act.ctypes.data, n, pl.ctypes.data,
+                               near_dist, mid_dist, max_near, outs[0].ctypes.data, C.byref(cnt[0]),
+                               outs[1].ctypes.data, C.byref(cnt[1]), outs[2].ctypes.data, C.byref(cnt[2]))
+    return tuple(o[:c.value].astype(np.uint64) for o, c in zip(outs, cnt))
+
+
+def far_field_update(pos, vel, temperature, far_idx, coarse, coarse_dx, origin, far_dt):
+    """simulation.rs:612-679, in place on float32 arrays."""
+    idx = np.ascontiguousarray(far_idx, np.uint32)
+    coarse = np.ascontiguousarray(coarse, np.float32)
+    cn = int(round(coarse.size ** (1.0 / 3.0)))
+    o = np.ascontiguousarray(origin, np.float32)
+    load().oracle_far_field_update(pos.ctypes.data, vel.ctypes.data, temperature.ctypes.data, idx.ctypes.data,
+                                   idx.size, coarse.ctypes.data, cn, coarse_dx, o.ctypes.data, far_dt)
+
+
+def coarse_field_update(pos, mass, temperature, active, near_idx, coarse, coarse_dx, origin, dt):
+    """simulation.rs:877-966, coarse (float32, n^3) in place."""
+    idx = np.ascontiguousarray(near_idx, np.uint32)
+    cn = int(round(coarse.size ** (1.0 / 3.0)))
+    o = np.ascontiguousarray(origin, np.float32)
+    act = None if active is None else np.ascontiguousarray(active, np.uint8)
+    load().oracle_coarse_field_update(np.ascontiguousarray(pos, np.float32).ctypes.data,
+                                      np.ascontiguousarray(mass, np.float32).ctypes.data,
+                                      np.ascontiguousarray(temperature, np.float32).ctypes.data,
+                                      None if act is None else act.ctypes.data, idx.ctypes.data, idx.size,
+                                      coarse.ctypes.data, cn, coarse_dx, o.ctypes.data, dt)
