@@ -5,13 +5,14 @@
 //
 //   classify      stable 3-way partition of the particles by squared distance to the player
 //                 (count per 2048-particle tile, scan of the tile counts, scatter in index order).
-//                 When more than max_near fall within near_dist, the near candidates' squared
-//                 distances (non-negative floats, so their bit patterns order like the values) are
-//                 radix-sorted, the first max_near are flagged, and a second partition splits the
-//                 candidates into the kept near list and the tail appended to the mid list.
+//                 When more than max_near fall within near_dist, a one-block radix select over
+//                 the near candidates' squared distances (non-negative floats, so their bit patterns
+//                 order like the values) flags the max_near closest, and a second partition splits
+//                 the candidates into the kept near list and the tail appended to the mid list.
 //   far_field     one thread per far particle: gravity on y, position, nearest-cell sample.
 //   coarse_field  the near particles' cells are radix-sorted (stable, so each cell keeps the
-//                 reference's index order) and each cell's run is summed sequentially, which
+//                 reference's index order), each cell's run is located, and one thread per cell
+//                 sums its run sequentially, which
 //                 reproduces the reference's serial accumulation exactly; then relaxation and one
 //                 FTCS step, one thread per cell.
 #include "ae_mpm_lod.cuh"
@@ -183,9 +184,75 @@ __global__ void __launch_bounds__(kPT) part_scatter(Cls cls, uint64_t n, const u
   }
 }
 
-__global__ void mark_keep(const uint32_t* perm, uint64_t n_keep, uint8_t* keep) {
-  for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < n_keep; k += uint64_t(gridDim.x) * blockDim.x)
-    keep[perm[k]] = 1;
+// One block: flags the k smallest of n keys (k >= 1, k < n), equal keys by position.  Four 8-bit
+// radix-select passes find the k-th smallest key T and how many of the keys equal to T are kept;
+// the keys below T and the first of those equal to T (a block-wide scan of per-thread counts over
+// contiguous chunks gives their positional ranks) are flagged.
+constexpr uint32_t kSelectSmemKeys = 40960;  // 160 KB: candidates up to this count are read once
+__global__ void __launch_bounds__(1024) select_keep(const uint32_t* gkeys, uint32_t n, uint32_t k, uint8_t* keep) {
+  extern __shared__ uint32_t skeys[];  // n keys when n <= kSelectSmemKeys (dynamic size 0 otherwise)
+  __shared__ uint32_t hist[256];
+  __shared__ uint32_t s_prefix, s_mask, s_rem;
+  __shared__ uint32_t wsum[32];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const bool cached = n <= kSelectSmemKeys;
+  if (cached)
+    for (uint32_t i = tid; i < n; i += 1024) skeys[i] = gkeys[i];
+  const uint32_t* keys = cached ? skeys : gkeys;
+  if (tid == 0) {
+    s_prefix = 0;
+    s_mask = 0;
+    s_rem = k;
+  }
+  __syncthreads();
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    if (tid < 256) hist[tid] = 0;
+    __syncthreads();
+    const uint32_t prefix = s_prefix, mask = s_mask;
+    for (uint32_t i = tid; i < n; i += 1024) {
+      const uint32_t key = keys[i];
+      if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (w == 0) {  // the digit whose bucket holds the s_rem-th smallest remaining key
+      uint32_t c = 0;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) c += hist[8 * lane + b];
+      const uint32_t incl = warp_scan_incl(c, lane), rem = s_rem;
+      const uint32_t hit = __ballot_sync(0xffffffffu, incl >= rem);
+      if (lane == __ffs(hit) - 1) {
+        uint32_t cum = incl - c;
+        int d = 8 * lane;
+        for (int b = 0; b < 8; ++b, ++d) {
+          if (cum + hist[d] >= rem) break;
+          cum += hist[d];
+        }
+        s_prefix = prefix | (uint32_t(d) << shift);
+        s_mask = mask | (255u << shift);
+        s_rem = rem - cum;
+      }
+    }
+    __syncthreads();
+  }
+  const uint32_t T = s_prefix, rem = s_rem;
+  const uint32_t chunk = (n + 1023) / 1024, c0 = min(n, tid * chunk), c1 = min(n, c0 + chunk);
+  uint32_t eq = 0;
+  for (uint32_t i = c0; i < c1; ++i) eq += keys[i] == T;
+  const uint32_t incl = warp_scan_incl(eq, lane);
+  if (lane == 31) wsum[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    const uint32_t v = wsum[lane];
+    wsum[lane] = warp_scan_incl(v, lane) - v;
+  }
+  __syncthreads();
+  uint32_t before = wsum[w] + incl - eq;
+  for (uint32_t i = c0; i < c1; ++i) {
+    const uint32_t key = keys[i];
+    bool kp = key < T;
+    if (key == T) kp = before++ < rem;
+    keep[i] = kp ? 1 : 0;
+  }
 }
 
 // simulation.rs:626-650 per far particle
@@ -237,19 +304,44 @@ __global__ void coarse_gather(const float* mass, const float* temp, const uint64
   }
 }
 
-// the thread at the head of each cell's run sums it in order, as the reference's serial loop does
-__global__ void coarse_sums(const uint32_t* skeys, const float* tm, const float* m, uint64_t n, uint32_t dead,
-                            float* cell_tm, float* cell_m) {
+// each cell's run [start, end) in the sorted order (cells without particles keep start == end == 0)
+__global__ void coarse_runs(const uint32_t* skeys, uint64_t n, uint32_t dead, uint32_t* run_start, uint32_t* run_end) {
   for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < n; k += uint64_t(gridDim.x) * blockDim.x) {
     const uint32_t key = skeys[k];
-    if (key == dead || (k > 0 && skeys[k - 1] == key)) continue;
+    if (key == dead) continue;
+    if (k == 0 || skeys[k - 1] != key) run_start[key] = uint32_t(k);
+    if (k + 1 == n || skeys[k + 1] != key) run_end[key] = uint32_t(k + 1);
+  }
+}
+
+// One warp per cell: the warp stages its cell's run in shared memory 256 entries at a time
+// (coalesced loads) and lane 0 adds them in order, as the reference's serial loop does.
+constexpr int kSumBatch = 256;
+__global__ void __launch_bounds__(256) coarse_sums(const uint32_t* run_start, const uint32_t* run_end, const float* tm,
+                                                   const float* m, uint64_t cells, float* cell_tm, float* cell_m) {
+  __shared__ float st[8][2][kSumBatch];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint64_t c = blockIdx.x * 8ull + w; c < cells; c += uint64_t(gridDim.x) * 8) {
+    const uint32_t s0 = run_start[c], e0 = run_end[c];
     float a = 0.0f, b = 0.0f;
-    for (uint64_t j = k; j < n && skeys[j] == key; ++j) {
-      a = __fadd_rn(a, tm[j]);
-      b = __fadd_rn(b, m[j]);
+    for (uint32_t base = s0; base < e0; base += kSumBatch) {
+      const uint32_t cnt = min(uint32_t(kSumBatch), e0 - base);
+      for (uint32_t t = lane; t < cnt; t += 32) {
+        st[w][0][t] = tm[base + t];
+        st[w][1][t] = m[base + t];
+      }
+      __syncwarp();
+      if (lane == 0)
+        for (uint32_t t = 0; t < cnt; ++t) {
+          a = __fadd_rn(a, st[w][0][t]);
+          b = __fadd_rn(b, st[w][1][t]);
+        }
+      __syncwarp();
     }
-    cell_tm[key] = a;
-    cell_m[key] = b;
+    if (lane == 0) {
+      cell_tm[c] = a;
+      cell_m[c] = b;
+    }
   }
 }
 
@@ -305,7 +397,8 @@ int bits_for(uint64_t v) {  // bits needed to hold values 0..v
   } while (0)
 
 LodWork::~LodWork() {
-  void* ps[] = {tile_counts_, tile_offs_, totals_, near_tmp_, near_key_, keep_, tm_, m_, cell_a_, cell_b_, field_tmp_};
+  void* ps[] = {tile_counts_, tile_offs_, totals_, near_tmp_, near_key_, keep_, tm_, m_, cell_a_, cell_b_, field_tmp_,
+                run_start_, run_end_};
   for (void* p : ps)
     if (p) cudaFree(p);
   sort_scratch_free(sort_);
@@ -335,14 +428,17 @@ cudaError_t LodWork::grow(uint64_t count, uint64_t cells) {
     cap_ = cap;
   }
   if (cells > cells_cap_) {
-    void* ps[] = {cell_a_, cell_b_, field_tmp_};
+    void* ps[] = {cell_a_, cell_b_, field_tmp_, run_start_, run_end_};
     for (void* p : ps)
       if (p) cudaFree(p);
     cell_a_ = cell_b_ = field_tmp_ = nullptr;
+    run_start_ = run_end_ = nullptr;
     cells_cap_ = 0;
     LOD_TRY(cudaMalloc(&cell_a_, sizeof(float) * cells));
     LOD_TRY(cudaMalloc(&cell_b_, sizeof(float) * cells));
     LOD_TRY(cudaMalloc(&field_tmp_, sizeof(float) * cells));
+    LOD_TRY(cudaMalloc(&run_start_, sizeof(uint32_t) * cells));
+    LOD_TRY(cudaMalloc(&run_end_, sizeof(uint32_t) * cells));
     cells_cap_ = cells;
   }
   return cudaSuccess;
@@ -374,10 +470,17 @@ cudaError_t LodWork::classify(const float* pos, const uint8_t* active, uint64_t 
     return cudaSuccess;
   }
   // cap (simulation.rs:519-530): the max_near smallest squared distances stay near, ties by index
-  const uint32_t *sorted = nullptr, *perm = nullptr;
-  radix_sort_pairs(near_key_, n_near, 31, sort_, s, &sorted, &perm);
-  LOD_TRY(cudaMemsetAsync(keep_, 0, n_near, s));
-  if (max_near) mark_keep<<<grid_for(max_near, 256), 256, 0, s>>>(perm, max_near, keep_);
+  if (max_near) {
+    const size_t sm = n_near <= kSelectSmemKeys ? sizeof(uint32_t) * n_near : 0;
+    if (!select_smem_set_) {
+      LOD_TRY(cudaFuncSetAttribute(select_keep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(sizeof(uint32_t) * kSelectSmemKeys)));
+      select_smem_set_ = true;
+    }
+    select_keep<<<1, 1024, sm, s>>>(near_key_, uint32_t(n_near), uint32_t(max_near), keep_);
+  }
+  else
+    LOD_TRY(cudaMemsetAsync(keep_, 0, n_near, s));
   const uint32_t tiles2 = uint32_t((n_near + kPTile - 1) / kPTile);
   const KeepClass kc{near_tmp_, keep_};
   part_count<KeepClass><<<tiles2, kPT, 0, s>>>(kc, n_near, tile_counts_, tiles2);
@@ -406,8 +509,10 @@ cudaError_t LodWork::coarse_field(const float* pos, const float* mass, const flo
   const uint64_t cells = uint64_t(cn) * cn * cn;
   if (cells == 0) return cudaSuccess;
   LOD_TRY(grow(std::max<uint64_t>(n, 1), cells));
-  LOD_TRY(cudaMemsetAsync(cell_a_, 0, sizeof(float) * cells, s));
-  LOD_TRY(cudaMemsetAsync(cell_b_, 0, sizeof(float) * cells, s));
+  if (n == 0) {  // no particles: the injection adds nothing
+    LOD_TRY(cudaMemsetAsync(cell_a_, 0, sizeof(float) * cells, s));
+    LOD_TRY(cudaMemsetAsync(cell_b_, 0, sizeof(float) * cells, s));
+  }
   if (n > 0) {
     const uint32_t dead = uint32_t(cells);
     const float inv_dx = 1.0f / cdx;
@@ -416,7 +521,11 @@ cudaError_t LodWork::coarse_field(const float* pos, const float* mass, const flo
     const uint32_t *sorted = nullptr, *perm = nullptr;
     radix_sort_pairs(near_key_, n, bits_for(cells), sort_, s, &sorted, &perm);
     coarse_gather<<<grid_for(n, 256), 256, 0, s>>>(mass, temp, near_idx, perm, n, tm_, m_);
-    coarse_sums<<<grid_for(n, 256), 256, 0, s>>>(sorted, tm_, m_, n, dead, cell_a_, cell_b_);
+    LOD_TRY(cudaMemsetAsync(run_start_, 0, sizeof(uint32_t) * cells, s));
+    LOD_TRY(cudaMemsetAsync(run_end_, 0, sizeof(uint32_t) * cells, s));
+    coarse_runs<<<grid_for(n, 256), 256, 0, s>>>(sorted, n, dead, run_start_, run_end_);
+    coarse_sums<<<unsigned(std::min<uint64_t>((cells + 7) / 8, 148 * 16)), 256, 0, s>>>(run_start_, run_end_, tm_, m_,
+                                                                                      cells, cell_a_, cell_b_);
   }
   const float inject_rate = 0.1f;
   const float blend = std::fmin(inject_rate * dt, 1.0f);

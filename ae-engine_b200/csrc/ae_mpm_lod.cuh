@@ -39,6 +39,7 @@ class LodWork {
  private:
   cudaError_t grow(uint64_t count, uint64_t cells);
   uint64_t cap_ = 0, cells_cap_ = 0;
+  bool select_smem_set_ = false;
   uint32_t* tile_counts_ = nullptr;  // [3][tiles]
   uint32_t* tile_offs_ = nullptr;    // [3][tiles]
   uint32_t* totals_ = nullptr;       // [4]
@@ -50,6 +51,8 @@ class LodWork {
   float* cell_a_ = nullptr;          // [cells] sums of temperature x mass
   float* cell_b_ = nullptr;          // [cells] sums of mass
   float* field_tmp_ = nullptr;       // [cells]
+  uint32_t* run_start_ = nullptr;    // [cells] each cell's run in the cell-sorted near list
+  uint32_t* run_end_ = nullptr;      // [cells]
   SortScratch sort_;
 };
 

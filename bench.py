@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="snow", choices=["snow", "jelly", "dam", "batched", "served"])
+    ap.add_argument("--workload", default="snow", choices=["snow", "jelly", "dam", "batched", "served", "tick"])
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--e2e-substeps", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -229,6 +229,8 @@ def cpu_rate(scene, p, substeps: int, threads: int) -> tuple[float, float]:
 
 def run_reference(args, rank, pg):
     """CPU restatement of the reference substep on this host's cores, same workload and metric."""
+    if args.workload == "tick":
+        return run_tick(args, rank, 0, 1, pg, reference=True)
     if rank != 0:
         return
     scenes, parts, cfg = workload(args.workload, 0, args.scenes)
@@ -259,11 +261,171 @@ def run_reference(args, rank, pg):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------------------
+# "tick": the engine's particle passes around the substep (simulation.rs:495-532, 612-679,
+# 877-966) on one frame that reclassifies: LOD classification, far-field update and coarse
+# temperature field, over a 1M-particle MpssBuffer.  Synthetic: a 1.6 km cube around the player
+# with 3% of the particles within 40 m (so the 10 000 near cap binds), 95% active.
+# ---------------------------------------------------------------------------------------------
+TICK_N = 1 << 20
+TICK = dict(near=50.0, mid=200.0, max_near=10000, coarse_n=16, coarse_dx=50.0, far_dt=1.0)
+
+
+def tick_population(n, seed):
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(-800, 800, (n, 3))
+    k = n * 3 // 100
+    pos[:k] = rng.uniform(-40, 40, (k, 3))
+    pos = pos[rng.permutation(n)].astype(np.float32)
+    return {"pos": pos, "vel": rng.normal(0, 3, (n, 3)).astype(np.float32),
+            "temp": rng.uniform(250, 600, n).astype(np.float32), "mass": rng.uniform(0.5, 2, n).astype(np.float32),
+            "active": (rng.uniform(size=n) > 0.05).astype(np.uint8)}
+
+
+def tick_cfg(n):
+    return {"workload": "engine tick around the substep: LOD reclassify + far-field update + coarse field, "
+                        "%d particles, near cap %d, coarse field %d^3" % (n, TICK["max_near"], TICK["coarse_n"]),
+            "particles": n, "l2": "L2 flushed between ticks (256 MB write, outside the timed events): the tick's "
+                                  "33 B/particle would otherwise stay L2-resident"}
+
+
+def tick_oracle(d, player, origin):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    near, mid, far = O.lod_classify(d["pos"], d["active"], player, TICK["near"], TICK["mid"], TICK["max_near"])
+    O.far_field_update(d["pos"], d["vel"], d["temp"], far, d["coarse"], TICK["coarse_dx"], origin, TICK["far_dt"])
+    O.coarse_field_update(d["pos"], d["mass"], d["temp"], d["active"], np.sort(near), d["coarse"], TICK["coarse_dx"],
+                          origin, TICK["far_dt"])
+
+
+def run_tick(args, rank, local, world_size, pg, reference=False):
+    import ctypes as C
+
+    n = TICK_N
+    d = tick_population(n, 0xAE05 + 1000 * rank)
+    player = np.zeros(3, np.float32)
+    origin = (player - np.float32(TICK["coarse_n"] * TICK["coarse_dx"] / 2)).astype(np.float32)
+    d["coarse"] = np.full(TICK["coarse_n"] ** 3, 288.15, np.float32)
+    cfg = tick_cfg(n)
+    metric, unit = "engine-tick particles/s", "particles/s"
+    if reference:  # the CPU restatement on this host (single thread, as the reference's serial passes)
+        if rank != 0:
+            return
+        for _ in range(max(1, args.warmup)):
+            tick_oracle({k: v.copy() for k, v in d.items()}, player, origin)
+        steps = max(1, min(args.steps, 20))
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            tick_oracle(d, player, origin)
+        dt = time.perf_counter() - t0
+        value = n * steps / dt
+        print(json.dumps({"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
+                          "steps": steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / steps,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                          "data": "synthetic (seeded numpy)", "config": cfg,
+                          "cpu_baseline": {"value": value, "unit": unit, "cores": 1, "kind": "port",
+                                           "sample": "the whole %d-particle tick" % n},
+                          "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+    import torch
+
+    import ae_mpm as M
+
+    ctx = M.Context(local)
+    lib, h = ctx.lib, ctx.h
+    dev = {k: torch.from_numpy(v.copy()).cuda(local) for k, v in d.items()}
+    outs = [torch.empty(n, dtype=torch.int64, device="cuda:%d" % local) for _ in range(3)]
+    cnt = [C.c_uint64(0) for _ in range(3)]
+    pl, og = player.copy(), origin.copy()
+
+    def tick_device():
+        ctx.check(lib.ae_mpm_lod_classify(h, dev["pos"].data_ptr(), dev["active"].data_ptr(), n, pl.ctypes.data,
+                                          TICK["near"], TICK["mid"], TICK["max_near"], outs[0].data_ptr(),
+                                          C.byref(cnt[0]), outs[1].data_ptr(), C.byref(cnt[1]), outs[2].data_ptr(),
+                                          C.byref(cnt[2])))
+        ctx.check(lib.ae_mpm_far_field_update(h, dev["pos"].data_ptr(), dev["vel"].data_ptr(), dev["temp"].data_ptr(),
+                                              n, outs[2].data_ptr(), cnt[2].value, dev["coarse"].data_ptr(),
+                                              TICK["coarse_n"], TICK["coarse_dx"], og.ctypes.data, TICK["far_dt"]))
+        ctx.check(lib.ae_mpm_coarse_field_update(h, dev["pos"].data_ptr(), dev["mass"].data_ptr(),
+                                                 dev["temp"].data_ptr(), dev["active"].data_ptr(), n,
+                                                 outs[0].data_ptr(), cnt[0].value, dev["coarse"].data_ptr(),
+                                                 TICK["coarse_n"], TICK["coarse_dx"], og.ctypes.data, TICK["far_dt"]))
+
+    for _ in range(max(args.warmup, 3)):
+        tick_device()
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda:%d" % local)  # 256 MB > L2
+    clocks = Clocks(local)
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0.record()
+        tick_device()
+        e1.record()
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+    clk = clocks.stop()
+    ms = max_over_ranks(pg, ms)
+    value = n * world_size * args.steps / (ms / 1e3)
+    n_near, n_far = cnt[0].value, cnt[2].value
+    capped = n_near >= TICK["max_near"]
+    # kernels per tick: classify 3 (7 with the cap: radix select, second partition), far 1, coarse 12
+    # (cell keys, 2-pass sort, gather, runs, sums, relaxation, diffusion)
+    launches = args.steps * ((7 if capped else 3) + 1 + 12)
+    # algorithmic bytes per tick: classify reads pos + active twice and writes one 8-byte index per
+    # particle; far: index 8 + pos 12 read, pos.y, vel.y, temperature read and written; coarse: near
+    # index 8, pos 12, mass 4, temperature 4, active 1
+    alg = 34 * n + 40 * n_far + 29 * n_near
+    achieved = alg / (ms / args.steps * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    # end to end: the same tick through the drop-in call on host (MpssBuffer) arrays
+    hd = {k: v.copy() for k, v in d.items()}
+    e2e_steps = max(1, min(args.steps, 20))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        near, mid, far = ctx.lod_classify(hd["pos"], hd["active"], player, TICK["near"], TICK["mid"], TICK["max_near"])
+        ctx.far_field_update(hd["pos"], hd["vel"], hd["temp"], far, hd["coarse"], TICK["coarse_dx"], origin,
+                             TICK["far_dt"])
+        ctx.coarse_field_update(hd["pos"], hd["mass"], hd["temp"], hd["active"], near, hd["coarse"], TICK["coarse_dx"],
+                                origin, TICK["far_dt"])
+    e2e_dt = time.perf_counter() - t0
+    h2d = 13 * n + 28 * n_far + (29 - 8) * n_near + 4 * TICK["coarse_n"] ** 3 * 2
+    d2h = 8 * n + 28 * n_far + 4 * TICK["coarse_n"] ** 3
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        t0 = time.perf_counter()
+        tick_oracle({k: v.copy() for k, v in d.items()}, player, origin)
+        cdt = time.perf_counter() - t0
+        cpu = {"value": n / cdt, "unit": unit, "cores": 1, "kind": "port", "sample": "one whole %d-particle tick" % n}
+    if rank == 0:
+        print(json.dumps({
+            "metric": metric, "value": value, "unit": unit, "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy)",
+            "config": dict(cfg, parallelism="replicas" if world_size > 1 else "single GPU"),
+            "roofline": {"bound": "hbm", "kernel": "tick (all passes)", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg},
+            "tick_counts": {"near": n_near, "mid": cnt[1].value, "far": n_far},
+            "e2e": {"value": n * e2e_steps / e2e_dt, "unit": unit, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": 1000.0 * e2e_dt / e2e_steps},
+            "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk}), flush=True)
+
+
 def run_ours(args, rank, local, world_size, pg):
     import torch
 
     import ae_mpm as M
 
+    if args.workload == "tick":
+        return run_tick(args, rank, local, world_size, pg)
     ctx = M.Context(local)
     scenes, parts, cfg = workload(args.workload, rank, args.scenes)
     if args.workload == "served":
