@@ -100,6 +100,51 @@ extern "C" {
         n_indices: u64,
     ) -> c_int;
     pub fn ae_mpm_grid_download(ctx: *mut ae_mpm_ctx, mass: *mut f32, vel: *mut f32, n_nodes: u64) -> c_int;
+    pub fn ae_mpm_lod_classify(
+        ctx: *mut ae_mpm_ctx,
+        pos: *const f32,
+        active: *const u8,
+        count: u64,
+        player: *const f32,
+        near_dist: f32,
+        mid_dist: f32,
+        max_near: u64,
+        near_out: *mut u64,
+        n_near: *mut u64,
+        mid_out: *mut u64,
+        n_mid: *mut u64,
+        far_out: *mut u64,
+        n_far: *mut u64,
+    ) -> c_int;
+    pub fn ae_mpm_far_field_update(
+        ctx: *mut ae_mpm_ctx,
+        pos: *mut f32,
+        vel: *mut f32,
+        temperature: *mut f32,
+        count: u64,
+        far_idx: *const u64,
+        n_far: u64,
+        coarse_temperature: *const f32,
+        coarse_n: u32,
+        coarse_dx: f32,
+        coarse_origin: *const f32,
+        far_dt: f32,
+    ) -> c_int;
+    pub fn ae_mpm_coarse_field_update(
+        ctx: *mut ae_mpm_ctx,
+        pos: *const f32,
+        mass: *const f32,
+        temperature: *const f32,
+        active: *const u8,
+        count: u64,
+        near_idx: *const u64,
+        n_near: u64,
+        coarse_temperature: *mut f32,
+        coarse_n: u32,
+        coarse_dx: f32,
+        coarse_origin: *const f32,
+        dt: f32,
+    ) -> c_int;
 }
 
 /// Library context on device 0, created on first use (one per process, like the rayon pool).
@@ -204,6 +249,108 @@ pub fn mpm_step_velocity_only_parallel(
 pub fn grid_download(mass: &mut [f32], vel: &mut [[f32; 3]]) -> Result<(), String> {
     assert_eq!(mass.len(), vel.len());
     check(unsafe { ae_mpm_grid_download(ctx(), mass.as_mut_ptr(), vel.as_mut_ptr() as *mut f32, mass.len() as u64) })
+}
+
+/// The reclassify branch of SimulationManager::update_fields_and_particles (simulation.rs:495-532):
+/// returns (near, mid, far).  `active` is MpssBuffer::active (Vec<bool>, one byte per entry).
+/// The near list comes back in ascending index order; the engine's Vec<(usize, f32)> keeps
+/// only the indices downstream.
+pub fn lod_classify(
+    pos: &[[f32; 3]],
+    active: &[bool],
+    player: [f32; 3],
+    near_dist: f32,
+    mid_dist: f32,
+    max_near: usize,
+) -> Result<(Vec<usize>, Vec<usize>, Vec<usize>), String> {
+    let n = pos.len();
+    assert_eq!(active.len(), n);
+    let (mut near, mut mid, mut far) = (vec![0u64; n], vec![0u64; n], vec![0u64; n]);
+    let (mut nn, mut nm, mut nf) = (0u64, 0u64, 0u64);
+    check(unsafe {
+        ae_mpm_lod_classify(
+            ctx(),
+            pos.as_ptr() as *const f32,
+            active.as_ptr() as *const u8,
+            n as u64,
+            player.as_ptr(),
+            near_dist,
+            mid_dist,
+            max_near as u64,
+            near.as_mut_ptr(),
+            &mut nn,
+            mid.as_mut_ptr(),
+            &mut nm,
+            far.as_mut_ptr(),
+            &mut nf,
+        )
+    })?;
+    let cut = |v: Vec<u64>, k: u64| v[..k as usize].iter().map(|&i| i as usize).collect::<Vec<usize>>();
+    Ok((cut(near, nn), cut(mid, nm), cut(far, nf)))
+}
+
+/// The far-field pass of update_fields_and_particles (simulation.rs:612-679) over `far_idx`.
+pub fn far_field_update(
+    pos: &mut [[f32; 3]],
+    vel: &mut [[f32; 3]],
+    temperature: &mut [f32],
+    far_idx: &[usize],
+    coarse_temperature: &[f32],
+    coarse_n: usize,
+    coarse_dx: f32,
+    coarse_origin: [f32; 3],
+    far_dt: f32,
+) -> Result<(), String> {
+    let idx: Vec<u64> = far_idx.iter().map(|&i| i as u64).collect();
+    check(unsafe {
+        ae_mpm_far_field_update(
+            ctx(),
+            pos.as_mut_ptr() as *mut f32,
+            vel.as_mut_ptr() as *mut f32,
+            temperature.as_mut_ptr(),
+            pos.len() as u64,
+            idx.as_ptr(),
+            idx.len() as u64,
+            coarse_temperature.as_ptr(),
+            coarse_n as u32,
+            coarse_dx,
+            coarse_origin.as_ptr(),
+            far_dt,
+        )
+    })
+}
+
+/// SimulationManager::update_coarse_field (simulation.rs:877-966) with the near indices.
+pub fn coarse_field_update(
+    pos: &[[f32; 3]],
+    mass: &[f32],
+    temperature: &[f32],
+    active: &[bool],
+    near_idx: &[usize],
+    coarse_temperature: &mut [f32],
+    coarse_n: usize,
+    coarse_dx: f32,
+    coarse_origin: [f32; 3],
+    dt: f32,
+) -> Result<(), String> {
+    let idx: Vec<u64> = near_idx.iter().map(|&i| i as u64).collect();
+    check(unsafe {
+        ae_mpm_coarse_field_update(
+            ctx(),
+            pos.as_ptr() as *const f32,
+            mass.as_ptr(),
+            temperature.as_ptr(),
+            active.as_ptr() as *const u8,
+            pos.len() as u64,
+            idx.as_ptr(),
+            idx.len() as u64,
+            coarse_temperature.as_mut_ptr(),
+            coarse_n as u32,
+            coarse_dx,
+            coarse_origin.as_ptr(),
+            dt,
+        )
+    })
 }
 
 #[allow(dead_code)]
