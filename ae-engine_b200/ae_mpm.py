@@ -127,6 +127,8 @@ SIGNATURES = {
                                           C.c_float]),
     "ae_mpm_coarse_field_update": (C.c_int, [_P, _P, _P, _P, _P, C.c_uint64, _P, C.c_uint64, _P, C.c_uint32,
                                              C.c_float, _P, C.c_float]),
+    "ae_mpm_mpss_housekeeping": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.c_uint64, _P, _P, C.c_float, C.c_float,
+                                           C.c_uint32, C.POINTER(C.c_uint32)]),
     "ae_mpm_world_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(TuneResult)]),
     "ae_mpm_server_create": (C.c_int, [_P, C.POINTER(ServerOpts), C.POINTER(_P)]),
     "ae_mpm_server_submit": (C.c_int, [_P, C.POINTER(SceneDesc), C.POINTER(ParticlesView), C.c_uint64, C.c_uint32,
@@ -338,6 +340,22 @@ class Context:
                                                        None if act is None else act.ctypes.data, pos.shape[0],
                                                        idx.ctypes.data, idx.size, coarse.ctypes.data, cn, coarse_dx,
                                                        o.ctypes.data, dt))
+
+    def mpss_housekeeping(self, pos, vel, temperature, phase, material_idx, active, bounds_min, bounds_max,
+                          min_temp, max_temp, passes=7):
+        """ae_engine/src/lib.rs:347-358 in place on pos, vel (float32 (n,3)), temperature (float32),
+        phase (uint8); returns the number of phase transitions."""
+        mat = np.ascontiguousarray(material_idx, np.uint16)
+        act = None if active is None else np.ascontiguousarray(active, np.uint8)
+        lo = np.ascontiguousarray(bounds_min, np.float32)
+        hi = np.ascontiguousarray(bounds_max, np.float32)
+        tr = C.c_uint32(0)
+        self.check(self.lib.ae_mpm_mpss_housekeeping(self.h, pos.ctypes.data, vel.ctypes.data, temperature.ctypes.data,
+                                                     phase.ctypes.data, mat.ctypes.data,
+                                                     None if act is None else act.ctypes.data, pos.shape[0],
+                                                     lo.ctypes.data, hi.ctypes.data, min_temp, max_temp, passes,
+                                                     C.byref(tr)))
+        return tr.value
 
     def radix_sort(self, keys: np.ndarray, key_bits: int):
         keys = np.ascontiguousarray(keys, np.uint32)

@@ -600,6 +600,60 @@ int ae_mpm_coarse_field_update(ae_mpm_ctx* ctx, const float* pos, const float* m
   return AE_MPM_OK;
 }
 
+int ae_mpm_mpss_housekeeping(ae_mpm_ctx* ctx, float* pos, float* vel, float* temperature, uint8_t* phase,
+                             const uint16_t* material_idx, const uint8_t* active, uint64_t count,
+                             const float bounds_min[3], const float bounds_max[3], float min_temp, float max_temp,
+                             uint32_t passes, uint32_t* transitions) {
+  if (!ctx) return AE_MPM_EINVAL;
+  if (!transitions || !bounds_min || !bounds_max || (passes & ~7u) ||
+      (count && (((passes & 1u) && (!pos || !vel)) || ((passes & 6u) && !temperature) ||
+                 ((passes & 4u) && (!phase || !material_idx)))))
+    return fail(ctx, AE_MPM_EINVAL, "mpss_housekeeping: null array for a selected pass, or unknown pass bits");
+  *transitions = 0;
+  if (count == 0 || passes == 0) return AE_MPM_OK;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  aemp::LodWork* lw = lod_work(ctx);
+  const bool b1 = passes & 1u, b2 = (passes & 6u) != 0, b4 = passes & 4u;
+  const void* probe = b1 ? static_cast<const void*>(pos) : static_cast<const void*>(temperature);
+  cudaError_t e;
+  if (is_device_ptr(probe)) {
+    e = lw->housekeeping(pos, vel, temperature, phase, material_idx, active, count, bounds_min, bounds_max, min_temp,
+                         max_temp, passes, transitions, 0);
+  } else {
+    // device copies of the arrays the selected passes use, 16-byte aligned regions
+    auto up16 = [](size_t b) { return (b + 15) & ~size_t(15); };
+    const size_t bp = b1 ? up16(12 * count) : 0, bt = b2 ? up16(4 * count) : 0, bph = b4 ? up16(count) : 0,
+                 bm = b4 ? up16(2 * count) : 0, ba = active ? up16(count) : 0;
+    rc = ensure_dstage(ctx, 2 * bp + bt + bph + bm + ba);
+    if (rc) return rc;
+    char* d = static_cast<char*>(ctx->dstage);
+    float* dpos = b1 ? reinterpret_cast<float*>(d) : nullptr;
+    float* dvel = b1 ? reinterpret_cast<float*>(d + bp) : nullptr;
+    float* dt = b2 ? reinterpret_cast<float*>(d + 2 * bp) : nullptr;
+    uint8_t* dph = b4 ? reinterpret_cast<uint8_t*>(d + 2 * bp + bt) : nullptr;
+    uint16_t* dm = b4 ? reinterpret_cast<uint16_t*>(d + 2 * bp + bt + bph) : nullptr;
+    uint8_t* da = active ? reinterpret_cast<uint8_t*>(d + 2 * bp + bt + bph + bm) : nullptr;
+    e = cudaSuccess;
+    if (b1) e = cudaMemcpyAsync(dpos, pos, 12 * count, cudaMemcpyHostToDevice, 0);
+    if (b1 && e == cudaSuccess) e = cudaMemcpyAsync(dvel, vel, 12 * count, cudaMemcpyHostToDevice, 0);
+    if (b2 && e == cudaSuccess) e = cudaMemcpyAsync(dt, temperature, 4 * count, cudaMemcpyHostToDevice, 0);
+    if (b4 && e == cudaSuccess) e = cudaMemcpyAsync(dph, phase, count, cudaMemcpyHostToDevice, 0);
+    if (b4 && e == cudaSuccess) e = cudaMemcpyAsync(dm, material_idx, 2 * count, cudaMemcpyHostToDevice, 0);
+    if (active && e == cudaSuccess) e = cudaMemcpyAsync(da, active, count, cudaMemcpyHostToDevice, 0);
+    if (e == cudaSuccess)
+      e = lw->housekeeping(dpos, dvel, dt, dph, dm, da, count, bounds_min, bounds_max, min_temp, max_temp, passes,
+                           transitions, 0);
+    if (b1 && e == cudaSuccess) e = cudaMemcpyAsync(pos, dpos, 12 * count, cudaMemcpyDeviceToHost, 0);
+    if (b1 && e == cudaSuccess) e = cudaMemcpyAsync(vel, dvel, 12 * count, cudaMemcpyDeviceToHost, 0);
+    if ((passes & 2u) && e == cudaSuccess) e = cudaMemcpyAsync(temperature, dt, 4 * count, cudaMemcpyDeviceToHost, 0);
+    if (b4 && e == cudaSuccess) e = cudaMemcpyAsync(phase, dph, count, cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  }
+  if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("mpss_housekeeping: ") + cudaGetErrorString(e));
+  return AE_MPM_OK;
+}
+
 // Autotuner: P2G variant x particles per block x sort interval, timed with CUDA events on the
 // world's stream from the same starting state (snapshot restored between trials).
 int ae_mpm_world_autotune(ae_mpm_world* world, uint32_t substeps_per_trial, ae_mpm_tune_result* out) {

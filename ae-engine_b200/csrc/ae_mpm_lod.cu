@@ -377,6 +377,79 @@ __global__ void coarse_diffuse(const float* f, uint32_t cn, float coef, float* o
   }
 }
 
+// MpssPhase (mpss.rs:67-75): Solid 0, Liquid 1, Gas 2, Plasma 3, Granular 4, Crystal 5, Amorphous 6.
+// One hop of apply_phase_transitions' table (mpss.rs:512-524): the arms in order, a failing guard
+// falling through to the next arm.
+__device__ __forceinline__ uint8_t phase_hop(uint16_t m, uint8_t cur, float t) {
+  if (m == 1 && cur == 0 && t >= 273.0f) return 1;
+  if (m == 1 && cur == 1 && t >= 373.0f) return 2;
+  if (m == 1 && cur == 2 && t < 373.0f) return 1;
+  if (m == 1 && cur == 1 && t < 273.0f) return 0;
+  if (m == 3 && cur == 0 && t >= 1811.0f) return 1;
+  if (m == 3 && cur == 1 && t >= 3134.0f) return 2;
+  if (m == 3 && cur == 2 && t < 3134.0f) return 1;
+  if (m == 3 && cur == 1 && t < 1811.0f) return 0;
+  if (m == 0 && cur == 0 && t >= 500.0f) return 2;
+  if (m == 2 && cur == 0 && t >= 1923.0f) return 2;
+  return cur;
+}
+
+// MpssBuffer housekeeping after the substep (ae_engine/src/lib.rs:347-358): per active particle,
+// reflecting world bounds (mpss.rs:449-476), temperature clamp (:479-497), phase transitions with
+// up to 3 hops (:500-548), in that order; passes selects them (1, 2, 4).  The loop bounds are
+// warp-uniform so the transition count is a warp ballot.
+__global__ void housekeeping_kernel(float* pos, float* vel, float* temp, uint8_t* phase, const uint16_t* mat,
+                                    const uint8_t* active, uint64_t n, float x0, float y0, float z0, float x1, float y1,
+                                    float z1, float tmin, float tmax, uint32_t passes, uint32_t* transitions) {
+  const float lo[3] = {x0, y0, z0}, hi[3] = {x1, y1, z1};
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t base = uint64_t(blockIdx.x) * blockDim.x; base < n; base += stride) {
+    const uint64_t i = base + threadIdx.x;
+    bool changed = false;
+    if (i < n && (!active || active[i])) {
+      if (passes & 1u) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const float p = pos[3 * i + d];
+          if (p < lo[d]) {
+            pos[3 * i + d] = lo[d];
+            const float v = vel[3 * i + d];
+            if (v < 0.0f) vel[3 * i + d] = __fmul_rn(-v, 0.5f);
+          } else if (p > hi[d]) {
+            pos[3 * i + d] = hi[d];
+            const float v = vel[3 * i + d];
+            if (v > 0.0f) vel[3 * i + d] = __fmul_rn(-v, 0.5f);
+          }
+        }
+      }
+      if (passes & 2u) {
+        const float t = temp[i];
+        if (t > tmax)
+          temp[i] = tmax;
+        else if (t < tmin)
+          temp[i] = tmin;
+      }
+      if (passes & 4u) {
+        const float t = temp[i];
+        const uint16_t m = mat[i];
+        const uint8_t cur = phase[i];
+        uint8_t next = cur;
+        for (int hop = 0; hop < 3; ++hop) {
+          const uint8_t h = phase_hop(m, next, t);
+          if (h == next) break;
+          next = h;
+        }
+        if (next != cur) {
+          phase[i] = next;
+          changed = true;
+        }
+      }
+    }
+    const uint32_t c = __popc(__ballot_sync(0xffffffffu, changed));
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(transitions, c);
+  }
+}
+
 inline unsigned grid_for(uint64_t n, int threads) {
   const uint64_t b = (n + threads - 1) / threads;
   return unsigned(std::max<uint64_t>(1, std::min<uint64_t>(b, 148ull * 16)));
@@ -492,6 +565,22 @@ cudaError_t LodWork::classify(const float* pos, const uint8_t* active, uint64_t 
   counts[1] = n_mid + (n_near - max_near);
   counts[2] = n_far;
   return cudaSuccess;
+}
+
+cudaError_t LodWork::housekeeping(float* pos, float* vel, float* temp, uint8_t* phase, const uint16_t* material,
+                                  const uint8_t* active, uint64_t n, const float bmin[3], const float bmax[3],
+                                  float min_temp, float max_temp, uint32_t passes, uint32_t* transitions,
+                                  cudaStream_t s) {
+  *transitions = 0;
+  if (n == 0) return cudaSuccess;
+  LOD_TRY(grow(1, 0));
+  LOD_TRY(cudaMemsetAsync(totals_ + 3, 0, sizeof(uint32_t), s));
+  housekeeping_kernel<<<grid_for(n, 256), 256, 0, s>>>(pos, vel, temp, phase, material, active, n, bmin[0], bmin[1],
+                                                      bmin[2], bmax[0], bmax[1], bmax[2], min_temp, max_temp, passes,
+                                                      totals_ + 3);
+  LOD_TRY(cudaGetLastError());
+  LOD_TRY(cudaMemcpyAsync(transitions, totals_ + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  return cudaStreamSynchronize(s);
 }
 
 cudaError_t LodWork::far_field(float* pos, float* vel, float* temp, const uint64_t* far_idx, uint64_t n,

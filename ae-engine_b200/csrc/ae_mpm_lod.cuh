@@ -30,6 +30,13 @@ class LodWork {
   cudaError_t far_field(float* pos, float* vel, float* temp, const uint64_t* far_idx, uint64_t n, const float* coarse,
                         uint32_t cn, float cdx, const float origin[3], float far_dt, cudaStream_t s);
 
+  // MpssBuffer housekeeping (ae_engine/src/lib.rs:347-358) over particles 0..n: passes 1 = world
+  // bounds (reflect, halve the velocity), 2 = temperature clamp, 4 = phase transitions.
+  // *transitions (host) = particles whose phase changed.
+  cudaError_t housekeeping(float* pos, float* vel, float* temp, uint8_t* phase, const uint16_t* material,
+                           const uint8_t* active, uint64_t n, const float bmin[3], const float bmax[3], float min_temp,
+                           float max_temp, uint32_t passes, uint32_t* transitions, cudaStream_t s);
+
   // coarse field (cn^3 floats, updated in place): mass-weighted temperature of the near particles
   // near_idx[0..n) (null: 0..n; inactive ones skipped), relaxation, one FTCS diffusion step.
   cudaError_t coarse_field(const float* pos, const float* mass, const float* temp, const uint8_t* active,
@@ -42,7 +49,7 @@ class LodWork {
   bool select_smem_set_ = false;
   uint32_t* tile_counts_ = nullptr;  // [3][tiles]
   uint32_t* tile_offs_ = nullptr;    // [3][tiles]
-  uint32_t* totals_ = nullptr;       // [4]
+  uint32_t* totals_ = nullptr;       // [4]: class totals, housekeeping transition count
   uint64_t* near_tmp_ = nullptr;     // [cap] near candidates (ascending index)
   uint32_t* near_key_ = nullptr;     // [cap] their squared distance, as bits; later cell keys
   uint8_t* keep_ = nullptr;          // [cap]

@@ -335,6 +335,22 @@ int ae_mpm_coarse_field_update(ae_mpm_ctx* ctx, const float* pos, const float* m
                                float* coarse_temperature, uint32_t coarse_n, float coarse_dx,
                                const float coarse_origin[3], float dt);
 
+/* MpssBuffer housekeeping after the substep, the three calls of ae_engine/src/lib.rs:347-358 in
+ * their order, over particles 0..count (active ones only):
+ *   passes & 1  MpssBuffer::apply_boundary_conditions_par (ae_particle/src/mpss.rs:449-476): a
+ *               coordinate outside [bounds_min, bounds_max] is clamped and its velocity component,
+ *               when it points outward, reversed and halved;
+ *   passes & 2  MpssBuffer::clamp_temperatures_par (mpss.rs:479-497) to [min_temp, max_temp];
+ *   passes & 4  MpssBuffer::apply_phase_transitions_par (mpss.rs:500-548): material 1 water, 3
+ *               iron, 0 wood, 2 concrete, up to 3 hops; phase holds MpssPhase values (Solid 0,
+ *               Liquid 1, Gas 2, ...) as bytes, material_idx MpssBuffer::material_idx.
+ * *transitions receives the number of particles whose phase changed (the u32 the reference
+ * returns).  pos/vel are count x 3 floats.  Host or device pointers, as above (decided by pos). */
+int ae_mpm_mpss_housekeeping(ae_mpm_ctx* ctx, float* pos, float* vel, float* temperature, uint8_t* phase,
+                             const uint16_t* material_idx, const uint8_t* active, uint64_t count,
+                             const float bounds_min[3], const float bounds_max[3], float min_temp, float max_temp,
+                             uint32_t passes, uint32_t* transitions);
+
 /* ---------------------------------------------------------------------------------------------
  * Autotuner: times the P2G variants, block sizes and sort intervals on a world and writes the
  * fastest choice back into the world's options.  Choices are cached per workload signature.

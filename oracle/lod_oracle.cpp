@@ -8,6 +8,8 @@
 //                                                          simulation.rs:612-679
 //   * coarse temperature field update (mass-weighted injection from the near particles,
 //     relaxation, one 6-neighbour FTCS diffusion step)       simulation.rs:877-966
+//   * MpssBuffer housekeeping after the substep (ae_engine/src/lib.rs:347-358): reflecting world
+//     bounds, temperature clamp, material phase transitions   ae_particle/src/mpss.rs:449-548
 // Only tests/ and bench.py's CPU baseline load it, as the checker; the library never does.
 //
 // Rounding follows Rust's f32 semantics: this file is built with -ffp-contract=off (Rust never
@@ -140,6 +142,70 @@ void oracle_coarse_field_update(const float* pos, const float* mass, const float
         }
       }
   std::copy(next.begin(), next.end(), coarse);
+}
+
+// MpssPhase (mpss.rs:67-75): Solid 0, Liquid 1, Gas 2, Plasma 3, Granular 4, Crystal 5, Amorphous 6.
+// One hop of the transition table of apply_phase_transitions (mpss.rs:401-416, 512-524): the arms
+// in order, a failing guard falling through to the next arm.
+static uint8_t phase_hop(uint16_t m, uint8_t cur, float t) {
+  if (m == 1 && cur == 0 && t >= 273.0f) return 1;
+  if (m == 1 && cur == 1 && t >= 373.0f) return 2;
+  if (m == 1 && cur == 2 && t < 373.0f) return 1;
+  if (m == 1 && cur == 1 && t < 273.0f) return 0;
+  if (m == 3 && cur == 0 && t >= 1811.0f) return 1;
+  if (m == 3 && cur == 1 && t >= 3134.0f) return 2;
+  if (m == 3 && cur == 2 && t < 3134.0f) return 1;
+  if (m == 3 && cur == 1 && t < 1811.0f) return 0;
+  if (m == 0 && cur == 0 && t >= 500.0f) return 2;
+  if (m == 2 && cur == 0 && t >= 1923.0f) return 2;
+  return cur;
+}
+
+// The three passes ae_engine/src/lib.rs:347-358 runs after update_fields_and_particles, as their
+// serial forms (mpss.rs:344-430; the _par forms do the same per particle).  passes: 1 boundary,
+// 2 temperature clamp, 4 phase transitions, applied in that order.  Returns the transition count.
+uint32_t oracle_mpss_housekeeping(float* pos, float* vel, float* temperature, uint8_t* phase, const uint16_t* material,
+                                  const uint8_t* active, uint64_t count, const float* bmin, const float* bmax,
+                                  float min_temp, float max_temp, uint32_t passes) {
+  if (passes & 1u)
+    for (uint64_t i = 0; i < count; ++i) {
+      if (active && !active[i]) continue;
+      for (int d = 0; d < 3; ++d) {
+        float& p = pos[3 * i + d];
+        float& v = vel[3 * i + d];
+        if (p < bmin[d]) {
+          p = bmin[d];
+          if (v < 0.0f) v = -v * 0.5f;
+        } else if (p > bmax[d]) {
+          p = bmax[d];
+          if (v > 0.0f) v = -v * 0.5f;
+        }
+      }
+    }
+  if (passes & 2u)
+    for (uint64_t i = 0; i < count; ++i) {
+      if (active && !active[i]) continue;
+      if (temperature[i] > max_temp)
+        temperature[i] = max_temp;
+      else if (temperature[i] < min_temp)
+        temperature[i] = min_temp;
+    }
+  uint32_t transitions = 0;
+  if (passes & 4u)
+    for (uint64_t i = 0; i < count; ++i) {
+      if (active && !active[i]) continue;
+      uint8_t cur = phase[i];
+      for (int hop = 0; hop < 3; ++hop) {
+        const uint8_t next = phase_hop(material[i], cur, temperature[i]);
+        if (next == cur) break;
+        cur = next;
+      }
+      if (cur != phase[i]) {
+        phase[i] = cur;
+        ++transitions;
+      }
+    }
+  return transitions;
 }
 
 }  // extern "C"

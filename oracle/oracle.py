@@ -65,6 +65,8 @@ def load():
                                         C.POINTER(C.c_uint64), V, C.POINTER(C.c_uint64)]
     lib.oracle_far_field_update.argtypes = [V, V, V, V, C.c_uint64, V, C.c_uint64, f, V, f]
     lib.oracle_coarse_field_update.argtypes = [V, V, V, V, V, C.c_uint64, V, C.c_uint64, f, V, f]
+    lib.oracle_mpss_housekeeping.restype = C.c_uint32
+    lib.oracle_mpss_housekeeping.argtypes = [V, V, V, V, V, V, C.c_uint64, V, V, f, f, C.c_uint32]
     _lib = lib
     return lib
 
@@ -211,3 +213,15 @@ def coarse_field_update(pos, mass, temperature, active, near_idx, coarse, coarse
                                       np.ascontiguousarray(temperature, np.float32).ctypes.data,
                                       None if act is None else act.ctypes.data, idx.ctypes.data, idx.size,
                                       coarse.ctypes.data, cn, coarse_dx, o.ctypes.data, dt)
+
+
+def mpss_housekeeping(pos, vel, temperature, phase, material_idx, active, bounds_min, bounds_max, min_temp, max_temp,
+                      passes=7):
+    """ae_engine/src/lib.rs:347-358 (mpss.rs serial forms), in place; returns the transition count."""
+    mat = np.ascontiguousarray(material_idx, np.uint16)
+    act = None if active is None else np.ascontiguousarray(active, np.uint8)
+    lo = np.ascontiguousarray(bounds_min, np.float32)
+    hi = np.ascontiguousarray(bounds_max, np.float32)
+    return load().oracle_mpss_housekeeping(pos.ctypes.data, vel.ctypes.data, temperature.ctypes.data,
+                                           phase.ctypes.data, mat.ctypes.data, None if act is None else act.ctypes.data,
+                                           pos.shape[0], lo.ctypes.data, hi.ctypes.data, min_temp, max_temp, passes)

@@ -179,3 +179,60 @@ def test_engine_tick_sequence_matches_oracle(ctx):
     O.coarse_field_update(r[0], mass, r[2], active, np.sort(rn), r[3], 50.0, origin, 1.0)
     for x, y in zip(g, r):
         assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+
+
+# ---------------------------------------------------------------- MpssBuffer housekeeping
+def housekeeping_case(n, seed):
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(-1200, 1200, (n, 3)).astype(f32)
+    vel = rng.normal(0, 10, (n, 3)).astype(f32)
+    temp = rng.uniform(-100, 9000, n).astype(f32)
+    temp[::53] = np.nan
+    temp[1::61] = np.inf
+    pos[2::71, 1] = np.nan
+    phase = rng.integers(0, 8, n).astype(np.uint8)
+    mat = rng.choice([0, 1, 2, 3, 3, 1, 5], n).astype(np.uint16)
+    active = (rng.uniform(size=n) > 0.1).astype(np.uint8)
+    return pos, vel, temp, phase, mat, active
+
+
+@pytest.mark.parametrize("n,passes", [(1, 7), (1000, 7), (1000003, 7), (200000, 1), (200000, 2), (200000, 4),
+                                      (200000, 5)])
+def test_housekeeping_matches_oracle_bitwise(ctx, n, passes):
+    lo, hi = np.array([-1000, -50, -1000], f32), np.array([1000, 900, 1000], f32)
+    a = housekeeping_case(n, n + passes)
+    b = tuple(x.copy() for x in a)
+    ca = ctx.mpss_housekeeping(a[0], a[1], a[2], a[3], a[4], a[5], lo, hi, 10.0, 8000.0, passes)
+    cb = O.mpss_housekeeping(b[0], b[1], b[2], b[3], b[4], b[5], lo, hi, 10.0, 8000.0, passes)
+    assert ca == cb
+    for x, y in zip(a[:4], b[:4]):
+        assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
+
+
+def test_housekeeping_reference_phase_cases_and_device_pointers(ctx):
+    import json
+    import os
+    torch = pytest.importorskip("torch")
+    cases = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "phase_cases.json")))
+    temps = np.array(sum((c["temps"] for c in cases), []), f32)
+    mats = np.array(sum(([c["material"]] * len(c["temps"]) for c in cases), []), np.uint16)
+    expected = sum((c["expected"] for c in cases), [])
+    n = temps.size
+    pos, vel = np.zeros((n, 3), f32), np.zeros((n, 3), f32)
+    phase = np.zeros(n, np.uint8)
+    ctx.mpss_housekeeping(pos, vel, temps.copy(), phase, mats, None, [-1e9] * 3, [1e9] * 3, 10.0, 8000.0, 4)
+    assert phase.tolist() == expected
+    # device pointers: the same pass in place on device arrays
+    a = housekeeping_case(300000, 77)
+    b = tuple(x.copy() for x in a)
+    d = [torch.from_numpy(x.copy()).cuda() for x in a]
+    lo, hi = np.array([-1000, -50, -1000], f32), np.array([1000, 900, 1000], f32)
+    tr = M.C.c_uint32(0)
+    ctx.check(ctx.lib.ae_mpm_mpss_housekeeping(ctx.h, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                               d[3].data_ptr(), d[4].data_ptr(), d[5].data_ptr(), a[0].shape[0],
+                                               lo.ctypes.data, hi.ctypes.data, 10.0, 8000.0, 7, M.C.byref(tr)))
+    torch.cuda.synchronize()
+    cb = O.mpss_housekeeping(b[0], b[1], b[2], b[3], b[4], b[5], lo, hi, 10.0, 8000.0, 7)
+    assert tr.value == cb
+    for x, y in zip(d[:4], b[:4]):
+        assert np.array_equal(x.cpu().numpy().view(np.uint8), y.view(np.uint8))

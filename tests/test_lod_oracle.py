@@ -128,3 +128,93 @@ def test_lod_oracle_partitions_by_distance_and_caps_near():
     # under the cap the near list keeps index order
     near2, _, _ = O.lod_classify(pos, active, player, 50.0, 200.0, 10 ** 9)
     assert np.array_equal(near2, within)
+
+
+# ---------------------------------------------------------------- MpssBuffer housekeeping
+import json  # noqa: E402
+import os  # noqa: E402
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "phase_cases.json")
+
+
+def test_phase_transitions_match_the_reference_scenario_cases():
+    # game/src/bin/scenario_test.rs:217-265, extracted by tests/golden/extract_phase_cases.py
+    cases = json.load(open(GOLDEN))
+    assert len(cases) == 3
+    for c in cases:
+        n = len(c["temps"])
+        pos = np.zeros((n, 3), f32)
+        vel = np.zeros((n, 3), f32)
+        temp = np.array(c["temps"], f32)
+        phase = np.full(n, c["start"], np.uint8)
+        mat = np.full(n, c["material"], np.uint16)
+        changed = O.mpss_housekeeping(pos, vel, temp, phase, mat, None, [-1e9] * 3, [1e9] * 3, 0.0, 1e9, passes=4)
+        assert phase.tolist() == c["expected"], c["name"]
+        assert changed == sum(e != c["start"] for e in c["expected"])
+
+
+def np_housekeeping(pos, vel, temp, phase, mat, active, lo, hi, tmin, tmax, passes):
+    n = pos.shape[0]
+    arms = [(1, 0, ">=", 273.0, 1), (1, 1, ">=", 373.0, 2), (1, 2, "<", 373.0, 1), (1, 1, "<", 273.0, 0),
+            (3, 0, ">=", 1811.0, 1), (3, 1, ">=", 3134.0, 2), (3, 2, "<", 3134.0, 1), (3, 1, "<", 1811.0, 0),
+            (0, 0, ">=", 500.0, 2), (2, 0, ">=", 1923.0, 2)]
+    changed = 0
+    for i in range(n):
+        if active is not None and not active[i]:
+            continue
+        if passes & 1:
+            for d in range(3):
+                if pos[i, d] < lo[d]:
+                    pos[i, d] = lo[d]
+                    if vel[i, d] < 0:
+                        vel[i, d] = f32(-vel[i, d] * f32(0.5))
+                elif pos[i, d] > hi[d]:
+                    pos[i, d] = hi[d]
+                    if vel[i, d] > 0:
+                        vel[i, d] = f32(-vel[i, d] * f32(0.5))
+        if passes & 2:
+            if temp[i] > tmax:
+                temp[i] = tmax
+            elif temp[i] < tmin:
+                temp[i] = tmin
+        if passes & 4:
+            cur = int(phase[i])
+            for _ in range(3):
+                nxt = cur
+                for m, p, op, th, to in arms:
+                    if mat[i] == m and cur == p and ((temp[i] >= th) if op == ">=" else (temp[i] < th)):
+                        nxt = to
+                        break
+                if nxt == cur:
+                    break
+                cur = nxt
+            if cur != phase[i]:
+                phase[i] = cur
+                changed += 1
+    return changed
+
+
+def housekeeping_case(n, seed):
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(-1200, 1200, (n, 3)).astype(f32)
+    vel = rng.normal(0, 10, (n, 3)).astype(f32)
+    temp = rng.uniform(-100, 9000, n).astype(f32)
+    temp[::53] = np.nan
+    temp[1::61] = np.inf
+    pos[2::71, 1] = np.nan
+    phase = rng.integers(0, 8, n).astype(np.uint8)
+    mat = rng.choice([0, 1, 2, 3, 3, 1, 5], n).astype(np.uint16)
+    active = (rng.uniform(size=n) > 0.1).astype(np.uint8)
+    return pos, vel, temp, phase, mat, active
+
+
+def test_housekeeping_oracle_matches_numpy_restatement_bitwise():
+    lo, hi = np.array([-1000, -50, -1000], f32), np.array([1000, 900, 1000], f32)
+    for passes in (7, 1, 2, 4, 6):
+        a = housekeeping_case(3000, passes)
+        b = tuple(x.copy() for x in a)
+        ca = O.mpss_housekeeping(a[0], a[1], a[2], a[3], a[4], a[5], lo, hi, 10.0, 8000.0, passes)
+        cb = np_housekeeping(b[0], b[1], b[2], b[3], b[4], b[5], lo, hi, f32(10.0), f32(8000.0), passes)
+        assert ca == cb, passes
+        for x, y in zip(a[:4], b[:4]):
+            assert np.array_equal(x.view(np.uint8), y.view(np.uint8)), passes
