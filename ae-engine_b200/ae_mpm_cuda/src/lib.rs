@@ -145,6 +145,22 @@ extern "C" {
         coarse_origin: *const f32,
         dt: f32,
     ) -> c_int;
+    pub fn ae_mpm_mpss_housekeeping(
+        ctx: *mut ae_mpm_ctx,
+        pos: *mut f32,
+        vel: *mut f32,
+        temperature: *mut f32,
+        phase: *mut u8,
+        material_idx: *const u16,
+        active: *const u8,
+        count: u64,
+        bounds_min: *const f32,
+        bounds_max: *const f32,
+        min_temp: f32,
+        max_temp: f32,
+        passes: u32,
+        transitions: *mut u32,
+    ) -> c_int;
 }
 
 /// Library context on device 0, created on first use (one per process, like the rayon pool).
@@ -351,6 +367,44 @@ pub fn coarse_field_update(
             dt,
         )
     })
+}
+
+/// The three MpssBuffer calls of ae_engine/src/lib.rs:347-358 (apply_boundary_conditions_par,
+/// clamp_temperatures_par, apply_phase_transitions_par) in one device pass; returns the number of
+/// phase transitions.  `phase` holds MpssPhase discriminants as bytes (`p as u8` and back, or
+/// MpssPhase declared #[repr(u8)] and the slice reinterpreted).
+pub fn mpss_housekeeping(
+    pos: &mut [[f32; 3]],
+    vel: &mut [[f32; 3]],
+    temperature: &mut [f32],
+    phase: &mut [u8],
+    material_idx: &[u16],
+    active: &[bool],
+    bounds_min: [f32; 3],
+    bounds_max: [f32; 3],
+    min_temp: f32,
+    max_temp: f32,
+) -> Result<u32, String> {
+    let mut transitions = 0u32;
+    check(unsafe {
+        ae_mpm_mpss_housekeeping(
+            ctx(),
+            pos.as_mut_ptr() as *mut f32,
+            vel.as_mut_ptr() as *mut f32,
+            temperature.as_mut_ptr(),
+            phase.as_mut_ptr(),
+            material_idx.as_ptr(),
+            active.as_ptr() as *const u8,
+            pos.len() as u64,
+            bounds_min.as_ptr(),
+            bounds_max.as_ptr(),
+            min_temp,
+            max_temp,
+            7,
+            &mut transitions,
+        )
+    })?;
+    Ok(transitions)
 }
 
 #[allow(dead_code)]

@@ -262,13 +262,15 @@ def run_reference(args, rank, pg):
 
 
 # ---------------------------------------------------------------------------------------------
-# "tick": the engine's particle passes around the substep (simulation.rs:495-532, 612-679,
-# 877-966) on one frame that reclassifies: LOD classification, far-field update and coarse
-# temperature field, over a 1M-particle MpssBuffer.  Synthetic: a 1.6 km cube around the player
-# with 3% of the particles within 40 m (so the 10 000 near cap binds), 95% active.
+# "tick": the engine's particle passes around the substep on one frame that reclassifies: LOD
+# classification, far-field update and coarse temperature field (simulation.rs:495-532, 612-679,
+# 877-966), then the MpssBuffer housekeeping (ae_engine/src/lib.rs:347-358), over a 1M-particle
+# MpssBuffer.  Synthetic: a 1.6 km cube around the player with 3% of the particles within 40 m
+# (so the 10 000 near cap binds), 95% active, materials wood/water/concrete/iron.
 # ---------------------------------------------------------------------------------------------
 TICK_N = 1 << 20
-TICK = dict(near=50.0, mid=200.0, max_near=10000, coarse_n=16, coarse_dx=50.0, far_dt=1.0)
+TICK = dict(near=50.0, mid=200.0, max_near=10000, coarse_n=16, coarse_dx=50.0, far_dt=1.0, bounds=750.0,
+            min_temp=10.0, max_temp=8000.0)
 
 
 def tick_population(n, seed):
@@ -278,15 +280,17 @@ def tick_population(n, seed):
     pos[:k] = rng.uniform(-40, 40, (k, 3))
     pos = pos[rng.permutation(n)].astype(np.float32)
     return {"pos": pos, "vel": rng.normal(0, 3, (n, 3)).astype(np.float32),
-            "temp": rng.uniform(250, 600, n).astype(np.float32), "mass": rng.uniform(0.5, 2, n).astype(np.float32),
-            "active": (rng.uniform(size=n) > 0.05).astype(np.uint8)}
+            "temp": rng.uniform(250, 2500, n).astype(np.float32), "mass": rng.uniform(0.5, 2, n).astype(np.float32),
+            "active": (rng.uniform(size=n) > 0.05).astype(np.uint8), "phase": np.zeros(n, np.uint8),
+            "mat": rng.integers(0, 4, n).astype(np.uint16)}
 
 
 def tick_cfg(n):
-    return {"workload": "engine tick around the substep: LOD reclassify + far-field update + coarse field, "
-                        "%d particles, near cap %d, coarse field %d^3" % (n, TICK["max_near"], TICK["coarse_n"]),
+    return {"workload": "engine tick around the substep: LOD reclassify + far-field update + coarse field + "
+                        "MpssBuffer housekeeping, %d particles, near cap %d, coarse field %d^3"
+                        % (n, TICK["max_near"], TICK["coarse_n"]),
             "particles": n, "l2": "L2 flushed between ticks (256 MB write, outside the timed events): the tick's "
-                                  "33 B/particle would otherwise stay L2-resident"}
+                                  "36 B/particle would otherwise stay L2-resident"}
 
 
 def tick_oracle(d, player, origin):
@@ -297,6 +301,9 @@ def tick_oracle(d, player, origin):
     O.far_field_update(d["pos"], d["vel"], d["temp"], far, d["coarse"], TICK["coarse_dx"], origin, TICK["far_dt"])
     O.coarse_field_update(d["pos"], d["mass"], d["temp"], d["active"], np.sort(near), d["coarse"], TICK["coarse_dx"],
                           origin, TICK["far_dt"])
+    b = TICK["bounds"]
+    O.mpss_housekeeping(d["pos"], d["vel"], d["temp"], d["phase"], d["mat"], d["active"], [-b] * 3, [b] * 3,
+                        TICK["min_temp"], TICK["max_temp"], 7)
 
 
 def run_tick(args, rank, local, world_size, pg, reference=False):
@@ -339,6 +346,9 @@ def run_tick(args, rank, local, world_size, pg, reference=False):
     outs = [torch.empty(n, dtype=torch.int64, device="cuda:%d" % local) for _ in range(3)]
     cnt = [C.c_uint64(0) for _ in range(3)]
     pl, og = player.copy(), origin.copy()
+    blo = np.full(3, -TICK["bounds"], np.float32)
+    bhi = np.full(3, TICK["bounds"], np.float32)
+    trans = C.c_uint32(0)
 
     def tick_device():
         ctx.check(lib.ae_mpm_lod_classify(h, dev["pos"].data_ptr(), dev["active"].data_ptr(), n, pl.ctypes.data,
@@ -352,6 +362,10 @@ def run_tick(args, rank, local, world_size, pg, reference=False):
                                                  dev["temp"].data_ptr(), dev["active"].data_ptr(), n,
                                                  outs[0].data_ptr(), cnt[0].value, dev["coarse"].data_ptr(),
                                                  TICK["coarse_n"], TICK["coarse_dx"], og.ctypes.data, TICK["far_dt"]))
+        ctx.check(lib.ae_mpm_mpss_housekeeping(h, dev["pos"].data_ptr(), dev["vel"].data_ptr(), dev["temp"].data_ptr(),
+                                               dev["phase"].data_ptr(), dev["mat"].data_ptr(), dev["active"].data_ptr(),
+                                               n, blo.ctypes.data, bhi.ctypes.data, TICK["min_temp"],
+                                               TICK["max_temp"], 7, C.byref(trans)))
 
     for _ in range(max(args.warmup, 3)):
         tick_device()
@@ -377,12 +391,13 @@ def run_tick(args, rank, local, world_size, pg, reference=False):
     n_near, n_far = cnt[0].value, cnt[2].value
     capped = n_near >= TICK["max_near"]
     # kernels per tick: classify 3 (7 with the cap: radix select, second partition), far 1, coarse 12
-    # (cell keys, 2-pass sort, gather, runs, sums, relaxation, diffusion)
-    launches = args.steps * ((7 if capped else 3) + 1 + 12)
+    # (cell keys, 2-pass sort, gather, runs, sums, relaxation, diffusion), housekeeping 1
+    launches = args.steps * ((7 if capped else 3) + 1 + 12 + 1)
     # algorithmic bytes per tick: classify reads pos + active twice and writes one 8-byte index per
     # particle; far: index 8 + pos 12 read, pos.y, vel.y, temperature read and written; coarse: near
-    # index 8, pos 12, mass 4, temperature 4, active 1
-    alg = 34 * n + 40 * n_far + 29 * n_near
+    # index 8, pos 12, mass 4, temperature 4, active 1; housekeeping: pos, vel, temperature and
+    # phase read and written, material and active read (61 B)
+    alg = 34 * n + 40 * n_far + 29 * n_near + 61 * n
     achieved = alg / (ms / args.steps * 1e-3) / 1e9
     peak, peak_kind = peaks()
     # end to end: the same tick through the drop-in call on host (MpssBuffer) arrays
@@ -395,9 +410,11 @@ def run_tick(args, rank, local, world_size, pg, reference=False):
                              TICK["far_dt"])
         ctx.coarse_field_update(hd["pos"], hd["mass"], hd["temp"], hd["active"], near, hd["coarse"], TICK["coarse_dx"],
                                 origin, TICK["far_dt"])
+        ctx.mpss_housekeeping(hd["pos"], hd["vel"], hd["temp"], hd["phase"], hd["mat"], hd["active"], blo, bhi,
+                              TICK["min_temp"], TICK["max_temp"], 7)
     e2e_dt = time.perf_counter() - t0
-    h2d = 13 * n + 28 * n_far + (29 - 8) * n_near + 4 * TICK["coarse_n"] ** 3 * 2
-    d2h = 8 * n + 28 * n_far + 4 * TICK["coarse_n"] ** 3
+    h2d = 13 * n + 28 * n_far + (29 - 8) * n_near + 4 * TICK["coarse_n"] ** 3 * 2 + 32 * n
+    d2h = 8 * n + 28 * n_far + 4 * TICK["coarse_n"] ** 3 + 29 * n
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         t0 = time.perf_counter()
@@ -413,7 +430,7 @@ def run_tick(args, rank, local, world_size, pg, reference=False):
             "roofline": {"bound": "hbm", "kernel": "tick (all passes)", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
                          "algorithmic_bytes": alg},
-            "tick_counts": {"near": n_near, "mid": cnt[1].value, "far": n_far},
+            "tick_counts": {"near": n_near, "mid": cnt[1].value, "far": n_far, "phase_transitions": trans.value},
             "e2e": {"value": n * e2e_steps / e2e_dt, "unit": unit, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": 1000.0 * e2e_dt / e2e_steps},
             "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk}), flush=True)
