@@ -88,6 +88,60 @@ class RequestResult(C.Structure):
                 ("admit_s", C.c_double), ("done_s", C.c_double)]
 
 
+class CkConfig(C.Structure):
+    """ae_mpm_ck_config: CkMpmConfig (ae_compute/src/ck_mpm.rs:41-59)."""
+    _fields_ = [("dt", C.c_float), ("grid_h", C.c_float), ("grid_n", C.c_uint32), ("gravity", C.c_float * 3),
+                ("youngs_modulus", C.c_float), ("poissons_ratio", C.c_float), ("density", C.c_float),
+                ("bounds_min", C.c_float * 3), ("bounds_max", C.c_float * 3), ("restitution", C.c_float),
+                ("dual_grid", C.c_uint8), ("pad", C.c_uint8 * 3)]
+
+
+class CkStats(C.Structure):
+    _fields_ = [("kinetic_energy", C.c_float), ("average_velocity", C.c_float * 3),
+                ("average_volume_ratio", C.c_float)]
+
+
+CK_RECORD = 26  # floats per CkMpmParticle record: position, velocity, affine, deformation, rest_volume, mass
+
+
+def ck_config(**overrides) -> CkConfig:
+    """CkMpmConfig::default() (ck_mpm.rs:61-77) with `overrides` applied, like the reference's
+    `CkMpmConfig { grid_n: 16, ..CkMpmConfig::default() }`."""
+    c = CkConfig()
+    c.dt = 1.0 / 240.0
+    c.grid_h = 0.05
+    c.grid_n = 32
+    c.gravity[:] = (0.0, -9.81, 0.0)
+    c.youngs_modulus = 1e5
+    c.poissons_ratio = 0.3
+    c.density = 1000.0
+    c.bounds_min[:] = (-1.0, -1.0, -1.0)
+    c.bounds_max[:] = (1.0, 1.0, 1.0)
+    c.restitution = 0.3
+    c.dual_grid = 1
+    for k, v in overrides.items():
+        if k in ("gravity", "bounds_min", "bounds_max"):
+            getattr(c, k)[:] = tuple(float(x) for x in v)
+        else:
+            setattr(c, k, v)
+    return c
+
+
+def ck_particles(positions, mass, rest_volume, velocity=None) -> np.ndarray:
+    """(n, 26) float32 CkMpmParticle records as CkMpmParticle::new (ck_mpm.rs:97-108) makes them:
+    zero velocity and affine matrix, identity deformation gradient."""
+    pos = np.asarray(positions, np.float32).reshape(-1, 3)
+    n = pos.shape[0]
+    r = np.zeros((n, CK_RECORD), np.float32)
+    r[:, 0:3] = pos
+    if velocity is not None:
+        r[:, 3:6] = np.asarray(velocity, np.float32).reshape(-1, 3)
+    r[:, 15] = r[:, 19] = r[:, 23] = 1.0
+    r[:, 24] = rest_volume
+    r[:, 25] = mass
+    return r
+
+
 # every function include/ae_mpm.h declares: name -> (restype, argtypes)
 _P = C.c_void_p
 SIGNATURES = {
@@ -129,6 +183,11 @@ SIGNATURES = {
                                              C.c_float, _P, C.c_float]),
     "ae_mpm_mpss_housekeeping": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.c_uint64, _P, _P, C.c_float, C.c_float,
                                            C.c_uint32, C.POINTER(C.c_uint32)]),
+    "ae_mpm_ck_config_default": (None, [C.POINTER(CkConfig)]),
+    "ae_mpm_ck_step": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(CkConfig), C.c_uint32]),
+    "ae_mpm_ck_step_timed": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(CkConfig), C.c_uint32, C.POINTER(C.c_double)]),
+    "ae_mpm_ck_stats_compute": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(CkStats)]),
+    "ae_mpm_ck_weights": (C.c_int, [_P, _P, C.c_uint64, C.c_float, _P, _P]),
     "ae_mpm_world_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(TuneResult)]),
     "ae_mpm_server_create": (C.c_int, [_P, C.POINTER(ServerOpts), C.POINTER(_P)]),
     "ae_mpm_server_submit": (C.c_int, [_P, C.POINTER(SceneDesc), C.POINTER(ParticlesView), C.c_uint64, C.c_uint32,
@@ -356,6 +415,29 @@ class Context:
                                                      lo.ctypes.data, hi.ctypes.data, min_temp, max_temp, passes,
                                                      C.byref(tr)))
         return tr.value
+
+    # CK-MPM solver (ae_compute/src/ck_mpm.rs): particles are (n, 26) float32 records
+    def ck_step(self, particles: np.ndarray, config: CkConfig, steps: int = 1) -> None:
+        """`steps` x CkMpmSolver::step, in place."""
+        if particles.dtype != np.float32 or not particles.flags.c_contiguous or particles.shape[-1] != CK_RECORD:
+            raise ValueError("particles must be a C-contiguous (n, 26) float32 array")
+        self.check(self.lib.ae_mpm_ck_step(self.h, particles.ctypes.data, particles.shape[0], C.byref(config), steps))
+
+    def ck_stats(self, particles: np.ndarray):
+        """(kinetic_energy, average_velocity (3,), average_volume_ratio)."""
+        p = np.ascontiguousarray(particles, np.float32)
+        st = CkStats()
+        self.check(self.lib.ae_mpm_ck_stats_compute(self.h, p.ctypes.data if p.size else None, p.shape[0],
+                                                    C.byref(st)))
+        return st.kinetic_energy, np.array(st.average_velocity[:], np.float32), st.average_volume_ratio
+
+    def ck_weights(self, x, h: float):
+        """CkMpmSolver::weight / weight_grad evaluated on the device."""
+        x = np.ascontiguousarray(x, np.float32).ravel()
+        w = np.empty_like(x)
+        dw = np.empty_like(x)
+        self.check(self.lib.ae_mpm_ck_weights(self.h, x.ctypes.data, x.size, h, w.ctypes.data, dw.ctypes.data))
+        return w, dw
 
     def radix_sort(self, keys: np.ndarray, key_bits: int):
         keys = np.ascontiguousarray(keys, np.uint32)

@@ -8,12 +8,23 @@ fn main() {
     let csrc = PathBuf::from(env::var("CARGO_MANIFEST_DIR").unwrap()).join("../csrc");
     let out = PathBuf::from(env::var("OUT_DIR").unwrap());
     let nvcc = env::var("NVCC").unwrap_or_else(|_| "nvcc".to_string());
-    let sources = ["radix_sort.cu", "mpm_world.cu", "ae_mpm_api.cu", "ae_mpm_server.cu", "ae_mpm_noalloc.cu"];
+    let sources = [
+        "radix_sort.cu",
+        "mpm_world.cu",
+        "ae_mpm_api.cu",
+        "ae_mpm_server.cu",
+        "ae_mpm_noalloc.cu",
+        "ae_mpm_lod.cu",
+        "ae_mpm_ck.cu",
+    ];
     let mut objects = Vec::new();
     for src in sources.iter() {
         let obj = out.join(src.replace(".cu", ".o"));
+        // the CK-MPM kernels round every operation separately, as Rust's f32 arithmetic does
+        let extra: &[&str] = if *src == "ae_mpm_ck.cu" { &["--fmad=false"] } else { &[] };
         let status = Command::new(&nvcc)
             .args(["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-lineinfo", "-Xptxas", "-v"])
+            .args(extra)
             .args(["-Xcompiler", "-fPIC", "-c"])
             .arg(csrc.join(src))
             .arg("-o")

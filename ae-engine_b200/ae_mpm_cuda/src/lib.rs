@@ -71,6 +71,45 @@ pub struct ae_mpm_ctx {
 
 pub const AE_MPM_OK: c_int = 0;
 
+/// CkMpmConfig (ae_compute/src/ck_mpm.rs:41-59) in the library's layout.
+#[repr(C)]
+#[derive(Clone, Copy, Debug, Default)]
+pub struct ae_mpm_ck_config {
+    pub dt: f32,
+    pub grid_h: f32,
+    pub grid_n: u32,
+    pub gravity: [f32; 3],
+    pub youngs_modulus: f32,
+    pub poissons_ratio: f32,
+    pub density: f32,
+    pub bounds_min: [f32; 3],
+    pub bounds_max: [f32; 3],
+    pub restitution: f32,
+    pub dual_grid: u8,
+    pub pad: [u8; 3],
+}
+
+/// CkMpmParticle (ck_mpm.rs:84-95): glam Vec3 / Mat3 are #[repr(C)] (Mat3 = three column Vec3s),
+/// so a CkMpmParticle declared #[repr(C)] has exactly this layout and its slice can be passed as is.
+#[repr(C)]
+#[derive(Clone, Copy, Debug, Default)]
+pub struct ae_mpm_ck_particle {
+    pub position: [f32; 3],
+    pub velocity: [f32; 3],
+    pub affine: [f32; 9],
+    pub deformation: [f32; 9],
+    pub rest_volume: f32,
+    pub mass: f32,
+}
+
+#[repr(C)]
+#[derive(Clone, Copy, Debug, Default)]
+pub struct ae_mpm_ck_stats {
+    pub kinetic_energy: f32,
+    pub average_velocity: [f32; 3],
+    pub average_volume_ratio: f32,
+}
+
 extern "C" {
     pub fn ae_mpm_ctx_create(device: c_int, out: *mut *mut ae_mpm_ctx) -> c_int;
     pub fn ae_mpm_ctx_destroy(ctx: *mut ae_mpm_ctx);
@@ -161,6 +200,29 @@ extern "C" {
         passes: u32,
         transitions: *mut u32,
     ) -> c_int;
+    pub fn ae_mpm_ck_config_default(out: *mut ae_mpm_ck_config);
+    pub fn ae_mpm_ck_step(
+        ctx: *mut ae_mpm_ctx,
+        particles: *mut ae_mpm_ck_particle,
+        n: u64,
+        config: *const ae_mpm_ck_config,
+        steps: u32,
+    ) -> c_int;
+    pub fn ae_mpm_ck_step_timed(
+        ctx: *mut ae_mpm_ctx,
+        particles: *mut ae_mpm_ck_particle,
+        n: u64,
+        config: *const ae_mpm_ck_config,
+        steps: u32,
+        kernel_ms: *mut f64,
+    ) -> c_int;
+    pub fn ae_mpm_ck_stats_compute(
+        ctx: *mut ae_mpm_ctx,
+        particles: *const ae_mpm_ck_particle,
+        n: u64,
+        out: *mut ae_mpm_ck_stats,
+    ) -> c_int;
+    pub fn ae_mpm_ck_weights(ctx: *mut ae_mpm_ctx, x: *const f32, n: u64, h: f32, w: *mut f32, dw: *mut f32) -> c_int;
 }
 
 /// Library context on device 0, created on first use (one per process, like the rayon pool).
@@ -405,6 +467,18 @@ pub fn mpss_housekeeping(
         )
     })?;
     Ok(transitions)
+}
+
+/// `steps` x CkMpmSolver::step (ck_mpm.rs:187-480) on the caller's particles, in place.
+pub fn ck_step(particles: &mut [ae_mpm_ck_particle], config: &ae_mpm_ck_config, steps: u32) -> Result<(), String> {
+    check(unsafe { ae_mpm_ck_step(ctx(), particles.as_mut_ptr(), particles.len() as u64, config, steps) })
+}
+
+/// kinetic_energy, average_velocity, average_volume_ratio (ck_mpm.rs:484-503).
+pub fn ck_stats(particles: &[ae_mpm_ck_particle]) -> Result<ae_mpm_ck_stats, String> {
+    let mut out = ae_mpm_ck_stats::default();
+    check(unsafe { ae_mpm_ck_stats_compute(ctx(), particles.as_ptr(), particles.len() as u64, &mut out) })?;
+    Ok(out)
 }
 
 #[allow(dead_code)]

@@ -26,7 +26,11 @@ LIB = os.path.join(BUILD, "libae_mpm.so")
 HOST_TEST = os.path.join(BUILD, "test_host_mirror")
 ORACLE_LIB = os.path.join(ORACLE_BUILD, "libae_mpm_oracle.so")
 
-CU_SOURCES = ["radix_sort.cu", "mpm_world.cu", "ae_mpm_api.cu", "ae_mpm_server.cu", "ae_mpm_noalloc.cu", "ae_mpm_lod.cu"]
+CU_SOURCES = ["radix_sort.cu", "mpm_world.cu", "ae_mpm_api.cu", "ae_mpm_server.cu", "ae_mpm_noalloc.cu", "ae_mpm_lod.cu",
+              "ae_mpm_ck.cu"]
+# per-source flags: the CK-MPM kernels round every operation separately, as the reference's f32
+# arithmetic does (no fused multiply-add)
+SOURCE_FLAGS = {"ae_mpm_ck.cu": ["--fmad=false"]}
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
@@ -70,7 +74,7 @@ def build_cuda(force: bool = False) -> str:
         o = os.path.join(BUILD, "obj", src.replace(".cu", ".o"))
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
-            jobs.append([nvcc] + NVCC_FLAGS + ["-c", s, "-o", o])
+            jobs.append([nvcc] + NVCC_FLAGS + SOURCE_FLAGS.get(src, []) + ["-c", s, "-o", o])
     with cf.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
         list(ex.map(_run, jobs))
     if force or jobs or _stale(LIB, objs):
@@ -91,7 +95,7 @@ def build_host_test(force: bool = False) -> str:
 
 def build_oracle(force: bool = False) -> str:
     os.makedirs(ORACLE_BUILD, exist_ok=True)
-    srcs = [os.path.join(ORACLE, "mpm_oracle.cpp"), os.path.join(ORACLE, "lod_oracle.cpp")]
+    srcs = [os.path.join(ORACLE, f) for f in ("mpm_oracle.cpp", "lod_oracle.cpp", "ck_oracle.cpp")]
     if force or _stale(ORACLE_LIB, srcs + [os.path.join(ROOT, "include", "ae_mpm.h")]):
         # x86-64-v3 so the binary also runs on the GPU hosts' CPUs; no FMA contraction, as in Rust
         _run(["g++", "-O3", "-std=c++17", "-march=x86-64-v3", "-ffp-contract=off", "-fPIC", "-shared", "-o", ORACLE_LIB]

@@ -17,6 +17,7 @@
 
 #include "../../include/ae_mpm.h"
 #include "mpm_world.cuh"
+#include "ae_mpm_ck.cuh"
 #include "ae_mpm_lod.cuh"
 #include "radix_sort.cuh"
 
@@ -40,6 +41,8 @@ struct ae_mpm_ctx {
   std::map<std::string, ae_mpm_tune_result> tuned;
   // engine tick passes (LOD, far field, coarse field) and their device staging for host arrays
   aemp::LodWork* lod = nullptr;
+  // CK-MPM solver buffers
+  aemp::CkWork* ck = nullptr;
   void* dstage = nullptr;
   size_t dstage_bytes = 0;
 };
@@ -123,6 +126,11 @@ bool is_device_ptr(const void* p) {
 aemp::LodWork* lod_work(ae_mpm_ctx* ctx) {
   if (!ctx->lod) ctx->lod = new aemp::LodWork();
   return ctx->lod;
+}
+
+aemp::CkWork* ck_work(ae_mpm_ctx* ctx) {
+  if (!ctx->ck) ctx->ck = new aemp::CkWork();
+  return ctx->ck;
 }
 
 // reference-layout view over the pinned staging for n particles
@@ -269,6 +277,7 @@ void ae_mpm_ctx_destroy(ae_mpm_ctx* ctx) {
   cudaSetDevice(ctx->device);
   delete ctx->dropin;
   delete ctx->lod;
+  delete ctx->ck;
   cudaFree(ctx->dstage);
   if (ctx->pin) cudaFreeHost(ctx->pin);
   aemp::sort_scratch_free(ctx->sort);
@@ -651,6 +660,105 @@ int ae_mpm_mpss_housekeeping(ae_mpm_ctx* ctx, float* pos, float* vel, float* tem
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
   }
   if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("mpss_housekeeping: ") + cudaGetErrorString(e));
+  return AE_MPM_OK;
+}
+
+void ae_mpm_ck_config_default(ae_mpm_ck_config* out) {
+  if (!out) return;
+  // CkMpmConfig::default(), ck_mpm.rs:61-77
+  *out = ae_mpm_ck_config{};
+  out->dt = 1.0f / 240.0f;
+  out->grid_h = 0.05f;
+  out->grid_n = 32;
+  out->gravity[1] = -9.81f;
+  out->youngs_modulus = 1e5f;
+  out->poissons_ratio = 0.3f;
+  out->density = 1000.0f;
+  for (int k = 0; k < 3; ++k) out->bounds_min[k] = -1.0f, out->bounds_max[k] = 1.0f;
+  out->restitution = 0.3f;
+  out->dual_grid = 1;
+}
+
+int ae_mpm_ck_step(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm_ck_config* config,
+                   uint32_t steps) {
+  return ae_mpm_ck_step_timed(ctx, particles, n, config, steps, nullptr);
+}
+
+int ae_mpm_ck_step_timed(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm_ck_config* config,
+                         uint32_t steps, double kernel_ms[2]) {
+  if (!ctx) return AE_MPM_EINVAL;
+  if (kernel_ms) kernel_ms[0] = kernel_ms[1] = 0.0;
+  if (!config || (n && !particles)) return fail(ctx, AE_MPM_EINVAL, "ck_step: null config or particles");
+  if (config->grid_n > 1024) return fail(ctx, AE_MPM_EINVAL, "ck_step: grid_n above 1024");
+  if (n == 0 || steps == 0) return AE_MPM_OK;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  aemp::CkWork* ck = ck_work(ctx);
+  cudaError_t e;
+  if (is_device_ptr(particles)) {
+    e = ck->step(particles, n, *config, steps, 0, kernel_ms);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  } else {
+    const size_t bytes = n * sizeof(ae_mpm_ck_particle);
+    rc = ensure_dstage(ctx, bytes);
+    if (rc) return rc;
+    auto* d = static_cast<ae_mpm_ck_particle*>(ctx->dstage);
+    e = cudaMemcpyAsync(d, particles, bytes, cudaMemcpyHostToDevice, 0);
+    if (e == cudaSuccess) e = ck->step(d, n, *config, steps, 0, kernel_ms);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(particles, d, bytes, cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  }
+  if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("ck_step: ") + cudaGetErrorString(e));
+  return AE_MPM_OK;
+}
+
+int ae_mpm_ck_stats_compute(ae_mpm_ctx* ctx, const ae_mpm_ck_particle* particles, uint64_t n, ae_mpm_ck_stats* out) {
+  if (!ctx) return AE_MPM_EINVAL;
+  if (!out || (n && !particles)) return fail(ctx, AE_MPM_EINVAL, "ck_stats: null particles or output");
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  aemp::CkWork* ck = ck_work(ctx);
+  cudaError_t e;
+  if (n == 0 || is_device_ptr(particles)) {
+    e = ck->stats(particles, n, out, 0);
+  } else {
+    const size_t bytes = n * sizeof(ae_mpm_ck_particle);
+    rc = ensure_dstage(ctx, bytes);
+    if (rc) return rc;
+    auto* d = static_cast<ae_mpm_ck_particle*>(ctx->dstage);
+    e = cudaMemcpyAsync(d, particles, bytes, cudaMemcpyHostToDevice, 0);
+    if (e == cudaSuccess) e = ck->stats(d, n, out, 0);
+  }
+  if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("ck_stats: ") + cudaGetErrorString(e));
+  return AE_MPM_OK;
+}
+
+int ae_mpm_ck_weights(ae_mpm_ctx* ctx, const float* x, uint64_t n, float h, float* w, float* dw) {
+  if (!ctx) return AE_MPM_EINVAL;
+  if (n && (!x || !w || !dw)) return fail(ctx, AE_MPM_EINVAL, "ck_weights: null array");
+  if (n == 0) return AE_MPM_OK;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  aemp::CkWork* ck = ck_work(ctx);
+  cudaError_t e;
+  if (is_device_ptr(x)) {
+    e = ck->weights(x, n, h, w, dw, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  } else {
+    const size_t b = (4 * n + 15) & ~size_t(15);
+    rc = ensure_dstage(ctx, 3 * b);
+    if (rc) return rc;
+    char* d = static_cast<char*>(ctx->dstage);
+    float* dx = reinterpret_cast<float*>(d);
+    float* dwt = reinterpret_cast<float*>(d + b);
+    float* dg = reinterpret_cast<float*>(d + 2 * b);
+    e = cudaMemcpyAsync(dx, x, 4 * n, cudaMemcpyHostToDevice, 0);
+    if (e == cudaSuccess) e = ck->weights(dx, n, h, dwt, dg, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(w, dwt, 4 * n, cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dw, dg, 4 * n, cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  }
+  if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("ck_weights: ") + cudaGetErrorString(e));
   return AE_MPM_OK;
 }
 

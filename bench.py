@@ -15,7 +15,7 @@ the grid exceeds the 126 MB L2, so no flush is needed between steps.
 
 --impl reference times that CPU restatement alone (the reference is Rust and cannot be built
 here).  --gpus N runs N independent replicas (one scene per GPU; the substep does
-not shard within a scene).  Other workloads: --workload jelly|dam|batched|served.
+not shard within a scene).  Other workloads: --workload jelly|dam|batched|served|tick|ck.
 """
 from __future__ import annotations
 
@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="snow", choices=["snow", "jelly", "dam", "batched", "served", "tick"])
+    ap.add_argument("--workload", default="snow", choices=["snow", "jelly", "dam", "batched", "served", "tick", "ck"])
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--e2e-substeps", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -231,6 +231,8 @@ def run_reference(args, rank, pg):
     """CPU restatement of the reference substep on this host's cores, same workload and metric."""
     if args.workload == "tick":
         return run_tick(args, rank, 0, 1, pg, reference=True)
+    if args.workload == "ck":
+        return run_ck(args, rank, 0, 1, pg, reference=True)
     if rank != 0:
         return
     scenes, parts, cfg = workload(args.workload, 0, args.scenes)
@@ -436,6 +438,149 @@ def run_tick(args, rank, local, world_size, pg, reference=False):
             "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk}), flush=True)
 
 
+# "ck": CK-MPM (ae_compute/src/ck_mpm.rs, CkMpmSolver::step) on an elastic block: 128^3 particles
+# on a jittered lattice at half the cell size (8 per cell, in lattice order as the reference's
+# tests add them) in a 128^3 grid of h = 1 m, falling at 1 m/s; E 1e5, nu 0.3, density 1000,
+# dt 5e-3 (0.05 of the elastic CFL limit).  At h = 1 the kernel's weights sum to ~1 over a node
+# stencil, so the solver stays far below its 50 m/s speed cap; at the reference's default
+# h = 0.05 the weights sum to ~6000 and every moving particle runs at the cap.
+CK_SIDE = 128
+CK_E2E_STEPS = 200  # steps per host call in the end-to-end leg (the reference's longest test runs 200-300)
+# algorithmic bytes per particle-step of the particle kernel: the 104-byte record read, the 96
+# bytes that change (position, velocity, affine matrix, deformation gradient) written
+CK_BYTES_PER_PARTICLE = 104 + 96
+
+
+def ck_scene(seed=0xC4):
+    import ae_mpm as M
+
+    grid_n, h = 128, 1.0
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(*[np.arange(CK_SIDE)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    spacing = 0.5 * h
+    pos = np.array([32.0, 40.0, 32.0]) + (g + rng.uniform(0.25, 0.75, g.shape)) * spacing
+    vel = np.zeros_like(pos)
+    vel[:, 1] = -1.0
+    vol = spacing ** 3
+    p = M.ck_particles(pos, 1000.0 * vol, vol, velocity=vel + rng.normal(0, 0.05, pos.shape))
+    cfg = M.ck_config(dt=5e-3, grid_n=grid_n, grid_h=h, bounds_min=(0, 0, 0), bounds_max=(128, 128, 128))
+    n = p.shape[0]
+    info = {"workload": "CK-MPM elastic block: %d particles (128^3 jittered lattice, 8 per cell), 128^3 grid "
+                        "h=1, dt 5e-3, E 1e5, nu 0.3, falling at 1 m/s" % n,
+            "particles": n, "grid_n": grid_n,
+            "l2": "inputs larger than L2 (%.0f MB of particle records), no flush" % (104 * n / 1e6)}
+    return p, cfg, info
+
+
+def ck_oracle_rate(p, cfg, steps):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    q = p.copy()
+    t0 = time.perf_counter()
+    O.ck_step(q, cfg, steps)
+    return p.shape[0] * steps / (time.perf_counter() - t0)
+
+
+def run_ck(args, rank, local, world_size, pg, reference=False):
+    import ctypes as C
+
+    p, cfg, info = ck_scene(0xC4 + rank)
+    n = p.shape[0]
+    metric, unit = "CK-MPM particle-updates/s", "particle-updates/s"
+    if reference:  # the CPU restatement of CkMpmSolver::step (serial, as the reference's loops)
+        if rank != 0:
+            return
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        q = p.copy()
+        O.ck_step(q, cfg, max(1, min(args.warmup, 1)))
+        steps = max(1, min(args.steps, 5))
+        t0 = time.perf_counter()
+        O.ck_step(q, cfg, steps)
+        dt = time.perf_counter() - t0
+        value = n * steps / dt
+        print(json.dumps({"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
+                          "steps": steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / steps,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                          "data": "synthetic (seeded numpy)", "config": info,
+                          "cpu_baseline": {"value": value, "unit": unit, "cores": 1, "kind": "port",
+                                           "sample": "%d whole steps of the %d-particle scene" % (steps, n)},
+                          "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+    import torch
+
+    import ae_mpm as M
+
+    ctx = M.Context(local)
+    lib, h = ctx.lib, ctx.h
+    dp = torch.from_numpy(p.ravel().copy()).cuda(local)
+    steps = args.steps
+
+    def run(k, timed=None):
+        ctx.check(lib.ae_mpm_ck_step_timed(h, dp.data_ptr(), n, C.byref(cfg), k, timed))
+
+    run(max(args.warmup, 3))
+    clocks = Clocks(local)
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run(steps)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    ms = max_over_ranks(pg, ms)
+    value = n * world_size * steps / (ms / 1e3)
+    # per-kernel durations from events around every launch, on a separate run of the same length
+    km = (C.c_double * 2)()
+    run(steps, km)
+    part_us = 1000.0 * km[0] / (steps + 1)
+    grid_us = 1000.0 * km[1] / steps  # block compaction + grid update
+    achieved = CK_BYTES_PER_PARTICLE * n / (part_us * 1e-6) / 1e9
+    peak, peak_kind = peaks()
+    # end to end: host records through the drop-in call, CK_E2E_STEPS steps per call, pinned memory
+    hp = torch.from_numpy(p.ravel().copy()).pin_memory()
+    e2e_calls = max(1, args.e2e_reps)
+    t0 = time.perf_counter()
+    for _ in range(e2e_calls):
+        ctx.check(lib.ae_mpm_ck_step(h, hp.data_ptr(), n, C.byref(cfg), CK_E2E_STEPS))
+    e2e_dt = time.perf_counter() - t0
+    e2e_value = n * CK_E2E_STEPS * e2e_calls / e2e_dt
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = {"value": ck_oracle_rate(p, cfg, 2), "unit": unit, "cores": 1, "kind": "port",
+               "sample": "2 whole steps of the %d-particle scene" % n}
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        t = json.load(open(tpath)).get("ck")
+        if t:
+            traffic = t["particles_bytes_per_particle"] * n
+    if rank == 0:
+        print(json.dumps({
+            "metric": metric, "value": value, "unit": unit, "n_gpus": world_size, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy)",
+            "config": dict(info, parallelism="replicas" if world_size > 1 else "single GPU"),
+            "roofline": {"bound": "hbm", "kernel": "ck_particles_kernel (G2P + next P2G + forces)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "algorithmic_bytes": CK_BYTES_PER_PARTICLE * n},
+            "kernel_us": {"particles": part_us, "grid": grid_us},
+            "e2e": {"value": e2e_value, "unit": unit, "h2d_bytes_per_step": 104 * n / CK_E2E_STEPS,
+                    "d2h_bytes_per_step": 104 * n / CK_E2E_STEPS,
+                    "ms_per_step": 1000.0 * e2e_dt / (CK_E2E_STEPS * e2e_calls),
+                    "call": "ae_mpm_ck_step on pinned host records, %d steps per call" % CK_E2E_STEPS},
+            "cpu_baseline": cpu, "gpu_launches": 1 + 3 * steps, "clocks": clk}), flush=True)
+
+
 def run_ours(args, rank, local, world_size, pg):
     import torch
 
@@ -443,6 +588,8 @@ def run_ours(args, rank, local, world_size, pg):
 
     if args.workload == "tick":
         return run_tick(args, rank, local, world_size, pg)
+    if args.workload == "ck":
+        return run_ck(args, rank, local, world_size, pg)
     ctx = M.Context(local)
     scenes, parts, cfg = workload(args.workload, rank, args.scenes)
     if args.workload == "served":

@@ -352,6 +352,70 @@ int ae_mpm_mpss_housekeeping(ae_mpm_ctx* ctx, float* pos, float* vel, float* tem
                              uint32_t passes, uint32_t* transitions);
 
 /* ---------------------------------------------------------------------------------------------
+ * CK-MPM, the compact-kernel MPM solver (ae_compute/src/ck_mpm.rs, CkMpmSolver): C^2 kernel
+ * w(x) = (1 - (x/h)^2)^3 / h on the 2 nodes per axis around a particle (nodes at (i + 1/2) h,
+ * i = floor(x/h) + {0, 1}, 0 <= i < grid_n), APIC transfer, neo-Hookean forces, guarded grid and
+ * particle updates.  Particles are CkMpmParticle records; matrices are glam Mat3, column-major.
+ * The particle pointer of a call is host memory (staged through the context) or device memory
+ * (updated in place); which one is decided from the pointer.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ae_mpm_ck_config {  /* CkMpmConfig, ck_mpm.rs:41-59                          */
+  float dt;
+  float grid_h;
+  uint32_t grid_n;                 /* usize in the reference; at most 1024 here            */
+  float gravity[3];
+  float youngs_modulus;
+  float poissons_ratio;
+  float density;                   /* carried, read by no step (as in the reference)       */
+  float bounds_min[3];
+  float bounds_max[3];
+  float restitution;
+  uint8_t dual_grid;               /* carried, read by no step (as in the reference)       */
+  uint8_t pad[3];
+} ae_mpm_ck_config;
+
+typedef struct ae_mpm_ck_particle {  /* CkMpmParticle, ck_mpm.rs:84-95; 104 bytes            */
+  float position[3];
+  float velocity[3];
+  float affine[9];                   /* APIC matrix B, columns x_axis, y_axis, z_axis         */
+  float deformation[9];              /* deformation gradient F, same layout                   */
+  float rest_volume;
+  float mass;
+} ae_mpm_ck_particle;
+
+typedef struct ae_mpm_ck_stats {
+  float kinetic_energy;        /* CkMpmSolver::kinetic_energy, ck_mpm.rs:484-486        */
+  float average_velocity[3];   /* CkMpmSolver::average_velocity, :489-494               */
+  float average_volume_ratio;  /* CkMpmSolver::average_volume_ratio, :497-503           */
+} ae_mpm_ck_stats;
+
+/* CkMpmConfig::default() (ck_mpm.rs:61-77). */
+void ae_mpm_ck_config_default(ae_mpm_ck_config* out);
+
+/* `steps` calls of CkMpmSolver::step (ck_mpm.rs:187-480) over particles[0..n), in place.  Each
+ * particle's contribution to a node and each particle update from the node velocities round as
+ * the reference's f32 arithmetic does; node sums are accumulated in atomic order (not particle
+ * order), so results agree with the reference to rounding, not bit for bit, where several
+ * particles share a node.  Invalid: null config, grid_n > 1024 (AE_MPM_EINVAL). */
+int ae_mpm_ck_step(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm_ck_config* config,
+                   uint32_t steps);
+
+/* ae_mpm_ck_step with CUDA events around each kernel: kernel_ms[0] receives the summed duration
+ * of the particle kernels (G2P fused with the next step's P2G and force scatter), kernel_ms[1]
+ * that of the grid kernels (touched-block compaction and grid update), in milliseconds. */
+int ae_mpm_ck_step_timed(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm_ck_config* config,
+                         uint32_t steps, double kernel_ms[2]);
+
+/* The solver's diagnostics over particles[0..n), summed on the device in double precision;
+ * n = 0 gives 0, (0, 0, 0) and 1, as the reference's empty-solver cases do. */
+int ae_mpm_ck_stats_compute(ae_mpm_ctx* ctx, const ae_mpm_ck_particle* particles, uint64_t n,
+                            ae_mpm_ck_stats* out);
+
+/* CkMpmSolver::weight and weight_grad (ck_mpm.rs:163-185) at x[0..n) with support h, evaluated
+ * by the device code the solver uses.  Host or device arrays (decided from x). */
+int ae_mpm_ck_weights(ae_mpm_ctx* ctx, const float* x, uint64_t n, float h, float* w, float* dw);
+
+/* ---------------------------------------------------------------------------------------------
  * Autotuner: times the P2G variants, block sizes and sort intervals on a world and writes the
  * fastest choice back into the world's options.  Choices are cached per workload signature.
  * ------------------------------------------------------------------------------------------- */

@@ -65,6 +65,11 @@ def load():
                                         C.POINTER(C.c_uint64), V, C.POINTER(C.c_uint64)]
     lib.oracle_far_field_update.argtypes = [V, V, V, V, C.c_uint64, V, C.c_uint64, f, V, f]
     lib.oracle_coarse_field_update.argtypes = [V, V, V, V, V, C.c_uint64, V, C.c_uint64, f, V, f]
+    lib.oracle_ck_step.argtypes = [V, C.c_uint64, C.POINTER(M.CkConfig), C.c_uint32]
+    lib.oracle_ck_weight.restype = f
+    lib.oracle_ck_weight.argtypes = [f, f]
+    lib.oracle_ck_weight_grad.restype = f
+    lib.oracle_ck_weight_grad.argtypes = [f, f]
     lib.oracle_mpss_housekeeping.restype = C.c_uint32
     lib.oracle_mpss_housekeeping.argtypes = [V, V, V, V, V, V, C.c_uint64, V, V, f, f, C.c_uint32]
     _lib = lib
@@ -225,3 +230,43 @@ def mpss_housekeeping(pos, vel, temperature, phase, material_idx, active, bounds
     return load().oracle_mpss_housekeeping(pos.ctypes.data, vel.ctypes.data, temperature.ctypes.data,
                                            phase.ctypes.data, mat.ctypes.data, None if act is None else act.ctypes.data,
                                            pos.shape[0], lo.ctypes.data, hi.ctypes.data, min_temp, max_temp, passes)
+
+
+# ---------------------------------------------------------------- CK-MPM (ae_compute/src/ck_mpm.rs)
+def ck_step(particles: np.ndarray, config: M.CkConfig, steps: int = 1) -> None:
+    """`steps` x CkMpmSolver::step (ck_mpm.rs:187-480) in place on (n, 26) float32 records."""
+    if particles.dtype != np.float32 or not particles.flags.c_contiguous or particles.shape[-1] != M.CK_RECORD:
+        raise ValueError("particles must be a C-contiguous (n, 26) float32 array")
+    load().oracle_ck_step(particles.ctypes.data if particles.size else None, particles.shape[0], C.byref(config),
+                          steps)
+
+
+def ck_weight(x: float, h: float) -> float:
+    return load().oracle_ck_weight(x, h)
+
+
+def ck_weight_grad(x: float, h: float) -> float:
+    return load().oracle_ck_weight_grad(x, h)
+
+
+def ck_stats(particles: np.ndarray):
+    """kinetic_energy, average_velocity, average_volume_ratio (ck_mpm.rs:484-503): sequential f32
+    sums in particle order, as the reference's iterator sums."""
+    p = np.asarray(particles, np.float32)
+    n = p.shape[0]
+    if n == 0:
+        return np.float32(0.0), np.zeros(3, np.float32), np.float32(1.0)
+    ke = np.float32(0.0)
+    vs = np.zeros(3, np.float32)
+    ds = np.float32(0.0)
+    f32 = np.float32
+    for r in p:
+        v = r[3:6]
+        lsq = f32(f32(v[0] * v[0]) + f32(v[1] * v[1])) + f32(v[2] * v[2])
+        ke = f32(ke + f32(f32(f32(0.5) * r[25]) * lsq))
+        vs = (vs + v).astype(np.float32)
+        x, y, z = r[15:18], r[18:21], r[21:24]
+        cx = np.array([f32(x[1] * y[2]) - f32(y[1] * x[2]), f32(x[2] * y[0]) - f32(y[2] * x[0]),
+                       f32(x[0] * y[1]) - f32(y[0] * x[1])], np.float32)
+        ds = f32(ds + (f32(f32(z[0] * cx[0]) + f32(z[1] * cx[1])) + f32(z[2] * cx[2])))
+    return ke, (vs / f32(n)).astype(np.float32), f32(ds / f32(n))

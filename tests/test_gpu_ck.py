@@ -1,0 +1,327 @@
+"""GPU parity of CK-MPM (ae_compute/src/ck_mpm.rs, CkMpmSolver) through the C ABI against the
+CPU oracle.
+
+What is bit-exact and what is not:
+* the kernel weights, and any step in which no node has two contributing particles and no
+  logarithm is taken (E = 0, or F = I on the first step): each particle's contribution and update
+  round exactly as the reference's f32 arithmetic (no FMA contraction, glam's operand order);
+* ln(det F) is the correctly rounded logarithm on the device and glibc's logf in the reference,
+  which is off by one ulp for a few percent of arguments (its documented error is ~0.82 ulp);
+* where particles share nodes the device adds their contributions in atomic order, not particle
+  order, so results agree to rounding.
+
+The reference's own scenarios are chaotic at their settings: the kernel's weights sum to
+~(0.9/h)^3 over a node stencil (~700 at h = 0.1), so G2P amplifies node velocities by that factor
+and most particles run at the 50 m/s speed cap, whose direction comes from sums that cancel.
+One ulp on one input coordinate moves the oracle's own trajectories by up to 0.7 within 20 steps.
+Multi-step comparisons are therefore made against that rounding envelope: the device result must
+lie within 10x the largest deviation of oracle runs whose input positions differ by one ulp.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import ae_mpm as M
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+f32 = np.float32
+
+
+def ref(cfg, p, steps):
+    q = np.array(p, np.float32, order="C")
+    O.ck_step(q, cfg, steps)
+    return q
+
+
+def dev(ctx, cfg, p, steps):
+    q = np.array(p, np.float32, order="C")
+    ctx.ck_step(q, cfg, steps)
+    return q
+
+
+def envelope(cfg, p0, steps, k=3, seed=0):
+    """The oracle's result and, per record field, the largest deviation of k oracle runs whose
+    input positions differ from p0 by one ulp (random direction per coordinate)."""
+    base = ref(cfg, p0, steps)
+    rng = np.random.default_rng(seed)
+    env = np.zeros(26)
+    for _ in range(k):
+        q = p0.copy()
+        up = rng.integers(0, 2, q[:, :3].shape).astype(bool)
+        q[:, :3] = np.where(up, np.nextafter(q[:, :3], f32(np.inf)), np.nextafter(q[:, :3], f32(-np.inf)))
+        r = ref(cfg, q, steps)
+        d = np.abs(r.astype(np.float64) - base)
+        env = np.maximum(env, np.nan_to_num(d, nan=0.0).max(axis=0) if d.size else 0)
+    return base, env
+
+
+def assert_in_envelope(got, base, env, factor=10.0, floor=1e-6):
+    """Field groups (position, velocity, affine, deformation) within factor x the envelope."""
+    assert got.shape == base.shape
+    assert np.array_equal(np.isnan(got), np.isnan(base))
+    np.testing.assert_array_equal(got[:, 24:26], base[:, 24:26])
+    for lo, hi, name in ((0, 3, "position"), (3, 6, "velocity"), (6, 15, "affine"), (15, 24, "deformation")):
+        d = np.nan_to_num(np.abs(got[:, lo:hi].astype(np.float64) - base[:, lo:hi]), nan=0.0)
+        scale = max(float(np.nanmax(np.abs(base[:, lo:hi]))), 1.0) if base.size else 1.0
+        tol = factor * float(env[lo:hi].max()) + floor * scale
+        assert d.max() <= tol, "%s: max |device - oracle| %.3g > %.3g (envelope %.3g)" % (
+            name, d.max(), tol, env[lo:hi].max())
+
+
+def assert_close(got, want, pos_tol, vel_rel=1e-4, f_tol=1e-4):
+    assert got.shape == want.shape
+    assert np.array_equal(np.isnan(got), np.isnan(want))
+    vmax = max(float(np.nanmax(np.abs(want[:, 3:6]))), 1e-3)
+    np.testing.assert_allclose(got[:, 0:3], want[:, 0:3], rtol=0, atol=pos_tol)
+    np.testing.assert_allclose(got[:, 3:6], want[:, 3:6], rtol=0, atol=vel_rel * vmax)
+    np.testing.assert_allclose(got[:, 15:24], want[:, 15:24], rtol=0, atol=f_tol)
+    np.testing.assert_array_equal(got[:, 24:26], want[:, 24:26])
+
+
+def block(n, origin, spacing, mass, vol):
+    g = np.arange(n, dtype=np.float32) * f32(spacing)
+    pts = [(f32(origin[0]) + g[i], f32(origin[1]) + g[j], f32(origin[2]) + g[k])
+           for i in range(n) for j in range(n) for k in range(n)]
+    return M.ck_particles(pts, mass, vol)
+
+
+def test_weights_match_oracle_bitwise(ctx):
+    rng = np.random.default_rng(5)
+    for h in (0.1, 0.05, 0.0125):
+        x = np.concatenate([rng.uniform(-1.5 * h, 1.5 * h, 20000), [0.0, h, -h, 0.5 * h, np.nextafter(h, 0)]])
+        x = x.astype(f32)
+        w, dw = ctx.ck_weights(x, h)
+        rw = np.array([O.ck_weight(float(v), h) for v in x], f32)
+        rdw = np.array([O.ck_weight_grad(float(v), h) for v in x], f32)
+        assert np.array_equal(w.view(np.uint32), rw.view(np.uint32))
+        assert np.array_equal(dw.view(np.uint32), rdw.view(np.uint32))
+    # the reference's own assertions (ck_mpm.rs:538-553)
+    w, _ = ctx.ck_weights([0.15, -0.15, 0.0, 0.05], 0.1)
+    assert w[0] == 0 and w[1] == 0 and w[2] > 0 and 0 < w[3] < w[2]
+
+
+# ------------------------------------------------ the reference's unit-test scenarios, on the device
+SINGLE = [
+    # (name, config overrides, position, steps) from ck_mpm.rs:555-612, 724-737
+    ("single_particle_no_crash", dict(grid_n=16, grid_h=0.1), (0.5, 0.5, 0.5), 1),
+    ("falls_under_gravity", dict(dt=0.01, grid_n=16, grid_h=0.1, bounds_min=(-2, -2, -2), bounds_max=(2, 2, 2)),
+     (0.8, 1.5, 0.8), 1),
+    ("boundary_collision", dict(dt=0.01, grid_n=32, grid_h=0.05, gravity=(0, -20, 0), bounds_min=(0, 0, 0),
+                                bounds_max=(1.6, 1.6, 1.6)), (0.8, 1.5, 0.8), 300),
+    ("volume_ratio_finite", dict(), (0.5, 0.5, 0.5), 10),
+    ("dual_grid_off", dict(grid_n=16, grid_h=0.1, dual_grid=0), (0.5, 0.5, 0.5), 1),
+]
+
+
+@pytest.mark.parametrize("name,over,pos,steps", SINGLE, ids=[s[0] for s in SINGLE])
+def test_single_particle_scenarios(ctx, name, over, pos, steps):
+    cfg = M.ck_config(**over)
+    p0 = M.ck_particles([pos], 1.0, 0.001)
+    got = dev(ctx, cfg, p0, steps)
+    want = ref(cfg, p0, steps)
+    if steps == 1:  # one contributor per node and F = I: bit for bit
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert_close(got, want, pos_tol=1e-5)
+    if name == "falls_under_gravity":
+        assert got[0, 1] < p0[0, 1]
+    if name == "boundary_collision":
+        assert -0.1 <= got[0, 1] < 0.5
+    if name == "volume_ratio_finite":
+        assert np.isfinite(ctx.ck_stats(got)[2])
+
+
+BLOCKS = [
+    # (name, config overrides, block args, steps) from ck_mpm.rs:614-646, 660-722, 739-779
+    ("multiple_particles", dict(grid_n=16, grid_h=0.1, bounds_min=(-1, -1, -1), bounds_max=(2, 2, 2)),
+     (3, (0.5, 0.5, 0.5), 0.05, 1.0, 0.0001), 20),
+    ("elastic_deformation", dict(dt=0.001, grid_n=16, grid_h=0.1, youngs_modulus=1e4, bounds_min=(-1, -1, -1),
+                                 bounds_max=(2, 2, 2)), (4, (0.6, 0.6, 0.6), 0.04, 0.01, 0.0001), 50),
+    ("no_nan_long_run", dict(dt=0.002, grid_n=24, grid_h=0.05, youngs_modulus=1e3, bounds_min=(0, 0, 0),
+                             bounds_max=(1.2, 1.2, 1.2)), (3, (0.5, 0.8, 0.5), 0.03, 0.01, 0.0001), 200),
+]
+
+
+@pytest.mark.parametrize("name,over,blk,steps", BLOCKS, ids=[b[0] for b in BLOCKS])
+def test_block_scenarios(ctx, name, over, blk, steps):
+    cfg = M.ck_config(**over)
+    p0 = block(*blk)
+    for k in (1, 2, steps):
+        got = dev(ctx, cfg, p0, k)
+        base, env = envelope(cfg, p0, k)
+        assert_in_envelope(got, base, env)
+    # the reference's own assertions on the full run
+    assert np.isfinite(got[:, 0:6]).all()
+    dets = [np.linalg.det(r[15:24].reshape(3, 3).astype(np.float64)) for r in got]
+    assert all(np.isfinite(d) and abs(d) < 100 for d in dets)
+
+
+def test_apic_affine_scenario(ctx):  # ck_mpm.rs:660-684
+    cfg = M.ck_config(dt=0.005, grid_n=16, grid_h=0.1, bounds_min=(-1, -1, -1), bounds_max=(2, 2, 2))
+    p0 = M.ck_particles([(0.5 + i * 0.05, 1.0, 0.5) for i in range(3)], 1.0, 0.0001)
+    got = dev(ctx, cfg, p0, 1)
+    assert_close(got, ref(cfg, p0, 1), pos_tol=1e-6)
+    assert np.abs(got[:, 6:15]).max() > 1e-10
+
+
+def test_kinetic_energy_and_stats(ctx):  # ck_mpm.rs:648-658 and the diagnostics :484-503
+    p = M.ck_particles([[0.5, 0.5, 0.5]], 2.0, 0.001, velocity=[[1.0, 0.0, 0.0]])
+    ke, v, ratio = ctx.ck_stats(p)
+    assert abs(ke - 1.0) < 1e-4 and list(v) == [1.0, 0.0, 0.0] and ratio == 1.0
+    ke, v, ratio = ctx.ck_stats(np.zeros((0, 26), f32))
+    assert ke == 0 and not v.any() and ratio == 1.0
+    rng = np.random.default_rng(3)
+    q = M.ck_particles(rng.uniform(0, 1, (50000, 3)), 0.01, 1e-4, velocity=rng.normal(0, 2, (50000, 3)))
+    q[:, 15:24] += rng.normal(0, 0.05, (50000, 9)).astype(f32)
+    got = ctx.ck_stats(q)
+    want = O.ck_stats(q)
+    assert abs(got[0] - want[0]) <= 1e-4 * abs(want[0])
+    np.testing.assert_allclose(got[1], want[1], rtol=0, atol=1e-5)
+    assert abs(got[2] - want[2]) <= 1e-5
+
+
+# ------------------------------------------------ larger populations
+def jittered_block(n_side, spacing, origin, seed, mass=2.5e-4, vol=2.5e-7):
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(*[np.arange(n_side)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    pos = np.asarray(origin) + (g + rng.uniform(0.25, 0.75, g.shape)) * spacing
+    p = M.ck_particles(pos, mass, vol, velocity=rng.normal(0, 0.5, g.shape))
+    return p
+
+
+def test_sparse_particles_are_bit_exact(ctx):
+    # particles at least 2.5 cells apart on every axis share no node: every step is bit for bit
+    # the reference's, except where the device's correctly rounded ln(det F) and the C library's
+    # logf differ
+    h = 0.0125
+    p0 = jittered_block(24, 5 * h, (0.05, 0.05, 0.05), 7)
+    p0[:, 15:24] += np.random.default_rng(8).normal(0, 0.02, (p0.shape[0], 9)).astype(f32)
+    cfg = M.ck_config(dt=5e-4, grid_n=128, grid_h=h, bounds_min=(0, 0, 0), bounds_max=(1.6, 1.6, 1.6))
+    got = dev(ctx, cfg, p0, 1)
+    want = ref(cfg, p0, 1)
+    same = np.all(got.view(np.uint32) == want.view(np.uint32), axis=1)
+    assert same.mean() >= 0.9, same.mean()  # the rest: a one-ulp ln(det F) of glibc's logf
+    assert_close(got, want, pos_tol=1e-6)
+    got = dev(ctx, cfg, p0, 10)
+    base, env = envelope(cfg, p0, 10)
+    assert_in_envelope(got, base, env)
+
+
+def test_sparse_particles_without_stress_are_bit_exact_over_many_steps(ctx):
+    # E = 0: the stress is 0 and no logarithm enters; particles 2.5+ cells apart share no node:
+    # nothing is left to differ.  h = 1 keeps them slow (weights summing to ~1), so they stay apart.
+    p0 = jittered_block(20, 5.0, (2.0, 2.0, 2.0), 17, mass=125.0, vol=0.125)
+    p0[:, 6:15] = np.random.default_rng(18).normal(0, 0.5, (p0.shape[0], 9)).astype(f32)
+    cfg = M.ck_config(dt=5e-3, grid_n=128, grid_h=1.0, youngs_modulus=0.0, bounds_min=(0, 0, 0),
+                      bounds_max=(128, 128, 128))
+    got = dev(ctx, cfg, p0, 20)
+    want = ref(cfg, p0, 20)
+    assert np.abs(want[:, 3:6]).max() < 5  # still far from the cap: the premise holds
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_sparse_particles_at_a_non_power_of_two_spacing_match_bitwise(ctx):
+    # the same at h = 0.7 (divisions by h do not reduce to exact multiplications) for 3 steps
+    h = 0.7
+    p0 = jittered_block(16, 5 * h, (2.0, 2.0, 2.0), 19, mass=0.04, vol=4e-5)
+    cfg = M.ck_config(dt=2e-3, grid_n=128, grid_h=h, youngs_modulus=0.0, bounds_min=(0, 0, 0),
+                      bounds_max=(128 * h,) * 3)
+    got = dev(ctx, cfg, p0, 3)
+    want = ref(cfg, p0, 3)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_coarse_grid_stable_regime_multi_step(ctx):
+    # h = 1: the stencil weights sum to ~1, velocities stay far below the cap, and the
+    # comparison holds over 40 steps
+    g = np.stack(np.meshgrid(*[np.arange(16)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    rng = np.random.default_rng(4)
+    pos = np.array([20.0, 24.0, 20.0]) + (g + rng.uniform(0.25, 0.75, g.shape)) * 0.5
+    vel = np.tile([0.0, -1.0, 0.0], (g.shape[0], 1)) + rng.normal(0, 0.05, g.shape)
+    p0 = M.ck_particles(pos, 125.0, 0.125, velocity=vel)
+    cfg = M.ck_config(dt=5e-3, grid_n=64, grid_h=1.0, bounds_min=(0, 0, 0), bounds_max=(64, 64, 64))
+    got = dev(ctx, cfg, p0, 40)
+    base, env = envelope(cfg, p0, 40)
+    assert_in_envelope(got, base, env)
+    np.testing.assert_allclose(got[:, 0:3], base[:, 0:3], rtol=0, atol=1e-3)
+    assert np.abs(got[:, 3:6]).max() < 50
+
+
+@pytest.mark.parametrize("n_side,grid_n,steps", [(20, 32, 5), (40, 64, 3), (64, 128, 2)])
+def test_dense_blocks_match_oracle(ctx, n_side, grid_n, steps):
+    h = 1.6 / grid_n
+    p0 = jittered_block(n_side, 0.5 * h, (0.4, 0.5, 0.4), n_side)
+    cfg = M.ck_config(dt=5e-4, grid_n=grid_n, grid_h=h, bounds_min=(0, 0, 0), bounds_max=(1.6, 1.6, 1.6))
+    got = dev(ctx, cfg, p0, steps)
+    base, env = envelope(cfg, p0, steps, k=2)
+    assert_in_envelope(got, base, env)
+
+
+def test_edges_outside_grid_nan_and_empty(ctx):
+    cfg = M.ck_config(grid_n=16, grid_h=0.1, bounds_min=(-1, -1, -1), bounds_max=(3, 3, 3))
+    pts = [(-0.5, 0.5, 0.5),      # below the grid: no node, the velocity becomes 0
+           (-0.03, 0.5, 0.5),     # floor(-0.3) = -1: only the i = 0 nodes
+           (1.58, 1.55, 1.59),    # at the top of the 16-node grid
+           (2.5, 2.5, 2.5),       # beyond it
+           (0.5, 0.5, 0.5), (0.52, 0.5, 0.5)]
+    p0 = M.ck_particles(pts, 1.0, 0.001, velocity=[(1, 2, 3)] * len(pts))
+    got = dev(ctx, cfg, p0, 3)
+    assert_close(got, ref(cfg, p0, 3), pos_tol=1e-6)
+    # a NaN particle poisons the nodes it reaches (floor(NaN) as i32 is 0), as in the reference
+    p1 = p0.copy()
+    p1[4, 0] = np.nan
+    got = dev(ctx, cfg, p1, 2)
+    want = ref(cfg, p1, 2)
+    assert np.array_equal(np.isnan(got), np.isnan(want))
+    # nothing to do
+    e = np.zeros((0, 26), f32)
+    ctx.ck_step(e, cfg, 5)
+    q = p0.copy()
+    ctx.ck_step(q, cfg, 0)
+    assert np.array_equal(q, p0)
+    # grid_n = 0: no node exists anywhere
+    got = dev(ctx, M.ck_config(grid_n=0), p0, 2)
+    assert_close(got, ref(M.ck_config(grid_n=0), p0, 2), pos_tol=0)
+
+
+def test_invalid_arguments(ctx):
+    p = M.ck_particles([[0.5, 0.5, 0.5]], 1.0, 0.001)
+    with pytest.raises(M.MpmError) as e:
+        ctx.ck_step(p, M.ck_config(grid_n=2048), 1)
+    assert e.value.code == M.EINVAL
+    rc = ctx.lib.ae_mpm_ck_step(ctx.h, p.ctypes.data, 1, None, 1)
+    assert rc == M.EINVAL
+
+
+def test_split_calls_and_grid_changes(ctx):
+    h = 1.6 / 64
+    p0 = jittered_block(16, 0.5 * h, (0.5, 0.6, 0.5), 3)
+    cfg = M.ck_config(dt=5e-4, grid_n=64, grid_h=h, bounds_min=(0, 0, 0), bounds_max=(1.6, 1.6, 1.6))
+    base, env = envelope(cfg, p0, 6)
+    q = p0.copy()
+    for k in (1, 2, 3):
+        ctx.ck_step(q, cfg, k)
+    assert_in_envelope(q, base, env)
+    # another grid in between: the buffers are re-laid out and cleared
+    other = M.ck_config(grid_n=16, grid_h=0.1)
+    ctx.ck_step(M.ck_particles([[0.5, 0.5, 0.5]], 1.0, 0.001), other, 2)
+    q = p0.copy()
+    ctx.ck_step(q, cfg, 6)
+    assert_in_envelope(q, base, env)
+
+
+def test_device_pointers_aligned_and_not(ctx):
+    torch = pytest.importorskip("torch")
+    h = 0.0125
+    p0 = jittered_block(12, 5 * h, (0.3, 0.3, 0.3), 9)  # no shared nodes: order-independent results
+    cfg = M.ck_config(dt=5e-4, grid_n=128, grid_h=h, bounds_min=(0, 0, 0), bounds_max=(1.6, 1.6, 1.6))
+    want = dev(ctx, cfg, p0, 4)
+    for offset in (0, 1):  # records starting 4 bytes past a 16-byte boundary take the scalar staging path
+        buf = torch.zeros(p0.size + 4, dtype=torch.float32, device="cuda")
+        view = buf[offset:offset + p0.size]
+        view.copy_(torch.from_numpy(p0.ravel()))
+        ctx.check(ctx.lib.ae_mpm_ck_step(ctx.h, view.data_ptr(), p0.shape[0], C.byref(cfg), 4))
+        torch.cuda.synchronize()
+        got = view.cpu().numpy().reshape(p0.shape)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), offset
