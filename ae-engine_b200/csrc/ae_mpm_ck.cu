@@ -358,35 +358,59 @@ __global__ void __launch_bounds__(256) ck_compact_kernel(uint32_t* flags, uint64
 
 // Grid update (:245-251, :323-363) over the touched node blocks a.list[0..*a.count): velocity
 // from momentum, gravity and force, NaN guard, speed cap 50, reflection at the bounds.  Leaves
-// the accumulators zeroed.
+// the accumulators zeroed.  Each 64-thread group takes kGridU listed blocks per iteration and
+// issues all their accumulator loads before using any, so the list is not walked one
+// latency-bound load after another.
+constexpr int kGridU = 4;
+
+__device__ __forceinline__ void grid_node(const CkArgs& a, uint32_t b, int local, float4 a0, float4 a1, float4* vel) {
+  const uint32_t node = b * 64u + uint32_t(local);
+  const float m = a0.w;
+  V3 nv{0.0f, 0.0f, 0.0f};
+  if (m > 1e-10f) {
+    const V3 v{a0.x / m, a0.y / m, a0.z / m};
+    const V3 acc{a1.x / m + a.g[0], a1.y / m + a.g[1], a1.z / m + a.g[2]};
+    nv = v + acc * a.dt;
+    if (!finite3(nv)) nv = V3{0.0f, 0.0f, 0.0f};
+    float vl;
+    if (above(nv, 2475.0f, 50.0f, &vl)) nv = nv * (50.0f / vl);
+    const uint32_t nb = uint32_t(a.nb);
+    const int i = int((b % nb) * 4u + uint32_t(local & 3)), j = int(((b / nb) % nb) * 4u + uint32_t((local >> 2) & 3)),
+              k = int((b / (nb * nb)) * 4u + uint32_t(local >> 4));
+    const float h = a.h;
+    reflect_axis(nv.x, (float(i) + 0.5f) * h, a.bmin[0], a.bmax[0], a.restitution);
+    reflect_axis(nv.y, (float(j) + 0.5f) * h, a.bmin[1], a.bmax[1], a.restitution);
+    reflect_axis(nv.z, (float(k) + 0.5f) * h, a.bmin[2], a.bmax[2], a.restitution);
+  }
+  vel[node] = make_float4(nv.x, nv.y, nv.z, 0.0f);
+}
+
 __global__ void __launch_bounds__(kGridThreads) ck_grid_kernel(CkArgs a, float4* vel) {
-  const uint32_t count = __ldcg(a.count);
+  // written by the compaction, unchanged here: through the read-only cache, once per SM
+  const uint32_t count = __ldg(a.count);
   const int local = threadIdx.x & 63;
-  const float h = a.h, dt = a.dt;
-  for (uint32_t item = blockIdx.x * (kGridThreads / 64) + (threadIdx.x >> 6); item < count;
-       item += gridDim.x * (kGridThreads / 64)) {
-    const uint32_t b = a.list[item];
-    const uint32_t node = b * 64u + uint32_t(local);
-    const float4 a0 = a.acc[2 * node], a1 = a.acc[2 * node + 1];
-    a.acc[2 * node] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    a.acc[2 * node + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const float m = a0.w;
-    V3 nv{0.0f, 0.0f, 0.0f};
-    if (m > 1e-10f) {
-      const V3 v{a0.x / m, a0.y / m, a0.z / m};
-      const V3 acc{a1.x / m + a.g[0], a1.y / m + a.g[1], a1.z / m + a.g[2]};
-      nv = v + acc * dt;
-      if (!finite3(nv)) nv = V3{0.0f, 0.0f, 0.0f};
-      float vl;
-      if (above(nv, 2475.0f, 50.0f, &vl)) nv = nv * (50.0f / vl);
-      const uint32_t nb = uint32_t(a.nb);
-      const int i = int((b % nb) * 4u + uint32_t(local & 3)), j = int(((b / nb) % nb) * 4u + uint32_t((local >> 2) & 3)),
-                k = int((b / (nb * nb)) * 4u + uint32_t(local >> 4));
-      reflect_axis(nv.x, (float(i) + 0.5f) * h, a.bmin[0], a.bmax[0], a.restitution);
-      reflect_axis(nv.y, (float(j) + 0.5f) * h, a.bmin[1], a.bmax[1], a.restitution);
-      reflect_axis(nv.z, (float(k) + 0.5f) * h, a.bmin[2], a.bmax[2], a.restitution);
-    }
-    vel[node] = make_float4(nv.x, nv.y, nv.z, 0.0f);
+  const uint32_t groups = gridDim.x * (kGridThreads / 64);
+  for (uint32_t t0 = (blockIdx.x * (kGridThreads / 64) + (threadIdx.x >> 6)) * kGridU; t0 < count;
+       t0 += groups * kGridU) {
+    uint32_t b[kGridU];
+    float4 a0[kGridU], a1[kGridU];
+#pragma unroll
+    for (int u = 0; u < kGridU; ++u) b[u] = t0 + u < count ? a.list[t0 + u] : 0xffffffffu;
+#pragma unroll
+    for (int u = 0; u < kGridU; ++u)
+      if (b[u] != 0xffffffffu) {
+        const uint32_t node = b[u] * 64u + uint32_t(local);
+        a0[u] = a.acc[2 * node];
+        a1[u] = a.acc[2 * node + 1];
+      }
+#pragma unroll
+    for (int u = 0; u < kGridU; ++u)
+      if (b[u] != 0xffffffffu) {
+        const uint32_t node = b[u] * 64u + uint32_t(local);
+        a.acc[2 * node] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        a.acc[2 * node + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        grid_node(a, b[u], local, a0[u], a1[u], vel);
+      }
   }
 }
 
@@ -482,7 +506,7 @@ cudaError_t CkWork::step(ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm
   for (int k = 0; k < 3; ++k) a.g[k] = cfg.gravity[k], a.bmin[k] = cfg.bounds_min[k], a.bmax[k] = cfg.bounds_max[k];
   a.aligned16 = (reinterpret_cast<uintptr_t>(particles) & 15u) == 0;
   const unsigned pgrid = unsigned((n + kCkThreads - 1) / kCkThreads);
-  const unsigned ggrid = unsigned(std::min<uint64_t>(148 * 8, (blocks_ + 3) / 4));
+  const unsigned ggrid = unsigned(std::min<uint64_t>(148 * 4, (blocks_ + 4 * kGridU - 1) / (4 * kGridU)));
   const unsigned cgrid = unsigned(std::min<uint64_t>(148 * 8, (blocks_ + 255) / 256));
   // optional per-launch events: [2 k] before and [2 k + 1] after launch k
   const uint32_t n_launch = 1 + 3 * steps;

@@ -63,6 +63,11 @@ __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
+// A work counter that an earlier kernel wrote and that no thread of this kernel changes, read by
+// every thread: through the read-only cache, so each SM fetches it once.  (A volatile or L2-only
+// load would send every warp of the grid to the same L2 slice before any of them could start.)
+__device__ __forceinline__ uint32_t launch_count(const uint32_t* p) { return __ldg(p); }
+
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 template <class V4>
@@ -653,7 +658,7 @@ __device__ __forceinline__ void block_coords(const SceneDev<T>& sc, uint32_t gb,
 template <class T, int MODE>
 __global__ void __launch_bounds__(256) grid_update_kernel(WorldDev<T> w, uint32_t* blk_epoch, const uint32_t* epoch) {
   using V4 = typename V4T<T>::type;
-  const uint32_t count = *reinterpret_cast<volatile uint32_t*>(w.touched_count);
+  const uint32_t count = launch_count(w.touched_count);
   const uint32_t ep = *epoch;
   if (blockIdx.x == 0 && threadIdx.x == 0) *w.clamp_count = 0u;  // G2P of this substep refills it
   // each 64-thread group takes 4 touched blocks per iteration and issues their 4 accumulator loads
@@ -1236,7 +1241,7 @@ __global__ void __launch_bounds__(256, (MODE == AE_MPM_MODE_PHYSICS && sizeof(T)
 template <class T>
 __global__ void __launch_bounds__(128) snow_clamp_kernel(WorldDev<T> w) {
   using V4 = typename V4T<T>::type;
-  const uint32_t count = *reinterpret_cast<volatile uint32_t*>(w.clamp_count);
+  const uint32_t count = launch_count(w.clamp_count);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     const uint2 q = w.clamp_queue[i];
     const SceneDev<T>& sc = w.scenes[q.y];
@@ -1289,7 +1294,7 @@ __global__ void det_heads_kernel(const uint32_t* __restrict__ skeys, uint64_t n,
 template <class T, int MODE>
 __global__ void __launch_bounds__(128) det_cellsum_kernel(WorldDev<T> w, uint64_t n_sorted) {
   using V4 = typename V4T<T>::type;
-  const uint32_t count = *reinterpret_cast<volatile uint32_t*>(w.cell_count);
+  const uint32_t count = launch_count(w.cell_count);
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < count; s += gridDim.x * blockDim.x) {
     const uint32_t start = w.seg_start[s];
     const uint32_t key = w.sorted_keys[start];
@@ -1330,7 +1335,7 @@ __global__ void __launch_bounds__(128) det_cellsum_kernel(WorldDev<T> w, uint64_
 template <class T, int MODE>
 __global__ void __launch_bounds__(256) det_gather_kernel(WorldDev<T> w, uint32_t* blk_epoch, const uint32_t* epoch) {
   using V4 = typename V4T<T>::type;
-  const uint32_t count = *reinterpret_cast<volatile uint32_t*>(w.touched_count);
+  const uint32_t count = launch_count(w.touched_count);
   const uint32_t ep = *epoch;
   if (blockIdx.x == 0 && threadIdx.x == 0) *w.clamp_count = 0u;
   const int sub = threadIdx.x >> 6, l = threadIdx.x & 63;
@@ -1368,7 +1373,7 @@ __global__ void __launch_bounds__(256) det_gather_kernel(WorldDev<T> w, uint32_t
 
 __global__ void det_reset_kernel(const uint32_t* __restrict__ seg_start, const uint32_t* __restrict__ skeys,
                                  const uint32_t* cell_count, uint32_t* cell_slot) {
-  const uint32_t count = *reinterpret_cast<const volatile uint32_t*>(cell_count);
+  const uint32_t count = launch_count(cell_count);
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < count; s += gridDim.x * blockDim.x)
     cell_slot[skeys[seg_start[s]]] = 0xffffffffu;
 }
