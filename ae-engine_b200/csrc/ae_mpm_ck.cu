@@ -30,6 +30,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "ae_mpm_ck.cuh"
@@ -73,19 +74,37 @@ __device__ __forceinline__ M3 inversem(const M3& m) {
 }
 __device__ __forceinline__ float col_abs_len(V3 c) { return len3(V3{fabsf(c.x), fabsf(c.y), fabsf(c.z)}); }
 
+// The grid spacing and, when h = 2^k with |k| <= 40, its exact reciprocals 2^-k and 2^-3k.  Then
+// x / h and x / (h h h) equal x * 2^-k and x * 2^-3k bit for bit: both round the same real
+// number (subnormal results included), and the products cost one instruction instead of an IEEE
+// division sequence.  POW2 selects that form; otherwise the divisions are written as such.
+struct Spacing {
+  float h, inv_h, inv_h3;
+};
+template <bool POW2>
+__device__ __forceinline__ float div_h(float x, const Spacing& sp) {
+  return POW2 ? x * sp.inv_h : x / sp.h;
+}
+template <bool POW2>
+__device__ __forceinline__ float div_h3(float x, const Spacing& sp) {
+  return POW2 ? x * sp.inv_h3 : x / (sp.h * sp.h * sp.h);
+}
+
 // CkMpmSolver::weight (:163-176): (1 - r^2)^3 / h for r = |x| / h < 1
-__device__ __forceinline__ float ck_weight(float x, float h) {
-  const float r = fabsf(x) / h;
+template <bool POW2 = false>
+__device__ __forceinline__ float ck_weight(float x, const Spacing& sp) {
+  const float r = div_h<POW2>(fabsf(x), sp);
   if (r >= 1.0f) return 0.0f;
   const float a = 1.0f - r * r;
-  return a * a * a / h;
+  return div_h<POW2>(a * a * a, sp);
 }
 // CkMpmSolver::weight_grad (:178-185): -6 x (1 - r^2)^2 / h^3
-__device__ __forceinline__ float ck_weight_grad(float x, float h) {
-  const float r = fabsf(x) / h;
+template <bool POW2 = false>
+__device__ __forceinline__ float ck_weight_grad(float x, const Spacing& sp) {
+  const float r = div_h<POW2>(fabsf(x), sp);
   if (r >= 1.0f) return 0.0f;
   const float a = 1.0f - r * r;
-  return -6.0f * x * (a * a) / (h * h * h);
+  return div_h3<POW2>(-6.0f * x * (a * a), sp);
 }
 
 // Rust `f32 as i32`: truncation toward zero, NaN -> 0, saturating at the i32 range
@@ -106,6 +125,7 @@ struct CkArgs {
   uint32_t* count;
   uint32_t* next_count;  // the counter the next step's compaction appends to
   int gn, nb;
+  Spacing sp;
   float h, dt, youngs, poisson, restitution;
   float g[3], bmin[3], bmax[3];
   int aligned16;
@@ -129,11 +149,13 @@ struct Stencil {
   float diff[3][2], w[3][2], gw[3][2];
 };
 
-__device__ __forceinline__ void make_stencil(Stencil& st, V3 pos, float h, int gn, bool grads) {
+template <bool POW2>
+__device__ __forceinline__ void make_stencil(Stencil& st, V3 pos, const Spacing& sp, int gn, bool grads) {
   const float p[3] = {pos.x, pos.y, pos.z};
+  const float h = sp.h;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const int c = as_i32(floorf(p[a] / h));
+    const int c = as_i32(floorf(div_h<POW2>(p[a], sp)));
 #pragma unroll
     for (int d = 0; d < 2; ++d) {
       const int i = int(uint32_t(c) + uint32_t(d));  // i32 add, wrapping like the reference's release build
@@ -141,8 +163,8 @@ __device__ __forceinline__ void make_stencil(Stencil& st, V3 pos, float h, int g
       st.ok[a][d] = i >= 0 && i < gn;
       const float df = (float(i) + 0.5f) * h - p[a];
       st.diff[a][d] = df;
-      st.w[a][d] = ck_weight(df, h);
-      st.gw[a][d] = grads ? ck_weight_grad(df, h) : 0.0f;
+      st.w[a][d] = ck_weight<POW2>(df, sp);
+      st.gw[a][d] = grads ? ck_weight_grad<POW2>(df, sp) : 0.0f;
       st.zero[a][d] = st.w[a][d] == 0.0f && st.gw[a][d] == 0.0f;
     }
   }
@@ -176,11 +198,12 @@ __device__ __forceinline__ void mark_block(const CkArgs& a, uint32_t b, uint32_t
 }
 
 // P2G (:200-242) and the force pass (:253-320) of one particle
+template <bool POW2>
 __device__ __forceinline__ void scatter(const CkArgs& a, V3 pos, V3 vel, const M3& B, const M3& F, float rest_volume,
                                         float mass) {
   const float h = a.h;
   Stencil st;
-  make_stencil(st, pos, h, a.gn, true);
+  make_stencil<POW2>(st, pos, a.sp, a.gn, true);
   const float mu = a.youngs / (2.0f * (1.0f + a.poisson));
   const float lambda = a.youngs * a.poisson / ((1.0f + a.poisson) * (1.0f - 2.0f * a.poisson));
   const float fdet = fmaxf(detm(F), 1e-10f);
@@ -232,10 +255,11 @@ __device__ __forceinline__ void reflect_axis(float& v, float node_pos, float lo,
 }
 
 // G2P (:365-459) and the particle bounds (:462-478) of one particle
+template <bool POW2>
 __device__ __forceinline__ void gather_update(const CkArgs& a, V3& pos, V3& vel, M3& B, M3& F) {
   const float h = a.h, dt = a.dt;
   Stencil st;
-  make_stencil(st, pos, h, a.gn, false);
+  make_stencil<POW2>(st, pos, a.sp, a.gn, false);
   const float d_inv = 4.0f / (h * h);
   // all eight node loads first, so their latencies overlap
   float4 vnode[8];
@@ -287,7 +311,7 @@ __device__ __forceinline__ void gather_update(const CkArgs& a, V3& pos, V3& vel,
 
 // One CTA = 256 consecutive particles.  G2P: gather from a.vel and update the record in place.
 // P2G: scatter the (updated) particle into a.acc for the next grid update.
-template <bool G2P, bool P2G>
+template <bool G2P, bool P2G, bool POW2>
 __global__ void __launch_bounds__(kCkThreads, 3) ck_particles_kernel(CkArgs a) {
   __shared__ __align__(16) float srec[kCkThreads * kRecFloats];
   const uint64_t base = uint64_t(blockIdx.x) * kCkThreads;
@@ -312,7 +336,7 @@ __global__ void __launch_bounds__(kCkThreads, 3) ck_particles_kernel(CkArgs a) {
     M3 F{{r[15], r[16], r[17]}, {r[18], r[19], r[20]}, {r[21], r[22], r[23]}};
     const float rest_volume = r[24], mass = r[25];
     if (G2P) {
-      gather_update(a, pos, vel, B, F);
+      gather_update<POW2>(a, pos, vel, B, F);
       r[0] = pos.x, r[1] = pos.y, r[2] = pos.z;
       r[3] = vel.x, r[4] = vel.y, r[5] = vel.z;
       r[6] = B.c0.x, r[7] = B.c0.y, r[8] = B.c0.z, r[9] = B.c1.x, r[10] = B.c1.y, r[11] = B.c1.z;
@@ -320,7 +344,7 @@ __global__ void __launch_bounds__(kCkThreads, 3) ck_particles_kernel(CkArgs a) {
       r[15] = F.c0.x, r[16] = F.c0.y, r[17] = F.c0.z, r[18] = F.c1.x, r[19] = F.c1.y, r[20] = F.c1.z;
       r[21] = F.c2.x, r[22] = F.c2.y, r[23] = F.c2.z;
     }
-    if (P2G) scatter(a, pos, vel, B, F, rest_volume, mass);
+    if (P2G) scatter<POW2>(a, pos, vel, B, F, rest_volume, mass);
   }
   if (G2P) {
     __syncthreads();
@@ -435,10 +459,10 @@ __global__ void __launch_bounds__(256) ck_stats_kernel(const float* rec, uint64_
   }
 }
 
-__global__ void ck_weights_kernel(const float* x, uint64_t n, float h, float* w, float* dw) {
+__global__ void ck_weights_kernel(const float* x, uint64_t n, Spacing sp, float* w, float* dw) {
   for (uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += uint64_t(gridDim.x) * blockDim.x) {
-    w[q] = ck_weight(x[q], h);
-    dw[q] = ck_weight_grad(x[q], h);
+    w[q] = ck_weight(x[q], sp);
+    dw[q] = ck_weight_grad(x[q], sp);
   }
 }
 
@@ -502,6 +526,11 @@ cudaError_t CkWork::step(ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm
   a.gn = int(cfg.grid_n);
   a.nb = int(cfg.grid_n ? (cfg.grid_n + 3) / 4 : 1);
   a.h = cfg.grid_h, a.dt = cfg.dt, a.youngs = cfg.youngs_modulus, a.poisson = cfg.poissons_ratio;
+  a.sp = Spacing{cfg.grid_h, 0.0f, 0.0f};
+  int e2 = 0;
+  const bool pow2 = std::isfinite(cfg.grid_h) && cfg.grid_h > 0.0f && std::frexp(cfg.grid_h, &e2) == 0.5f &&
+                    e2 - 1 >= -40 && e2 - 1 <= 40;
+  if (pow2) a.sp.inv_h = std::ldexp(1.0f, 1 - e2), a.sp.inv_h3 = std::ldexp(1.0f, 3 * (1 - e2));
   a.restitution = cfg.restitution;
   for (int k = 0; k < 3; ++k) a.g[k] = cfg.gravity[k], a.bmin[k] = cfg.bounds_min[k], a.bmax[k] = cfg.bounds_max[k];
   a.aligned16 = (reinterpret_cast<uintptr_t>(particles) & 15u) == 0;
@@ -532,7 +561,10 @@ cudaError_t CkWork::step(ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm
   };
   a.list = lists_;
   before();
-  ck_particles_kernel<false, true><<<pgrid, kCkThreads, 0, s>>>(a);
+  if (pow2)
+    ck_particles_kernel<false, true, true><<<pgrid, kCkThreads, 0, s>>>(a);
+  else
+    ck_particles_kernel<false, true, false><<<pgrid, kCkThreads, 0, s>>>(a);
   after(true);
   for (uint32_t st = 0; st < steps; ++st) {
     // counters alternate by step: this step's compaction appends to one and zeroes the other
@@ -545,10 +577,14 @@ cudaError_t CkWork::step(ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm
     ck_grid_kernel<<<ggrid, kGridThreads, 0, s>>>(a, vel_);
     after(false);
     before();
-    if (st + 1 < steps)
-      ck_particles_kernel<true, true><<<pgrid, kCkThreads, 0, s>>>(a);
+    if (st + 1 < steps && pow2)
+      ck_particles_kernel<true, true, true><<<pgrid, kCkThreads, 0, s>>>(a);
+    else if (st + 1 < steps)
+      ck_particles_kernel<true, true, false><<<pgrid, kCkThreads, 0, s>>>(a);
+    else if (pow2)
+      ck_particles_kernel<true, false, true><<<pgrid, kCkThreads, 0, s>>>(a);
     else
-      ck_particles_kernel<true, false><<<pgrid, kCkThreads, 0, s>>>(a);
+      ck_particles_kernel<true, false, false><<<pgrid, kCkThreads, 0, s>>>(a);
     after(true);
   }
   e = cudaGetLastError();
@@ -590,7 +626,7 @@ cudaError_t CkWork::stats(const ae_mpm_ck_particle* particles, uint64_t n, ae_mp
 cudaError_t CkWork::weights(const float* x, uint64_t n, float h, float* w, float* dw, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   const unsigned grid = unsigned(std::min<uint64_t>(148 * 4, (n + 255) / 256));
-  ck_weights_kernel<<<grid, 256, 0, s>>>(x, n, h, w, dw);
+  ck_weights_kernel<<<grid, 256, 0, s>>>(x, n, Spacing{h, 0.0f, 0.0f}, w, dw);
   return cudaGetLastError();
 }
 

@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="snow", choices=["snow", "jelly", "dam", "batched", "served", "tick", "ck"])
+    ap.add_argument("--ck-h", type=float, default=1.0,
+                    help="ck: grid spacing (the scene scales with it); 1 takes the exact power-of-two division path")
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--e2e-substeps", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -451,22 +453,22 @@ CK_E2E_STEPS = 200  # steps per host call in the end-to-end leg (the reference's
 CK_BYTES_PER_PARTICLE = 104 + 96
 
 
-def ck_scene(seed=0xC4):
+def ck_scene(seed=0xC4, h=1.0):
     import ae_mpm as M
 
-    grid_n, h = 128, 1.0
+    grid_n = 128
     rng = np.random.default_rng(seed)
     g = np.stack(np.meshgrid(*[np.arange(CK_SIDE)] * 3, indexing="ij"), -1).reshape(-1, 3)
     spacing = 0.5 * h
-    pos = np.array([32.0, 40.0, 32.0]) + (g + rng.uniform(0.25, 0.75, g.shape)) * spacing
+    pos = np.array([32.0, 40.0, 32.0]) * h + (g + rng.uniform(0.25, 0.75, g.shape)) * spacing
     vel = np.zeros_like(pos)
     vel[:, 1] = -1.0
     vol = spacing ** 3
     p = M.ck_particles(pos, 1000.0 * vol, vol, velocity=vel + rng.normal(0, 0.05, pos.shape))
-    cfg = M.ck_config(dt=5e-3, grid_n=grid_n, grid_h=h, bounds_min=(0, 0, 0), bounds_max=(128, 128, 128))
+    cfg = M.ck_config(dt=5e-3, grid_n=grid_n, grid_h=h, bounds_min=(0, 0, 0), bounds_max=(128 * h,) * 3)
     n = p.shape[0]
     info = {"workload": "CK-MPM elastic block: %d particles (128^3 jittered lattice, 8 per cell), 128^3 grid "
-                        "h=1, dt 5e-3, E 1e5, nu 0.3, falling at 1 m/s" % n,
+                        "h=%g, dt 5e-3, E 1e5, nu 0.3, falling at 1 m/s" % (n, h),
             "particles": n, "grid_n": grid_n,
             "l2": "inputs larger than L2 (%.0f MB of particle records), no flush" % (104 * n / 1e6)}
     return p, cfg, info
@@ -485,7 +487,7 @@ def ck_oracle_rate(p, cfg, steps):
 def run_ck(args, rank, local, world_size, pg, reference=False):
     import ctypes as C
 
-    p, cfg, info = ck_scene(0xC4 + rank)
+    p, cfg, info = ck_scene(0xC4 + rank, args.ck_h)
     n = p.shape[0]
     metric, unit = "CK-MPM particle-updates/s", "particle-updates/s"
     if reference:  # the CPU restatement of CkMpmSolver::step (serial, as the reference's loops)

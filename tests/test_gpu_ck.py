@@ -221,11 +221,12 @@ def test_sparse_particles_without_stress_are_bit_exact_over_many_steps(ctx):
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
 
 
-def test_sparse_particles_at_a_non_power_of_two_spacing_match_bitwise(ctx):
-    # the same at h = 0.7 (divisions by h do not reduce to exact multiplications) for 3 steps
-    h = 0.7
-    p0 = jittered_block(16, 5 * h, (2.0, 2.0, 2.0), 19, mass=0.04, vol=4e-5)
-    cfg = M.ck_config(dt=2e-3, grid_n=128, grid_h=h, youngs_modulus=0.0, bounds_min=(0, 0, 0),
+@pytest.mark.parametrize("h,gap,dt", [(0.7, 5, 2e-3), (0.0625, 6, 1e-4)])
+def test_sparse_particles_at_other_spacings_match_bitwise(ctx, h, gap, dt):
+    # the same for 3 steps at h = 0.7, where the divisions by h are IEEE divisions, and at
+    # h = 2^-4, where they are exact multiplications by 2^4 and 2^12
+    p0 = jittered_block(16, gap * h, (2 * h, 2 * h, 2 * h), 19, mass=0.04, vol=4e-5)
+    cfg = M.ck_config(dt=dt, grid_n=128, grid_h=h, youngs_modulus=0.0, bounds_min=(0, 0, 0),
                       bounds_max=(128 * h,) * 3)
     got = dev(ctx, cfg, p0, 3)
     want = ref(cfg, p0, 3)
