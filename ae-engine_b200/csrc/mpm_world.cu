@@ -115,6 +115,20 @@ __device__ __forceinline__ uint32_t cell_key(const SceneDev<T>& sc, int mode, T 
   return node_index(sc, b[0], b[1], b[2]);
 }
 
+// The chunk a CTA works on: {scene, first slot, end of the live particles, end of capacity}.
+// A world of one scene needs no table (its chunks are consecutive ranges of blockDim.x slots),
+// so its CTAs start their particle loads without first waiting for a descriptor load.
+template <class T>
+__device__ __forceinline__ int4 cta_chunk(const WorldDev<T>& w) {
+  if (w.one_scene) {
+    const uint64_t lo = uint64_t(w.one_off) + uint64_t(blockIdx.x) * blockDim.x;
+    const uint64_t live = lo + blockDim.x < w.one_live_end ? lo + blockDim.x : w.one_live_end;
+    const uint64_t cap = lo + blockDim.x < w.one_cap_end ? lo + blockDim.x : w.one_cap_end;
+    return make_int4(0, int(lo), int(live > lo ? live : lo), int(cap));
+  }
+  return w.chunks[blockIdx.x];
+}
+
 template <class T>
 __device__ __forceinline__ void mark_block(const WorldDev<T>& w, uint32_t gb) {
   volatile uint32_t* f = w.blk_flag + gb;
@@ -297,7 +311,7 @@ __global__ void __launch_bounds__(512) p2g_kernel(WorldDev<T> w) {
   V4* tile = reinterpret_cast<V4*>(smem);
   __shared__ int s_lo[3], s_hi[3];
   const int tid = threadIdx.x, lane = tid & 31;
-  const int4 ch = w.chunks[blockIdx.x];
+  const int4 ch = cta_chunk(w);
   const SceneDev<T>& sc = w.scenes[ch.x];
   if (tid < 3) {
     s_lo[tid] = INT_MAX;
@@ -463,7 +477,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) p2g_lanes_kernel(
   V4* acol = wxm + nt;                            // acol[q]
   int4* gk = reinterpret_cast<int4*>(acol + nt);  // gk[q] = (stencil base, cell key)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int4 ch = w.chunks[blockIdx.x];
+  const int4 ch = cta_chunk(w);
   const SceneDev<T>& sc = w.scenes[ch.x];
   const int n0 = sc.n[0], n1 = sc.n[1], n2 = sc.n[2];
   const int j = ch.y + tid;
@@ -1099,7 +1113,7 @@ __global__ void __launch_bounds__(256, (MODE == AE_MPM_MODE_PHYSICS && sizeof(T)
   constexpr bool kTile = MODE != AE_MPM_MODE_PHYSICS;
   V4* stage = kTile ? tile + w.max_tile_nodes : tile;  // a1..a3 of this block's particles: stage[k * nt + tid]
   __shared__ int s_lo[3], s_hi[3];
-  const int4 ch = w.chunks[blockIdx.x];
+  const int4 ch = cta_chunk(w);
   const SceneDev<T>& sc = w.scenes[ch.x];
   const int tid = threadIdx.x, lane = tid & 31, nt = blockDim.x;
   const int j = ch.y + tid;
@@ -1383,7 +1397,7 @@ __global__ void det_reset_kernel(const uint32_t* __restrict__ seg_start, const u
 // ============================================================================================
 template <class T, int MODE>
 __global__ void init_keys_kernel(WorldDev<T> w) {
-  const int4 ch = w.chunks[blockIdx.x];
+  const int4 ch = cta_chunk(w);
   const SceneDev<T>& sc = w.scenes[ch.x];
   const int j = ch.y + threadIdx.x;
   if (j < ch.z) {
@@ -1480,7 +1494,7 @@ __global__ void unpack_kernel(const typename V4T<T>::type* const* src, T* __rest
 template <class T>
 __global__ void __launch_bounds__(256) totals_kernel(WorldDev<T> w, double* partial) {
   __shared__ double sm[8][5];
-  const int4 ch = w.chunks[blockIdx.x];
+  const int4 ch = cta_chunk(w);
   const int j = ch.y + threadIdx.x;
   double v[5] = {0, 0, 0, 0, 0};
   if (j < ch.z) {
@@ -2216,6 +2230,13 @@ class World final : public WorldBase {
     w.scenes = d_scenes_;
     w.mats = d_mats_;
     w.chunks = d_chunks_;
+    if (h_scenes_.size() == 1) {
+      const SceneDev<T>& h = h_scenes_[0];
+      w.one_scene = 1u;
+      w.one_off = h.p_off;
+      w.one_live_end = h.p_off + h.p_count;
+      w.one_cap_end = h.p_off + h.p_cap;
+    }
     for (int k = 0; k < 7; ++k) {
       w.in[k] = in_buf()[k];
       w.out[k] = out_buf()[k];

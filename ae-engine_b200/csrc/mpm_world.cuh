@@ -58,6 +58,8 @@ struct WorldDev {
   const SceneDev<T>* scenes;
   const MatDev* mats;
   const int4* chunks;  // {scene, lo, hi_live, hi_cap}
+  // a world of one scene: its chunks are consecutive ranges of blockDim.x slots, given here
+  uint32_t one_scene, one_off, one_live_end, one_cap_end;
   const V4* in[7];
   V4* out[7];
   const uint32_t* perm;  // sorted position -> storage slot; nullptr = identity
