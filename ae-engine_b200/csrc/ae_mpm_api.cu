@@ -526,7 +526,35 @@ int ae_mpm_far_field_update(ae_mpm_ctx* ctx, float* pos, float* vel, float* temp
   } else {
     for (uint64_t k = 0; k < n_far; ++k)
       if (far_idx[k] >= count) return fail(ctx, AE_MPM_EINVAL, "far_field_update: index out of range");
-    // gather the far particles (pos, vel, temperature: 7 floats each) and the field, one copy each way
+    if (4 * n_far >= count) {
+      // most particles are far: copy the whole arrays and the index list, let the device gather
+      // and scatter, and copy the arrays back (no host-side loop over the particles)
+      auto up16 = [](size_t b) { return (b + 15) & ~size_t(15); };
+      const size_t b3 = up16(12 * count), b1 = up16(4 * count), bi = up16(8 * n_far), bc = up16(4 * cells);
+      rc = ensure_dstage(ctx, 2 * b3 + b1 + bi + bc);
+      if (rc) return rc;
+      char* d = static_cast<char*>(ctx->dstage);
+      float* dpos = reinterpret_cast<float*>(d);
+      float* dvel = reinterpret_cast<float*>(d + b3);
+      float* dtemp = reinterpret_cast<float*>(d + 2 * b3);
+      uint64_t* didx = reinterpret_cast<uint64_t*>(d + 2 * b3 + b1);
+      float* dcoarse = reinterpret_cast<float*>(d + 2 * b3 + b1 + bi);
+      e = cudaMemcpyAsync(dpos, pos, 12 * count, cudaMemcpyHostToDevice, 0);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(dvel, vel, 12 * count, cudaMemcpyHostToDevice, 0);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(dtemp, temperature, 4 * count, cudaMemcpyHostToDevice, 0);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(didx, far_idx, 8 * n_far, cudaMemcpyHostToDevice, 0);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(dcoarse, coarse_temperature, 4 * cells, cudaMemcpyHostToDevice, 0);
+      if (e == cudaSuccess)
+        e = lw->far_field(dpos, dvel, dtemp, didx, n_far, dcoarse, coarse_n, coarse_dx, coarse_origin, far_dt, 0);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(pos, dpos, 12 * count, cudaMemcpyDeviceToHost, 0);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(vel, dvel, 12 * count, cudaMemcpyDeviceToHost, 0);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(temperature, dtemp, 4 * count, cudaMemcpyDeviceToHost, 0);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+      if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("far_field_update: ") + cudaGetErrorString(e));
+      return AE_MPM_OK;
+    }
+    // few far particles: gather them (pos, vel, temperature: 7 floats each) and the field, one
+    // copy each way
     const size_t bytes = sizeof(float) * (7 * n_far + cells);
     rc = ensure_pinned(ctx, bytes);
     if (rc) return rc;

@@ -443,8 +443,16 @@ def run_tick(args, rank, local, world_size, pg, reference=False):
     for _ in range(e2e_steps):
         tick_host()
     e2e_dt = time.perf_counter() - t0
-    h2d = 13 * n + 28 * n_far + (29 - 8) * n_near + 4 * TICK["coarse_n"] ** 3 * 2 + 32 * n
-    d2h = 8 * n + 28 * n_far + 4 * TICK["coarse_n"] ** 3 + 29 * n
+    # bytes copied by the library's host paths: classify (pos, active in; the three lists out), far
+    # field (whole pos, vel, temperature and the far list when at least a quarter of the particles
+    # are far, else the gathered far particles), coarse field (the gathered near particles and the
+    # field in, the field out), housekeeping (pos, vel, temperature, phase, material, active in;
+    # pos, vel, temperature, phase out)
+    cells = TICK["coarse_n"] ** 3
+    far_in, far_out = (28 * n + 8 * n_far + 4 * cells, 28 * n) if 4 * n_far >= n else (28 * n_far + 4 * cells,
+                                                                                        28 * n_far)
+    h2d = 13 * n + far_in + 21 * n_near + 4 * cells + 32 * n
+    d2h = 8 * n + far_out + 4 * cells + 29 * n
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         t0 = time.perf_counter()

@@ -67,20 +67,23 @@ def test_lod_classify_all_inactive_and_empty(ctx):
     assert near.size == mid.size == far.size == 0
 
 
-def far_case(n, seed):
+def far_case(n, seed, frac=2):
     rng = np.random.default_rng(seed)
     pos = rng.uniform(-500, 500, (n, 3)).astype(f32)
     vel = rng.normal(0, 5, (n, 3)).astype(f32)
     temp = rng.uniform(250, 600, n).astype(f32)
     coarse = rng.uniform(270, 330, 16 ** 3).astype(f32)
     origin = np.array([-400.0, -400.0, -400.0], f32)
-    idx = np.sort(rng.choice(n, n // 2, replace=False)).astype(np.uint64)
+    idx = np.sort(rng.choice(n, max(n // frac, 1), replace=False)).astype(np.uint64)
     return pos, vel, temp, coarse, origin, idx
 
 
+# half the particles far: the host path copies whole arrays and gathers on the device; an eighth:
+# it gathers the far particles on the host
+@pytest.mark.parametrize("frac", [2, 8])
 @pytest.mark.parametrize("n", [1, 3001, 200000])
-def test_far_field_update_matches_oracle_bitwise(ctx, n):
-    pos, vel, temp, coarse, origin, idx = far_case(n, n)
+def test_far_field_update_matches_oracle_bitwise(ctx, n, frac):
+    pos, vel, temp, coarse, origin, idx = far_case(n, n, frac)
     a = [pos.copy(), vel.copy(), temp.copy()]
     b = [pos.copy(), vel.copy(), temp.copy()]
     ctx.far_field_update(*a, idx, coarse, 50.0, origin, 1.0)
