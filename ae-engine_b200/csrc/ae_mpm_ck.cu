@@ -201,7 +201,6 @@ __device__ __forceinline__ void mark_block(const CkArgs& a, uint32_t b, uint32_t
 template <bool POW2>
 __device__ __forceinline__ void scatter(const CkArgs& a, V3 pos, V3 vel, const M3& B, const M3& F, float rest_volume,
                                         float mass) {
-  const float h = a.h;
   Stencil st;
   make_stencil<POW2>(st, pos, a.sp, a.gn, true);
   const float mu = a.youngs / (2.0f * (1.0f + a.poisson));

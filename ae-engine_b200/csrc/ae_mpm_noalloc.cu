@@ -32,6 +32,7 @@ constexpr uint64_t kHistWords = uint64_t(aemp::kMaxRadix) * kTiles;
 constexpr uint64_t kTotalsWords = 4 * uint64_t(aemp::kMaxRadix);
 constexpr uint64_t kScratchWords = 2 * kHistWords + kTotalsWords + 2 * kMaxKeys;
 constexpr uint64_t kNoallocScratchBytes = kScratchWords * sizeof(uint32_t);
+static_assert(kNoallocScratchBytes <= (16ull << 20), "the no-allocation scratch array stays under 16 MB per device");
 
 static __device__ __align__(256) uint32_t g_sort_scratch[kScratchWords];
 
