@@ -85,8 +85,8 @@ def build_cuda(force: bool = False) -> str:
 
 def build_host_test(force: bool = False) -> str:
     src = os.path.join(ROOT, "tests", "cpp", "test_host_mirror.cpp")
-    hdr = os.path.join(HERE, "host", "ae_mpm_host.hpp")
-    deps = [src, hdr, os.path.join(ROOT, "include", "ae_mpm.h"), LIB]
+    hdrs = [os.path.join(HERE, "host", h) for h in ("ae_mpm_host.hpp", "ae_ck_mpm_host.hpp")]
+    deps = [src] + hdrs + [os.path.join(ROOT, "include", "ae_mpm.h"), LIB]
     if force or _stale(HOST_TEST, deps):
         _run(["g++", "-O2", "-std=c++17", "-o", HOST_TEST, src, "-I" + os.path.join(ROOT, "include"),
               "-I" + os.path.join(HERE, "host"), "-L" + BUILD, "-lae_mpm", "-Wl,-rpath,$ORIGIN", "-lpthread"])

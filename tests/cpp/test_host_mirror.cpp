@@ -5,13 +5,16 @@
 //   test_water_pressure          ae_particle/src/mpm_solver.rs:1659-1711
 //   test_steel_rigid_fall        ae_particle/src/mpm_solver.rs:1713-1745
 // plus the engine's near-field call shape (ae_engine/src/managers/simulation.rs:573-581) with an
-// index list, the velocity-only mid-field call (:598-607), and the panic paths.
+// index list, the velocity-only mid-field call (:598-607), and the panic paths; and the CK-MPM
+// module's own tests (ae_compute/src/ck_mpm.rs:510-781) through the CkMpmSolver mirror
+// (ae-engine_b200/host/ae_ck_mpm_host.hpp), with the assertions the Rust tests make.
 // Prints one line per test and exits non-zero if any failed.
 #include <cmath>
 #include <cstdio>
 #include <functional>
 #include <string>
 
+#include "ae_ck_mpm_host.hpp"
 #include "ae_mpm_host.hpp"
 
 using namespace ae_particle;
@@ -178,6 +181,150 @@ int main() {
     Grid grid = Grid::create(8, 8, 8, 0.25f);
     mpm_step_parallel_with_grid(buf, grid, MpmConfig{}, {}, {}, 0.016f, {});
     if (buf.count != 1) return std::string("lifetimes were updated on an empty call");
+    return std::string();
+  });
+
+  // ---------------------------------------------------------------- CK-MPM (ck_mpm.rs:510-781)
+  using ae_compute::CkMpmConfig;
+  using ae_compute::CkMpmParticle;
+  using ae_compute::CkMpmSolver;
+  using ae_compute::Mat3;
+  using ae_compute::Vec3;
+  auto cfg = [](auto f) {
+    CkMpmConfig c;
+    f(c);
+    return c;
+  };
+  auto block = [](CkMpmSolver& s, int n, Vec3 o, float d, float mass, float vol) {
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j)
+        for (int k = 0; k < n; ++k)
+          s.add_particle(CkMpmParticle::new_(Vec3{o.x + i * d, o.y + j * d, o.z + k * d}, mass, vol));
+  };
+  auto finite_state = [](const CkMpmSolver& s) {
+    for (const auto& p : s.particles)
+      if (!std::isfinite(p.position.x) || !std::isfinite(p.velocity.x) || !std::isfinite(p.deformation.determinant()))
+        return false;
+    return true;
+  };
+
+  run("test_ckmpm_config_default", [] {
+    CkMpmConfig c;
+    if (!(c.dt > 0 && c.grid_h > 0 && c.grid_n > 0 && c.density > 0)) return std::string("bad defaults");
+    return std::string();
+  });
+  run("test_ckmpm_particle_creation", [] {
+    CkMpmParticle p = CkMpmParticle::new_(Vec3{0.5f, 0.5f, 0.5f}, 1.0f, 0.001f);
+    if (!(p.position.x == 0.5f && p.position.y == 0.5f && p.position.z == 0.5f)) return std::string("position");
+    if (p.mass != 1.0f || !(p.deformation == Mat3::identity())) return std::string("mass or deformation");
+    return std::string();
+  });
+  run("test_ckmpm_solver_creation", [] {
+    CkMpmSolver s(CkMpmConfig{});
+    if (!s.particles.empty() || s.grid_a.empty()) return std::string("solver state");
+    return std::string();
+  });
+  run("test_ckmpm_weight_zero_outside_support", [] {
+    if (CkMpmSolver::weight(0.15f, 0.1f) != 0.0f || CkMpmSolver::weight(-0.15f, 0.1f) != 0.0f)
+      return std::string("nonzero weight outside the support");
+    return std::string();
+  });
+  run("test_ckmpm_weight_nonzero_inside", [] {
+    const float w = CkMpmSolver::weight(0.0f, 0.1f), w2 = CkMpmSolver::weight(0.05f, 0.1f);
+    if (!(w > 0.0f && w2 > 0.0f && w2 < w)) return "weights " + std::to_string(w) + " " + std::to_string(w2);
+    return std::string();
+  });
+  run("test_ckmpm_single_particle_no_crash", [&] {
+    CkMpmSolver s(cfg([](CkMpmConfig& c) { c.grid_n = 16, c.grid_h = 0.1f; }));
+    s.add_particle(CkMpmParticle::new_(Vec3{0.5f, 0.5f, 0.5f}, 1.0f, 0.001f));
+    s.step();
+    return s.particles.size() == 1 ? std::string() : std::string("particle count");
+  });
+  run("test_ckmpm_particle_falls_under_gravity", [&] {
+    CkMpmSolver s(cfg([](CkMpmConfig& c) {
+      c.dt = 0.01f, c.grid_n = 16, c.grid_h = 0.1f, c.gravity = Vec3{0, -9.81f, 0};
+      c.bounds_min = Vec3{-2, -2, -2}, c.bounds_max = Vec3{2, 2, 2};
+    }));
+    s.add_particle(CkMpmParticle::new_(Vec3{0.8f, 1.5f, 0.8f}, 1.0f, 0.001f));
+    const float y0 = s.particles[0].position.y;
+    s.step();
+    const float y1 = s.particles[0].position.y;
+    return y1 < y0 ? std::string() : "should fall: " + std::to_string(y0) + " -> " + std::to_string(y1);
+  });
+  run("test_ckmpm_boundary_collision", [&] {
+    CkMpmSolver s(cfg([](CkMpmConfig& c) {
+      c.dt = 0.01f, c.grid_n = 32, c.grid_h = 0.05f, c.gravity = Vec3{0, -20, 0};
+      c.bounds_min = Vec3{0, 0, 0}, c.bounds_max = Vec3{1.6f, 1.6f, 1.6f};
+    }));
+    s.add_particle(CkMpmParticle::new_(Vec3{0.8f, 1.5f, 0.8f}, 1.0f, 0.001f));
+    for (int i = 0; i < 300; ++i) s.step();
+    const float y = s.particles[0].position.y;
+    return (y < 0.5f && y >= -0.1f) ? std::string() : "y = " + std::to_string(y);
+  });
+  run("test_ckmpm_volume_ratio_finite", [] {
+    CkMpmSolver s(CkMpmConfig{});
+    s.add_particle(CkMpmParticle::new_(Vec3{0.5f, 0.5f, 0.5f}, 1.0f, 0.001f));
+    for (int i = 0; i < 10; ++i) s.step();
+    const float r = s.average_volume_ratio();
+    return std::isfinite(r) ? std::string() : "ratio " + std::to_string(r);
+  });
+  run("test_ckmpm_multiple_particles", [&] {
+    CkMpmSolver s(cfg([](CkMpmConfig& c) {
+      c.grid_n = 16, c.grid_h = 0.1f, c.bounds_min = Vec3{-1, -1, -1}, c.bounds_max = Vec3{2, 2, 2};
+    }));
+    block(s, 3, Vec3{0.5f, 0.5f, 0.5f}, 0.05f, 1.0f, 0.0001f);
+    for (int i = 0; i < 20; ++i) s.step();
+    return finite_state(s) ? std::string() : std::string("NaN in the state");
+  });
+  run("test_ckmpm_kinetic_energy", [&] {
+    CkMpmSolver s(cfg([](CkMpmConfig& c) { c.gravity = Vec3{0, 0, 0}; }));
+    CkMpmParticle p = CkMpmParticle::new_(Vec3{0.5f, 0.5f, 0.5f}, 2.0f, 0.001f);
+    p.velocity = Vec3{1.0f, 0.0f, 0.0f};
+    s.add_particle(p);
+    const float ke = s.kinetic_energy();
+    return std::fabs(ke - 1.0f) < 1e-4f ? std::string() : "ke " + std::to_string(ke);
+  });
+  run("test_ckmpm_apic_affine_nonzero", [&] {  // the reference asserts only that the step runs
+    CkMpmSolver s(cfg([](CkMpmConfig& c) {
+      c.dt = 0.005f, c.grid_n = 16, c.grid_h = 0.1f;
+      c.bounds_min = Vec3{-1, -1, -1}, c.bounds_max = Vec3{2, 2, 2};
+    }));
+    for (int i = 0; i < 3; ++i) s.add_particle(CkMpmParticle::new_(Vec3{0.5f + i * 0.05f, 1.0f, 0.5f}, 1.0f, 0.0001f));
+    s.step();
+    return finite_state(s) ? std::string() : std::string("NaN in the state");
+  });
+  run("test_ckmpm_elastic_deformation", [&] {
+    CkMpmSolver s(cfg([](CkMpmConfig& c) {
+      c.dt = 0.001f, c.grid_n = 16, c.grid_h = 0.1f, c.youngs_modulus = 1e4f;
+      c.bounds_min = Vec3{-1, -1, -1}, c.bounds_max = Vec3{2, 2, 2};
+    }));
+    block(s, 4, Vec3{0.6f, 0.6f, 0.6f}, 0.04f, 0.01f, 0.0001f);
+    for (int i = 0; i < 50; ++i) s.step();
+    const float f1 = s.particles[0].deformation.determinant();
+    return (std::isfinite(f1) && std::fabs(f1) < 100.0f) ? std::string() : "det " + std::to_string(f1);
+  });
+  run("test_ckmpm_dual_grid_flag", [&] {
+    for (bool dual : {true, false}) {
+      CkMpmSolver s(cfg([dual](CkMpmConfig& c) { c.grid_n = 16, c.grid_h = 0.1f, c.dual_grid = dual; }));
+      s.add_particle(CkMpmParticle::new_(Vec3{0.5f, 0.5f, 0.5f}, 1.0f, 0.001f));
+      s.step();
+      if (!std::isfinite(s.particles[0].position.x)) return std::string("dual_grid=") + (dual ? "true" : "false");
+    }
+    return std::string();
+  });
+  run("test_ckmpm_no_nan_long_run", [&] {
+    CkMpmSolver s(cfg([](CkMpmConfig& c) {
+      c.dt = 0.002f, c.grid_n = 24, c.grid_h = 0.05f, c.youngs_modulus = 1e3f;
+      c.bounds_min = Vec3{0, 0, 0}, c.bounds_max = Vec3{1.2f, 1.2f, 1.2f};
+    }));
+    block(s, 3, Vec3{0.5f, 0.8f, 0.5f}, 0.03f, 0.01f, 0.0001f);
+    for (int step = 0; step < 200; ++step) {
+      s.step();
+      if (step % 50 == 49)
+        for (const auto& p : s.particles)
+          if (!std::isfinite(p.position.x) || !std::isfinite(p.velocity.x))
+            return "NaN at step " + std::to_string(step);
+    }
     return std::string();
   });
 
