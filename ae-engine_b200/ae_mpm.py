@@ -186,6 +186,7 @@ SIGNATURES = {
     "ae_mpm_ck_config_default": (None, [C.POINTER(CkConfig)]),
     "ae_mpm_ck_step": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(CkConfig), C.c_uint32]),
     "ae_mpm_ck_step_timed": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(CkConfig), C.c_uint32, C.POINTER(C.c_double)]),
+    "ae_mpm_ck_step_deterministic": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(CkConfig), C.c_uint32]),
     "ae_mpm_ck_stats_compute": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(CkStats)]),
     "ae_mpm_ck_weights": (C.c_int, [_P, _P, C.c_uint64, C.c_float, _P, _P]),
     "ae_mpm_world_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(TuneResult)]),
@@ -417,11 +418,13 @@ class Context:
         return tr.value
 
     # CK-MPM solver (ae_compute/src/ck_mpm.rs): particles are (n, 26) float32 records
-    def ck_step(self, particles: np.ndarray, config: CkConfig, steps: int = 1) -> None:
-        """`steps` x CkMpmSolver::step, in place."""
+    def ck_step(self, particles: np.ndarray, config: CkConfig, steps: int = 1, deterministic: bool = False) -> None:
+        """`steps` x CkMpmSolver::step, in place.  deterministic: node sums in particle order
+        (bitwise reproducible, the reference's summation order)."""
         if particles.dtype != np.float32 or not particles.flags.c_contiguous or particles.shape[-1] != CK_RECORD:
             raise ValueError("particles must be a C-contiguous (n, 26) float32 array")
-        self.check(self.lib.ae_mpm_ck_step(self.h, particles.ctypes.data, particles.shape[0], C.byref(config), steps))
+        fn = self.lib.ae_mpm_ck_step_deterministic if deterministic else self.lib.ae_mpm_ck_step
+        self.check(fn(self.h, particles.ctypes.data, particles.shape[0], C.byref(config), steps))
 
     def ck_stats(self, particles: np.ndarray):
         """(kinetic_energy, average_velocity (3,), average_volume_ratio)."""

@@ -208,6 +208,13 @@ extern "C" {
         config: *const ae_mpm_ck_config,
         steps: u32,
     ) -> c_int;
+    pub fn ae_mpm_ck_step_deterministic(
+        ctx: *mut ae_mpm_ctx,
+        particles: *mut ae_mpm_ck_particle,
+        n: u64,
+        config: *const ae_mpm_ck_config,
+        steps: u32,
+    ) -> c_int;
     pub fn ae_mpm_ck_step_timed(
         ctx: *mut ae_mpm_ctx,
         particles: *mut ae_mpm_ck_particle,
@@ -472,6 +479,15 @@ pub fn mpss_housekeeping(
 /// `steps` x CkMpmSolver::step (ck_mpm.rs:187-480) on the caller's particles, in place.
 pub fn ck_step(particles: &mut [ae_mpm_ck_particle], config: &ae_mpm_ck_config, steps: u32) -> Result<(), String> {
     check(unsafe { ae_mpm_ck_step(ctx(), particles.as_mut_ptr(), particles.len() as u64, config, steps) })
+}
+
+/// The same steps with node sums in the reference's particle order: bitwise reproducible.
+pub fn ck_step_deterministic(
+    particles: &mut [ae_mpm_ck_particle],
+    config: &ae_mpm_ck_config,
+    steps: u32,
+) -> Result<(), String> {
+    check(unsafe { ae_mpm_ck_step_deterministic(ctx(), particles.as_mut_ptr(), particles.len() as u64, config, steps) })
 }
 
 /// kinetic_energy, average_velocity, average_volume_ratio (ck_mpm.rs:484-503).

@@ -707,15 +707,14 @@ void ae_mpm_ck_config_default(ae_mpm_ck_config* out) {
   out->dual_grid = 1;
 }
 
-int ae_mpm_ck_step(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm_ck_config* config,
-                   uint32_t steps) {
-  return ae_mpm_ck_step_timed(ctx, particles, n, config, steps, nullptr);
-}
-
-int ae_mpm_ck_step_timed(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm_ck_config* config,
-                         uint32_t steps, double kernel_ms[2]) {
+namespace {
+// ae_mpm_ck_step / _timed / _deterministic: host records are staged through the context
+int ck_run(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm_ck_config* config, uint32_t steps,
+           double* kernel_ms, bool deterministic) {
   if (!ctx) return AE_MPM_EINVAL;
   if (kernel_ms) kernel_ms[0] = kernel_ms[1] = 0.0;
+  if (deterministic && n >= (1ull << 32))
+    return fail(ctx, AE_MPM_EINVAL, "ck_step_deterministic: more than 2^32 - 1 particles");
   if (!config || (n && !particles)) return fail(ctx, AE_MPM_EINVAL, "ck_step: null config or particles");
   if (config->grid_n > 1024) return fail(ctx, AE_MPM_EINVAL, "ck_step: grid_n above 1024");
   if (n == 0 || steps == 0) return AE_MPM_OK;
@@ -723,8 +722,11 @@ int ae_mpm_ck_step_timed(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_
   if (rc) return rc;
   aemp::CkWork* ck = ck_work(ctx);
   cudaError_t e;
+  auto run = [&](ae_mpm_ck_particle* p) {
+    return deterministic ? ck->step_deterministic(p, n, *config, steps, 0) : ck->step(p, n, *config, steps, 0, kernel_ms);
+  };
   if (is_device_ptr(particles)) {
-    e = ck->step(particles, n, *config, steps, 0, kernel_ms);
+    e = run(particles);
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
   } else {
     const size_t bytes = n * sizeof(ae_mpm_ck_particle);
@@ -732,12 +734,28 @@ int ae_mpm_ck_step_timed(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_
     if (rc) return rc;
     auto* d = static_cast<ae_mpm_ck_particle*>(ctx->dstage);
     e = cudaMemcpyAsync(d, particles, bytes, cudaMemcpyHostToDevice, 0);
-    if (e == cudaSuccess) e = ck->step(d, n, *config, steps, 0, kernel_ms);
+    if (e == cudaSuccess) e = run(d);
     if (e == cudaSuccess) e = cudaMemcpyAsync(particles, d, bytes, cudaMemcpyDeviceToHost, 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
   }
   if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("ck_step: ") + cudaGetErrorString(e));
   return AE_MPM_OK;
+}
+}  // namespace
+
+int ae_mpm_ck_step(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm_ck_config* config,
+                   uint32_t steps) {
+  return ck_run(ctx, particles, n, config, steps, nullptr, false);
+}
+
+int ae_mpm_ck_step_timed(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm_ck_config* config,
+                         uint32_t steps, double kernel_ms[2]) {
+  return ck_run(ctx, particles, n, config, steps, kernel_ms, false);
+}
+
+int ae_mpm_ck_step_deterministic(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_t n,
+                                 const ae_mpm_ck_config* config, uint32_t steps) {
+  return ck_run(ctx, particles, n, config, steps, nullptr, true);
 }
 
 int ae_mpm_ck_stats_compute(ae_mpm_ctx* ctx, const ae_mpm_ck_particle* particles, uint64_t n, ae_mpm_ck_stats* out) {

@@ -197,18 +197,38 @@ __device__ __forceinline__ void mark_block(const CkArgs& a, uint32_t b, uint32_t
   a.flags[b] = 1u;
 }
 
+// The first Piola stress of the force pass (:262-268): P = mu (F - F^-T) + lambda ln(max(det F, 1e-10)) F^-T
+__device__ __forceinline__ M3 piola_stress(const CkArgs& a, const M3& F) {
+  const float mu = a.youngs / (2.0f * (1.0f + a.poisson));
+  const float lambda = a.youngs * a.poisson / ((1.0f + a.poisson) * (1.0f - 2.0f * a.poisson));
+  const float fdet = fmaxf(detm(F), 1e-10f);
+  const M3 fit = inversem(transposem(F));
+  const float ln_j = float(log(double(fdet)));
+  return addm(scalem(subm(F, fit), mu), scalem(fit, lambda * ln_j));
+}
+
+// One particle's contribution to one node (:221-240 and :276-318): wm = w m to the mass, (v + B d) wm
+// to the momentum, -V0 P grad w (clamped to |f| <= 1e4) to the force.  Both the atomic scatter and
+// the deterministic node gather call this, so their contributions are the same bits.
+__device__ __forceinline__ void node_contribution(float wx, float wy, float wz, float gx, float gy, float gz, V3 diff,
+                                                  V3 vel, const M3& B, const M3& P, float mass, float coeff, float& wm,
+                                                  V3& mom, V3& force) {
+  wm = wx * wy * wz * mass;
+  const V3 vg = vel + mulv(B, diff);
+  mom = vg * wm;
+  const V3 grad{gx * wy * wz, wx * gy * wz, wx * wy * gz};
+  force = mulv(P, grad) * coeff;
+  float fl;
+  if (above(force, 9.9e7f, 1e4f, &fl)) force = force * (1e4f / fl);
+}
+
 // P2G (:200-242) and the force pass (:253-320) of one particle
 template <bool POW2>
 __device__ __forceinline__ void scatter(const CkArgs& a, V3 pos, V3 vel, const M3& B, const M3& F, float rest_volume,
                                         float mass) {
   Stencil st;
   make_stencil<POW2>(st, pos, a.sp, a.gn, true);
-  const float mu = a.youngs / (2.0f * (1.0f + a.poisson));
-  const float lambda = a.youngs * a.poisson / ((1.0f + a.poisson) * (1.0f - 2.0f * a.poisson));
-  const float fdet = fmaxf(detm(F), 1e-10f);
-  const M3 fit = inversem(transposem(F));
-  const float ln_j = float(log(double(fdet)));
-  const M3 P = addm(scalem(subm(F, fit), mu), scalem(fit, lambda * ln_j));
+  const M3 P = piola_stress(a, F);
   const float coeff = -rest_volume;
   uint32_t last = 0xffffffffu;
 #pragma unroll
@@ -219,14 +239,10 @@ __device__ __forceinline__ void scatter(const CkArgs& a, V3 pos, V3 vel, const M
       for (int di = 0; di < 2; ++di) {
         if (!live(st, di, dj, dk)) continue;
         const V3 diff{st.diff[0][di], st.diff[1][dj], st.diff[2][dk]};
-        const float wx = st.w[0][di], wy = st.w[1][dj], wz = st.w[2][dk];
-        const float wm = wx * wy * wz * mass;
-        const V3 vg = vel + mulv(B, diff);
-        const V3 mom = vg * wm;
-        const V3 grad{st.gw[0][di] * wy * wz, wx * st.gw[1][dj] * wz, wx * wy * st.gw[2][dk]};
-        V3 force = mulv(P, grad) * coeff;
-        float fl;
-        if (above(force, 9.9e7f, 1e4f, &fl)) force = force * (1e4f / fl);
+        float wm;
+        V3 mom, force;
+        node_contribution(st.w[0][di], st.w[1][dj], st.w[2][dk], st.gw[0][di], st.gw[1][dj], st.gw[2][dk], diff, vel, B,
+                          P, mass, coeff, wm, mom, force);
         const uint32_t node = node_index(st.i[0][di], st.i[1][dj], st.i[2][dk], a.nb);
         atomicAdd(a.acc + 2 * node, make_float4(mom.x, mom.y, mom.z, wm));
         atomicAdd(a.acc + 2 * node + 1, make_float4(force.x, force.y, force.z, 0.0f));
@@ -437,6 +453,133 @@ __global__ void __launch_bounds__(kGridThreads) ck_grid_kernel(CkArgs a, float4*
   }
 }
 
+// ------------------------------------------------------------------ deterministic mode
+// P2G as a gather in particle order: particles are sorted (stably) by base cell, every touched node
+// merges the particle lists of the 8 cells whose stencils reach it by particle index, and adds the
+// contributions in that order, which is the order of the reference's serial loops (:201, :262).
+// Each contribution is the atomic scatter's (node_contribution), so node sums, and with them the
+// whole step, equal the reference's bit for bit except where ln(det F) differs.
+//
+// Cell key of a particle with base cell c = floor(x / h) (per axis): ((cz+1)(gn+1) + cy+1)(gn+1)
+// + cx+1 when -1 <= c <= gn-1 on every axis (the particle has a node in the grid), else the dead
+// key (gn+1)^3, which sorts last and belongs to no cell.
+
+template <bool POW2>
+__global__ void __launch_bounds__(256) ck_det_prep_kernel(CkArgs a, uint32_t* keys, float* stress) {
+  const uint32_t g1 = uint32_t(a.gn) + 1u;
+  for (uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < a.n; q += uint64_t(gridDim.x) * blockDim.x) {
+    const float* r = a.rec + q * kRecFloats;
+    const V3 pos{r[0], r[1], r[2]};
+    const M3 F{{r[15], r[16], r[17]}, {r[18], r[19], r[20]}, {r[21], r[22], r[23]}};
+    Stencil st;
+    make_stencil<POW2>(st, pos, a.sp, a.gn, true);
+    uint32_t last = 0xffffffffu;
+#pragma unroll
+    for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+      for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+        for (int di = 0; di < 2; ++di)
+          if (live(st, di, dj, dk)) mark_block(a, node_index(st.i[0][di], st.i[1][dj], st.i[2][dk], a.nb) >> 6, last);
+    bool in = true;
+    uint32_t kc[3];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      const int c = st.i[ax][0];
+      in = in && c >= -1 && c <= a.gn - 1;
+      kc[ax] = uint32_t(c + 1);
+    }
+    keys[q] = in ? (kc[2] * g1 + kc[1]) * g1 + kc[0] : g1 * g1 * g1;
+    const M3 P = piola_stress(a, F);
+    float* o = stress + 9 * q;
+    o[0] = P.c0.x, o[1] = P.c0.y, o[2] = P.c0.z, o[3] = P.c1.x, o[4] = P.c1.y, o[5] = P.c1.z;
+    o[6] = P.c2.x, o[7] = P.c2.y, o[8] = P.c2.z;
+  }
+}
+
+// [begin, end) of every cell's run in the sorted order (set), or back to empty (clear)
+template <bool SET>
+__global__ void __launch_bounds__(256) ck_det_ranges_kernel(const uint32_t* skeys, uint64_t n, uint32_t dead,
+                                                            uint2* range) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t k = skeys[i];
+    if (k == dead) continue;
+    const bool first = i == 0 || skeys[i - 1] != k;
+    if (SET) {
+      if (first) range[k].x = uint32_t(i);
+      if (i + 1 == n || skeys[i + 1] != k) range[k].y = uint32_t(i + 1);
+    } else if (first) {
+      range[k] = make_uint2(0u, 0u);
+    }
+  }
+}
+
+// Every node of the listed blocks: the in-order merge of its 8 cells' particles, accumulated the
+// way the reference accumulates; nodes outside the grid (padding blocks) get zeros.
+template <bool POW2>
+__global__ void __launch_bounds__(256) ck_det_nodes_kernel(CkArgs a, const uint32_t* perm, const uint2* range,
+                                                           const float* stress) {
+  const uint32_t count = __ldg(a.count);
+  const int local = threadIdx.x & 63;
+  const uint32_t nb = uint32_t(a.nb), g1 = uint32_t(a.gn) + 1u;
+  const float h = a.h;
+  for (uint32_t item = blockIdx.x * (kGridThreads / 64) + (threadIdx.x >> 6); item < count;
+       item += gridDim.x * (kGridThreads / 64)) {
+    const uint32_t b = a.list[item];
+    const int i = int((b % nb) * 4u + uint32_t(local & 3)), j = int(((b / nb) % nb) * 4u + uint32_t((local >> 2) & 3)),
+              k = int((b / (nb * nb)) * 4u + uint32_t(local >> 4));
+    float m = 0.0f;
+    V3 mom_sum{0.0f, 0.0f, 0.0f}, force_sum{0.0f, 0.0f, 0.0f};
+    if (i < a.gn && j < a.gn && k < a.gn) {
+      uint32_t head[8], end[8], cur[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const uint32_t key = (uint32_t(k - (q >> 2) + 1) * g1 + uint32_t(j - ((q >> 1) & 1) + 1)) * g1 +
+                             uint32_t(i - (q & 1) + 1);
+        const uint2 r = range[key];
+        head[q] = r.x;
+        end[q] = r.y;
+        cur[q] = r.x < r.y ? perm[r.x] : 0xffffffffu;
+      }
+      const V3 node{(float(i) + 0.5f) * h, (float(j) + 0.5f) * h, (float(k) + 0.5f) * h};
+      for (;;) {
+        uint32_t p = 0xffffffffu;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) p = cur[q] < p ? cur[q] : p;
+        if (p == 0xffffffffu) break;
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (cur[q] == p) {  // particle indices are unique: exactly one list holds p
+            ++head[q];
+            cur[q] = head[q] < end[q] ? perm[head[q]] : 0xffffffffu;
+          }
+        const float* r = a.rec + uint64_t(p) * kRecFloats;
+        const V3 pos{r[0], r[1], r[2]};
+        const V3 diff = node - pos;
+        const float wx = ck_weight<POW2>(diff.x, a.sp), wy = ck_weight<POW2>(diff.y, a.sp),
+                    wz = ck_weight<POW2>(diff.z, a.sp);
+        const float gx = ck_weight_grad<POW2>(diff.x, a.sp), gy = ck_weight_grad<POW2>(diff.y, a.sp),
+                    gz = ck_weight_grad<POW2>(diff.z, a.sp);
+        const bool fin = isfinite(pos.x) && isfinite(pos.y) && isfinite(pos.z);
+        if (fin && ((wx == 0.0f && gx == 0.0f) || (wy == 0.0f && gy == 0.0f) || (wz == 0.0f && gz == 0.0f))) continue;
+        const V3 vel{r[3], r[4], r[5]};
+        const M3 B{{r[6], r[7], r[8]}, {r[9], r[10], r[11]}, {r[12], r[13], r[14]}};
+        const float* ps = stress + 9 * uint64_t(p);
+        const M3 P{{ps[0], ps[1], ps[2]}, {ps[3], ps[4], ps[5]}, {ps[6], ps[7], ps[8]}};
+        float wm;
+        V3 mom, force;
+        node_contribution(wx, wy, wz, gx, gy, gz, diff, vel, B, P, r[25], -r[24], wm, mom, force);
+        m = m + wm;
+        mom_sum = mom_sum + mom;
+        force_sum = force_sum + force;
+      }
+    }
+    const uint32_t node_id = b * 64u + uint32_t(local);
+    a.acc[2 * node_id] = make_float4(mom_sum.x, mom_sum.y, mom_sum.z, m);
+    a.acc[2 * node_id + 1] = make_float4(force_sum.x, force_sum.y, force_sum.z, 0.0f);
+  }
+}
+
 // kinetic_energy, average_velocity, average_volume_ratio (:484-503), summed in double
 __global__ void __launch_bounds__(256) ck_stats_kernel(const float* rec, uint64_t n, double* sums) {
   double s[5] = {0, 0, 0, 0, 0};
@@ -468,6 +611,10 @@ __global__ void ck_weights_kernel(const float* x, uint64_t n, Spacing sp, float*
 }  // namespace
 
 CkWork::~CkWork() {
+  cudaFree(det_keys_);
+  cudaFree(det_stress_);
+  cudaFree(det_range_);
+  sort_scratch_free(det_sort_);
   cudaFree(acc_);
   cudaFree(vel_);
   cudaFree(flags_);
@@ -502,11 +649,35 @@ cudaError_t CkWork::ensure(uint32_t grid_n) {
   return cudaSuccess;
 }
 
-cudaError_t CkWork::step(ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm_ck_config& cfg, uint32_t steps,
-                         cudaStream_t s, double* kernel_ms) {
-  launches_ = 0;
-  if (n == 0 || steps == 0) return cudaSuccess;
-  cudaError_t e = ensure(cfg.grid_n);
+namespace {
+// Kernel arguments for a call over grid buffers laid out for cfg.grid_n.  Sets *pow2 when the
+// divisions by h can be exact reciprocal multiplications.
+CkArgs make_args(float4* acc, float4* vel, uint32_t* flags, uint32_t* lists, ae_mpm_ck_particle* particles, uint64_t n,
+                 const ae_mpm_ck_config& cfg, bool* pow2) {
+  CkArgs a{};
+  a.rec = reinterpret_cast<float*>(particles);
+  a.n = n;
+  a.acc = acc;
+  a.vel = vel;
+  a.flags = flags;
+  a.list = lists;
+  a.gn = int(cfg.grid_n);
+  a.nb = int(cfg.grid_n ? (cfg.grid_n + 3) / 4 : 1);
+  a.h = cfg.grid_h, a.dt = cfg.dt, a.youngs = cfg.youngs_modulus, a.poisson = cfg.poissons_ratio;
+  a.sp = Spacing{cfg.grid_h, 0.0f, 0.0f};
+  int e2 = 0;
+  *pow2 = std::isfinite(cfg.grid_h) && cfg.grid_h > 0.0f && std::frexp(cfg.grid_h, &e2) == 0.5f && e2 - 1 >= -40 &&
+          e2 - 1 <= 40;
+  if (*pow2) a.sp.inv_h = std::ldexp(1.0f, 1 - e2), a.sp.inv_h3 = std::ldexp(1.0f, 3 * (1 - e2));
+  a.restitution = cfg.restitution;
+  for (int k = 0; k < 3; ++k) a.g[k] = cfg.gravity[k], a.bmin[k] = cfg.bounds_min[k], a.bmax[k] = cfg.bounds_max[k];
+  a.aligned16 = (reinterpret_cast<uintptr_t>(particles) & 15u) == 0;
+  return a;
+}
+}  // namespace
+
+cudaError_t CkWork::begin_call(uint32_t grid_n, cudaStream_t s) {
+  cudaError_t e = ensure(grid_n);
   if (e != cudaSuccess) return e;
   if (!clean_) {
     e = cudaMemsetAsync(acc_, 0, blocks_ * 64 * 2 * sizeof(float4), s);
@@ -514,25 +685,17 @@ cudaError_t CkWork::step(ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm
     if (e != cudaSuccess) return e;
     clean_ = true;
   }
-  e = cudaMemsetAsync(counts_, 0, 2 * sizeof(uint32_t), s);
+  return cudaMemsetAsync(counts_, 0, 2 * sizeof(uint32_t), s);
+}
+
+cudaError_t CkWork::step(ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm_ck_config& cfg, uint32_t steps,
+                         cudaStream_t s, double* kernel_ms) {
+  launches_ = 0;
+  if (n == 0 || steps == 0) return cudaSuccess;
+  cudaError_t e = begin_call(cfg.grid_n, s);
   if (e != cudaSuccess) return e;
-  CkArgs a{};
-  a.rec = reinterpret_cast<float*>(particles);
-  a.n = n;
-  a.acc = acc_;
-  a.vel = vel_;
-  a.flags = flags_;
-  a.gn = int(cfg.grid_n);
-  a.nb = int(cfg.grid_n ? (cfg.grid_n + 3) / 4 : 1);
-  a.h = cfg.grid_h, a.dt = cfg.dt, a.youngs = cfg.youngs_modulus, a.poisson = cfg.poissons_ratio;
-  a.sp = Spacing{cfg.grid_h, 0.0f, 0.0f};
-  int e2 = 0;
-  const bool pow2 = std::isfinite(cfg.grid_h) && cfg.grid_h > 0.0f && std::frexp(cfg.grid_h, &e2) == 0.5f &&
-                    e2 - 1 >= -40 && e2 - 1 <= 40;
-  if (pow2) a.sp.inv_h = std::ldexp(1.0f, 1 - e2), a.sp.inv_h3 = std::ldexp(1.0f, 3 * (1 - e2));
-  a.restitution = cfg.restitution;
-  for (int k = 0; k < 3; ++k) a.g[k] = cfg.gravity[k], a.bmin[k] = cfg.bounds_min[k], a.bmax[k] = cfg.bounds_max[k];
-  a.aligned16 = (reinterpret_cast<uintptr_t>(particles) & 15u) == 0;
+  bool pow2 = false;
+  CkArgs a = make_args(acc_, vel_, flags_, lists_, particles, n, cfg, &pow2);
   const unsigned pgrid = unsigned((n + kCkThreads - 1) / kCkThreads);
   const unsigned ggrid = unsigned(std::min<uint64_t>(148 * 4, (blocks_ + 4 * kGridU - 1) / (4 * kGridU)));
   const unsigned cgrid = unsigned(std::min<uint64_t>(148 * 8, (blocks_ + 255) / 256));
@@ -597,6 +760,78 @@ cudaError_t CkWork::step(ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm
     }
     for (auto x : ev) cudaEventDestroy(x);
   }
+  if (e != cudaSuccess) clean_ = false;
+  launches_ = launches;
+  return e;
+}
+
+cudaError_t CkWork::ensure_det(uint64_t n, uint32_t grid_n) {
+  const uint64_t g1 = uint64_t(grid_n) + 1, cells = g1 * g1 * g1;
+  cudaError_t e = cudaSuccess;
+  if (n > det_cap_) {
+    cudaFree(det_keys_);
+    cudaFree(det_stress_);
+    det_keys_ = nullptr, det_stress_ = nullptr, det_cap_ = 0;
+    sort_scratch_free(det_sort_);
+    e = cudaMalloc(&det_keys_, n * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&det_stress_, 9 * n * sizeof(float));
+    if (e == cudaSuccess) e = sort_scratch_alloc(det_sort_, n);
+    if (e != cudaSuccess) return e;
+    det_cap_ = n;
+  }
+  if (cells != det_cells_) {
+    cudaFree(det_range_);
+    det_range_ = nullptr, det_cells_ = 0;
+    e = cudaMalloc(&det_range_, cells * sizeof(uint2));
+    if (e == cudaSuccess) e = cudaMemset(det_range_, 0, cells * sizeof(uint2));  // every cell empty
+    if (e != cudaSuccess) return e;
+    det_cells_ = cells;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t CkWork::step_deterministic(ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm_ck_config& cfg,
+                                       uint32_t steps, cudaStream_t s) {
+  launches_ = 0;
+  if (n == 0 || steps == 0) return cudaSuccess;
+  cudaError_t e = begin_call(cfg.grid_n, s);
+  if (e == cudaSuccess) e = ensure_det(n, cfg.grid_n);
+  if (e != cudaSuccess) return e;
+  bool pow2 = false;
+  CkArgs a = make_args(acc_, vel_, flags_, lists_, particles, n, cfg, &pow2);
+  const uint32_t g1 = cfg.grid_n + 1u, dead = g1 * g1 * g1;
+  int key_bits = 1;
+  while (key_bits < 32 && (dead >> key_bits) != 0u) ++key_bits;
+  const unsigned pgrid = unsigned((n + kCkThreads - 1) / kCkThreads);
+  const unsigned sgrid = unsigned(std::min<uint64_t>(148 * 8, (n + 255) / 256));
+  const unsigned ngrid = unsigned(std::min<uint64_t>(148 * 8, (blocks_ + 3) / 4));
+  const unsigned ggrid = unsigned(std::min<uint64_t>(148 * 4, (blocks_ + 4 * kGridU - 1) / (4 * kGridU)));
+  const unsigned cgrid = unsigned(std::min<uint64_t>(148 * 8, (blocks_ + 255) / 256));
+  uint32_t launches = 0;
+  for (uint32_t st = 0; st < steps; ++st) {
+    a.count = counts_ + (st & 1);
+    a.next_count = counts_ + ((st + 1) & 1);
+    if (pow2)
+      ck_det_prep_kernel<true><<<sgrid, 256, 0, s>>>(a, det_keys_, det_stress_);
+    else
+      ck_det_prep_kernel<false><<<sgrid, 256, 0, s>>>(a, det_keys_, det_stress_);
+    const uint32_t *skeys = nullptr, *perm = nullptr;
+    launches += 1 + uint32_t(radix_sort_pairs(det_keys_, n, key_bits, det_sort_, s, &skeys, &perm));
+    ck_det_ranges_kernel<true><<<sgrid, 256, 0, s>>>(skeys, n, dead, det_range_);
+    ck_compact_kernel<<<cgrid, 256, 0, s>>>(flags_, blocks_, lists_, a.count, a.next_count);
+    if (pow2)
+      ck_det_nodes_kernel<true><<<ngrid, kGridThreads, 0, s>>>(a, perm, det_range_, det_stress_);
+    else
+      ck_det_nodes_kernel<false><<<ngrid, kGridThreads, 0, s>>>(a, perm, det_range_, det_stress_);
+    ck_grid_kernel<<<ggrid, kGridThreads, 0, s>>>(a, vel_);
+    ck_det_ranges_kernel<false><<<sgrid, 256, 0, s>>>(skeys, n, dead, det_range_);
+    if (pow2)
+      ck_particles_kernel<true, false, true><<<pgrid, kCkThreads, 0, s>>>(a);
+    else
+      ck_particles_kernel<true, false, false><<<pgrid, kCkThreads, 0, s>>>(a);
+    launches += 6;
+  }
+  e = cudaGetLastError();
   if (e != cudaSuccess) clean_ = false;
   launches_ = launches;
   return e;

@@ -93,6 +93,8 @@ class CkMpmSolver {
   CkMpmConfig config;
   std::vector<CkMpmParticle> particles;
   std::vector<GridNode> grid_a, grid_b;
+  // add node sums in particle order, as the reference does (bitwise reproducible, slower)
+  bool deterministic = false;
 
   explicit CkMpmSolver(const CkMpmConfig& c) : config(c) {
     const size_t n = c.grid_n + 2;
@@ -112,8 +114,10 @@ class CkMpmSolver {
   void step_n(uint32_t steps) {
     if (particles.empty()) return;
     const ae_mpm_ck_config c = to_c();
-    ae_particle::check(ae_mpm_ck_step(ae_particle::gpu_context(), reinterpret_cast<ae_mpm_ck_particle*>(particles.data()),
-                                      particles.size(), &c, steps));
+    auto* recs = reinterpret_cast<ae_mpm_ck_particle*>(particles.data());
+    ae_particle::check(deterministic
+                           ? ae_mpm_ck_step_deterministic(ae_particle::gpu_context(), recs, particles.size(), &c, steps)
+                           : ae_mpm_ck_step(ae_particle::gpu_context(), recs, particles.size(), &c, steps));
   }
 
   // :484-503

@@ -406,6 +406,15 @@ int ae_mpm_ck_step(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_t n, c
 int ae_mpm_ck_step_timed(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_t n, const ae_mpm_ck_config* config,
                          uint32_t steps, double kernel_ms[2]);
 
+/* ae_mpm_ck_step with each node's sums added in particle order, as the reference's serial loops
+ * add them (a per-node merge over particles sorted by cell instead of atomics): results are the
+ * same bits on every run, and equal the reference's bit for bit wherever ln(det F) agrees (the
+ * device takes the correctly rounded logarithm; glibc's logf differs from it by one ulp for a few
+ * percent of arguments).  Slower than ae_mpm_ck_step; at most 2^32 - 1 particles, and
+ * (grid_n + 1)^3 x 8 bytes of cell table on the device. */
+int ae_mpm_ck_step_deterministic(ae_mpm_ctx* ctx, ae_mpm_ck_particle* particles, uint64_t n,
+                                 const ae_mpm_ck_config* config, uint32_t steps);
+
 /* The solver's diagnostics over particles[0..n), summed on the device in double precision;
  * n = 0 gives 0, (0, 0, 0) and 1, as the reference's empty-solver cases do. */
 int ae_mpm_ck_stats_compute(ae_mpm_ctx* ctx, const ae_mpm_ck_particle* particles, uint64_t n,

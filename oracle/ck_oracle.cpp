@@ -90,7 +90,12 @@ struct OracleCkParticle {
   float position[3], velocity[3], affine[9], deformation[9], rest_volume, mass;
 };
 
-void oracle_ck_step(OracleCkParticle* ps, uint64_t n, const OracleCkConfig* cfg, uint32_t steps) {
+// correctly_rounded_ln: take f32::ln as the correctly rounded logarithm (the double-precision
+// log rounded to f32) instead of the C library's logf.  Only a checker for the device's
+// deterministic mode uses it, to isolate the one operation where the device and the reference's
+// libm may differ; the reference's semantics are correctly_rounded_ln = 0.
+void oracle_ck_step_ln(OracleCkParticle* ps, uint64_t n, const OracleCkConfig* cfg, uint32_t steps,
+                       int correctly_rounded_ln) {
   const float h = cfg->grid_h, dt = cfg->dt;
   const int32_t gn = int32_t(cfg->grid_n);
   const uint64_t np = uint64_t(gn) + 2;
@@ -149,7 +154,8 @@ void oracle_ck_step(OracleCkParticle* ps, uint64_t n, const OracleCkConfig* cfg,
       const M3 F = load(p.deformation);
       const float fdet = std::fmax(det(F), 1e-10f);
       const M3 fit = inverse(transpose(F));
-      const M3 P = add(scale(sub(F, fit), mu), scale(fit, lambda * std::log(fdet)));
+      const float ln_j = correctly_rounded_ln ? float(std::log(double(fdet))) : std::log(fdet);
+      const M3 P = add(scale(sub(F, fit), mu), scale(fit, lambda * ln_j));
       const float coeff = -p.rest_volume;
       for (int dk = 0; dk <= 1; ++dk)
         for (int dj = 0; dj <= 1; ++dj)
@@ -250,6 +256,10 @@ void oracle_ck_step(OracleCkParticle* ps, uint64_t n, const OracleCkConfig* cfg,
       }
     }
   }
+}
+
+void oracle_ck_step(OracleCkParticle* ps, uint64_t n, const OracleCkConfig* cfg, uint32_t steps) {
+  oracle_ck_step_ln(ps, n, cfg, steps, 0);
 }
 
 // CkMpmSolver::weight / weight_grad (:163-185), for known-answer tests

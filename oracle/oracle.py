@@ -66,6 +66,7 @@ def load():
     lib.oracle_far_field_update.argtypes = [V, V, V, V, C.c_uint64, V, C.c_uint64, f, V, f]
     lib.oracle_coarse_field_update.argtypes = [V, V, V, V, V, C.c_uint64, V, C.c_uint64, f, V, f]
     lib.oracle_ck_step.argtypes = [V, C.c_uint64, C.POINTER(M.CkConfig), C.c_uint32]
+    lib.oracle_ck_step_ln.argtypes = [V, C.c_uint64, C.POINTER(M.CkConfig), C.c_uint32, C.c_int]
     lib.oracle_ck_weight.restype = f
     lib.oracle_ck_weight.argtypes = [f, f]
     lib.oracle_ck_weight_grad.restype = f
@@ -233,12 +234,14 @@ def mpss_housekeeping(pos, vel, temperature, phase, material_idx, active, bounds
 
 
 # ---------------------------------------------------------------- CK-MPM (ae_compute/src/ck_mpm.rs)
-def ck_step(particles: np.ndarray, config: M.CkConfig, steps: int = 1) -> None:
-    """`steps` x CkMpmSolver::step (ck_mpm.rs:187-480) in place on (n, 26) float32 records."""
+def ck_step(particles: np.ndarray, config: M.CkConfig, steps: int = 1, correctly_rounded_ln: bool = False) -> None:
+    """`steps` x CkMpmSolver::step (ck_mpm.rs:187-480) in place on (n, 26) float32 records.
+    correctly_rounded_ln replaces the C library's logf (the reference's f32::ln) by the correctly
+    rounded logarithm, for checking the device's deterministic mode bit for bit."""
     if particles.dtype != np.float32 or not particles.flags.c_contiguous or particles.shape[-1] != M.CK_RECORD:
         raise ValueError("particles must be a C-contiguous (n, 26) float32 array")
-    load().oracle_ck_step(particles.ctypes.data if particles.size else None, particles.shape[0], C.byref(config),
-                          steps)
+    load().oracle_ck_step_ln(particles.ctypes.data if particles.size else None, particles.shape[0], C.byref(config),
+                             steps, 1 if correctly_rounded_ln else 0)
 
 
 def ck_weight(x: float, h: float) -> float:

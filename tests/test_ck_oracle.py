@@ -210,8 +210,9 @@ def finite(v):
     return all(np.isfinite(x) for x in v)
 
 
-def np_step(ps, cfg):
-    """One CkMpmSolver::step (ck_mpm.rs:187-480) on (n, 26) float32 records, in place."""
+def np_step(ps, cfg, cr_ln=False):
+    """One CkMpmSolver::step (ck_mpm.rs:187-480) on (n, 26) float32 records, in place.  cr_ln: the
+    correctly rounded logarithm instead of the C library's logf."""
     h, dt, gn = f32(cfg.grid_h), f32(cfg.dt), int(cfg.grid_n)
     grid = {}
 
@@ -245,7 +246,7 @@ def np_step(ps, cfg):
         pos, F = r[0:3], cols(r, 15)
         fdet = max(det(F), f32(1e-10))
         fit = inverse(transpose(F))
-        ln = f32(_libm.logf(float(fdet)))
+        ln = f32(np.log(np.float64(fdet))) if cr_ln else f32(_libm.logf(float(fdet)))
         P = [[f32(f32(f32(F[c][i] - fit[c][i]) * mu) + f32(fit[c][i] * f32(lam * ln))) for i in range(3)]
              for c in range(3)]
         coeff = f32(-r[24])
@@ -339,3 +340,18 @@ def test_oracle_matches_numpy_restatement_bitwise():
         np_step(b, cfg)
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     assert not np.array_equal(a, p)
+
+
+def test_oracle_with_correctly_rounded_ln_matches_numpy_restatement_bitwise():
+    # the oracle's checker option for the device's deterministic mode: only f32::ln changes
+    rng = np.random.default_rng(12)
+    n = 30
+    p = M.ck_particles(rng.uniform(0.3, 0.9, (n, 3)), 0.01, 1e-4, velocity=rng.normal(0, 1, (n, 3)))
+    p[:, 15:24] += rng.normal(0, 0.05, (n, 9)).astype(np.float32)
+    cfg = M.ck_config(dt=0.002, bounds_min=(0, 0, 0), bounds_max=(1.6, 1.6, 1.6))
+    a, b = p.copy(), p.copy()
+    for _ in range(2):
+        O.ck_step(a, cfg, 1, correctly_rounded_ln=True)
+        np_step(b, cfg, cr_ln=True)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+

@@ -326,3 +326,72 @@ def test_device_pointers_aligned_and_not(ctx):
         torch.cuda.synchronize()
         got = view.cpu().numpy().reshape(p0.shape)
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), offset
+
+
+# ------------------------------------------------ deterministic mode: node sums in particle order
+def ref_cr(cfg, p, steps):
+    """The oracle with the correctly rounded logarithm the device takes for f32::ln."""
+    q = np.array(p, np.float32, order="C")
+    O.ck_step(q, cfg, steps, correctly_rounded_ln=True)
+    return q
+
+
+def det(ctx, cfg, p, steps):
+    q = np.array(p, np.float32, order="C")
+    ctx.ck_step(q, cfg, steps, deterministic=True)
+    return q
+
+
+def assert_bitwise(got, want):
+    assert np.array_equal(np.isnan(got), np.isnan(want))
+    ok = ~np.isnan(want)
+    assert np.array_equal(got.view(np.uint32)[ok], want.view(np.uint32)[ok])
+
+
+@pytest.mark.parametrize("name,over,blk,steps", BLOCKS, ids=[b[0] for b in BLOCKS])
+def test_deterministic_reference_scenarios_are_bit_exact(ctx, name, over, blk, steps):
+    # the reference's chaotic block scenarios, every step bit for bit (given the same logarithm)
+    cfg = M.ck_config(**over)
+    p0 = block(*blk)
+    assert_bitwise(det(ctx, cfg, p0, steps), ref_cr(cfg, p0, steps))
+
+
+@pytest.mark.parametrize("n_side,grid_n,h,steps", [(20, 32, 0.05, 5), (64, 128, 1.0, 3), (40, 64, 0.7, 3)])
+def test_deterministic_dense_blocks_are_bit_exact(ctx, n_side, grid_n, h, steps):
+    # dense jittered blocks (8 particles per cell): IEEE-division and power-of-two paths
+    p0 = jittered_block(n_side, 0.5 * h, (8 * h, 9 * h, 8 * h), n_side, mass=1000 * (0.5 * h) ** 3,
+                        vol=(0.5 * h) ** 3)
+    p0[:, 15:24] += np.random.default_rng(n_side).normal(0, 0.01, (p0.shape[0], 9)).astype(f32)
+    cfg = M.ck_config(dt=min(5e-4, 0.05 * h / 10), grid_n=grid_n, grid_h=h, bounds_min=(0, 0, 0),
+                      bounds_max=(grid_n * h,) * 3)
+    assert_bitwise(det(ctx, cfg, p0, steps), ref_cr(cfg, p0, steps))
+
+
+def test_deterministic_runs_repeat_bitwise_and_agree_with_the_atomic_path(ctx):
+    cfg = M.ck_config(dt=0.002, grid_n=24, grid_h=0.05, youngs_modulus=1e3, bounds_min=(0, 0, 0),
+                      bounds_max=(1.2, 1.2, 1.2))
+    p0 = jittered_block(12, 0.025, (0.4, 0.6, 0.4), 5, mass=1e-3, vol=1e-6)
+    a, b = det(ctx, cfg, p0, 50), det(ctx, cfg, p0, 50)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    base, env = envelope(cfg, p0, 2)
+    assert_in_envelope(dev(ctx, cfg, p0, 2), base, env)
+    assert_in_envelope(det(ctx, cfg, p0, 2), base, env)
+
+
+def test_deterministic_edges(ctx):
+    # particles outside the grid (no cell), a NaN particle, an empty call, split calls
+    cfg = M.ck_config(grid_n=16, grid_h=0.1, bounds_min=(-1, -1, -1), bounds_max=(3, 3, 3))
+    pts = [(-0.5, 0.5, 0.5), (-0.03, 0.5, 0.5), (1.58, 1.55, 1.59), (2.5, 2.5, 2.5), (0.5, 0.5, 0.5),
+           (0.52, 0.5, 0.5), (0.53, 0.51, 0.5)]
+    p0 = M.ck_particles(pts, 1.0, 0.001, velocity=[(1, 2, 3)] * len(pts))
+    assert_bitwise(det(ctx, cfg, p0, 4), ref_cr(cfg, p0, 4))
+    p1 = p0.copy()
+    p1[4, 0] = np.nan
+    assert_bitwise(det(ctx, cfg, p1, 2), ref_cr(cfg, p1, 2))
+    e = np.zeros((0, 26), f32)
+    ctx.ck_step(e, cfg, 3, deterministic=True)
+    q = p0.copy()
+    for k in (1, 3):
+        ctx.ck_step(q, cfg, k, deterministic=True)
+    assert_bitwise(q, ref_cr(cfg, p0, 4))
+
