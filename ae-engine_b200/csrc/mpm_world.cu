@@ -1865,8 +1865,13 @@ class World final : public WorldBase {
                                                                       d_scenes_ + s, d_mats_);
       AE_TRY(cudaGetLastError());
     }
-    h_scenes_[s].p_count = uint32_t(n);
-    scenes_dirty_ = chunks_dirty_ = keys_stale_ = true;
+    // the same count keeps the scene table, the chunks and the captured graph (which replays from
+    // the upload's buffers); the cell keys are recomputed before the next substep either way
+    if (h_scenes_[s].p_count != uint32_t(n)) {
+      h_scenes_[s].p_count = uint32_t(n);
+      scenes_dirty_ = chunks_dirty_ = true;
+    }
+    keys_stale_ = true;
     return AE_MPM_OK;
   }
 
