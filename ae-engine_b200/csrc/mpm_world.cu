@@ -558,6 +558,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) p2g_lanes_kernel(
     if (uint32_t(run.w) == 0xffffffffu) continue;
     const int X = run.x, Y = run.y + nb, Z = run.z + nc;
     T m0 = 0, x0 = 0, y0 = 0, z0 = 0, m1 = 0, x1 = 0, y1 = 0, z1 = 0, m2 = 0, x2 = 0, y2 = 0, z2 = 0;
+#pragma unroll 2
     for (int i = s0 + grp; i < e0; i += 3) {
       const V4 u = colw[i * 9];
       const V4 r = wxw[i];
