@@ -874,6 +874,16 @@ def run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
     except Exception:
         pass
     budget = int(min(free * 0.6, 64 << 30)) if free else (32 << 30)
+    # warm-up, untimed: a few requests through a server of their own, so that first-use costs
+    # (module loading, the caching allocator's first blocks) do not land in the first rate's window
+    wrng = S.Rng(0xAE05 - 1 - 1000 * rank)
+    srv = M.Server(ctx, hbm_budget_bytes=budget, substeps_per_tick=20)
+    for _ in range(8):
+        sc, p, k = S.config5_request(wrng)
+        srv.submit(sc, p, min(k, 200))
+    srv.drain(600.0)
+    srv.poll(4096)
+    srv.close()
     out = []
     for ri, rate in enumerate(rates):
         rng = S.Rng(0xAE05 + 100 * ri + 1000 * rank)
