@@ -691,7 +691,7 @@ __global__ void __launch_bounds__(256) grid_update_kernel(WorldDev<T> w, uint32_
 #pragma unroll
     for (int u = 0; u < kU; ++u) {
       if (gb[u] == 0xffffffffu) continue;
-      const SceneDev<T>& sc = w.scenes[w.blk_scene[gb[u]]];
+      const SceneDev<T>& sc = w.scenes[w.one_scene ? 0u : w.blk_scene[gb[u]]];  // one scene: no lookup
       int i, j, k;
       block_coords(sc, gb[u], l, i, j, k);
       const uint64_t gi = uint64_t(gb[u]) * 64u + l;
