@@ -220,3 +220,36 @@ def test_config3_deterministic_runs_are_bitwise_equal(ctx):
         w.close()
     for f in ("pos", "vel", "F", "J", "C"):
         assert np.array_equal(getattr(outs[0], f), getattr(outs[1], f)), f
+
+
+# ------------------------------------------------------------------ chunking of the particle slots
+@pytest.mark.parametrize("spare", [0, 61, 700])
+@pytest.mark.parametrize("threads", [128, 256])
+def test_one_scene_chunks_equal_the_chunk_table(ctx, spare, threads):
+    # a world of one scene derives its CTA chunks arithmetically; a world of several reads them
+    # from a table.  With spare capacity the last live chunk is partial and later chunks hold only
+    # dead slots.  In deterministic mode scene 0 must come out bitwise the same either way.
+    import dataclasses
+    sc, p = S.tiny_scene(3001, 32, S.snow(), v=(1.0, -0.5, 0.25))
+    sc = dataclasses.replace(sc, max_particles=p.n + spare)
+    opts = dict(deterministic=1, block_threads=threads)
+    one = world_of(ctx, [sc], [p], **opts)
+    two = world_of(ctx, [sc, dataclasses.replace(sc)], [p, p], **opts)
+    for w in (one, two):
+        w.step(24)
+        assert w.sync(raise_on_error=False) == M.OK
+    a, b = one.download(0, p.n), two.download(0, p.n)
+    one.close()
+    two.close()
+    for f in ("pos", "vel", "F", "J", "C"):
+        assert np.array_equal(getattr(a, f), getattr(b, f)), f
+    assert np.isfinite(a.pos).all() and not np.array_equal(a.pos, p.pos)
+    # the atomic path (LANES P2G, chunked G2P): against the FP64 oracle, 1e-5 relative in positions
+    ref = p.astype(np.float64)
+    O.run(sc, ref, 24)
+    fast = world_of(ctx, [sc], [p], p2g_variant=M.P2G_LANES, block_threads=threads, sort_interval=4)
+    fast.step(24)
+    assert fast.sync(raise_on_error=False) == M.OK
+    g = fast.download(0, p.n)
+    fast.close()
+    assert rel(g.pos, ref.pos) <= 1e-5
