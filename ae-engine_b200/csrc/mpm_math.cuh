@@ -391,26 +391,31 @@ AE_HD void svd3(const T* F, T* U, T* s, T* V) {
 // relative gap below which two FP32 singular values count as near-degenerate (sqrt(eps_f32))
 constexpr double kSvdGapTol = 3.5e-4;
 
-// every singular value of F provably in [lo, hi] and det F > 0 (Gershgorin discs of F^T F inside
-// [lo^2, hi^2]): the snow clamp is then the identity map and needs no SVD
+// Whether the symmetric matrix [[a d e] [d b f] [e f c]] is positive definite: its leading
+// principal minors are all positive (Sylvester's criterion).
+template <class T>
+AE_HD bool sym3_positive_definite(T a, T b, T c, T d, T e, T f) {
+  const T m2 = a * b - d * d;
+  const T m3 = a * (b * c - f * f) - d * (d * c - f * e) + e * (d * f - b * e);
+  return a > T(0) && m2 > T(0) && m3 > T(0);
+}
+
+// Every singular value of F strictly inside (lo, hi) and det F > 0, so the snow clamp is the
+// identity map and needs no SVD.  The squared singular values are the eigenvalues of M = F^T F,
+// so the test is that M - lo^2 I and hi^2 I - M are both positive definite.  It is exact up to
+// rounding in the minors: F whose singular values come within rounding of lo or hi may go either
+// way, and those are clamped by at most that rounding.
 template <class T>
 AE_HD bool clamp_is_identity(const T* F, T lo, T hi) {
-  T a[9];
+  T m[3][3];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) a[i * 3 + j] = F[0 * 3 + i] * F[0 * 3 + j] + F[1 * 3 + i] * F[1 * 3 + j] + F[2 * 3 + i] * F[2 * 3 + j];
+    for (int j = i; j < 3; ++j) m[i][j] = F[0 * 3 + i] * F[0 * 3 + j] + F[1 * 3 + i] * F[1 * 3 + j] + F[2 * 3 + i] * F[2 * 3 + j];
   const T lo2 = lo * lo, hi2 = hi * hi;
-  bool ok = true;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    T r = T(0);
-#pragma unroll
-    for (int j = 0; j < 3; ++j)
-      if (j != i) r += t_abs(a[i * 3 + j]);
-    ok = ok && !(a[i * 4] - r < lo2) && !(a[i * 4] + r > hi2);
-  }
-  return ok && det3(F) > T(0);
+  return sym3_positive_definite(m[0][0] - lo2, m[1][1] - lo2, m[2][2] - lo2, m[0][1], m[0][2], m[1][2]) &&
+         sym3_positive_definite(hi2 - m[0][0], hi2 - m[1][1], hi2 - m[2][2], -m[0][1], -m[0][2], -m[1][2]) &&
+         det3(F) > T(0);
 }
 
 // FP32 SVD, redone in FP64 when a near-degenerate pair straddles a clamp threshold

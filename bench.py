@@ -57,14 +57,16 @@ def l2_note(n_particles):
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps; default: the workload's run length in substeps (RUN_LENGTH), else 200")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="snow", choices=["snow", "jelly", "dam", "batched", "served", "tick", "ck"])
     ap.add_argument("--ck-h", type=float, default=1.0,
                     help="ck: grid spacing (the scene scales with it); 1 takes the exact power-of-two division path")
     ap.add_argument("--e2e-reps", type=int, default=3)
-    ap.add_argument("--e2e-substeps", type=int, default=500)
+    ap.add_argument("--e2e-substeps", type=int, default=None,
+                    help="substeps per end-to-end call; default: the workload's run length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--variant", choices=["lanes", "tile", "warp_agg", "global"],
@@ -619,6 +621,9 @@ def run_ck(args, rank, local, world_size, pg, reference=False):
             "cpu_baseline": cpu, "gpu_launches": 1 + 3 * steps, "clocks": clk}), flush=True)
 
 
+STAGE_SUBSTEPS = 20
+
+
 def run_ours(args, rank, local, world_size, pg):
     import torch
 
@@ -655,7 +660,13 @@ def run_ours(args, rank, local, world_size, pg):
                 "us_per_substep": round(r.us_per_substep, 2)}
     world.step(max(args.warmup, 3))
     world.sync()
-    stages = world.stage_times(20)
+    # per-kernel event times over the next STAGE_SUBSTEPS substeps (eager, one event per stage)
+    stages = world.stage_times(STAGE_SUBSTEPS)
+    t0_sub = max(args.warmup, 3) + STAGE_SUBSTEPS  # the timed substeps start here, counted from the initial state
+    # active grid nodes of the state the kernel times were taken on (for the roofline's node bytes)
+    A = sum(active_nodes(s, world.download(i, p.n)) for i, (s, p) in enumerate(zip(scenes[:64], parts[:64])))
+    if len(scenes) > 64:
+        A = int(A * len(scenes) / 64)
     stream = torch.cuda.ExternalStream(world.stream(), device=local)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -675,11 +686,10 @@ def run_ours(args, rank, local, world_size, pg):
     ms = e0.elapsed_time(e1)
     ms = max_over_ranks(pg, ms)
     value = n_total * world_size * args.steps / (ms / 1e3)
+    # the same per-kernel times where the timed region ended (the state evolves: boxes collide, fluid spreads)
+    stages_end = world.stage_times(STAGE_SUBSTEPS)
 
     # roofline of the dominant kernel (P2G or G2P), from its event-timed mean duration
-    A = sum(active_nodes(s, world.download(i, p.n)) for i, (s, p) in enumerate(zip(scenes[:64], parts[:64])))
-    if len(scenes) > 64:
-        A = int(A * len(scenes) / 64)
     kern = "g2p" if stages["g2p"] >= stages["p2g"] else "p2g"
     per_p = G2P_BYTES_PER_PARTICLE if kern == "g2p" else P2G_BYTES_PER_PARTICLE
     per_n = G2P_BYTES_PER_NODE if kern == "g2p" else P2G_BYTES_PER_NODE
@@ -723,23 +733,27 @@ def run_ours(args, rank, local, world_size, pg):
         world.upload(0, hin)
         world.step(args.e2e_substeps)
         world.download_into(0, hout)
-        times = []
+        times, phases = [], []
         for _ in range(args.e2e_reps):
             barrier(pg)
             torch.cuda.synchronize(local)
-            a0 = torch.cuda.Event(enable_timing=True)
-            a1 = torch.cuda.Event(enable_timing=True)
-            a0.record(stream)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            ev[0].record(stream)
             world.upload(0, hin)
+            ev[1].record(stream)
             world.step(args.e2e_substeps)
+            ev[2].record(stream)
             world.download_into(0, hout)
-            a1.record(stream)
-            a1.synchronize()
-            times.append(max_over_ranks(pg, a0.elapsed_time(a1)))
+            ev[3].record(stream)
+            ev[3].synchronize()
+            times.append(max_over_ranks(pg, ev[0].elapsed_time(ev[3])))
+            phases.append([ev[k].elapsed_time(ev[k + 1]) for k in range(3)])
         t = statistics.median(times)
+        ph = [statistics.median(p[k] for p in phases) for k in range(3)]
         e2e = {"value": n_total * world_size * args.e2e_substeps / (t / 1e3), "unit": "particle-updates/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "substeps_per_step": args.e2e_substeps, "ms_per_step": t}
+               "substeps_per_step": args.e2e_substeps, "ms_per_step": t,
+               "phases_ms": {"upload": round(ph[0], 3), "substeps": round(ph[1], 3), "download": round(ph[2], 3)}}
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
@@ -757,11 +771,14 @@ def run_ours(args, rank, local, world_size, pg):
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64 scenes)",
             "config": dict(cfg, parallelism="replicas" if world_size > 1 else "single GPU",
-                           l2=l2_note(n_total)),
+                           l2=l2_note(n_total), timed_substeps=[t0_sub, t0_sub + args.steps]),
             "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "algorithmic_bytes": alg_bytes, "active_nodes": A, "kernel_us": stages[kern]},
+                         "algorithmic_bytes": alg_bytes, "active_nodes": A, "kernel_us": stages[kern],
+                         "kernel_substeps": [t0_sub - STAGE_SUBSTEPS, t0_sub]},
             "stages_us": {k: round(v, 2) for k, v in stages.items()},
+            "stages_us_end": dict({k: round(v, 2) for k, v in stages_end.items()},
+                                  substeps=[t0_sub + args.steps, t0_sub + args.steps + STAGE_SUBSTEPS]),
             "autotune": tune,
             "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,
         }
@@ -925,8 +942,16 @@ def run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
         print(json.dumps(line), flush=True)
 
 
+# substeps of one run of each configuration (the default number of timed steps)
+RUN_LENGTH = {"snow": 500, "dam": 1000, "jelly": 200, "batched": 200}
+
+
 def main():
     args = parse()
+    if args.steps is None:
+        args.steps = RUN_LENGTH.get(args.workload, 200)
+    if args.e2e_substeps is None:
+        args.e2e_substeps = RUN_LENGTH.get(args.workload, 500)
     rank, local, world_size, pg = dist_setup(args)
     try:
         if args.impl == "reference":

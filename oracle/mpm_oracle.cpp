@@ -353,21 +353,28 @@ void svd3(const T* F, T* U, T* s, T* V) {
 // the gap at which FP32 singular vectors keep only half their digits.
 constexpr double kSvdGapTol = 3.5e-4;
 
-// True when every singular value of F provably lies in [lo, hi] and det F > 0, so the snow clamp
-// is the identity map: Gershgorin discs of F^T F inside [lo^2, hi^2].
+// Whether the symmetric matrix [[a d e] [d b f] [e f c]] is positive definite (Sylvester's
+// criterion: every leading principal minor is positive).
+template <class T>
+bool sym3_positive_definite(T a, T b, T c, T d, T e, T f) {
+  T m2 = a * b - d * d;
+  T m3 = a * (b * c - f * f) - d * (d * c - f * e) + e * (d * f - b * e);
+  return a > T(0) && m2 > T(0) && m3 > T(0);
+}
+
+// True when every singular value of F lies strictly inside (lo, hi) and det F > 0, so the snow
+// clamp of ae_physics/src/mpm.rs:565-606 is the identity map and its SVD can be skipped: the
+// eigenvalues of F^T F (the squared singular values) lie in (lo^2, hi^2) exactly when
+// F^T F - lo^2 I and hi^2 I - F^T F are positive definite.  Exact up to rounding in the minors.
 template <class T>
 bool clamp_is_identity(const T* F, T lo, T hi) {
-  T a[9];
+  T m[3][3];
   for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) a[i * 3 + j] = F[0 * 3 + i] * F[0 * 3 + j] + F[1 * 3 + i] * F[1 * 3 + j] + F[2 * 3 + i] * F[2 * 3 + j];
+    for (int j = i; j < 3; ++j) m[i][j] = F[0 * 3 + i] * F[0 * 3 + j] + F[1 * 3 + i] * F[1 * 3 + j] + F[2 * 3 + i] * F[2 * 3 + j];
   T lo2 = lo * lo, hi2 = hi * hi;
-  for (int i = 0; i < 3; ++i) {
-    T r = T(0);
-    for (int j = 0; j < 3; ++j)
-      if (j != i) r += std::fabs(a[i * 3 + j]);
-    if (a[i * 4] - r < lo2 || a[i * 4] + r > hi2) return false;
-  }
-  return det3(F) > T(0);
+  return sym3_positive_definite(m[0][0] - lo2, m[1][1] - lo2, m[2][2] - lo2, m[0][1], m[0][2], m[1][2]) &&
+         sym3_positive_definite(hi2 - m[0][0], hi2 - m[1][1], hi2 - m[2][2], -m[0][1], -m[0][2], -m[1][2]) &&
+         det3(F) > T(0);
 }
 
 // FP32 SVD, redone in FP64 when a near-degenerate pair of singular values straddles a clamp

@@ -156,6 +156,32 @@ def test_clamp_identity_fast_path_is_exact():
     th = 0.4
     R = np.array([[math.cos(th), -math.sin(th), 0], [math.sin(th), math.cos(th), 0], [0, 0, 1]])
     assert O.clamp_is_identity(R, lo, hi)  # pure rotations need no SVD
+
+
+def rotation(rng):
+    q, r = np.linalg.qr(rng.normal(size=(3, 3)))
+    q = q * np.sign(np.diag(r))
+    return q if np.linalg.det(q) > 0 else -q
+
+
+def test_clamp_identity_is_tight_for_rotated_f():
+    # F = R1 diag(s) R2^T with the singular values spread across the band: the test is exact, so
+    # every such F whose singular values are inside by a margin skips the SVD, whatever its rotations
+    # (a Gershgorin bound on F^T F rejects most of them), and every F with one outside takes it
+    lo, hi = 1 - 2.5e-2, 1 + 7.5e-3
+    rng = np.random.default_rng(11)
+    margin = 1e-5
+    for _ in range(400):
+        R1, R2 = rotation(rng), rotation(rng)
+        s = rng.uniform(lo + margin, hi - margin, 3)
+        F = (R1 @ np.diag(s) @ R2.T).astype(np.float32)
+        assert O.clamp_is_identity(F, lo, hi), s
+        k = rng.integers(0, 3)
+        t = s.copy()
+        t[k] = rng.choice([rng.uniform(lo - 0.02, lo - margin), rng.uniform(hi + margin, hi + 0.02)])
+        G = (R1 @ np.diag(t) @ R2.T).astype(np.float32)
+        assert not O.clamp_is_identity(G, lo, hi), t
+        assert not O.clamp_is_identity((R1 @ np.diag(s * [1, 1, -1]) @ R2.T).astype(np.float32), lo, hi)
     assert not O.clamp_is_identity(np.diag([1.0, 1.0, -1.0]), lo, hi)  # inverted
 
 
