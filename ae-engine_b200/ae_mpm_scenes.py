@@ -126,6 +126,21 @@ def config2_snow(seed: int = 0xAE02):
     return sc, p
 
 
+def snow_collision_small(n_box: int = 4096, grid: int = 32, seed: int = 0xAE22, v: float = 2.0):
+    """Config 2 in miniature for parity tests: two snow boxes 0.2 x 0.2 x 0.2 half a cell apart,
+    closing at 2v, so the Stomakhin clamp is active from the first tens of substeps."""
+    rng = Rng(seed)
+    dx = 1.0 / grid
+    w, c, gap = 0.2, 0.5, 0.5 * dx
+    a = jittered_box(rng, (c - gap / 2 - w, 0.4, 0.4), (c - gap / 2, 0.6, 0.6), n_box)
+    b = jittered_box(rng, (c + gap / 2, 0.4, 0.4), (c + gap / 2 + w, 0.6, 0.6), n_box)
+    m = 400.0 * w ** 3 / n_box
+    p = concat([make_particles(a, (v, 0, 0), m, 0), make_particles(b, (-v, 0, 0), m, 0)])
+    p.J[:] = 1.0
+    sc = M.Scene(n=(grid, grid, grid), dx=dx, dt=1e-4, materials=[snow()], max_particles=2 * n_box)
+    return sc, p
+
+
 def config3_dam(seed: int = 0xAE03, scale: float = 1.0):
     """Mixed dam break.  `scale` < 1 shrinks the particle counts (same boxes) for tests."""
     rng = Rng(seed)

@@ -285,14 +285,37 @@ struct SvdTol<double> {
   static constexpr double off = 7.9e-31;
 };
 
+// Quotient and reciprocal square root for the rotation angles.  FP32 on the device uses the
+// hardware approximations (MUFU reciprocal, 2 ulp reciprocal square root): a rotation only has to
+// shrink the off-diagonal entry, the next sweep removes what it leaves, and c^2 + s^2 = 1 holds to
+// a few ulp, so U, V stay orthogonal to FP32 accuracy.  FP64 and the host keep IEEE operations.
+AE_HD float rot_div(float a, float b) {
+#ifdef __CUDA_ARCH__
+  return __fdividef(a, b);
+#else
+  return a / b;
+#endif
+}
+AE_HD double rot_div(double a, double b) { return a / b; }
+AE_HD float rot_rsqrt(float x) {
+#ifdef __CUDA_ARCH__
+  return rsqrtf(x);
+#else
+  return 1.0f / sqrtf(x);
+#endif
+}
+AE_HD double rot_rsqrt(double x) { return 1.0 / sqrt(x); }
+
 template <class T>
 AE_HD void jacobi_rot(T* a, T* v, int p, int q) {
   T apq = a[p * 3 + q];
   if (apq == T(0)) return;
   T app = a[p * 3 + p], aqq = a[q * 3 + q];
-  T tau = (aqq - app) / (T(2) * apq);
-  T t = (tau >= T(0) ? T(1) : T(-1)) / (t_abs(tau) + t_sqrt(T(1) + tau * tau));
-  T c = T(1) / t_sqrt(T(1) + t * t);
+  const T dq = aqq - app;
+  T tau = dq == T(0) ? T(0) : rot_div(dq, T(2) * apq);  // 0 * rcp(tiny) would be NaN
+  // |tau| + sqrt(1 + tau^2) overflows to +inf for huge tau: t is then 0 (no rotation needed)
+  T t = rot_div(tau >= T(0) ? T(1) : T(-1), t_abs(tau) + t_sqrt(T(1) + tau * tau));
+  T c = rot_rsqrt(T(1) + t * t);  // 1 + t^2 in [1, 2]
   T sn = t * c;
   int o = 3 - p - q;
   T aop = a[o * 3 + p], aoq = a[o * 3 + q];

@@ -1253,8 +1253,10 @@ __global__ void __launch_bounds__(256, (MODE == AE_MPM_MODE_PHYSICS && sizeof(T)
 // Snow return mapping for the particles G2P queued: F = U S V^T, singular values clamped to
 // [1-theta_c, 1+theta_s], J_p *= prod(S)/prod(S_clamped) (ae_physics/src/mpm.rs:565-606 plus
 // Stomakhin's J_p), with the FP64 SVD redo where a near-degenerate pair straddles a threshold.
+// 64 registers, 8 blocks of 128 per SM: the FP64 redo, taken by few particles, would otherwise set
+// the register count (94) and leave three quarters of the SM's warp slots empty.
 template <class T>
-__global__ void __launch_bounds__(128) snow_clamp_kernel(WorldDev<T> w) {
+__global__ void __launch_bounds__(128, 8) snow_clamp_kernel(WorldDev<T> w) {
   using V4 = typename V4T<T>::type;
   const uint32_t count = launch_count(w.clamp_count);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
@@ -2322,7 +2324,7 @@ class World final : public WorldBase {
     g2p_kernel<T, MODE><<<n_chunks_, chunk_threads_, g2p_smem, stream_>>>(w, counters_ + 2, write_keys ? 1 : 0);
     ++launches_;
     if (MODE == AE_MPM_MODE_PHYSICS && has_snow_) {
-      snow_clamp_kernel<T><<<sms * 4, 128, 0, stream_>>>(w);
+      snow_clamp_kernel<T><<<sms * 8, 128, 0, stream_>>>(w);
       ++launches_;
     }
     mark(4);

@@ -115,6 +115,27 @@ def test_physics_materials_match_fp64_oracle(ctx, mat):
     assert rel(g64.J, ref.J) <= 1e-9
 
 
+def test_snow_collision_through_plastic_flow_matches_fp64_oracle(ctx):
+    # two snow boxes collide: most particles reach the clamp band and take the SVD return mapping
+    # (and its FP64 redo near degenerate pairs) every substep.  Tolerances: f32 GPU vs f64 oracle
+    # 1e-5 in positions, 2e-4 in F and J_p (the f32 oracle itself is 2e-6 / 2e-5 from f64 here);
+    # f64 GPU vs f64 oracle 1e-10 / 1e-9.
+    sc, p = S.snow_collision_small()
+    ref = p.astype(np.float64)
+    O.run(sc, ref, 80)
+    lo, hi = 1 - 2.5e-2, 1 + 7.5e-3
+    s = np.linalg.svd(ref.F.reshape(-1, 3, 3), compute_uv=False)
+    assert ((np.abs(s - lo) < 1e-9) | (np.abs(s - hi) < 1e-9)).any(1).mean() > 0.5  # the clamp is active
+    g = run_gpu(ctx, sc, p, 80)
+    assert rel(g.pos, ref.pos) <= 1e-5
+    assert rel(g.F, ref.F) <= 2e-4
+    assert rel(g.J, ref.J) <= 2e-4
+    g64 = run_gpu(ctx, sc, p.astype(np.float64), 80)
+    assert rel(g64.pos, ref.pos) <= 1e-10
+    assert rel(g64.F, ref.F) <= 1e-9
+    assert rel(g64.J, ref.J) <= 1e-9
+
+
 @pytest.mark.parametrize("interval", [2, 5, 32])
 def test_sort_interval_does_not_change_results(ctx, interval):
     sc, p = S.tiny_scene(4096, 32, S.jelly(), v=(0.5, 0.5, 0.0))
