@@ -1258,9 +1258,17 @@ __global__ void __launch_bounds__(256, (MODE == AE_MPM_MODE_PHYSICS && sizeof(T)
 template <class T>
 __global__ void __launch_bounds__(128, 8) snow_clamp_kernel(WorldDev<T> w) {
   using V4 = typename V4T<T>::type;
+  // the particle's mass and C slots arrive here while its SVD runs (each thread its own column)
+  __shared__ V4 pre[4][128];
+  const int tid = threadIdx.x;
   const uint32_t count = launch_count(w.clamp_count);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     const uint2 q = w.clamp_queue[i];
+    cp_async_v4(&pre[0][tid], w.out[0] + q.x);
+    cp_async_v4(&pre[1][tid], w.out[4] + q.x);
+    cp_async_v4(&pre[2][tid], w.out[5] + q.x);
+    cp_async_v4(&pre[3][tid], w.out[6] + q.x);
+    cp_async_commit();
     const SceneDev<T>& sc = w.scenes[q.y];
     V4 a1 = w.out[1][q.x], a2 = w.out[2][q.x], a3 = w.out[3][q.x];
     const MatDev& md = mat_of(w, sc, Bits<T>::unpack(a3.z) & 0xffffu);
@@ -1282,7 +1290,8 @@ __global__ void __launch_bounds__(128, 8) snow_clamp_kernel(WorldDev<T> w) {
     w.out[2][q.x] = mk4(nF[4], nF[5], nF[6], nF[7]);
     w.out[3][q.x] = mk4(nF[8], J, a3.z, a3.w);
     // G2P left C in the C slot of queued particles: turn it into A with the returned F and J_p
-    const V4 a0 = w.out[0][q.x], a4 = w.out[4][q.x], a5 = w.out[5][q.x], a6 = w.out[6][q.x];
+    cp_async_wait_all();
+    const V4 a0 = pre[0][tid], a4 = pre[1][tid], a5 = pre[2][tid], a6 = pre[3][tid];
     const T C[9] = {a4.w, a5.x, a5.y, a5.z, a5.w, a6.x, a6.y, a6.z, a6.w};
     T A[9];
     affine_from_c(sc, md, a0.w, C, nF, J, A);
