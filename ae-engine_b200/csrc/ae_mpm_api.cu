@@ -147,6 +147,71 @@ ae_mpm_particles pinned_view(ae_mpm_ctx* ctx, uint64_t n) {
   return v;
 }
 
+// Drop-in calls whose indices are ascending and select a quarter or more of the buffer copy the
+// buffer's arrays whole and gather / scatter the selected particles on the device.  `full`: every
+// field travels (reference mode); otherwise position, velocity and mass only, with F = I, C = 0,
+// J = 1 (the velocity-only substep reads none of them and writes back position and velocity).
+__global__ void dropin_gather_kernel(ae_mpm_particles src, const uint64_t* __restrict__ idx, uint64_t n,
+                                     ae_mpm_particles dst, int full) {
+  const uint64_t k = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint64_t i = idx[k];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    dst.pos[3 * k + a] = src.pos[3 * i + a];
+    dst.vel[3 * k + a] = src.vel[3 * i + a];
+  }
+  dst.mass[k] = src.mass[i];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    dst.strain[9 * k + q] = full ? src.strain[9 * i + q] : ((q % 4 == 0) ? 1.0f : 0.0f);
+    dst.c[9 * k + q] = full ? src.c[9 * i + q] : 0.0f;
+  }
+  dst.jacobian[k] = full ? src.jacobian[i] : 1.0f;
+  dst.material_idx[k] = full ? src.material_idx[i] : uint16_t(0);
+}
+
+__global__ void dropin_scatter_kernel(ae_mpm_particles src, const uint64_t* __restrict__ idx, uint64_t n,
+                                      ae_mpm_particles dst, int full) {
+  const uint64_t k = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint64_t i = idx[k];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    dst.pos[3 * i + a] = src.pos[3 * k + a];
+    dst.vel[3 * i + a] = src.vel[3 * k + a];
+  }
+  if (full) {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      dst.strain[9 * i + q] = src.strain[9 * k + q];
+      dst.c[9 * i + q] = src.c[9 * k + q];
+    }
+    dst.jacobian[i] = src.jacobian[k];
+  }
+}
+
+// Carves the device staging of a whole-array drop-in call: the buffer's arrays (capacity particles),
+// the index list and the selected particles (n), each region on a 16-byte boundary.
+struct DropinLayout {
+  size_t off[16];
+  size_t bytes;
+};
+DropinLayout dropin_layout(uint64_t capacity, uint64_t n, bool full) {
+  const size_t sz[15] = {12 * capacity, 12 * capacity, 4 * capacity, full ? 36 * capacity : 0, full ? 36 * capacity : 0,
+                         full ? 4 * capacity : 0, full ? 2 * capacity : 0, 8 * n, 12 * n, 12 * n, 36 * n, 4 * n, 36 * n,
+                         4 * n, 2 * n};
+  DropinLayout l{};
+  size_t o = 0;
+  for (int r = 0; r < 15; ++r) {
+    l.off[r] = o;
+    o += (sz[r] + 15) & ~size_t(15);
+  }
+  l.off[15] = o;
+  l.bytes = o;
+  return l;
+}
+
 int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64_t capacity, const ae_mpm_grid* grid,
                const ae_mpm_config* config, const std::vector<ae_mpm_material>& mats, float total_dt,
                const uint64_t* idx, uint64_t n) {
@@ -158,8 +223,11 @@ int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64
   if (!buffer->pos || !buffer->vel || !buffer->mass ||
       (mode == AE_MPM_MODE_REFERENCE && (!buffer->strain || !buffer->jacobian || !buffer->c || !buffer->material_idx)))
     return fail(ctx, AE_MPM_EINVAL, "particle buffer has a null array");
-  for (uint64_t k = 0; k < n; ++k)
+  bool ascending = true;
+  for (uint64_t k = 0; k < n; ++k) {
     if (idx[k] >= capacity) return fail(ctx, AE_MPM_EINVAL, "particle index " + std::to_string(idx[k]) + " >= capacity");
+    if (k > 0 && idx[k] <= idx[k - 1]) ascending = false;
+  }
   int rc = set_device(ctx);
   if (rc) return rc;
   ae_mpm_scene_desc d{};
@@ -200,6 +268,70 @@ int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64
     rc = ctx->dropin->set_scene_params(0, d);
     if (rc) return fail(ctx, rc, ctx->dropin->err);
   }
+  WorldBase* w = ctx->dropin;
+  const bool full = mode == AE_MPM_MODE_REFERENCE;
+  if (ascending && 4 * n >= capacity) {
+    // whole arrays in, gather and scatter on the device, whole arrays out: the unselected particles
+    // travel both ways unchanged (the caller holds the buffer exclusively for the call)
+    const DropinLayout l = dropin_layout(capacity, n, full);
+    rc = ensure_dstage(ctx, l.bytes);
+    if (rc) return rc;
+    char* d = static_cast<char*>(ctx->dstage);
+    ae_mpm_particles dfull{}, dsel{};
+    dfull.pos = reinterpret_cast<float*>(d + l.off[0]);
+    dfull.vel = reinterpret_cast<float*>(d + l.off[1]);
+    dfull.mass = reinterpret_cast<float*>(d + l.off[2]);
+    if (full) {
+      dfull.strain = reinterpret_cast<float*>(d + l.off[3]);
+      dfull.c = reinterpret_cast<float*>(d + l.off[4]);
+      dfull.jacobian = reinterpret_cast<float*>(d + l.off[5]);
+      dfull.material_idx = reinterpret_cast<uint16_t*>(d + l.off[6]);
+    }
+    uint64_t* didx = reinterpret_cast<uint64_t*>(d + l.off[7]);
+    dsel.pos = reinterpret_cast<float*>(d + l.off[8]);
+    dsel.vel = reinterpret_cast<float*>(d + l.off[9]);
+    dsel.strain = reinterpret_cast<float*>(d + l.off[10]);
+    dsel.jacobian = reinterpret_cast<float*>(d + l.off[11]);
+    dsel.c = reinterpret_cast<float*>(d + l.off[12]);
+    dsel.mass = reinterpret_cast<float*>(d + l.off[13]);
+    dsel.material_idx = reinterpret_cast<uint16_t*>(d + l.off[14]);
+    cudaStream_t st = w->stream();
+    cudaError_t e = cudaSuccess;
+    auto copy = [&](void* dst, const void* src, size_t b, cudaMemcpyKind kind) {
+      if (e == cudaSuccess) e = cudaMemcpyAsync(dst, src, b, kind, st);
+    };
+    copy(dfull.pos, buffer->pos, 12 * capacity, cudaMemcpyHostToDevice);
+    copy(dfull.vel, buffer->vel, 12 * capacity, cudaMemcpyHostToDevice);
+    copy(dfull.mass, buffer->mass, 4 * capacity, cudaMemcpyHostToDevice);
+    if (full) {
+      copy(dfull.strain, buffer->strain, 36 * capacity, cudaMemcpyHostToDevice);
+      copy(dfull.c, buffer->c, 36 * capacity, cudaMemcpyHostToDevice);
+      copy(dfull.jacobian, buffer->jacobian, 4 * capacity, cudaMemcpyHostToDevice);
+      copy(dfull.material_idx, buffer->material_idx, 2 * capacity, cudaMemcpyHostToDevice);
+    }
+    copy(didx, idx, 8 * n, cudaMemcpyHostToDevice);
+    const unsigned blocks = unsigned((n + 255) / 256);
+    if (e == cudaSuccess) {
+      dropin_gather_kernel<<<blocks, 256, 0, st>>>(dfull, didx, n, dsel, full ? 1 : 0);
+      e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("drop-in gather: ") + cudaGetErrorString(e));
+    if ((rc = w->upload(0, &dsel, n, false)) || (rc = w->step(uint32_t(config->substeps))) ||
+        (rc = w->download(0, &dsel, false)))
+      return fail(ctx, rc, w->err);
+    dropin_scatter_kernel<<<blocks, 256, 0, st>>>(dsel, didx, n, dfull, full ? 1 : 0);
+    e = cudaGetLastError();
+    copy(buffer->pos, dfull.pos, 12 * capacity, cudaMemcpyDeviceToHost);
+    copy(buffer->vel, dfull.vel, 12 * capacity, cudaMemcpyDeviceToHost);
+    if (full) {
+      copy(buffer->strain, dfull.strain, 36 * capacity, cudaMemcpyDeviceToHost);
+      copy(buffer->c, dfull.c, 36 * capacity, cudaMemcpyDeviceToHost);
+      copy(buffer->jacobian, dfull.jacobian, 4 * capacity, cudaMemcpyDeviceToHost);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("drop-in scatter: ") + cudaGetErrorString(e));
+    return AE_MPM_OK;
+  }
   // gather the selected particles into pinned staging
   rc = ensure_pinned(ctx, sizeof(float) * 26 * n + sizeof(uint16_t) * n + 64);
   if (rc) return rc;
@@ -222,7 +354,6 @@ int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64
     v.jacobian[k] = buffer->jacobian ? buffer->jacobian[i] : 1.0f;
     v.material_idx[k] = buffer->material_idx ? buffer->material_idx[i] : 0;
   }
-  WorldBase* w = ctx->dropin;
   if ((rc = w->upload(0, &v, n, false)) || (rc = w->step(uint32_t(config->substeps))) || (rc = w->download(0, &v, false)))
     return fail(ctx, rc, w->err);
   for (uint64_t k = 0; k < n; ++k) {

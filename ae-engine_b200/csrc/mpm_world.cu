@@ -1864,13 +1864,14 @@ class World final : public WorldBase {
     int rc = ensure_stage(n);
     if (rc) return rc;
     if (n > 0) {
-      AE_TRY(cudaMemcpyAsync(stage_, f[0], sizeof(T) * 3 * n, cudaMemcpyHostToDevice, stream_));
-      AE_TRY(cudaMemcpyAsync(stage_ + 3 * n, f[1], sizeof(T) * 3 * n, cudaMemcpyHostToDevice, stream_));
-      AE_TRY(cudaMemcpyAsync(stage_ + 6 * n, f[2], sizeof(T) * 9 * n, cudaMemcpyHostToDevice, stream_));
-      AE_TRY(cudaMemcpyAsync(stage_ + 15 * n, f[3], sizeof(T) * n, cudaMemcpyHostToDevice, stream_));
-      AE_TRY(cudaMemcpyAsync(stage_ + 16 * n, f[4], sizeof(T) * 9 * n, cudaMemcpyHostToDevice, stream_));
-      AE_TRY(cudaMemcpyAsync(stage_ + 25 * n, f[5], sizeof(T) * n, cudaMemcpyHostToDevice, stream_));
-      AE_TRY(cudaMemcpyAsync(stage_ + 26 * n, hv.mat, sizeof(uint16_t) * n, cudaMemcpyHostToDevice, stream_));
+      // the view's arrays may be host or device memory (unified addressing picks the direction)
+      AE_TRY(cudaMemcpyAsync(stage_, f[0], sizeof(T) * 3 * n, cudaMemcpyDefault, stream_));
+      AE_TRY(cudaMemcpyAsync(stage_ + 3 * n, f[1], sizeof(T) * 3 * n, cudaMemcpyDefault, stream_));
+      AE_TRY(cudaMemcpyAsync(stage_ + 6 * n, f[2], sizeof(T) * 9 * n, cudaMemcpyDefault, stream_));
+      AE_TRY(cudaMemcpyAsync(stage_ + 15 * n, f[3], sizeof(T) * n, cudaMemcpyDefault, stream_));
+      AE_TRY(cudaMemcpyAsync(stage_ + 16 * n, f[4], sizeof(T) * 9 * n, cudaMemcpyDefault, stream_));
+      AE_TRY(cudaMemcpyAsync(stage_ + 25 * n, f[5], sizeof(T) * n, cudaMemcpyDefault, stream_));
+      AE_TRY(cudaMemcpyAsync(stage_ + 26 * n, hv.mat, sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
       rc = sync_tables();
       if (rc) return rc;
       pack_kernel<T><<<unsigned((n + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), stage_, n, h_scenes_[s].p_off,
@@ -1911,13 +1912,13 @@ class World final : public WorldBase {
     unpack_kernel<T><<<unsigned((n + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), stage_, n, h_scenes_[s].p_off,
                                                                       d_scenes_ + s, d_mats_);
     AE_TRY(cudaGetLastError());
-    AE_TRY(cudaMemcpyAsync(f[0], stage_, sizeof(T) * 3 * n, cudaMemcpyDeviceToHost, stream_));
-    AE_TRY(cudaMemcpyAsync(f[1], stage_ + 3 * n, sizeof(T) * 3 * n, cudaMemcpyDeviceToHost, stream_));
-    AE_TRY(cudaMemcpyAsync(f[2], stage_ + 6 * n, sizeof(T) * 9 * n, cudaMemcpyDeviceToHost, stream_));
-    AE_TRY(cudaMemcpyAsync(f[3], stage_ + 15 * n, sizeof(T) * n, cudaMemcpyDeviceToHost, stream_));
-    AE_TRY(cudaMemcpyAsync(f[4], stage_ + 16 * n, sizeof(T) * 9 * n, cudaMemcpyDeviceToHost, stream_));
-    AE_TRY(cudaMemcpyAsync(f[5], stage_ + 25 * n, sizeof(T) * n, cudaMemcpyDeviceToHost, stream_));
-    AE_TRY(cudaMemcpyAsync(hv.mat, stage_ + 26 * n, sizeof(uint16_t) * n, cudaMemcpyDeviceToHost, stream_));
+    AE_TRY(cudaMemcpyAsync(f[0], stage_, sizeof(T) * 3 * n, cudaMemcpyDefault, stream_));
+    AE_TRY(cudaMemcpyAsync(f[1], stage_ + 3 * n, sizeof(T) * 3 * n, cudaMemcpyDefault, stream_));
+    AE_TRY(cudaMemcpyAsync(f[2], stage_ + 6 * n, sizeof(T) * 9 * n, cudaMemcpyDefault, stream_));
+    AE_TRY(cudaMemcpyAsync(f[3], stage_ + 15 * n, sizeof(T) * n, cudaMemcpyDefault, stream_));
+    AE_TRY(cudaMemcpyAsync(f[4], stage_ + 16 * n, sizeof(T) * 9 * n, cudaMemcpyDefault, stream_));
+    AE_TRY(cudaMemcpyAsync(f[5], stage_ + 25 * n, sizeof(T) * n, cudaMemcpyDefault, stream_));
+    AE_TRY(cudaMemcpyAsync(hv.mat, stage_ + 26 * n, sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
     AE_TRY(cudaStreamSynchronize(stream_));
     return AE_MPM_OK;
   }

@@ -61,7 +61,7 @@ def parse():
                     help="timed steps; default: the workload's run length in substeps (RUN_LENGTH), else 200")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="snow", choices=["snow", "jelly", "dam", "batched", "served", "tick", "ck"])
+    ap.add_argument("--workload", default="snow", choices=["snow", "jelly", "dam", "batched", "served", "tick", "ck", "midfield"])
     ap.add_argument("--ck-h", type=float, default=1.0,
                     help="ck: grid spacing (the scene scales with it); 1 takes the exact power-of-two division path")
     ap.add_argument("--e2e-reps", type=int, default=3)
@@ -237,6 +237,8 @@ def run_reference(args, rank, pg):
         return run_tick(args, rank, 0, 1, pg, reference=True)
     if args.workload == "ck":
         return run_ck(args, rank, 0, 1, pg, reference=True)
+    if args.workload == "midfield":
+        return run_midfield(args, rank, 0, 1, pg, reference=True)
     if rank != 0:
         return
     scenes, parts, cfg = workload(args.workload, 0, args.scenes)
@@ -311,6 +313,159 @@ def tick_oracle(d, player, origin):
     b = TICK["bounds"]
     O.mpss_housekeeping(d["pos"], d["vel"], d["temp"], d["phase"], d["mat"], d["active"], [-b] * 3, [b] * 3,
                         TICK["min_temp"], TICK["max_temp"], 7)
+
+
+# The mid-field call of the engine tick (simulation.rs:598-607 -> mpm_step_velocity_only_parallel): the
+# reference's own measurement is 490 045 mid particles of a 1M-particle MpssBuffer on a 32^3 grid, one
+# substep of mid_dt = 12 / 60 s, in 32-47 ms on its CPU (ARCHITECTURE_V7_CRITIQUE.md:542-549).
+MID = dict(n_near=10000, n_mid=490045, n_far=500010, near=50.0, mid=200.0, far=400.0, grid=32, dx=12.5,
+           origin=-200.0, total_dt=0.2)
+MID_PUBLISHED = MID["n_mid"] / 0.032  # the best of the quoted 32-47 ms, as particle-updates/s
+
+
+def midfield_setup(seed):
+    """A 1 000 055-particle buffer: near, mid and far shells around the player at the origin, in shuffled
+    buffer order; the mid indices ascending, as the LOD scan builds them."""
+    import ae_mpm as M
+
+    rng = np.random.default_rng(seed)
+
+    def shell(n, r0, r1):
+        d = rng.normal(size=(n, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        return d * (rng.uniform(r0 ** 3, r1 ** 3, n) ** (1.0 / 3.0))[:, None]
+
+    pos = np.concatenate([shell(MID["n_near"], 0.0, MID["near"]), shell(MID["n_mid"], MID["near"], MID["mid"]),
+                          shell(MID["n_far"], MID["mid"], MID["far"])])
+    cls = np.repeat([0, 1, 2], [MID["n_near"], MID["n_mid"], MID["n_far"]])
+    perm = rng.permutation(pos.shape[0])
+    pos, cls = pos[perm], cls[perm]
+    p = M.Particles.empty(pos.shape[0])
+    p.pos[:] = pos.astype(np.float32)
+    p.vel[:] = rng.normal(0.0, 3.0, p.pos.shape).astype(np.float32)
+    p.mass[:] = 1.0
+    idx = np.flatnonzero(cls == 1).astype(np.uint64)
+    n = MID["grid"]
+    grid = M.Grid(n, n, n, MID["dx"], (MID["origin"],) * 3)
+    cfg = M.Config(grid_dx=MID["dx"], grid_size=(n, n, n), substeps=1, gravity=(0, -9.81, 0), damping=0.995)
+    return p, idx, grid, cfg
+
+
+def midfield_cfg():
+    return {"workload": "mid-field velocity-only MPM call (mpm_step_velocity_only_parallel): %d mid particles of a "
+                        "%d-particle buffer, %d^3 grid, dx %.1f m, 1 substep of %.1f s"
+                        % (MID["n_mid"], MID["n_near"] + MID["n_mid"] + MID["n_far"], MID["grid"], MID["dx"],
+                           MID["total_dt"]),
+            "particles": MID["n_mid"], "grid": MID["grid"],
+            "baseline": "reference's own CPU measurement of this call: 32-47 ms (vs_baseline uses 32 ms)"}
+
+
+def run_midfield(args, rank, local, world_size, pg, reference=False):
+    metric, unit = "mid-field MPM particle-updates/s", "particle-updates/s"
+    p, idx, grid, mcfg = midfield_setup(0xAE06 + 1000 * rank)
+    n = int(idx.size)
+    cfg = midfield_cfg()
+    steps = max(1, min(args.steps, 50))
+    if reference:  # the CPU restatement of mpm_step_velocity_only_parallel on all host threads
+        if rank != 0:
+            return
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        threads = os.cpu_count() or 1
+        for _ in range(max(1, min(args.warmup, 3))):
+            O.step_velocity_only_parallel(p, grid, mcfg, MID["total_dt"], idx, threads=threads)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            O.step_velocity_only_parallel(p, grid, mcfg, MID["total_dt"], idx, threads=threads)
+        dt = time.perf_counter() - t0
+        value = n * steps / dt
+        print(json.dumps({"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
+                          "steps": steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / steps,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": value / MID_PUBLISHED,
+                          "dtype": "f32", "data": "synthetic (seeded numpy)", "config": cfg,
+                          "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
+                                           "sample": "the whole call, %d calls" % steps},
+                          "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+    import torch
+
+    import ae_mpm as M
+
+    ctx = M.Context(local)
+    # end to end: the drop-in call on the host buffer, as the engine makes it (host gather, upload, substep,
+    # download, host scatter); timed on the host clock, since the host work is part of the call
+    for _ in range(max(args.warmup, 3)):
+        ctx.step_velocity_only_parallel(p, grid, mcfg, MID["total_dt"], idx)
+    clocks = Clocks(local)
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    clocks.start()
+    time.sleep(0.3)
+    calls = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ctx.step_velocity_only_parallel(p, grid, mcfg, MID["total_dt"], idx)
+        calls.append(time.perf_counter() - t0)
+    clk = clocks.stop()
+    t_call = max_over_ranks(pg, statistics.median(calls))
+    e2e_value = n * world_size / t_call
+    # ascending indices selecting a quarter or more of the buffer: the call copies the buffer's position,
+    # velocity and mass arrays whole plus the index list in, and position and velocity out
+    cap = p.n
+    h2d, d2h = 28 * cap + 8 * n, 24 * cap
+
+    # device-resident: the same substep in a velocity-only world holding the mid particles
+    sub = p.subset(idx.astype(np.int64))
+    sc = M.Scene(n=(MID["grid"],) * 3, dx=MID["dx"], dt=MID["total_dt"], materials=[M.material()],
+                 mode=M.MODE_VELOCITY_ONLY, origin=(MID["origin"],) * 3, gravity=(0.0, -9.81, 0.0), wall_margin=0,
+                 damping=0.995, wall_origin=1, max_particles=n)
+    world = M.World(ctx, [sc], M.exec_opts())
+    world.upload(0, sub)
+    world.step(max(args.warmup, 3))
+    world.sync()
+    stages = world.stage_times(STAGE_SUBSTEPS)
+    stream = torch.cuda.ExternalStream(world.stream(), device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    e0.record(stream)
+    world.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    world.sync(raise_on_error=False)
+    launches = world.launches()
+    ms = max_over_ranks(pg, e0.elapsed_time(e1))
+    value = n * world_size * args.steps / (ms / 1e3)
+    world.close()
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        threads = os.cpu_count() or 1
+        q = p.copy()
+        O.step_velocity_only_parallel(q, grid, mcfg, MID["total_dt"], idx, threads=threads)
+        t0 = time.perf_counter()
+        O.step_velocity_only_parallel(q, grid, mcfg, MID["total_dt"], idx, threads=threads)
+        dt = time.perf_counter() - t0
+        cpu = {"value": n / dt, "unit": unit, "cores": threads, "kind": "port",
+               "sample": "one whole call (%d mid particles), %.2f s" % (n, dt)}
+    if rank == 0:
+        print(json.dumps({
+            "metric": metric, "value": value, "unit": unit, "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": value / MID_PUBLISHED, "dtype": "f32", "data": "synthetic (seeded numpy)",
+            "config": dict(cfg, parallelism="replicas" if world_size > 1 else "single GPU",
+                           l2="the mid particles' state (%.0f MB) exceeds L2" % (224 * n / 1e6)),
+            "stages_us": {k: round(v, 2) for k, v in stages.items()},
+            "e2e": {"value": e2e_value, "unit": unit, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": 1000.0 * t_call, "calls": steps, "timer": "host clock around each call",
+                    "vs_baseline": e2e_value / MID_PUBLISHED},
+            "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk}), flush=True)
+    ctx.close()
 
 
 def run_tick(args, rank, local, world_size, pg, reference=False):
@@ -633,6 +788,8 @@ def run_ours(args, rank, local, world_size, pg):
         return run_tick(args, rank, local, world_size, pg)
     if args.workload == "ck":
         return run_ck(args, rank, local, world_size, pg)
+    if args.workload == "midfield":
+        return run_midfield(args, rank, local, world_size, pg)
     ctx = M.Context(local)
     scenes, parts, cfg = workload(args.workload, rank, args.scenes)
     if args.workload == "served":

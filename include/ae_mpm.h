@@ -244,6 +244,7 @@ int ae_mpm_world_create(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32
                         const ae_mpm_exec_opts* opts, ae_mpm_world** out);
 int ae_mpm_world_destroy(ae_mpm_world* world);
 /* Copy n particles (indices 0..n-1 of the view) into scene `scene`; n <= max_particles.
+ * The view's arrays may be host memory or memory of the world's device.
  * The _f64 variants are for precision-64 worlds. */
 int ae_mpm_world_upload(ae_mpm_world* world, uint32_t scene, const ae_mpm_particles* host, uint64_t n);
 int ae_mpm_world_upload_f64(ae_mpm_world* world, uint32_t scene, const ae_mpm_particles_f64* host, uint64_t n);
@@ -254,7 +255,7 @@ int ae_mpm_world_set_scene(ae_mpm_world* world, uint32_t scene, const ae_mpm_sce
 int ae_mpm_world_step(ae_mpm_world* world, uint32_t n_substeps);
 /* Wait for queued work; returns AE_MPM_ENAN / AE_MPM_EDOMAIN if a scene raised its error word. */
 int ae_mpm_world_sync(ae_mpm_world* world);
-/* Copy scene particles back in their upload order. */
+/* Copy scene particles back in their upload order (into host memory or memory of the world's device). */
 int ae_mpm_world_download(ae_mpm_world* world, uint32_t scene, ae_mpm_particles* host);
 int ae_mpm_world_download_f64(ae_mpm_world* world, uint32_t scene, ae_mpm_particles_f64* host);
 /* FP64 totals of a scene: [mass, px, py, pz, kinetic energy] of its particles, now. */

@@ -261,15 +261,43 @@ def test_dropin_parallel_path_rules_with_moving_window(ctx):
     assert rel(a.pos, b.pos) <= 2e-5
 
 
-def test_dropin_velocity_only_matches_oracle(ctx):
+# index lists: ascending and a quarter or more of the buffer take the whole-array device gather; sparse
+# or unordered lists take the host gather
+INDEX_PATTERNS = {
+    "all": lambda n: np.arange(n),
+    "every_other": lambda n: np.arange(0, n, 2),
+    "sparse": lambda n: np.arange(3, n, 7),
+    "descending": lambda n: np.arange(n)[::-1],
+}
+
+
+@pytest.mark.parametrize("pattern", sorted(INDEX_PATTERNS))
+def test_dropin_velocity_only_matches_oracle(ctx, pattern):
     p, g, cfg, mats, mods = _ref_setup(n=5000, grid=16, dx=25.0)
-    idx = np.arange(p.n, dtype=np.uint64)
+    idx = INDEX_PATTERNS[pattern](p.n).astype(np.uint64)
     a, b = p.copy(), p.copy()
     ctx.step_velocity_only_parallel(a, g, cfg, 0.2, idx)
     assert O.step_velocity_only_parallel(b, g, cfg, 0.2, idx) == 0
     assert rel(a.pos, b.pos) <= 2e-5
     assert rel(a.vel, b.vel) <= 1e-4
-    assert np.array_equal(a.F, p.F) and np.array_equal(a.C, p.C)
+    assert np.array_equal(a.F, p.F) and np.array_equal(a.C, p.C) and np.array_equal(a.J, p.J)
+    untouched = np.setdiff1d(np.arange(p.n), idx.astype(np.int64))
+    assert np.array_equal(a.pos[untouched], p.pos[untouched]) and np.array_equal(a.vel[untouched], p.vel[untouched])
+
+
+@pytest.mark.parametrize("pattern", ["every_other", "sparse", "descending"])
+def test_dropin_reference_index_patterns_match_oracle(ctx, pattern):
+    p, g, cfg, mats, mods = _ref_setup(n=4000, models=(M.NEO_HOOKEAN, M.NEWTONIAN_FLUID))
+    idx = INDEX_PATTERNS[pattern](p.n).astype(np.uint64)
+    a, b = p.copy(), p.copy()
+    ctx.step_parallel_with_grid(a, g, cfg, mats, mods, 0.016, idx)
+    assert O.step_parallel_with_grid(b, g, cfg, mats, mods, 0.016, idx) == 0
+    assert rel(a.pos, b.pos) <= 2e-5
+    assert rel(a.F, b.F) <= 1e-4
+    assert rel(a.J, b.J) <= 1e-4
+    untouched = np.setdiff1d(np.arange(p.n), idx.astype(np.int64))
+    for f in ("pos", "vel", "F", "J", "C", "mass", "mat"):
+        assert np.array_equal(getattr(a, f)[untouched], getattr(p, f)[untouched]), f
 
 
 def test_dropin_empty_and_invalid_calls(ctx):
