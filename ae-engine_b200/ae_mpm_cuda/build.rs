@@ -21,7 +21,11 @@ fn main() {
     for src in sources.iter() {
         let obj = out.join(src.replace(".cu", ".o"));
         // the CK-MPM kernels round every operation separately, as Rust's f32 arithmetic does
-        let extra: &[&str] = if *src == "ae_mpm_ck.cu" { &["--fmad=false"] } else { &[] };
+        let extra: &[&str] = match *src {
+            "ae_mpm_ck.cu" => &["--fmad=false"],
+            "ae_mpm_api.cu" => &["-Xcompiler", "-fopenmp"],
+            _ => &[],
+        };
         let status = Command::new(&nvcc)
             .args(["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-lineinfo", "-Xptxas", "-v"])
             .args(extra)
@@ -46,6 +50,7 @@ fn main() {
     println!("cargo:rustc-link-lib=dylib=stdc++");
     println!("cargo:rustc-link-lib=dylib=dl");
     println!("cargo:rustc-link-lib=dylib=rt");
+    println!("cargo:rustc-link-lib=dylib=gomp");
     println!("cargo:rustc-link-lib=dylib=pthread");
     println!("cargo:rerun-if-changed=../../include/ae_mpm.h");
 }

@@ -30,7 +30,9 @@ CU_SOURCES = ["radix_sort.cu", "mpm_world.cu", "ae_mpm_api.cu", "ae_mpm_server.c
               "ae_mpm_ck.cu"]
 # per-source flags: the CK-MPM kernels round every operation separately, as the reference's f32
 # arithmetic does (no fused multiply-add)
-SOURCE_FLAGS = {"ae_mpm_ck.cu": ["--fmad=false"]}
+SOURCE_FLAGS = {"ae_mpm_ck.cu": ["--fmad=false"],
+                # the drop-in's host copies to and from pinned staging run on an OpenMP team
+                "ae_mpm_api.cu": ["-Xcompiler", "-fopenmp"]}
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
@@ -79,7 +81,7 @@ def build_cuda(force: bool = False) -> str:
         list(ex.map(_run, jobs))
     if force or jobs or _stale(LIB, objs):
         _run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-cudart", "static",
-              "-o", LIB] + objs + ["-lpthread"])
+              "-o", LIB] + objs + ["-lgomp", "-lpthread"])
     return LIB
 
 

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <omp.h>
 #include <map>
 #include <mutex>
 #include <string>
@@ -45,6 +46,8 @@ struct ae_mpm_ctx {
   aemp::CkWork* ck = nullptr;
   void* dstage = nullptr;
   size_t dstage_bytes = 0;
+  // completion events of the drop-in's whole-array copies back to the host
+  cudaEvent_t out_ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 struct ae_mpm_world {
@@ -191,6 +194,24 @@ __global__ void dropin_scatter_kernel(ae_mpm_particles src, const uint64_t* __re
   }
 }
 
+// Host copy between the caller's (pageable) arrays and pinned staging, split over up to 8 threads
+// for large arrays: the driver's own pageable copies run on one thread at a fraction of the link's
+// bandwidth, while copies from pinned staging run at the link's speed.
+void host_copy(void* dst, const void* src, size_t bytes) {
+  const int t_max = bytes >= (size_t(8) << 20) ? std::min(8, omp_get_max_threads()) : 1;
+  if (t_max <= 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t chunk = ((bytes + size_t(t_max) - 1) / size_t(t_max) + 63) & ~size_t(63);
+#pragma omp parallel for num_threads(t_max) schedule(static)
+  for (int t = 0; t < t_max; ++t) {
+    const size_t lo = size_t(t) * chunk;
+    if (lo < bytes)
+      std::memcpy(static_cast<char*>(dst) + lo, static_cast<const char*>(src) + lo, std::min(chunk, bytes - lo));
+  }
+}
+
 // Carves the device staging of a whole-array drop-in call: the buffer's arrays (capacity particles),
 // the index list and the selected particles (n), each region on a 16-byte boundary.
 struct DropinLayout {
@@ -223,11 +244,21 @@ int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64
   if (!buffer->pos || !buffer->vel || !buffer->mass ||
       (mode == AE_MPM_MODE_REFERENCE && (!buffer->strain || !buffer->jacobian || !buffer->c || !buffer->material_idx)))
     return fail(ctx, AE_MPM_EINVAL, "particle buffer has a null array");
-  bool ascending = true;
-  for (uint64_t k = 0; k < n; ++k) {
-    if (idx[k] >= capacity) return fail(ctx, AE_MPM_EINVAL, "particle index " + std::to_string(idx[k]) + " >= capacity");
-    if (k > 0 && idx[k] <= idx[k - 1]) ascending = false;
+  // bounds and order of the index list (split over threads for long lists; the message names the
+  // first index out of range)
+  uint64_t max_idx = 0;
+  int descents = 0;
+  const int t_idx = n >= (uint64_t(1) << 16) ? std::min(8, omp_get_max_threads()) : 1;
+#pragma omp parallel for num_threads(t_idx) schedule(static) reduction(max : max_idx) reduction(+ : descents)
+  for (int64_t k = 0; k < int64_t(n); ++k) {
+    max_idx = std::max(max_idx, idx[k]);
+    if (k > 0 && idx[k] <= idx[k - 1]) ++descents;
   }
+  if (max_idx >= capacity)
+    for (uint64_t k = 0; k < n; ++k)
+      if (idx[k] >= capacity)
+        return fail(ctx, AE_MPM_EINVAL, "particle index " + std::to_string(idx[k]) + " >= capacity");
+  const bool ascending = descents == 0;
   int rc = set_device(ctx);
   if (rc) return rc;
   ae_mpm_scene_desc d{};
@@ -295,21 +326,28 @@ int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64
     dsel.c = reinterpret_cast<float*>(d + l.off[12]);
     dsel.mass = reinterpret_cast<float*>(d + l.off[13]);
     dsel.material_idx = reinterpret_cast<uint16_t*>(d + l.off[14]);
+    // pinned staging mirrors the device layout of the whole arrays and the index list
+    rc = ensure_pinned(ctx, l.off[8]);
+    if (rc) return rc;
+    char* hp = reinterpret_cast<char*>(ctx->pin);
     cudaStream_t st = w->stream();
     cudaError_t e = cudaSuccess;
-    auto copy = [&](void* dst, const void* src, size_t b, cudaMemcpyKind kind) {
-      if (e == cudaSuccess) e = cudaMemcpyAsync(dst, src, b, kind, st);
+    // each array: host copy into pinned staging, then its DMA, which overlaps the next host copy
+    auto in = [&](int r, const void* src, size_t b) {
+      if (e != cudaSuccess) return;
+      host_copy(hp + l.off[r], src, b);
+      e = cudaMemcpyAsync(d + l.off[r], hp + l.off[r], b, cudaMemcpyHostToDevice, st);
     };
-    copy(dfull.pos, buffer->pos, 12 * capacity, cudaMemcpyHostToDevice);
-    copy(dfull.vel, buffer->vel, 12 * capacity, cudaMemcpyHostToDevice);
-    copy(dfull.mass, buffer->mass, 4 * capacity, cudaMemcpyHostToDevice);
+    in(0, buffer->pos, 12 * capacity);
+    in(1, buffer->vel, 12 * capacity);
+    in(2, buffer->mass, 4 * capacity);
     if (full) {
-      copy(dfull.strain, buffer->strain, 36 * capacity, cudaMemcpyHostToDevice);
-      copy(dfull.c, buffer->c, 36 * capacity, cudaMemcpyHostToDevice);
-      copy(dfull.jacobian, buffer->jacobian, 4 * capacity, cudaMemcpyHostToDevice);
-      copy(dfull.material_idx, buffer->material_idx, 2 * capacity, cudaMemcpyHostToDevice);
+      in(3, buffer->strain, 36 * capacity);
+      in(4, buffer->c, 36 * capacity);
+      in(5, buffer->jacobian, 4 * capacity);
+      in(6, buffer->material_idx, 2 * capacity);
     }
-    copy(didx, idx, 8 * n, cudaMemcpyHostToDevice);
+    in(7, idx, 8 * n);
     const unsigned blocks = unsigned((n + 255) / 256);
     if (e == cudaSuccess) {
       dropin_gather_kernel<<<blocks, 256, 0, st>>>(dfull, didx, n, dsel, full ? 1 : 0);
@@ -321,14 +359,22 @@ int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64
       return fail(ctx, rc, w->err);
     dropin_scatter_kernel<<<blocks, 256, 0, st>>>(dsel, didx, n, dfull, full ? 1 : 0);
     e = cudaGetLastError();
-    copy(buffer->pos, dfull.pos, 12 * capacity, cudaMemcpyDeviceToHost);
-    copy(buffer->vel, dfull.vel, 12 * capacity, cudaMemcpyDeviceToHost);
-    if (full) {
-      copy(buffer->strain, dfull.strain, 36 * capacity, cudaMemcpyDeviceToHost);
-      copy(buffer->c, dfull.c, 36 * capacity, cudaMemcpyDeviceToHost);
-      copy(buffer->jacobian, dfull.jacobian, 4 * capacity, cudaMemcpyDeviceToHost);
+    // the written arrays back: DMA into pinned staging, then host copies into the caller's arrays
+    const int outs[5] = {0, 1, 3, 4, 5};
+    const size_t out_b[5] = {12 * capacity, 12 * capacity, 36 * capacity, 36 * capacity, 4 * capacity};
+    void* const out_dst[5] = {buffer->pos, buffer->vel, buffer->strain, buffer->c, buffer->jacobian};
+    const int n_out = full ? 5 : 2;
+    // each array's host copy starts when its own DMA has landed, while the next one transfers
+    for (int k = 0; k < n_out && e == cudaSuccess; ++k) {
+      if (!ctx->out_ev[k]) e = cudaEventCreateWithFlags(&ctx->out_ev[k], cudaEventDisableTiming);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hp + l.off[outs[k]], d + l.off[outs[k]], out_b[k], cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaEventRecord(ctx->out_ev[k], st);
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    for (int k = 0; k < n_out && e == cudaSuccess; ++k) {
+      e = cudaEventSynchronize(ctx->out_ev[k]);
+      if (e == cudaSuccess) host_copy(out_dst[k], hp + l.off[outs[k]], out_b[k]);
+    }
     if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, std::string("drop-in scatter: ") + cudaGetErrorString(e));
     return AE_MPM_OK;
   }
@@ -410,6 +456,8 @@ void ae_mpm_ctx_destroy(ae_mpm_ctx* ctx) {
   delete ctx->lod;
   delete ctx->ck;
   cudaFree(ctx->dstage);
+  for (cudaEvent_t ev : ctx->out_ev)
+    if (ev) cudaEventDestroy(ev);
   if (ctx->pin) cudaFreeHost(ctx->pin);
   aemp::sort_scratch_free(ctx->sort);
   cudaFree(ctx->sort_keys);
