@@ -9,13 +9,13 @@ the grid exceeds the 126 MB L2, so no flush is needed between steps.
   value      particle-updates/s with the scene resident in HBM (CUDA events on the world's
              stream around K substeps; max over ranks)
   e2e        the same metric through the public C ABI with host buffers: upload from pinned
-             host memory, 500 substeps (the config's run length), download, per call
+             host memory, the config's run length of substeps, download, per call
   roofline   the dominant kernel (P2G or G2P): algorithmic bytes / its mean event-timed duration
   cpu_baseline  the CPU restatement of the reference substep (oracle/) on this host's cores
 
---impl reference times that CPU restatement alone (the reference is Rust and cannot be built
-here).  --gpus N runs N independent replicas (one scene per GPU; the substep does
-not shard within a scene).  Other workloads: --workload jelly|dam|batched|served|tick|ck.
+--impl reference times that CPU restatement alone (the reference is Rust, and no Rust toolchain is
+available to build it).  --gpus N runs N independent replicas (one scene per GPU; the substep does
+not shard within a scene).  Other workloads: --workload jelly|dam|batched|served|tick|ck|midfield.
 """
 from __future__ import annotations
 

@@ -1,6 +1,6 @@
 """GPU tests of the features around the substep: scene updates, error words and host-side fault
 injection, FP64 totals and conservation, the autotuner, the continuous-batching server, and the
-BASELINE configurations at (or near) full size.
+benchmark configurations at (or near) full size.
 
 Tolerances are stated per check.  Faults are injected on the host only (NaN and out-of-domain
 inputs, oversize requests, cancellation); nothing here faults, traps or hangs the GPU.
@@ -180,9 +180,9 @@ def test_server_budget_and_cancel(ctx):
     srv.close()
 
 
-# ------------------------------------------------------------------ BASELINE configurations
+# ------------------------------------------------------------------ the benchmark configurations
 def test_config1_fp32_vs_fp64_after_200_substeps(ctx):
-    # north-star target: <= 1e-4 relative position error vs FP64 after 200 substeps
+    # target: <= 1e-4 relative position error against the FP64 kernels after 200 substeps
     sc, p = S.config1_jelly()
     w32 = world_of(ctx, [sc], [p])
     w64 = world_of(ctx, [sc], [p.astype(np.float64)])
