@@ -382,7 +382,12 @@ int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64
   rc = ensure_pinned(ctx, sizeof(float) * 26 * n + sizeof(uint16_t) * n + 64);
   if (rc) return rc;
   ae_mpm_particles v = pinned_view(ctx, n);
-  for (uint64_t k = 0; k < n; ++k) {
+  // long lists gather on the OpenMP team (reads only); the scatter back is parallel only for
+  // ascending (hence distinct) indices, so a repeated index keeps the reference's last-write-wins
+  const int t_host = n >= 4096 ? std::min(8, omp_get_max_threads()) : 1;
+#pragma omp parallel for num_threads(t_host) schedule(static)
+  for (int64_t kk = 0; kk < int64_t(n); ++kk) {
+    const uint64_t k = uint64_t(kk);
     const uint64_t i = idx[k];
     std::memcpy(v.pos + 3 * k, buffer->pos + 3 * i, 3 * sizeof(float));
     std::memcpy(v.vel + 3 * k, buffer->vel + 3 * i, 3 * sizeof(float));
@@ -402,7 +407,9 @@ int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64
   }
   if ((rc = w->upload(0, &v, n, false)) || (rc = w->step(uint32_t(config->substeps))) || (rc = w->download(0, &v, false)))
     return fail(ctx, rc, w->err);
-  for (uint64_t k = 0; k < n; ++k) {
+#pragma omp parallel for num_threads(ascending ? t_host : 1) schedule(static)
+  for (int64_t kk = 0; kk < int64_t(n); ++kk) {
+    const uint64_t k = uint64_t(kk);
     const uint64_t i = idx[k];
     std::memcpy(buffer->pos + 3 * i, v.pos + 3 * k, 3 * sizeof(float));
     std::memcpy(buffer->vel + 3 * i, v.vel + 3 * k, 3 * sizeof(float));

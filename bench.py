@@ -15,7 +15,7 @@ the grid exceeds the 126 MB L2, so no flush is needed between steps.
 
 --impl reference times that CPU restatement alone (the reference is Rust, and no Rust toolchain is
 available to build it).  --gpus N runs N independent replicas (one scene per GPU; the substep does
-not shard within a scene).  Other workloads: --workload jelly|dam|batched|served|tick|ck|midfield.
+not shard within a scene).  Other workloads: --workload jelly|dam|batched|served|tick|ck|midfield|near.
 """
 from __future__ import annotations
 
@@ -61,7 +61,7 @@ def parse():
                     help="timed steps; default: the workload's run length in substeps (RUN_LENGTH), else 200")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="snow", choices=["snow", "jelly", "dam", "batched", "served", "tick", "ck", "midfield"])
+    ap.add_argument("--workload", default="snow", choices=["snow", "jelly", "dam", "batched", "served", "tick", "ck", "midfield", "near"])
     ap.add_argument("--ck-h", type=float, default=1.0,
                     help="ck: grid spacing (the scene scales with it); 1 takes the exact power-of-two division path")
     ap.add_argument("--e2e-reps", type=int, default=3)
@@ -239,6 +239,8 @@ def run_reference(args, rank, pg):
         return run_ck(args, rank, 0, 1, pg, reference=True)
     if args.workload == "midfield":
         return run_midfield(args, rank, 0, 1, pg, reference=True)
+    if args.workload == "near":
+        return run_near(args, rank, 0, 1, pg, reference=True)
     if rank != 0:
         return
     scenes, parts, cfg = workload(args.workload, 0, args.scenes)
@@ -465,6 +467,115 @@ def run_midfield(args, rank, local, world_size, pg, reference=False):
                     "ms_per_step": 1000.0 * t_call, "calls": steps, "timer": "host clock around each call",
                     "vs_baseline": e2e_value / MID_PUBLISHED},
             "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk}), flush=True)
+    ctx.close()
+
+
+# The engine's near-field call (simulation.rs:566-581 -> mpm_step_parallel_with_grid): the near set of the
+# same buffer (10 000 particles within 50 m, the LOD cap), the engine's 4-material table
+# (simulation.rs:251-294), a 64^3 grid of dx 1.6 m centred on the player (:218-226, :545-549), one
+# substep of the frame's dt.
+NEAR = dict(grid=64, dx=1.6, dt=1.0 / 60.0)
+
+
+def near_setup(seed):
+    import ae_mpm as M
+
+    p, _, _, _ = midfield_setup(seed)
+    r = np.linalg.norm(p.pos.astype(np.float64), axis=1)
+    idx = np.flatnonzero(r < MID["near"]).astype(np.uint64)
+    rng = np.random.default_rng(seed + 1)
+    p.mat[:] = rng.integers(0, 4, p.n).astype(np.uint16)
+    mats = [M.material(young_modulus=1.0e6, poisson_ratio=0.3, yield_stress=1.0e4, hardening=0.01, density=1000.0,
+                       friction_angle=35.0, cohesion=0.0),
+            M.material(young_modulus=2.0e6, poisson_ratio=0.45, yield_stress=0.0, hardening=0.0, density=1000.0,
+                       friction_angle=0.0, cohesion=0.0),
+            M.material(young_modulus=5.0e7, poisson_ratio=0.3, yield_stress=0.0, hardening=0.0, density=1600.0,
+                       friction_angle=35.0, cohesion=0.0),
+            M.material(young_modulus=2.0e11, poisson_ratio=0.3, yield_stress=2.5e8, hardening=0.01, density=7850.0,
+                       friction_angle=0.0, cohesion=0.0)]
+    models = [M.NEO_HOOKEAN, M.NEWTONIAN_FLUID, M.DRUCKER_PRAGER, M.VON_MISES]
+    n = NEAR["grid"]
+    half = n * NEAR["dx"] / 2
+    grid = M.Grid(n, n, n, NEAR["dx"], (-half,) * 3)
+    cfg = M.Config(grid_dx=NEAR["dx"], grid_size=(n, n, n), substeps=1, gravity=(0, -9.81, 0), damping=0.995)
+    return p, idx, grid, cfg, mats, models
+
+
+def run_near(args, rank, local, world_size, pg, reference=False):
+    metric, unit = "near-field MPM particle-updates/s", "particle-updates/s"
+    p, idx, grid, ncfg, mats, models = near_setup(0xAE07 + 1000 * rank)
+    n = int(idx.size)
+    cfg = {"workload": "near-field MPM call (mpm_step_parallel_with_grid): %d near particles of a %d-particle buffer, "
+                       "the engine's 4-material table, %d^3 grid, dx %.1f m, 1 substep of 1/60 s"
+                       % (n, p.n, NEAR["grid"], NEAR["dx"]),
+           "particles": n, "grid": NEAR["grid"]}
+    steps = max(1, min(args.steps, 100))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    if reference:  # the CPU restatement of the call (below 50 000 indices the reference's serial path)
+        if rank != 0:
+            return
+        import oracle as O
+
+        for _ in range(max(1, min(args.warmup, 3))):
+            O.step_parallel_with_grid(p, grid, ncfg, mats, models, NEAR["dt"], idx)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            O.step_parallel_with_grid(p, grid, ncfg, mats, models, NEAR["dt"], idx)
+        dt = time.perf_counter() - t0
+        value = n * steps / dt
+        print(json.dumps({"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
+                          "steps": steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / steps,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                          "data": "synthetic (seeded numpy)", "config": cfg,
+                          "cpu_baseline": {"value": value, "unit": unit, "cores": 1, "kind": "port",
+                                           "sample": "the whole call, %d calls" % steps},
+                          "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+    import torch
+
+    import ae_mpm as M
+
+    ctx = M.Context(local)
+    for _ in range(max(args.warmup, 3)):
+        ctx.step_parallel_with_grid(p, grid, ncfg, mats, models, NEAR["dt"], idx)
+    clocks = Clocks(local)
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    clocks.start()
+    time.sleep(0.3)
+    calls = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ctx.step_parallel_with_grid(p, grid, ncfg, mats, models, NEAR["dt"], idx)
+        calls.append(time.perf_counter() - t0)
+    clk = clocks.stop()
+    t_call = max_over_ranks(pg, statistics.median(calls))
+    value = n * world_size / t_call
+    staged = 106 * n  # a sparse index list: every field of the selected particles is gathered and staged
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        import oracle as O
+
+        q = p.copy()
+        O.step_parallel_with_grid(q, grid, ncfg, mats, models, NEAR["dt"], idx)
+        t0 = time.perf_counter()
+        reps = 5
+        for _ in range(reps):
+            O.step_parallel_with_grid(q, grid, ncfg, mats, models, NEAR["dt"], idx)
+        dt = (time.perf_counter() - t0) / reps
+        cpu = {"value": n / dt, "unit": unit, "cores": 1, "kind": "port",
+               "sample": "%d whole calls (%d near particles, the serial path), %.1f ms each" % (reps, n, 1e3 * dt)}
+    if rank == 0:
+        print(json.dumps({
+            "metric": metric, "value": value, "unit": unit, "n_gpus": world_size, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * t_call, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy)",
+            "config": dict(cfg, parallelism="replicas" if world_size > 1 else "single GPU",
+                           timer="host clock around each call: the call is the unit the engine waits on"),
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": staged, "d2h_bytes_per_step": staged,
+                    "ms_per_step": 1000.0 * t_call, "calls": steps},
+            "cpu_baseline": cpu, "clocks": clk}), flush=True)
     ctx.close()
 
 
@@ -790,6 +901,8 @@ def run_ours(args, rank, local, world_size, pg):
         return run_ck(args, rank, local, world_size, pg)
     if args.workload == "midfield":
         return run_midfield(args, rank, local, world_size, pg)
+    if args.workload == "near":
+        return run_near(args, rank, local, world_size, pg)
     ctx = M.Context(local)
     scenes, parts, cfg = workload(args.workload, rank, args.scenes)
     if args.workload == "served":
