@@ -1841,6 +1841,16 @@ class World final : public WorldBase {
     return AE_MPM_OK;
   }
 
+  // whether a particle view's seven arrays lie back to back in the staging order (pos, vel, F, J,
+  // C, mass at 0, 3n, 6n, 15n, 16n, 25n elements, the material indices at 26n)
+  static bool staging_layout(const HostView<T>& hv, uint64_t n) {
+    const uintptr_t b = reinterpret_cast<uintptr_t>(hv.f[0]);
+    const uint64_t at[6] = {0, 3, 6, 15, 16, 25};
+    for (int k = 1; k < 6; ++k)
+      if (reinterpret_cast<uintptr_t>(hv.f[k]) != b + sizeof(T) * at[k] * n) return false;
+    return reinterpret_cast<uintptr_t>(hv.mat) == b + sizeof(T) * 26 * n;
+  }
+
   int upload(uint32_t s, const void* host, uint64_t n, bool f64) override {
     if (s >= h_scenes_.size()) {
       err = "unknown scene";
@@ -1864,14 +1874,19 @@ class World final : public WorldBase {
     int rc = ensure_stage(n);
     if (rc) return rc;
     if (n > 0) {
-      // the view's arrays may be host or device memory (unified addressing picks the direction)
-      AE_TRY(cudaMemcpyAsync(stage_, f[0], sizeof(T) * 3 * n, cudaMemcpyDefault, stream_));
-      AE_TRY(cudaMemcpyAsync(stage_ + 3 * n, f[1], sizeof(T) * 3 * n, cudaMemcpyDefault, stream_));
-      AE_TRY(cudaMemcpyAsync(stage_ + 6 * n, f[2], sizeof(T) * 9 * n, cudaMemcpyDefault, stream_));
-      AE_TRY(cudaMemcpyAsync(stage_ + 15 * n, f[3], sizeof(T) * n, cudaMemcpyDefault, stream_));
-      AE_TRY(cudaMemcpyAsync(stage_ + 16 * n, f[4], sizeof(T) * 9 * n, cudaMemcpyDefault, stream_));
-      AE_TRY(cudaMemcpyAsync(stage_ + 25 * n, f[5], sizeof(T) * n, cudaMemcpyDefault, stream_));
-      AE_TRY(cudaMemcpyAsync(stage_ + 26 * n, hv.mat, sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+      // the view's arrays may be host or device memory (unified addressing picks the direction);
+      // a view laid out as the staging itself travels in one copy
+      if (staging_layout(hv, n)) {
+        AE_TRY(cudaMemcpyAsync(stage_, f[0], sizeof(T) * 26 * n + sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+      } else {
+        AE_TRY(cudaMemcpyAsync(stage_, f[0], sizeof(T) * 3 * n, cudaMemcpyDefault, stream_));
+        AE_TRY(cudaMemcpyAsync(stage_ + 3 * n, f[1], sizeof(T) * 3 * n, cudaMemcpyDefault, stream_));
+        AE_TRY(cudaMemcpyAsync(stage_ + 6 * n, f[2], sizeof(T) * 9 * n, cudaMemcpyDefault, stream_));
+        AE_TRY(cudaMemcpyAsync(stage_ + 15 * n, f[3], sizeof(T) * n, cudaMemcpyDefault, stream_));
+        AE_TRY(cudaMemcpyAsync(stage_ + 16 * n, f[4], sizeof(T) * 9 * n, cudaMemcpyDefault, stream_));
+        AE_TRY(cudaMemcpyAsync(stage_ + 25 * n, f[5], sizeof(T) * n, cudaMemcpyDefault, stream_));
+        AE_TRY(cudaMemcpyAsync(stage_ + 26 * n, hv.mat, sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+      }
       rc = sync_tables();
       if (rc) return rc;
       pack_kernel<T><<<unsigned((n + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), stage_, n, h_scenes_[s].p_off,
@@ -1912,13 +1927,17 @@ class World final : public WorldBase {
     unpack_kernel<T><<<unsigned((n + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), stage_, n, h_scenes_[s].p_off,
                                                                       d_scenes_ + s, d_mats_);
     AE_TRY(cudaGetLastError());
-    AE_TRY(cudaMemcpyAsync(f[0], stage_, sizeof(T) * 3 * n, cudaMemcpyDefault, stream_));
-    AE_TRY(cudaMemcpyAsync(f[1], stage_ + 3 * n, sizeof(T) * 3 * n, cudaMemcpyDefault, stream_));
-    AE_TRY(cudaMemcpyAsync(f[2], stage_ + 6 * n, sizeof(T) * 9 * n, cudaMemcpyDefault, stream_));
-    AE_TRY(cudaMemcpyAsync(f[3], stage_ + 15 * n, sizeof(T) * n, cudaMemcpyDefault, stream_));
-    AE_TRY(cudaMemcpyAsync(f[4], stage_ + 16 * n, sizeof(T) * 9 * n, cudaMemcpyDefault, stream_));
-    AE_TRY(cudaMemcpyAsync(f[5], stage_ + 25 * n, sizeof(T) * n, cudaMemcpyDefault, stream_));
-    AE_TRY(cudaMemcpyAsync(hv.mat, stage_ + 26 * n, sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+    if (staging_layout(hv, n)) {
+      AE_TRY(cudaMemcpyAsync(f[0], stage_, sizeof(T) * 26 * n + sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+    } else {
+      AE_TRY(cudaMemcpyAsync(f[0], stage_, sizeof(T) * 3 * n, cudaMemcpyDefault, stream_));
+      AE_TRY(cudaMemcpyAsync(f[1], stage_ + 3 * n, sizeof(T) * 3 * n, cudaMemcpyDefault, stream_));
+      AE_TRY(cudaMemcpyAsync(f[2], stage_ + 6 * n, sizeof(T) * 9 * n, cudaMemcpyDefault, stream_));
+      AE_TRY(cudaMemcpyAsync(f[3], stage_ + 15 * n, sizeof(T) * n, cudaMemcpyDefault, stream_));
+      AE_TRY(cudaMemcpyAsync(f[4], stage_ + 16 * n, sizeof(T) * 9 * n, cudaMemcpyDefault, stream_));
+      AE_TRY(cudaMemcpyAsync(f[5], stage_ + 25 * n, sizeof(T) * n, cudaMemcpyDefault, stream_));
+      AE_TRY(cudaMemcpyAsync(hv.mat, stage_ + 26 * n, sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+    }
     AE_TRY(cudaStreamSynchronize(stream_));
     return AE_MPM_OK;
   }
