@@ -247,7 +247,7 @@ int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64
   // bounds and order of the index list (split over threads for long lists; the message names the
   // first index out of range)
   uint64_t max_idx = 0;
-  int descents = 0;
+  uint64_t descents = 0;
   const int t_idx = n >= (uint64_t(1) << 16) ? std::min(8, omp_get_max_threads()) : 1;
 #pragma omp parallel for num_threads(t_idx) schedule(static) reduction(max : max_idx) reduction(+ : descents)
   for (int64_t k = 0; k < int64_t(n); ++k) {
@@ -277,7 +277,12 @@ int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64
   d.wall_margin = 0;
   d.n_materials = uint32_t(mats.size());
   d.materials = mats.data();
-  d.max_particles = n;
+  // capacity: the power of two at or above n, the particle bucket the cached world is keyed by, so a
+  // later call with a different count in the same bucket (the near set changes from tick to tick)
+  // reuses the world
+  uint64_t cap = 1;
+  while (cap < n) cap <<= 1;
+  d.max_particles = cap;
   ae_mpm_exec_opts o;
   ae_mpm_exec_opts_default(&o);
   std::string sig = world_signature(&d, 1, o) + "|" + std::to_string(mats.size());
@@ -307,25 +312,25 @@ int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64
     const DropinLayout l = dropin_layout(capacity, n, full);
     rc = ensure_dstage(ctx, l.bytes);
     if (rc) return rc;
-    char* d = static_cast<char*>(ctx->dstage);
+    char* dst = static_cast<char*>(ctx->dstage);
     ae_mpm_particles dfull{}, dsel{};
-    dfull.pos = reinterpret_cast<float*>(d + l.off[0]);
-    dfull.vel = reinterpret_cast<float*>(d + l.off[1]);
-    dfull.mass = reinterpret_cast<float*>(d + l.off[2]);
+    dfull.pos = reinterpret_cast<float*>(dst + l.off[0]);
+    dfull.vel = reinterpret_cast<float*>(dst + l.off[1]);
+    dfull.mass = reinterpret_cast<float*>(dst + l.off[2]);
     if (full) {
-      dfull.strain = reinterpret_cast<float*>(d + l.off[3]);
-      dfull.c = reinterpret_cast<float*>(d + l.off[4]);
-      dfull.jacobian = reinterpret_cast<float*>(d + l.off[5]);
-      dfull.material_idx = reinterpret_cast<uint16_t*>(d + l.off[6]);
+      dfull.strain = reinterpret_cast<float*>(dst + l.off[3]);
+      dfull.c = reinterpret_cast<float*>(dst + l.off[4]);
+      dfull.jacobian = reinterpret_cast<float*>(dst + l.off[5]);
+      dfull.material_idx = reinterpret_cast<uint16_t*>(dst + l.off[6]);
     }
-    uint64_t* didx = reinterpret_cast<uint64_t*>(d + l.off[7]);
-    dsel.pos = reinterpret_cast<float*>(d + l.off[8]);
-    dsel.vel = reinterpret_cast<float*>(d + l.off[9]);
-    dsel.strain = reinterpret_cast<float*>(d + l.off[10]);
-    dsel.jacobian = reinterpret_cast<float*>(d + l.off[11]);
-    dsel.c = reinterpret_cast<float*>(d + l.off[12]);
-    dsel.mass = reinterpret_cast<float*>(d + l.off[13]);
-    dsel.material_idx = reinterpret_cast<uint16_t*>(d + l.off[14]);
+    uint64_t* didx = reinterpret_cast<uint64_t*>(dst + l.off[7]);
+    dsel.pos = reinterpret_cast<float*>(dst + l.off[8]);
+    dsel.vel = reinterpret_cast<float*>(dst + l.off[9]);
+    dsel.strain = reinterpret_cast<float*>(dst + l.off[10]);
+    dsel.jacobian = reinterpret_cast<float*>(dst + l.off[11]);
+    dsel.c = reinterpret_cast<float*>(dst + l.off[12]);
+    dsel.mass = reinterpret_cast<float*>(dst + l.off[13]);
+    dsel.material_idx = reinterpret_cast<uint16_t*>(dst + l.off[14]);
     // pinned staging mirrors the device layout of the whole arrays and the index list
     rc = ensure_pinned(ctx, l.off[8]);
     if (rc) return rc;
@@ -336,7 +341,7 @@ int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64
     auto in = [&](int r, const void* src, size_t b) {
       if (e != cudaSuccess) return;
       host_copy(hp + l.off[r], src, b);
-      e = cudaMemcpyAsync(d + l.off[r], hp + l.off[r], b, cudaMemcpyHostToDevice, st);
+      e = cudaMemcpyAsync(dst + l.off[r], hp + l.off[r], b, cudaMemcpyHostToDevice, st);
     };
     in(0, buffer->pos, 12 * capacity);
     in(1, buffer->vel, 12 * capacity);
@@ -368,7 +373,7 @@ int dropin_run(ae_mpm_ctx* ctx, int mode, const ae_mpm_particles* buffer, uint64
     for (int k = 0; k < n_out && e == cudaSuccess; ++k) {
       if (!ctx->out_ev[k]) e = cudaEventCreateWithFlags(&ctx->out_ev[k], cudaEventDisableTiming);
       if (e == cudaSuccess)
-        e = cudaMemcpyAsync(hp + l.off[outs[k]], d + l.off[outs[k]], out_b[k], cudaMemcpyDeviceToHost, st);
+        e = cudaMemcpyAsync(hp + l.off[outs[k]], dst + l.off[outs[k]], out_b[k], cudaMemcpyDeviceToHost, st);
       if (e == cudaSuccess) e = cudaEventRecord(ctx->out_ev[k], st);
     }
     for (int k = 0; k < n_out && e == cudaSuccess; ++k) {

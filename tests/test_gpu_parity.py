@@ -300,6 +300,25 @@ def test_dropin_reference_index_patterns_match_oracle(ctx, pattern):
         assert np.array_equal(getattr(a, f)[untouched], getattr(p, f)[untouched]), f
 
 
+@pytest.mark.parametrize("order", ["ascending", "descending"])
+def test_dropin_counts_change_within_a_capacity_bucket(ctx, order):
+    # the drop-in world is cached per power-of-two particle bucket: counts that grow and shrink inside
+    # one bucket (the engine's near set from tick to tick) reuse it, on both data paths
+    p, g, cfg, mats, mods = _ref_setup(n=9000, models=(M.NEO_HOOKEAN, M.NEWTONIAN_FLUID))
+    for m in (3000, 3500, 2100, 4096):
+        idx = np.arange(m, dtype=np.uint64)
+        if order == "descending":
+            idx = idx[::-1].copy()
+        a, b = p.copy(), p.copy()
+        ctx.step_parallel_with_grid(a, g, cfg, mats, mods, 0.016, idx)
+        assert O.step_parallel_with_grid(b, g, cfg, mats, mods, 0.016, idx) == 0
+        assert rel(a.pos, b.pos) <= 2e-5, m
+        v1, v2 = p.copy(), p.copy()
+        ctx.step_velocity_only_parallel(v1, g, cfg, 0.016, idx)
+        assert O.step_velocity_only_parallel(v2, g, cfg, 0.016, idx) == 0
+        assert rel(v1.pos, v2.pos) <= 2e-5, m
+
+
 def test_dropin_empty_and_invalid_calls(ctx):
     p, g, cfg, mats, mods = _ref_setup(n=10)
     a = p.copy()
