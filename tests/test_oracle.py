@@ -204,6 +204,133 @@ def test_snow_collision_oracle_f32_tracks_f64_through_plastic_flow():
     assert rel(r32.J, r64.J) <= 1e-4
 
 
+def _velocity_only_substep_np(pos, vel, mass, idx, grid, dt, gravity, damping):
+    """mpm_substep_velocity_only (ae_particle/src/mpm_solver.rs:1353-1572) restated with numpy float32
+    scalars, one IEEE single rounding per operation: serial P2G in index order, the dense grid update
+    (Grid::update_parallel :112-139 without forces), G2P of velocity only with the NaN and |v| <= 50
+    guards, the mixed wall rules and damping."""
+    f = np.float32
+    nx, ny, nz = grid.nx, grid.ny, grid.nz
+    dx = f(grid.dx)
+    inv_dx = f(1.0) / dx
+    org = [f(o) for o in grid.origin]
+    gmass = np.zeros(nx * ny * nz, np.float32)
+    gvel = np.zeros((nx * ny * nz, 3), np.float32)
+
+    def bs(x):
+        ax = abs(x)
+        if ax < f(0.5):
+            return f(0.75) - ax * ax
+        if ax < f(1.5):
+            t = f(1.5) - ax
+            return f(0.5) * t * t
+        return f(0.0)
+
+    def stencil(p):
+        g, fr = [], []
+        for a in range(3):
+            q = (p[a] - org[a]) * inv_dx - f(0.5)
+            gi = int(np.floor(q))
+            fr.append((p[a] - org[a]) * inv_dx - f(0.5) - f(gi))
+            g.append(max(gi, 0))
+        w = [[bs(f(k) - fr[a]) for k in range(3)] for a in range(3)]
+        return g, w
+
+    for i in idx:
+        p = pos[i]
+        g, w = stencil(p)
+        wm = mass[i]
+        for dk in range(3):
+            if w[2][dk] < f(1e-10) or g[2] + dk >= nz:
+                continue
+            for dj in range(3):
+                if w[1][dj] < f(1e-10) or g[1] + dj >= ny:
+                    continue
+                wyz = w[1][dj] * w[2][dk]
+                for di in range(3):
+                    ww = w[0][di] * wyz
+                    if ww < f(1e-10) or g[0] + di >= nx:
+                        continue
+                    gid = (g[0] + di) + (g[1] + dj) * nx + (g[2] + dk) * nx * ny
+                    gmass[gid] += ww * wm
+                    for a in range(3):
+                        gvel[gid, a] += ww * wm * vel[i, a]
+    grav = [f(x) for x in gravity]
+    for gid in range(nx * ny * nz):
+        m = gmass[gid]
+        if m > f(1e-12):
+            for a in range(3):
+                gvel[gid, a] = gvel[gid, a] / m + (grav[a] + f(0.0) / m) * dt
+            if (gid % (nx * ny)) // nx == 0:
+                gvel[gid, 1] = max(gvel[gid, 1], f(0.0))
+                gvel[gid, 0] *= f(0.9)
+                gvel[gid, 2] *= f(0.9)
+    gmax_x = f(nx - 1) * dx
+    gmax_z = f(nz - 1) * dx
+    for i in idx:
+        p = pos[i].copy()
+        g, w = stencil(p)
+        nv = [f(0.0)] * 3
+        for dk in range(3):
+            if w[2][dk] < f(1e-10) or g[2] + dk >= nz:
+                continue
+            for dj in range(3):
+                if w[1][dj] < f(1e-10) or g[1] + dj >= ny:
+                    continue
+                wyz = w[1][dj] * w[2][dk]
+                for di in range(3):
+                    ww = w[0][di] * wyz
+                    if ww < f(1e-10) or g[0] + di >= nx:
+                        continue
+                    gid = (g[0] + di) + (g[1] + dj) * nx + (g[2] + dk) * nx * ny
+                    if gmass[gid] < f(1e-12):
+                        continue
+                    nv = [nv[a] + ww * gvel[gid, a] for a in range(3)]
+        if not all(np.isfinite(nv)):
+            nv = [f(0.0)] * 3
+        nv = [min(max(v, f(-50.0)), f(50.0)) for v in nv]
+        npos = [p[a] + nv[a] * dt for a in range(3)]
+        if not all(np.isfinite(npos)):
+            npos, nv = list(p), [f(0.0)] * 3
+        if npos[1] < f(0.0):
+            npos[1], nv[1] = f(0.0), max(nv[1], f(0.0)) * f(0.5)
+        if npos[0] < f(0.0):
+            npos[0], nv[0] = f(0.0), max(nv[0], f(0.0)) * f(0.5)
+        elif npos[0] > gmax_x + org[0]:
+            npos[0], nv[0] = gmax_x + org[0], min(nv[0], f(0.0)) * f(0.5)
+        if npos[2] < f(0.0):
+            npos[2], nv[2] = f(0.0), max(nv[2], f(0.0)) * f(0.5)
+        elif npos[2] > gmax_z + org[2]:
+            npos[2], nv[2] = gmax_z + org[2], min(nv[2], f(0.0)) * f(0.5)
+        pos[i] = npos
+        vel[i] = [v * f(damping) for v in nv]
+
+
+@pytest.mark.parametrize("origin", [(0.0, 0.0, 0.0), (-0.4, 0.0, -0.4)])
+def test_velocity_only_oracle_matches_a_numpy_restatement(origin):
+    # the oracle's mpm_step_velocity_only_parallel against an independent float32 restatement of the
+    # reference's substep, bit for bit; particles near the walls exercise the mixed wall rules
+    rng = np.random.default_rng(3)
+    n, grid_n, dx = 400, 8, 0.1
+    p = M.Particles.empty(n)
+    lo = np.asarray(origin) + 0.05
+    p.pos[:] = (lo + rng.random((n, 3)) * (grid_n - 1) * dx).astype(np.float32)
+    p.vel[:] = rng.normal(0, 2.0, (n, 3)).astype(np.float32)
+    p.mass[:] = rng.uniform(0.5, 2.0, n).astype(np.float32)
+    g = M.Grid(grid_n, grid_n, grid_n, dx, origin)
+    cfg = M.Config(grid_dx=dx, grid_size=(grid_n,) * 3, substeps=2, gravity=(0, -9.81, 0), damping=0.995)
+    idx = np.sort(rng.choice(n, 300, replace=False)).astype(np.uint64)
+    a = p.copy()
+    assert O.step_velocity_only_parallel(a, g, cfg, 0.02, idx) == 0
+    pos, vel = p.pos.copy(), p.vel.copy()
+    sub_dt = np.float32(0.02) / np.float32(cfg.substeps)
+    for _ in range(cfg.substeps):
+        _velocity_only_substep_np(pos, vel, p.mass, idx.astype(np.int64), g, sub_dt, (0, -9.81, 0), 0.995)
+    assert np.array_equal(a.pos, pos) and np.array_equal(a.vel, vel)
+    untouched = np.setdiff1d(np.arange(n), idx.astype(np.int64))
+    assert np.array_equal(a.pos[untouched], p.pos[untouched])
+
+
 def test_svd3_reflection_gives_negative_last_singular_value():
     F = np.diag([1.1, 0.9, -1.0])
     U, s, V, _ = O.svd3(F, f64=True)
