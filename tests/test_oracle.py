@@ -331,6 +331,193 @@ def test_velocity_only_oracle_matches_a_numpy_restatement(origin):
     assert np.array_equal(a.pos[untouched], p.pos[untouched])
 
 
+def _serial_substep_np(p, idx, grid, dt, gravity, damping, mats, models):
+    """mpm_substep_serial_active (ae_particle/src/mpm_solver.rs:812-1054) with the neo-Hookean and
+    Newtonian-fluid stresses (constitutive.rs:375-393, 603-617) restated with numpy float32 scalars,
+    one IEEE single rounding per operation, ln from the C library as Rust's f32::ln."""
+    import ctypes
+
+    logf = ctypes.CDLL("libm.so.6").logf
+    logf.restype, logf.argtypes = ctypes.c_float, [ctypes.c_float]
+    f = np.float32
+    nx, ny, nz = grid.nx, grid.ny, grid.nz
+    dx = f(grid.dx)
+    inv_dx = f(1.0) / dx
+    org = [f(o) for o in grid.origin]
+    n_nodes = nx * ny * nz
+    gm = np.zeros(n_nodes, np.float32)
+    gv = np.zeros((n_nodes, 3), np.float32)
+    gf = np.zeros((n_nodes, 3), np.float32)
+
+    def bs(x):
+        ax = abs(x)
+        if ax < f(0.5):
+            return f(0.75) - ax * ax
+        if ax < f(1.5):
+            t = f(1.5) - ax
+            return f(0.5) * t * t
+        return f(0.0)
+
+    def dbs(x):
+        ax = abs(x)
+        if ax < f(0.5):
+            return f(-2.0) * x
+        if ax < f(1.5):
+            return -(f(1.5) - ax) * f(math.copysign(1.0, float(x)))
+        return f(0.0)
+
+    def lame(m):
+        nu = min(max(f(m.poisson_ratio), f(-0.999)), f(0.4999))
+        e = f(m.young_modulus)
+        return e / (f(2.0) * (f(1.0) + nu)), e * nu / ((f(1.0) + nu) * (f(1.0) - f(2.0) * nu)), \
+            e / (f(3.0) * (f(1.0) - f(2.0) * nu))
+
+    def stress(model, m, F, J):
+        mu, la, k = lame(m)
+        if model == M.NEWTONIAN_FLUID:
+            sd = k * (J - f(1.0))
+            return [sd, f(0), f(0), f(0), sd, f(0), f(0), f(0), sd]
+        b = [F[r * 3 + 0] * F[c * 3 + 0] + F[r * 3 + 1] * F[c * 3 + 1] + F[r * 3 + 2] * F[c * 3 + 2]
+             for r in range(3) for c in range(3)]
+        p_term = la * f(logf(J)) / J if J > f(0.0) else f(0.0)
+        scale = mu / max(J, f(1e-10))
+        return [scale * ((b[i] - f(1.0) + p_term / scale) if i % 4 == 0 else b[i]) for i in range(9)]
+
+    def base(x):
+        g, fr = [], []
+        for a in range(3):
+            gi = int(np.floor((x[a] - org[a]) * inv_dx - f(0.5)))
+            fr.append((x[a] - org[a]) * inv_dx - f(0.5) - f(gi))
+            g.append(max(gi, 0))
+        return g, fr
+
+    def stencil(g, fr):
+        for dk in range(3):
+            for dj in range(3):
+                for di in range(3):
+                    w = bs(f(di) - fr[0]) * bs(f(dj) - fr[1]) * bs(f(dk) - fr[2])
+                    if w < f(1e-10):
+                        continue
+                    X, Y, Z = g[0] + di, g[1] + dj, g[2] + dk
+                    if X >= nx or Y >= ny or Z >= nz:
+                        continue
+                    dw = [dbs(f(di) - fr[0]) * inv_dx, dbs(f(dj) - fr[1]) * inv_dx, dbs(f(dk) - fr[2]) * inv_dx]
+                    d = [(f(X) + f(0.5)) * dx + org[0], (f(Y) + f(0.5)) * dx + org[1], (f(Z) + f(0.5)) * dx + org[2]]
+                    yield X + Y * nx + Z * nx * ny, w, dw, d
+
+    for i in idx:
+        mi = int(p.mat[i])
+        m = mats[mi] if mi < len(mats) else mats[0]
+        model = models[mi] if mi < len(models) else M.NEO_HOOKEAN
+        sig = stress(model, m, list(p.F[i]), p.J[i])
+        vol = p.mass[i] / f(m.density)
+        sv = [vol * x for x in sig]
+        g, fr = base(p.pos[i])
+        c, v, x, mass = p.C[i], p.vel[i], p.pos[i], p.mass[i]
+        for gid, w, dw, d in stencil(g, fr):
+            dg = [d[a] - x[a] for a in range(3)]
+            vv = [v[r] + c[3 * r] * dg[0] + c[3 * r + 1] * dg[1] + c[3 * r + 2] * dg[2] for r in range(3)]
+            gm[gid] += w * mass
+            for r in range(3):
+                gv[gid, r] += w * mass * vv[r]
+            for r in range(3):
+                gf[gid, r] += sv[3 * r] * dw[0] + sv[3 * r + 1] * dw[1] + sv[3 * r + 2] * dw[2]
+    grav = [f(a) for a in gravity]
+    for gid in range(n_nodes):
+        mm = gm[gid]
+        if mm > f(1e-12):
+            for r in range(3):
+                gv[gid, r] = gv[gid, r] / mm + (grav[r] + gf[gid, r] / mm) * dt
+            if (gid % (nx * ny)) // nx == 0:
+                gv[gid, 1] = max(gv[gid, 1], f(0.0))
+                gv[gid, 0] *= f(0.9)
+                gv[gid, 2] *= f(0.9)
+    gmax_x, gmax_z = f(nx - 1) * dx, f(nz - 1) * dx
+    for i in idx:
+        x = list(p.pos[i])
+        g, fr = base(x)
+        nv, nc, gr = [f(0)] * 3, [f(0)] * 9, [f(0)] * 9
+        for gid, w, dw, d in stencil(g, fr):
+            if gm[gid] < f(1e-12):
+                continue
+            u = gv[gid]
+            dg = [d[a] - x[a] for a in range(3)]
+            nv = [nv[r] + w * u[r] for r in range(3)]
+            sc = f(4.0) * inv_dx * inv_dx * w
+            nc = [nc[3 * r + a] + sc * u[r] * dg[a] for r in range(3) for a in range(3)]
+            gr = [gr[3 * r + a] - w * u[r] * dw[a] for r in range(3) for a in range(3)]
+        if not all(np.isfinite(nv)):
+            nv, nc = [f(0)] * 3, [f(0)] * 9
+        nv = [min(max(a, f(-50.0)), f(50.0)) for a in nv]
+        npos = [x[a] + nv[a] * dt for a in range(3)]
+        if not all(np.isfinite(npos)):
+            npos, nv = [f(6.0), f(5.0), f(6.0)], [f(0)] * 3
+        if npos[1] < f(0.0):
+            npos[1], nv[1] = f(0.0), max(nv[1], f(0.0)) * f(0.5)
+        if npos[0] < f(0.0):
+            npos[0], nv[0] = f(0.0), max(nv[0], f(0.0)) * f(0.5)
+        elif npos[0] > gmax_x:
+            npos[0], nv[0] = gmax_x, min(nv[0], f(0.0)) * f(0.5)
+        if npos[2] < f(0.0):
+            npos[2], nv[2] = f(0.0), max(nv[2], f(0.0)) * f(0.5)
+        elif npos[2] > gmax_z:
+            npos[2], nv[2] = gmax_z, min(nv[2], f(0.0)) * f(0.5)
+        F = p.F[i]
+        nf = []
+        for r in range(3):
+            for c2 in range(3):
+                acc = f(0.0)
+                for k in range(3):
+                    acc = acc + ((f(1.0) if r == k else f(0.0)) + gr[3 * r + k] * dt) * F[3 * k + c2]
+                nf.append(acc)
+        if all(np.isfinite(nf)) and all(abs(a) <= f(1e3) for a in nf):
+            J = nf[0] * (nf[4] * nf[8] - nf[5] * nf[7]) - nf[1] * (nf[3] * nf[8] - nf[5] * nf[6]) + \
+                nf[2] * (nf[3] * nf[7] - nf[4] * nf[6])
+            fin, jn = nf, min(max(J, f(0.1)), f(10.0))
+        else:
+            fin, jn = [f(1), f(0), f(0), f(0), f(1), f(0), f(0), f(0), f(1)], f(1.0)
+        p.vel[i] = [a * f(damping) for a in nv]
+        p.C[i] = nc
+        p.pos[i] = npos
+        p.F[i] = fin
+        p.J[i] = jn
+
+
+def test_reference_serial_oracle_matches_a_numpy_restatement():
+    # the oracle's drop-in substep (below 50 000 indices: mpm_substep_serial_active) against an
+    # independent float32 restatement, bit for bit, with the neo-Hookean and fluid models, a material
+    # index past the tables (material_table[0] with NeoHookean), deformed F and a nonzero C
+    rng = np.random.default_rng(9)
+    n, grid_n, dx = 300, 12, 0.05
+    p = M.Particles.empty(n)
+    p.pos[:] = (0.08 + rng.random((n, 3)) * 0.44).astype(np.float32)
+    p.vel[:] = rng.normal(0, 0.5, (n, 3)).astype(np.float32)
+    p.F[:] = (np.eye(3).reshape(9) + rng.normal(0, 0.03, (n, 9))).astype(np.float32)
+    p.J[:] = np.linalg.det(p.F.reshape(-1, 3, 3).astype(np.float64)).astype(np.float32)
+    p.C[:] = rng.normal(0, 0.5, (n, 9)).astype(np.float32)
+    p.mass[:] = rng.uniform(0.5e-3, 2e-3, n).astype(np.float32)
+    p.mat[:] = rng.integers(0, 3, n).astype(np.uint16)
+    p.pos[:20, 0], p.vel[:20, 0] = 0.001, -3.0  # into the x = 0 wall
+    p.pos[20:40, 1], p.vel[20:40, 1] = 0.001, -3.0  # into the floor
+    mats = [M.material(young_modulus=1e4, poisson_ratio=0.25, density=1000.0),
+            M.material(young_modulus=2e4, poisson_ratio=0.45, density=1000.0)]
+    models = [M.NEO_HOOKEAN, M.NEWTONIAN_FLUID]
+    g = M.Grid(grid_n, grid_n, grid_n, dx, (0.0, 0.0, 0.0))
+    cfg = M.Config(grid_dx=dx, grid_size=(grid_n,) * 3, substeps=2, gravity=(0, -9.81, 0), damping=0.995)
+    idx = np.sort(rng.choice(n, 240, replace=False)).astype(np.uint64)
+    a = p.copy()
+    assert O.step_parallel_with_grid(a, g, cfg, mats, models, 0.004, idx) == 0
+    b = p.copy()
+    sub_dt = np.float32(0.004) / np.float32(cfg.substeps)
+    for _ in range(cfg.substeps):
+        _serial_substep_np(b, idx.astype(np.int64), g, sub_dt, (0, -9.81, 0), 0.995, mats, models)
+    for fld in ("pos", "vel", "F", "J", "C"):
+        assert np.array_equal(getattr(a, fld), getattr(b, fld)), fld
+    assert not np.array_equal(a.pos, p.pos) and not np.array_equal(a.F, p.F)
+    sel = idx.astype(np.int64)
+    assert (a.pos[sel, 0] == 0).sum() > 0 and (a.pos[sel, 1] == 0).sum() > 0  # the wall rules ran
+
+
 def test_svd3_reflection_gives_negative_last_singular_value():
     F = np.diag([1.1, 0.9, -1.0])
     U, s, V, _ = O.svd3(F, f64=True)
