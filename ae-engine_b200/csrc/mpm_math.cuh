@@ -192,7 +192,8 @@ AE_HD void ref_stress(const MatDev& p, const T* F, T J, T* st) {
       T scale = T(1);
       bool plastic = false;
       if (p.model == kDruckerPrager) {
-        T phi = T(p.friction_angle) * T(3.14159265358979323846) / T(180);
+        // friction_angle.to_radians(): times the degree-to-radian constant pi / 180 rounded to T
+        T phi = T(p.friction_angle) * (T(3.14159265358979323846) / T(180));
         T sphi = t_sin(phi), cphi = t_cos(phi), s3 = t_sqrt(T(3));
         T alpha = (T(2) * sphi) / (s3 * (T(3) - sphi));
         T k = (T(6) * T(p.cohesion) * cphi) / (s3 * (T(3) - sphi));

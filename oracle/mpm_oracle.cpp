@@ -190,7 +190,8 @@ bool compute_stress(int model, const ae_mpm_material& p, const T* F, T J, T* str
       bool plastic = false;
       T scale = T(1);
       if (model == AE_MPM_DRUCKER_PRAGER) {
-        T phi = T(p.friction_angle) * T(3.14159265358979323846) / T(180);
+        // friction_angle.to_radians(): times the degree-to-radian constant pi / 180 rounded to T
+        T phi = T(p.friction_angle) * (T(3.14159265358979323846) / T(180));
         T sphi = std::sin(phi), cphi = std::cos(phi), s3 = std::sqrt(T(3));
         T alpha = (T(2) * sphi) / (s3 * (T(3) - sphi));
         T k = (T(6) * T(p.cohesion) * cphi) / (s3 * (T(3) - sphi));

@@ -331,15 +331,98 @@ def test_velocity_only_oracle_matches_a_numpy_restatement(origin):
     assert np.array_equal(a.pos[untouched], p.pos[untouched])
 
 
+# ---- float32 restatement of the reference's constitutive models (constitutive.rs), one IEEE single
+# rounding per operation; sin, cos and ln from the C library as Rust's f32 methods
+import ctypes  # noqa: E402
+
+_LIBM = ctypes.CDLL("libm.so.6")
+logf, sinf, cosf = _LIBM.logf, _LIBM.sinf, _LIBM.cosf
+for _fn in (logf, sinf, cosf):
+    _fn.restype, _fn.argtypes = ctypes.c_float, [ctypes.c_float]
+f = np.float32
+
+
+def _lame_np(m):
+    nu = min(max(f(m.poisson_ratio), f(-0.999)), f(0.4999))
+    e = f(m.young_modulus)
+    return e / (f(2.0) * (f(1.0) + nu)), e * nu / ((f(1.0) + nu) * (f(1.0) - f(2.0) * nu)), \
+        e / (f(3.0) * (f(1.0) - f(2.0) * nu))
+
+
+def _mm_np(a, b):
+    return [a[r * 3 + 0] * b[0 * 3 + c] + a[r * 3 + 1] * b[1 * 3 + c] + a[r * 3 + 2] * b[2 * 3 + c]
+            for r in range(3) for c in range(3)]
+
+def _inv_t_np(q):  # constitutive.rs:306-324 (the adjugate over the determinant: the inverse)
+    det = q[0] * (q[4] * q[8] - q[5] * q[7]) - q[1] * (q[3] * q[8] - q[5] * q[6]) + q[2] * (q[3] * q[7] - q[4] * q[6])
+    if abs(det) < f(1e-15):
+        return [f(1), f(0), f(0), f(0), f(1), f(0), f(0), f(0), f(1)]
+    i = f(1.0) / det
+    return [(q[4] * q[8] - q[5] * q[7]) * i, -(q[1] * q[8] - q[2] * q[7]) * i, (q[1] * q[5] - q[2] * q[4]) * i,
+            -(q[3] * q[8] - q[5] * q[6]) * i, (q[0] * q[8] - q[2] * q[6]) * i, -(q[0] * q[5] - q[2] * q[3]) * i,
+            (q[3] * q[7] - q[4] * q[6]) * i, -(q[0] * q[7] - q[1] * q[6]) * i, (q[0] * q[4] - q[1] * q[3]) * i]
+
+def _polar_np(F):  # constitutive.rs:284-304
+    r = list(F)
+    for _ in range(8):
+        ri = _inv_t_np(r)
+        nr = [f(0.5) * (r[i] + ri[i]) for i in range(9)]
+        diff = f(0.0)
+        for i in range(9):
+            diff = diff + abs(nr[i] - r[i])
+        r = nr
+        if diff < f(1e-10):
+            break
+    rt = [r[0], r[3], r[6], r[1], r[4], r[7], r[2], r[5], r[8]]
+    return r, _mm_np(rt, F)
+
+def _deviatoric_np(m, F):  # the shared trial of constitutive.rs:443-600
+    mu, la, _ = _lame_np(m)
+    _, sm = _polar_np(F)
+    eps = [sm[0] - f(1), sm[1], sm[2], sm[3], sm[4] - f(1), sm[5], sm[6], sm[7], sm[8] - f(1)]
+    tr = eps[0] + eps[4] + eps[8]
+    tr3 = tr / f(3.0)
+    for i in (0, 4, 8):
+        eps[i] = eps[i] - tr3
+    sd = [f(2.0) * mu * e for e in eps]
+    sn = np.sqrt(f(0.5) * (sd[0] * sd[0] + sd[4] * sd[4] + sd[8] * sd[8] + f(2.0) * (
+        sd[1] * sd[1] + sd[2] * sd[2] + sd[3] * sd[3] + sd[5] * sd[5] + sd[6] * sd[6] + sd[7] * sd[7])))
+    return sd, sn, -la * tr
+
+def _ref_stress_np(model, m, F, J):
+    mu, la, k = _lame_np(m)
+    if model == M.NEWTONIAN_FLUID:
+        sd = k * (J - f(1.0))
+        return [sd, f(0), f(0), f(0), sd, f(0), f(0), f(0), sd]
+    if model in (M.DRUCKER_PRAGER, M.VON_MISES):
+        sd, sn, pressure = _deviatoric_np(m, F)
+        if model == M.DRUCKER_PRAGER:
+            phi = f(m.friction_angle) * (f(math.pi) / f(180.0))  # f32::to_radians
+            sphi, cphi, s3 = f(sinf(phi)), f(cosf(phi)), np.sqrt(f(3.0))
+            alpha = (f(2.0) * sphi) / (s3 * (f(3.0) - sphi))
+            kk = (f(6.0) * f(m.cohesion) * cphi) / (s3 * (f(3.0) - sphi))
+            if sn + alpha * pressure - kk > f(0.0):
+                sc = max(kk - alpha * pressure, f(0.0)) / max(sn, f(1e-10))
+                sd = [x * sc for x in sd]
+        else:
+            thr = f(m.yield_stress) / np.sqrt(f(3.0))
+            if sn > thr:
+                sc = thr / sn
+                sd = [x * sc for x in sd]
+        for i in (0, 4, 8):
+            sd[i] = sd[i] - pressure
+        return sd
+    b = [F[r * 3 + 0] * F[c * 3 + 0] + F[r * 3 + 1] * F[c * 3 + 1] + F[r * 3 + 2] * F[c * 3 + 2]
+         for r in range(3) for c in range(3)]
+    p_term = la * f(logf(J)) / J if J > f(0.0) else f(0.0)
+    scale = mu / max(J, f(1e-10))
+    return [scale * ((b[i] - f(1.0) + p_term / scale) if i % 4 == 0 else b[i]) for i in range(9)]
+
+
 def _serial_substep_np(p, idx, grid, dt, gravity, damping, mats, models):
     """mpm_substep_serial_active (ae_particle/src/mpm_solver.rs:812-1054) with the neo-Hookean and
     Newtonian-fluid stresses (constitutive.rs:375-393, 603-617) restated with numpy float32 scalars,
     one IEEE single rounding per operation, ln from the C library as Rust's f32::ln."""
-    import ctypes
-
-    logf = ctypes.CDLL("libm.so.6").logf
-    logf.restype, logf.argtypes = ctypes.c_float, [ctypes.c_float]
-    f = np.float32
     nx, ny, nz = grid.nx, grid.ny, grid.nz
     dx = f(grid.dx)
     inv_dx = f(1.0) / dx
@@ -365,23 +448,6 @@ def _serial_substep_np(p, idx, grid, dt, gravity, damping, mats, models):
         if ax < f(1.5):
             return -(f(1.5) - ax) * f(math.copysign(1.0, float(x)))
         return f(0.0)
-
-    def lame(m):
-        nu = min(max(f(m.poisson_ratio), f(-0.999)), f(0.4999))
-        e = f(m.young_modulus)
-        return e / (f(2.0) * (f(1.0) + nu)), e * nu / ((f(1.0) + nu) * (f(1.0) - f(2.0) * nu)), \
-            e / (f(3.0) * (f(1.0) - f(2.0) * nu))
-
-    def stress(model, m, F, J):
-        mu, la, k = lame(m)
-        if model == M.NEWTONIAN_FLUID:
-            sd = k * (J - f(1.0))
-            return [sd, f(0), f(0), f(0), sd, f(0), f(0), f(0), sd]
-        b = [F[r * 3 + 0] * F[c * 3 + 0] + F[r * 3 + 1] * F[c * 3 + 1] + F[r * 3 + 2] * F[c * 3 + 2]
-             for r in range(3) for c in range(3)]
-        p_term = la * f(logf(J)) / J if J > f(0.0) else f(0.0)
-        scale = mu / max(J, f(1e-10))
-        return [scale * ((b[i] - f(1.0) + p_term / scale) if i % 4 == 0 else b[i]) for i in range(9)]
 
     def base(x):
         g, fr = [], []
@@ -409,7 +475,7 @@ def _serial_substep_np(p, idx, grid, dt, gravity, damping, mats, models):
         mi = int(p.mat[i])
         m = mats[mi] if mi < len(mats) else mats[0]
         model = models[mi] if mi < len(models) else M.NEO_HOOKEAN
-        sig = stress(model, m, list(p.F[i]), p.J[i])
+        sig = _ref_stress_np(model, m, list(p.F[i]), p.J[i])
         vol = p.mass[i] / f(m.density)
         sv = [vol * x for x in sig]
         g, fr = base(p.pos[i])
@@ -483,10 +549,40 @@ def _serial_substep_np(p, idx, grid, dt, gravity, damping, mats, models):
         p.J[i] = jn
 
 
-def test_reference_serial_oracle_matches_a_numpy_restatement():
+ENGINE_TABLE = (  # ae_engine/src/managers/simulation.rs:251-294
+    dict(young_modulus=1.0e6, poisson_ratio=0.3, yield_stress=1.0e4, hardening=0.01, density=1000.0,
+         friction_angle=35.0, cohesion=0.0),
+    dict(young_modulus=2.0e6, poisson_ratio=0.45, yield_stress=0.0, hardening=0.0, density=1000.0,
+         friction_angle=0.0, cohesion=0.0),
+    dict(young_modulus=5.0e7, poisson_ratio=0.3, yield_stress=0.0, hardening=0.0, density=1600.0,
+         friction_angle=35.0, cohesion=0.0),
+    dict(young_modulus=2.0e11, poisson_ratio=0.3, yield_stress=2.5e8, hardening=0.01, density=7850.0,
+         friction_angle=0.0, cohesion=0.0))
+
+
+@pytest.mark.parametrize("model,params", [
+    (M.NEO_HOOKEAN, ENGINE_TABLE[0]), (M.NEWTONIAN_FLUID, ENGINE_TABLE[1]), (M.DRUCKER_PRAGER, ENGINE_TABLE[2]),
+    (M.DRUCKER_PRAGER, dict(ENGINE_TABLE[2], cohesion=1e5)), (M.VON_MISES, ENGINE_TABLE[3]),
+    (M.VON_MISES, dict(ENGINE_TABLE[0], yield_stress=2e3))])
+def test_constitutive_oracle_matches_a_numpy_restatement(model, params):
+    # compute_stress of the oracle against the float32 restatement of constitutive.rs, bit for bit,
+    # on deformed F that put about half of the plastic models' samples past their yield surface
+    rng = np.random.default_rng(1)
+    m = M.material(**params)
+    for _ in range(200):
+        F = (np.eye(3).reshape(9) + rng.normal(0, 0.03, 9)).astype(np.float32)
+        J = np.float32(np.linalg.det(F.reshape(3, 3).astype(np.float64)))
+        r = O.compute_stress(model, m, F, float(J))
+        a = np.asarray(r[0] if isinstance(r, tuple) else r, np.float32)
+        assert np.array_equal(a, np.asarray(_ref_stress_np(model, m, list(F), J), np.float32))
+
+
+@pytest.mark.parametrize("table", ["neo_fluid", "engine"])
+def test_reference_serial_oracle_matches_a_numpy_restatement(table):
     # the oracle's drop-in substep (below 50 000 indices: mpm_substep_serial_active) against an
-    # independent float32 restatement, bit for bit, with the neo-Hookean and fluid models, a material
-    # index past the tables (material_table[0] with NeoHookean), deformed F and a nonzero C
+    # independent float32 restatement, bit for bit: the neo-Hookean and fluid models, or the engine's
+    # own 4-material table (NeoHookean, NewtonianFluid, DruckerPrager, VonMises); a material index past
+    # the tables (material_table[0] with NeoHookean), deformed F and a nonzero C
     rng = np.random.default_rng(9)
     n, grid_n, dx = 300, 12, 0.05
     p = M.Particles.empty(n)
@@ -499,9 +595,14 @@ def test_reference_serial_oracle_matches_a_numpy_restatement():
     p.mat[:] = rng.integers(0, 3, n).astype(np.uint16)
     p.pos[:20, 0], p.vel[:20, 0] = 0.001, -3.0  # into the x = 0 wall
     p.pos[20:40, 1], p.vel[20:40, 1] = 0.001, -3.0  # into the floor
-    mats = [M.material(young_modulus=1e4, poisson_ratio=0.25, density=1000.0),
-            M.material(young_modulus=2e4, poisson_ratio=0.45, density=1000.0)]
-    models = [M.NEO_HOOKEAN, M.NEWTONIAN_FLUID]
+    if table == "engine":
+        mats = [M.material(**kw) for kw in ENGINE_TABLE]
+        models = [M.NEO_HOOKEAN, M.NEWTONIAN_FLUID, M.DRUCKER_PRAGER, M.VON_MISES]
+        p.mat[:] = rng.integers(0, 5, n).astype(np.uint16)
+    else:
+        mats = [M.material(young_modulus=1e4, poisson_ratio=0.25, density=1000.0),
+                M.material(young_modulus=2e4, poisson_ratio=0.45, density=1000.0)]
+        models = [M.NEO_HOOKEAN, M.NEWTONIAN_FLUID]
     g = M.Grid(grid_n, grid_n, grid_n, dx, (0.0, 0.0, 0.0))
     cfg = M.Config(grid_dx=dx, grid_size=(grid_n,) * 3, substeps=2, gravity=(0, -9.81, 0), damping=0.995)
     idx = np.sort(rng.choice(n, 240, replace=False)).astype(np.uint64)
