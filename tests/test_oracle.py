@@ -394,6 +394,21 @@ def _ref_stress_np(model, m, F, J):
     if model == M.NEWTONIAN_FLUID:
         sd = k * (J - f(1.0))
         return [sd, f(0), f(0), f(0), sd, f(0), f(0), f(0), sd]
+    if model == M.RIGID:  # constitutive.rs:370-373
+        return [f(1), f(0), f(0), f(0), f(1), f(0), f(0), f(0), f(1)]
+    if model in (M.COROTATED, M.FIXED_COROTATED):  # constitutive.rs:395-442
+        r, _ = _polar_np(F)
+        if model == M.COROTATED:
+            out = [f(2.0) * mu * (F[i] - r[i]) for i in range(9)]
+            for i in (0, 4, 8):
+                out[i] = out[i] + la * (J - f(1.0))
+            return out
+        rt = [r[0], r[3], r[6], r[1], r[4], r[7], r[2], r[5], r[8]]
+        dr = _mm_np([F[i] - r[i] for i in range(9)], rt)
+        out = [f(2.0) * mu * dr[i] for i in range(9)]
+        for i in (0, 4, 8):
+            out[i] = out[i] + la * (J - f(1.0)) * J
+        return out
     if model in (M.DRUCKER_PRAGER, M.VON_MISES):
         sd, sn, pressure = _deviatoric_np(m, F)
         if model == M.DRUCKER_PRAGER:
@@ -563,7 +578,8 @@ ENGINE_TABLE = (  # ae_engine/src/managers/simulation.rs:251-294
 @pytest.mark.parametrize("model,params", [
     (M.NEO_HOOKEAN, ENGINE_TABLE[0]), (M.NEWTONIAN_FLUID, ENGINE_TABLE[1]), (M.DRUCKER_PRAGER, ENGINE_TABLE[2]),
     (M.DRUCKER_PRAGER, dict(ENGINE_TABLE[2], cohesion=1e5)), (M.VON_MISES, ENGINE_TABLE[3]),
-    (M.VON_MISES, dict(ENGINE_TABLE[0], yield_stress=2e3))])
+    (M.VON_MISES, dict(ENGINE_TABLE[0], yield_stress=2e3)), (M.COROTATED, ENGINE_TABLE[0]),
+    (M.FIXED_COROTATED, ENGINE_TABLE[2]), (M.RIGID, ENGINE_TABLE[3])])
 def test_constitutive_oracle_matches_a_numpy_restatement(model, params):
     # compute_stress of the oracle against the float32 restatement of constitutive.rs, bit for bit,
     # on deformed F that put about half of the plastic models' samples past their yield surface
@@ -577,7 +593,7 @@ def test_constitutive_oracle_matches_a_numpy_restatement(model, params):
         assert np.array_equal(a, np.asarray(_ref_stress_np(model, m, list(F), J), np.float32))
 
 
-@pytest.mark.parametrize("table", ["neo_fluid", "engine"])
+@pytest.mark.parametrize("table", ["neo_fluid", "engine", "all_models"])
 def test_reference_serial_oracle_matches_a_numpy_restatement(table):
     # the oracle's drop-in substep (below 50 000 indices: mpm_substep_serial_active) against an
     # independent float32 restatement, bit for bit: the neo-Hookean and fluid models, or the engine's
@@ -599,6 +615,12 @@ def test_reference_serial_oracle_matches_a_numpy_restatement(table):
         mats = [M.material(**kw) for kw in ENGINE_TABLE]
         models = [M.NEO_HOOKEAN, M.NEWTONIAN_FLUID, M.DRUCKER_PRAGER, M.VON_MISES]
         p.mat[:] = rng.integers(0, 5, n).astype(np.uint16)
+    elif table == "all_models":  # the seven ConstitutiveModel variants, softer materials
+        models = [M.NEO_HOOKEAN, M.DRUCKER_PRAGER, M.VON_MISES, M.NEWTONIAN_FLUID, M.COROTATED,
+                  M.FIXED_COROTATED, M.RIGID]
+        mats = [M.material(young_modulus=1e4 * (k + 1), poisson_ratio=0.3, yield_stress=50.0, density=1000.0,
+                           friction_angle=30.0, cohesion=10.0) for k in range(7)]
+        p.mat[:] = rng.integers(0, 8, n).astype(np.uint16)
     else:
         mats = [M.material(young_modulus=1e4, poisson_ratio=0.25, density=1000.0),
                 M.material(young_modulus=2e4, poisson_ratio=0.45, density=1000.0)]
