@@ -434,7 +434,7 @@ def _ref_stress_np(model, m, F, J):
     return [scale * ((b[i] - f(1.0) + p_term / scale) if i % 4 == 0 else b[i]) for i in range(9)]
 
 
-def _serial_substep_np(p, idx, grid, dt, gravity, damping, mats, models):
+def _serial_substep_np(p, idx, grid, dt, gravity, damping, mats, models, parallel=False):
     """mpm_substep_serial_active (ae_particle/src/mpm_solver.rs:812-1054) with the neo-Hookean and
     Newtonian-fluid stresses (constitutive.rs:375-393, 603-617) restated with numpy float32 scalars,
     one IEEE single rounding per operation, ln from the C library as Rust's f32::ln."""
@@ -535,14 +535,18 @@ def _serial_substep_np(p, idx, grid, dt, gravity, damping, mats, models):
             npos, nv = [f(6.0), f(5.0), f(6.0)], [f(0)] * 3
         if npos[1] < f(0.0):
             npos[1], nv[1] = f(0.0), max(nv[1], f(0.0)) * f(0.5)
-        if npos[0] < f(0.0):
-            npos[0], nv[0] = f(0.0), max(nv[0], f(0.0)) * f(0.5)
-        elif npos[0] > gmax_x:
-            npos[0], nv[0] = gmax_x, min(nv[0], f(0.0)) * f(0.5)
-        if npos[2] < f(0.0):
-            npos[2], nv[2] = f(0.0), max(nv[2], f(0.0)) * f(0.5)
-        elif npos[2] > gmax_z:
-            npos[2], nv[2] = gmax_z, min(nv[2], f(0.0)) * f(0.5)
+        # the serial path's x/z walls are [0, (n-1) dx]; the parallel path's (mpm_solver.rs:1282-1287)
+        # are offset by the grid origin
+        x_lo, z_lo = (org[0], org[2]) if parallel else (f(0.0), f(0.0))
+        x_hi, z_hi = (gmax_x + org[0], gmax_z + org[2]) if parallel else (gmax_x, gmax_z)
+        if npos[0] < x_lo:
+            npos[0], nv[0] = x_lo, max(nv[0], f(0.0)) * f(0.5)
+        elif npos[0] > x_hi:
+            npos[0], nv[0] = x_hi, min(nv[0], f(0.0)) * f(0.5)
+        if npos[2] < z_lo:
+            npos[2], nv[2] = z_lo, max(nv[2], f(0.0)) * f(0.5)
+        elif npos[2] > z_hi:
+            npos[2], nv[2] = z_hi, min(nv[2], f(0.0)) * f(0.5)
         F = p.F[i]
         nf = []
         for r in range(3):
@@ -573,6 +577,38 @@ ENGINE_TABLE = (  # ae_engine/src/managers/simulation.rs:251-294
          friction_angle=35.0, cohesion=0.0),
     dict(young_modulus=2.0e11, poisson_ratio=0.3, yield_stress=2.5e8, hardening=0.01, density=7850.0,
          friction_angle=0.0, cohesion=0.0))
+
+
+def test_reference_parallel_path_oracle_matches_a_numpy_restatement():
+    # 50 000 indices take the parallel path (mpm_solver.rs:1077): one fold adds into an empty grid
+    # exactly, so the serial summation order stands, and the x/z walls follow the grid origin
+    rng = np.random.default_rng(12)
+    n, grid_n, dx = 50000, 16, 0.1
+    origin = (-1.2, 0.0, -1.2)
+    p = M.Particles.empty(n)
+    p.pos[:] = (np.asarray(origin) + 0.15 + rng.random((n, 3)) * 1.3).astype(np.float32)
+    p.vel[:] = rng.normal(0, 0.5, (n, 3)).astype(np.float32)
+    p.pos[:300, 0], p.vel[:300, 0] = np.float32(origin[0] + 0.001), -3.0  # into the x wall at the origin
+    p.pos[300:600, 2], p.vel[300:600, 2] = np.float32(origin[2] + 1.499), 3.0  # into the upper z wall
+    p.F[:] = (np.eye(3).reshape(9) + rng.normal(0, 0.01, (n, 9))).astype(np.float32)
+    p.J[:] = np.linalg.det(p.F.reshape(-1, 3, 3).astype(np.float64)).astype(np.float32)
+    p.mass[:] = np.float32(1e-4)
+    p.mat[:] = rng.integers(0, 2, n).astype(np.uint16)
+    mats = [M.material(young_modulus=1e4, poisson_ratio=0.25, density=1000.0),
+            M.material(young_modulus=2e4, poisson_ratio=0.45, density=1000.0)]
+    models = [M.NEO_HOOKEAN, M.NEWTONIAN_FLUID]
+    g = M.Grid(grid_n, grid_n, grid_n, dx, origin)
+    cfg = M.Config(grid_dx=dx, grid_size=(grid_n,) * 3, substeps=1, gravity=(0, -9.81, 0), damping=0.995)
+    idx = np.arange(n, dtype=np.uint64)
+    a = p.copy()
+    assert O.step_parallel_with_grid(a, g, cfg, mats, models, 0.002, idx, threads=1) == 0
+    b = p.copy()
+    _serial_substep_np(b, idx.astype(np.int64), g, np.float32(0.002), (0, -9.81, 0), 0.995, mats, models,
+                       parallel=True)
+    for fld in ("pos", "vel", "F", "J", "C"):
+        assert np.array_equal(getattr(a, fld), getattr(b, fld)), fld
+    assert (a.pos[:300, 0] == np.float32(origin[0])).sum() > 0
+    assert (a.pos[300:600, 2] == np.float32(15 * dx) + np.float32(origin[2])).sum() > 0
 
 
 @pytest.mark.parametrize("model,params", [
