@@ -14,6 +14,10 @@
 // what must start at zero (the per-digit totals) is cleared by each call, and two calls whose
 // work overlaps on the GPU race on the array, so a caller queues them on one stream or otherwise
 // orders them.
+//
+// The device address of the array is looked up once per device and kept for the life of the
+// process.  A cudaDeviceReset after the first call unloads the module and leaves that address
+// stale, so a process that resets a device must not call this entry point on it again.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -81,6 +85,15 @@ extern "C" int ae_mpm_radix_sort_keys_noalloc(ae_mpm_ctx* ctx, const uint32_t* k
                                    " keys exceed the fixed scratch limit of " + std::to_string(kMaxKeys));
   if (!keys_dev || !sorted_keys_dev || !perm_dev || key_bits == 0 || key_bits > 32)
     return fail(AE_MPM_EINVAL, "ae_mpm_radix_sort_keys_noalloc: null buffer or key_bits outside 1..32");
+  // The passes read one buffer while other blocks write the next, and with an odd pass count the
+  // first pass writes straight into sorted_keys_dev: the three buffers must not overlap.
+  auto overlap = [n](const void* a, const void* b) {
+    const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+    const uintptr_t len = uintptr_t(n) * sizeof(uint32_t);
+    return x < y + len && y < x + len;
+  };
+  if (overlap(keys_dev, sorted_keys_dev) || overlap(keys_dev, perm_dev) || overlap(sorted_keys_dev, perm_dev))
+    return fail(AE_MPM_EINVAL, "ae_mpm_radix_sort_keys_noalloc: keys_dev, sorted_keys_dev and perm_dev must not overlap");
   if (ctx) {
     cudaError_t e = cudaSetDevice(aemp::ctx_device(ctx));
     if (e != cudaSuccess) return fail(AE_MPM_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));

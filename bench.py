@@ -1,21 +1,30 @@
 #!/usr/bin/env python
-"""MPM particle-updates/s on B200.
+"""MPM particle-updates/s on B200, batched vs plain, with p50/p99 scene latency.
 
-Default workload: 3D snow collision, 128^3 grid, 1 048 576 Stomakhin-snow particles in two
-0.2^3 boxes at +-2 m/s, dt 5e-5 (f32).  One bench step = one MPM substep of the whole scene
-(radix sort by cell key, P2G, grid update, G2P).  Particle state (2 x 112 B x 1M = 235 MB) plus
-the grid exceeds the 126 MB L2, so no flush is needed between steps.
+Default workload (config 4, "batched"): 512 independent scenes, grid per scene drawn from
+{32,48,64}^3, particle count log-uniform in [2k, 64k] (9.7 M particles in all), material jelly,
+snow or water, box velocities in [-1,1]^3 m/s, f32.  One bench step = one MPM substep of every
+scene (radix sort by cell key, P2G, grid update, G2P), all scenes in one world: one launch of each
+kernel per substep serves every scene.  The particle state (2 x 112 B x 9.7 M = 2.2 GB) exceeds
+the 126 MB L2, so no flush is needed between steps.
 
-  value      particle-updates/s with the scene resident in HBM (CUDA events on the world's
-             stream around K substeps; max over ranks)
-  e2e        the same metric through the public C ABI with host buffers: upload from pinned
-             host memory, the config's run length of substeps, download, per call
-  roofline   the dominant kernel (P2G or G2P): algorithmic bytes / its mean event-timed duration
-  cpu_baseline  the CPU restatement of the reference substep (oracle/) on this host's cores
+  value            particle-updates/s of the batched world with every scene resident in HBM
+                   (CUDA events on the world's stream around K substeps; max over ranks)
+  batched_vs_plain the same kernels stepping one world per scene, one scene after another, over
+                   every scene (device-resident and end to end)
+  scene_latency_s  p50/p99 scene completion latency of a full run (200 substeps per scene, every
+                   scene submitted at once) through the C ABI, batched and plain
+  e2e              the metric through the public C ABI with host buffers: upload every scene from
+                   pinned host memory, 200 substeps, download every scene, per call
+  error_vs_fp64    per-particle position error of that run against the FP64 instantiation of the
+                   same kernels after the same substeps
+  roofline         the dominant kernel: algorithmic bytes / its mean event-timed duration
+  cpu_baseline     the CPU restatement of the reference substep (oracle/) on this host's cores
 
---impl reference times that CPU restatement alone (the reference is Rust, and no Rust toolchain is
-available to build it).  --gpus N runs N independent replicas (one scene per GPU; the substep does
-not shard within a scene).  Other workloads: --workload jelly|dam|batched|served|tick|ck|midfield|near.
+--impl reference times that CPU restatement alone on the same scenes (the reference is Rust, and
+no Rust toolchain is available to build it).  --gpus N deals a scene list of N x 512 scenes
+round-robin to the ranks (weak scaling, no data-path collective).  Other workloads:
+--workload snow|jelly|dam|served|tick|ck|midfield|near.
 """
 from __future__ import annotations
 
@@ -35,14 +44,13 @@ sys.path.insert(0, os.path.join(ROOT, "ae-engine_b200"))
 
 import numpy as np  # noqa: E402
 
-# algorithmic bytes per particle-substep of each kernel (f32 layout of mpm_world.cuh, physics mode):
-# P2G reads 4 x 16 B (position+mass, velocity and the affine matrix); G2P reads 4 x 16 B
-# (position+mass, F, J, material) and writes 7 x 16 B plus a 4 B cell key.
-P2G_BYTES_PER_PARTICLE = 64
-G2P_BYTES_PER_PARTICLE = 64 + 112 + 4
-# per active grid node: P2G accumulator write 16, grid update read 16 + write 16 + clear 16, G2P read 16
-P2G_BYTES_PER_NODE = 16
-G2P_BYTES_PER_NODE = 16
+# Algorithmic bytes of each kernel per particle-substep and per active grid node, for the f32
+# particle state x 12, v 12, C 36, F 36, J_p 4, mass/material 4 B: P2G reads all of it (104 B);
+# G2P reads x, F, J_p and the material (56 B) and writes x, v, C, F, J_p (100 B); each touches
+# 16 B per active node; the grid update reads and writes 64 B per active node.  (The kernels'
+# own layout moves 64 B per particle in P2G and 180 B in G2P: P2G reads an affine matrix that
+# G2P folds the stress into, instead of F.)
+KERNEL_BYTES = {"p2g": (104, 16), "g2p": (156, 16), "grid": (0, 64)}
 
 
 def l2_note(n_particles):
@@ -61,20 +69,20 @@ def parse():
                     help="timed steps; default: the workload's run length in substeps (RUN_LENGTH), else 200")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="snow", choices=["snow", "jelly", "dam", "batched", "served", "tick", "ck", "midfield", "near"])
+    ap.add_argument("--workload", default="batched", choices=["snow", "jelly", "dam", "batched", "served", "tick", "ck", "midfield", "near"])
     ap.add_argument("--ck-h", type=float, default=1.0,
                     help="ck: grid spacing (the scene scales with it); 1 takes the exact power-of-two division path")
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--e2e-substeps", type=int, default=None,
                     help="substeps per end-to-end call; default: the workload's run length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 error reference run")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--variant", choices=["lanes", "tile", "warp_agg", "global"],
                     help="fixed P2G variant (with --block-threads and --sort-interval: no autotune)")
     ap.add_argument("--block-threads", type=int, choices=[128, 256])
     ap.add_argument("--sort-interval", type=int)
     ap.add_argument("--scenes", type=int, default=512, help="batched: number of scenes")
-    ap.add_argument("--plain-sample", type=int, default=48, help="batched: scenes timed one at a time")
     ap.add_argument("--rates", default="50,200,1000", help="served: Poisson arrival rates (scenes/s)")
     ap.add_argument("--served-seconds", type=float, default=1.5, help="served: arrival window per rate")
     ap.add_argument("--served-max", type=int, default=300, help="served: cap on requests per rate")
@@ -179,27 +187,72 @@ def shard(items, rank: int, world_size: int):
     return list(items[rank::world_size])
 
 
-def workload(name: str, rank: int, n_scenes: int):
+def workload(name: str, rank: int, n_scenes: int, world_size: int = 1):
+    """Scenes of a workload for one rank.  Single-scene workloads run one replica per rank (seed
+    offset by rank); the batched workload draws one list of world_size x n_scenes scenes and deals
+    it round-robin, so every rank steps n_scenes scenes of one seeded population."""
     import ae_mpm_scenes as S
 
     if name == "served":
         return [], [], {"workload": "served"}
+    single = {"parallelism": "replicas" if world_size > 1 else "single GPU"}
     if name == "snow":
         sc, p = S.config2_snow(0xAE02 + 1000 * rank)
-        return [sc], [p], {"workload": "snow collision 128^3, 1048576 Stomakhin snow particles, dt 5e-5",
-                           "grid": 128, "particles": p.n}
+        single["l2"] = l2_note(p.n)
+        return [sc], [p], dict({"workload": "snow collision 128^3, 1048576 Stomakhin snow particles, dt 5e-5",
+                                "grid": 128, "particles": p.n}, **single)
     if name == "jelly":
         sc, p = S.config1_jelly(0xAE01 + 1000 * rank)
-        return [sc], [p], {"workload": "jelly 64^3, 32768 neo-Hookean particles, dt 1e-4", "grid": 64,
-                           "particles": p.n}
+        single["l2"] = l2_note(p.n)
+        return [sc], [p], dict({"workload": "jelly 64^3, 32768 neo-Hookean particles, dt 1e-4", "grid": 64,
+                                "particles": p.n}, **single)
     if name == "dam":
         sc, p = S.config3_dam(0xAE03 + 1000 * rank)
-        return [sc], [p], {"workload": "mixed dam break 256^3, 8388608 particles (60% fluid, 25% jelly, 15% snow)",
-                           "grid": 256, "particles": p.n}
-    pairs = S.config4_batched(n_scenes, 0xAE04 + 1000 * rank)
+        single["l2"] = l2_note(p.n)
+        return [sc], [p], dict({"workload": "mixed dam break 256^3, 8388608 particles (60% fluid, 25% jelly, 15% snow)",
+                                "grid": 256, "particles": p.n}, **single)
+    pairs = shard(S.config4_batched(n_scenes * world_size, 0xAE04), rank, world_size)
+    n = int(sum(b.n for _, b in pairs))
     return [a for a, _ in pairs], [b for _, b in pairs], {
-        "workload": "%d independent scenes, grids {32,48,64}^3, 2k-64k particles, jelly/snow/water" % n_scenes,
-        "scenes": n_scenes, "particles": int(sum(b.n for _, b in pairs))}
+        "workload": "%d independent scenes, grids {32,48,64}^3, 2k-64k particles, jelly/snow/water, 200-substep runs"
+                    % n_scenes, "scenes": len(pairs), "particles": n, "l2": l2_note(n),
+        "parallelism": "%d scenes per GPU, dealt round-robin from one list of %d" % (len(pairs), n_scenes * world_size)
+        if world_size > 1 else "single GPU"}
+
+
+def traffic_record(workload_name: str, kernel: str):
+    """DRAM bytes per launch of `kernel` (dram__bytes_read.sum + dram__bytes_write.sum) from the
+    committed ncu capture of this workload, with the file it came from; None if not captured."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tr = json.load(f)
+    except Exception:
+        return None
+    rec = tr.get(workload_name, {})
+    if kernel not in rec:
+        return None
+    return {"bytes": rec[kernel], "source": "ncu capture, %s" % rec.get("source", "profiles/traffic.json")}
+
+
+def cpu_scenes_rate(scenes, parts, substeps: int, threads: int | None = None, inplace: bool = False):
+    """The CPU restatement over a set of scenes: each scene stepped by one host thread (the
+    reference's serial path below 50 000 particles; its rayon path above uses the same arithmetic),
+    the scenes spread over every host core.  Returns (particle-updates/s, threads, description)."""
+    import concurrent.futures as cf
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    threads = threads or os.cpu_count() or 1
+    qs = parts if inplace else [p.copy() for p in parts]
+    order = sorted(range(len(parts)), key=lambda i: -parts[i].n)  # largest first: even finish
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(threads) as ex:
+        list(ex.map(lambda i: O.run(scenes[i], qs[i], substeps, threads=1), order))
+    dt = time.perf_counter() - t0
+    n = sum(p.n for p in parts)
+    return n * substeps / dt, threads, ("all %d scenes (%d particles), %d substeps each, scenes spread over %d "
+                                        "threads, %.1f s" % (len(parts), n, substeps, threads, dt))
 
 
 def active_nodes(scene, p) -> int:
@@ -243,7 +296,30 @@ def run_reference(args, rank, pg):
         return run_near(args, rank, 0, 1, pg, reference=True)
     if rank != 0:
         return
-    scenes, parts, cfg = workload(args.workload, 0, args.scenes)
+    scenes, parts, cfg = workload(args.workload, 0, args.scenes, args.gpus)
+    base = {"impl": "reference", "metric": "MPM particle-updates/s", "unit": "particle-updates/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64)",
+            "config": cfg}
+    if args.workload == "batched":
+        # the reference steps one scene per call (simulation.rs:570-607); here every step is one
+        # substep of every scene, the scenes spread over all host threads, one scene per thread
+        threads = os.cpu_count() or 1
+        qs = [p.copy() for p in parts]
+        dt = 0.0
+        for k in range(args.warmup + args.steps):
+            rate, _, _ = cpu_scenes_rate(scenes, qs, 1, threads, inplace=True)
+            if k >= args.warmup:
+                dt += sum(p.n for p in parts) / rate
+        value = sum(p.n for p in parts) * args.steps / dt
+        desc = "all %d scenes (%d particles), 1 substep of every scene per step, scenes spread over %d threads" % (
+            len(parts), sum(p.n for p in parts), threads)
+        print(json.dumps(dict(base, value=value, ms_per_step=1000.0 * dt / args.steps,
+                              cpu_baseline={"value": value, "unit": "particle-updates/s", "cores": threads,
+                                            "kind": "port", "sample": desc},
+                              e2e={"value": value, "unit": "particle-updates/s", "h2d_bytes_per_step": 0,
+                                   "d2h_bytes_per_step": 0})), flush=True)
+        return
     scene, p = scenes[0], parts[0]
     threads = os.cpu_count() or 1
     # Each step is one substep of the whole scene when the K + W steps fit in about four minutes.
@@ -262,14 +338,11 @@ def run_reference(args, rank, pg):
     value = sample.n * args.steps / dt
     desc = ("the whole scene (%d particles), 1 substep per step" % p.n if sample.n == p.n else
             "%d of %d particles (first in scene order), 1 substep per step" % (sample.n, p.n))
-    line = {"impl": "reference", "metric": "MPM particle-updates/s", "value": value, "unit": "particle-updates/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64)", "config": cfg,
-            "cpu_baseline": {"value": value, "unit": "particle-updates/s", "cores": threads, "kind": "port",
-                             "sample": desc},
-            "e2e": {"value": value, "unit": "particle-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(dict(base, value=value, ms_per_step=1000.0 * dt / args.steps,
+                          cpu_baseline={"value": value, "unit": "particle-updates/s", "cores": threads,
+                                        "kind": "port", "sample": desc},
+                          e2e={"value": value, "unit": "particle-updates/s", "h2d_bytes_per_step": 0,
+                               "d2h_bytes_per_step": 0})), flush=True)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -904,7 +977,7 @@ def run_ours(args, rank, local, world_size, pg):
     if args.workload == "near":
         return run_near(args, rank, local, world_size, pg)
     ctx = M.Context(local)
-    scenes, parts, cfg = workload(args.workload, rank, args.scenes)
+    scenes, parts, cfg = workload(args.workload, rank, args.scenes, world_size)
     if args.workload == "served":
         return run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg)
     if args.workload == "batched":
@@ -923,8 +996,10 @@ def run_ours(args, rank, local, world_size, pg):
         world.upload(i, p)
     n_total = sum(p.n for p in parts)
     tune = {"fixed": {k: int(v) for k, v in fixed.items()}} if fixed else None
+    tuned_kw = dict(fixed)
     if not args.no_autotune and not fixed:
         r = world.autotune(8)
+        tuned_kw = {"p2g_variant": r.p2g_variant, "block_threads": r.block_threads, "sort_interval": r.sort_interval}
         tune = {"p2g_variant": {1: "tile", 2: "warp_agg", 3: "global", 4: "lanes"}.get(r.p2g_variant, r.p2g_variant),
                 "block_threads": r.block_threads, "sort_interval": r.sort_interval,
                 "us_per_substep": round(r.us_per_substep, 2)}
@@ -961,19 +1036,11 @@ def run_ours(args, rank, local, world_size, pg):
 
     # roofline of the dominant kernel (P2G or G2P), from its event-timed mean duration
     kern = "g2p" if stages["g2p"] >= stages["p2g"] else "p2g"
-    per_p = G2P_BYTES_PER_PARTICLE if kern == "g2p" else P2G_BYTES_PER_PARTICLE
-    per_n = G2P_BYTES_PER_NODE if kern == "g2p" else P2G_BYTES_PER_NODE
+    per_p, per_n = KERNEL_BYTES[kern]
     alg_bytes = per_p * n_total + per_n * A
     achieved = alg_bytes / (stages[kern] * 1e-6) / 1e9
     peak, peak_kind = peaks()
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            tr = json.load(f)
-        if args.workload in tr and kern in tr[args.workload]:
-            traffic = tr[args.workload][kern]
-    except Exception:
-        pass
+    traffic = traffic_record(args.workload, kern)
 
     # end to end through the public API with pinned host buffers
     e2e = None
@@ -1025,6 +1092,12 @@ def run_ours(args, rank, local, world_size, pg):
                "substeps_per_step": args.e2e_substeps, "ms_per_step": t,
                "phases_ms": {"upload": round(ph[0], 3), "substeps": round(ph[1], 3), "download": round(ph[2], 3)}}
 
+    # error of the end-to-end f32 run against the FP64 run of the same kernels, same substeps
+    err = None
+    if e2e is not None and not args.no_fp64:
+        ref = fp64_run(ctx, scenes, parts, tuned_kw, args.e2e_substeps)
+        err = dict(position_error(scenes, [hout], ref), substeps=args.e2e_substeps)
+
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -1040,11 +1113,13 @@ def run_ours(args, rank, local, world_size, pg):
             "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64 scenes)",
-            "config": dict(cfg, parallelism="replicas" if world_size > 1 else "single GPU",
-                           l2=l2_note(n_total), timed_substeps=[t0_sub, t0_sub + args.steps]),
+            "config": cfg, "timed_substeps": [t0_sub, t0_sub + args.steps],
+            "error_vs_fp64": err,
             "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "algorithmic_bytes": alg_bytes, "active_nodes": A, "kernel_us": stages[kern],
+                         "frac": achieved / peak, "traffic": traffic["bytes"] if traffic else None,
+                         "traffic_source": traffic["source"] if traffic else None, "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg_bytes, "bytes_per_particle": per_p, "bytes_per_node": per_n,
+                         "active_nodes": A, "kernel_us": stages[kern],
                          "kernel_substeps": [t0_sub - STAGE_SUBSTEPS, t0_sub]},
             "stages_us": {k: round(v, 2) for k, v in stages.items()},
             "stages_us_end": dict({k: round(v, 2) for k, v in stages_end.items()},
@@ -1079,9 +1154,73 @@ def time_world(torch, world, local, steps, warmup):
     return e0.elapsed_time(e1)
 
 
+def pinned_staging(torch, parts, fill=True):
+    """Pinned host buffers, one per scene, carved from one page-locked allocation and laid out as
+    the world's upload staging (pos, vel, F, J, C and mass back to back, then the material
+    indices), so each scene crosses PCIe in one copy.  Returns (owner, [Particles views])."""
+    import ae_mpm as M
+
+    offs, total = [], 0
+    for p in parts:
+        offs.append(total)
+        total += (106 * p.n + 255) // 256 * 256
+    owner = torch.empty(max(total, 256), dtype=torch.uint8, pin_memory=True)
+    raw = owner.numpy()
+    views = []
+    for p, o in zip(parts, offs):
+        n = p.n
+        f = raw[o:o + 104 * n].view(np.float32)
+        v = M.Particles(pos=f[0:3 * n].reshape(n, 3), vel=f[3 * n:6 * n].reshape(n, 3), F=f[6 * n:15 * n].reshape(n, 9),
+                        J=f[15 * n:16 * n], C=f[16 * n:25 * n].reshape(n, 9), mass=f[25 * n:26 * n],
+                        mat=raw[o + 104 * n:o + 106 * n].view(np.uint16))
+        if fill:
+            for k in ("pos", "vel", "F", "J", "C", "mass", "mat"):
+                getattr(v, k)[...] = getattr(p, k)
+        views.append(v)
+    return owner, views
+
+
+def particle_bytes(p) -> int:
+    return sum(getattr(p, k).nbytes for k in ("pos", "vel", "F", "J", "C", "mass", "mat"))
+
+
+def position_error(scenes, got, ref) -> dict:
+    """Per-particle position error of an f32 run against the FP64 run of the same kernels from the
+    same initial state: |x32 - x64| relative to |x64| (max and 99th percentile over every particle)
+    and in grid cells (|x32 - x64| / dx)."""
+    rel, cells, worst = [], [], []
+    for sc, a, b in zip(scenes, got, ref):
+        d = np.linalg.norm(a.pos.astype(np.float64) - b.pos, axis=1)
+        r = d / np.maximum(np.linalg.norm(b.pos, axis=1), 1e-30)
+        rel.append(r)
+        cells.append(d / sc.dx)
+        worst.append(float(r.max()) if r.size else 0.0)
+    rel = np.concatenate(rel)
+    cells = np.concatenate(cells)
+    return {"max_rel": float(rel.max()), "p99_rel": float(np.percentile(rel, 99)),
+            "max_cells": float(cells.max()), "p99_cells": float(np.percentile(cells, 99)),
+            "scenes_over_1e-4": int(sum(w > 1e-4 for w in worst)), "target_rel": 1e-4}
+
+
+def fp64_run(ctx, scenes, parts, opts_kw, substeps):
+    """The FP64 instantiation of the same kernels (precision 64), `substeps` from the initial state."""
+    import ae_mpm as M
+
+    w = M.World(ctx, scenes, M.exec_opts(precision=64, **opts_kw))
+    for i, p in enumerate(parts):
+        w.upload(i, p.astype(np.float64))
+    w.step(substeps)
+    w.sync(raise_on_error=False)
+    out = [w.download(i, p.n) for i, p in enumerate(parts)]
+    w.close()
+    return out
+
+
+
+
 def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
-    """Config 4: all scenes in one world (one launch per kernel per substep) against the plain
-    path, the same kernels stepping one scene at a time."""
+    """Config 4: every scene in one world (one launch per kernel per substep for all scenes) against
+    the plain path, the same kernels stepping one world per scene, one scene at a time."""
     import torch
 
     import ae_mpm as M
@@ -1090,59 +1229,149 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
     world = M.World(ctx, scenes, M.exec_opts())
     for i, p in enumerate(parts):
         world.upload(i, p)
-    tune = None
+    tune, tuned = None, {}
     if not args.no_autotune:
         r = world.autotune(8)
-        tune = {"p2g_variant": r.p2g_variant, "block_threads": r.block_threads, "sort_interval": r.sort_interval}
+        tuned = {"p2g_variant": r.p2g_variant, "block_threads": r.block_threads, "sort_interval": r.sort_interval}
+        tune = dict(tuned, p2g_variant={1: "tile", 2: "warp_agg", 3: "global", 4: "lanes"}.get(r.p2g_variant),
+                    us_per_substep=round(r.us_per_substep, 2))
+    warm = max(args.warmup, 3)
+    world.step(warm)
+    world.sync()
+    stages = world.stage_times(STAGE_SUBSTEPS)
+    t0_sub = warm + STAGE_SUBSTEPS
+    state = [world.download(i, p.n) for i, p in enumerate(parts)]
+    A = sum(active_nodes(s, q) for s, q in zip(scenes, state))
+    stream = torch.cuda.ExternalStream(world.stream(), device=local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
     clocks = Clocks(local)
     barrier(pg)
     torch.cuda.synchronize(local)
     clocks.start()
-    ms = time_world(torch, world, local, args.steps, max(args.warmup, 3))
+    time.sleep(0.3)
+    e0.record(stream)
+    world.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(local)
     clk = clocks.stop()
     launches = world.launches()
     world.sync(raise_on_error=False)
-    ms = max_over_ranks(pg, ms)
+    ms = max_over_ranks(pg, e0.elapsed_time(e1))
     value = n_total * world_size * args.steps / (ms / 1e3)
-    stages = world.stage_times(10)
-    world.close()
-    # plain path: a sample of the scenes, each its own world, stepped one after another
-    k = min(args.plain_sample, len(scenes))
-    idx = list(range(0, len(scenes), max(1, len(scenes) // k)))[:k]
-    t_plain, n_plain, per_scene_ms = 0.0, 0, []
-    for i in idx:
-        w1 = M.World(ctx, [scenes[i]], M.exec_opts())
-        w1.upload(0, parts[i])
-        t = time_world(torch, w1, local, args.steps, 3)
+
+    # plain path: every scene in a world of its own (same kernels and options), stepped one scene
+    # after another; the same K substeps per scene, each timed with events on that world's stream
+    plain = [M.World(ctx, [sc], M.exec_opts(**tuned)) for sc in scenes]
+    t_plain = 0.0
+    for w1, p in zip(plain, parts):
+        w1.upload(0, p)
+        t_plain += time_world(torch, w1, local, args.steps, 3)
+    t_plain = max_over_ranks(pg, t_plain)
+    plain_value = n_total * world_size * args.steps / (t_plain / 1e3)
+
+    # end to end through the C ABI: every scene submitted at once from pinned host memory, the
+    # config's run length of substeps, every scene downloaded; a scene completes when its results
+    # are in the caller's buffer.  Batched: one world; plain: one world per scene, in turn.
+    run = args.e2e_substeps
+    own_in, hin = pinned_staging(torch, parts)
+    own_out, hout = pinned_staging(torch, parts, fill=False)
+    own_pl, hpl = pinned_staging(torch, parts, fill=False)
+    h2d = sum(particle_bytes(p) for p in parts)
+    e2e_b, e2e_p, lat_b, lat_p = [], [], [], []
+    for rep in range(max(1, args.e2e_reps)):
+        barrier(pg)
+        torch.cuda.synchronize(local)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for i, q in enumerate(hin):
+            world.upload(i, q)
+        world.step(run)
+        done = []
+        for i, q in enumerate(hout):
+            world.download_into(i, q)
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(stream)
+            done.append(ev)
+        done[-1].synchronize()
+        lat = [ev0.elapsed_time(ev) / 1e3 for ev in done]
+        e2e_b.append(max_over_ranks(pg, lat[-1]))
+        lat_b.append(lat)
+        if rep == 0 or args.e2e_reps > 1:
+            barrier(pg)
+            torch.cuda.synchronize(local)
+            s0 = torch.cuda.ExternalStream(plain[0].stream(), device=local)
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev0.record(s0)
+            done = []
+            for w1, q, o in zip(plain, hin, hpl):
+                w1.upload(0, q)
+                w1.step(run)
+                w1.download_into(0, o)
+                ev = torch.cuda.Event(enable_timing=True)
+                ev.record(torch.cuda.ExternalStream(w1.stream(), device=local))
+                done.append(ev)
+            done[-1].synchronize()
+            lat = [ev0.elapsed_time(ev) / 1e3 for ev in done]
+            e2e_p.append(max_over_ranks(pg, lat[-1]))
+            lat_p.append(lat)
+    kb = int(np.argsort(e2e_b)[len(e2e_b) // 2])
+    kp = int(np.argsort(e2e_p)[len(e2e_p) // 2])
+    e2e = {"value": n_total * world_size * run / e2e_b[kb], "unit": "particle-updates/s",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d, "substeps_per_step": run,
+           "ms_per_step": 1e3 * e2e_b[kb],
+           "call": "ae_mpm_world_upload of every scene from pinned host memory, ae_mpm_world_step(%d), "
+                   "ae_mpm_world_download of every scene" % run}
+    plain_e2e = n_total * world_size * run / e2e_p[kp]
+    for w1 in plain:
         w1.close()
-        t_plain += t
-        n_plain += parts[i].n
-        per_scene_ms.append(t)
-    plain_rate = n_plain * args.steps / (t_plain / 1e3)
-    # scene completion latency for the whole set (each scene runs `steps` substeps): batched
-    # scenes all finish with the batch; plain scenes finish one after another
-    scale = len(scenes) / len(idx)
-    plain_done = []
-    acc = 0.0
-    for t in per_scene_ms * int(round(scale)):
-        acc += t
-        plain_done.append(acc)
+
+    # error of the batched f32 run against the FP64 run of the same kernels, same substeps
+    err = None
+    if not args.no_fp64:
+        ref = fp64_run(ctx, scenes, parts, tuned, run)
+        err = dict(position_error(scenes, hout, ref), substeps=run)
+
+    kern = max(("p2g", "g2p", "grid"), key=lambda k: stages[k])
+    per_p, per_n = KERNEL_BYTES[kern]
+    alg_bytes = per_p * n_total + per_n * A
+    achieved = alg_bytes / (stages[kern] * 1e-6) / 1e9
+    peak, peak_kind = peaks()
+    traffic = traffic_record("batched", kern)
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        rate, threads, desc = cpu_scenes_rate(scenes, parts, 2)
+        cpu = {"value": rate, "unit": "particle-updates/s", "cores": threads, "kind": "port", "sample": desc}
+    world.close()
     if rank == 0:
         line = {
             "metric": "MPM particle-updates/s", "value": value, "unit": "particle-updates/s", "n_gpus": world_size,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64 scenes)",
-            "config": dict(cfg, parallelism="replicas" if world_size > 1 else "single GPU",
-                           l2="inputs larger than L2, no flush"),
-            "batched_vs_plain": {"plain_value": plain_rate, "ratio": value / plain_rate,
-                                 "plain_sample_scenes": len(idx), "plain_kind": "one world per scene, same kernels"},
-            "scene_latency_s": {"batched_p50": ms / 1e3, "batched_p99": ms / 1e3,
-                                "plain_p50": percentile(plain_done, 50) / 1e3,
-                                "plain_p99": percentile(plain_done, 99) / 1e3},
-            "stages_us": {a: round(b, 2) for a, b in stages.items()}, "autotune": tune, "gpu_launches": launches,
-            "clocks": clk,
+            "config": cfg, "timed_substeps": [t0_sub, t0_sub + args.steps],
+            "batched_vs_plain": {"ratio": value / plain_value, "plain_value": plain_value,
+                                 "e2e_ratio": e2e["value"] / plain_e2e, "plain_e2e_value": plain_e2e,
+                                 "plain_scenes": len(scenes),
+                                 "plain_kind": "one world per scene (same kernels and options), scenes in turn"},
+            "scene_latency_s": {"substeps": run, "batched_p50": percentile(lat_b[kb], 50),
+                                "batched_p99": percentile(lat_b[kb], 99),
+                                "plain_p50": percentile(lat_p[kp], 50), "plain_p99": percentile(lat_p[kp], 99),
+                                "definition": "every scene submitted at t=0; done when its results are in the "
+                                              "caller's pinned buffer"},
+            "error_vs_fp64": err,
+            "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic["bytes"] if traffic else None,
+                         "traffic_source": traffic["source"] if traffic else None, "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg_bytes, "bytes_per_particle": per_p, "bytes_per_node": per_n,
+                         "active_nodes": A, "kernel_us": stages[kern],
+                         "kernel_substeps": [t0_sub - STAGE_SUBSTEPS, t0_sub]},
+            "stages_us": {a: round(b, 2) for a, b in stages.items()}, "autotune": tune,
+            "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,
         }
         print(json.dumps(line), flush=True)
+    del own_in, own_out, own_pl
 
 
 def run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):

@@ -291,7 +291,10 @@ int ae_mpm_radix_sort_keys(ae_mpm_ctx* ctx, const uint32_t* keys, uint64_t n, ui
  * or freed.  The work is queued on `stream` (a cudaStream_t; NULL = default stream).  ctx may be
  * NULL; when given, its device is made current and failures leave their text in it.  The first
  * call on a device looks up the array's device address, so make that first call before any stream
- * capture.  All calls on a device share the scratch: calls whose work overlaps on the GPU race. */
+ * capture; the address is kept for the life of the process, so a device that was reset
+ * (cudaDeviceReset) must not be given to this call again.  All calls on a device share the
+ * scratch: calls whose work overlaps on the GPU race.  keys_dev, sorted_keys_dev and perm_dev
+ * must not overlap (AE_MPM_EINVAL otherwise): no in-place sort. */
 #define AE_MPM_NOALLOC_MAX_KEYS (1u << 20)
 int ae_mpm_radix_sort_keys_noalloc(ae_mpm_ctx* ctx, const uint32_t* keys_dev, uint64_t n, uint32_t key_bits,
                                    uint32_t* sorted_keys_dev, uint32_t* perm_dev, void* stream);

@@ -33,7 +33,9 @@ def extract(ref_root: str) -> list[dict]:
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <reference checkout root>" % sys.argv[0])
+    root = sys.argv[1]
     rows = extract(root)
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "phase_cases.json"), "w") as f:

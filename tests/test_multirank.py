@@ -1,6 +1,7 @@
 """Multi-rank host logic of bench.py on CPU (gloo, world_size 2): the max-over-ranks timing and the
-round-robin scene sharding used when --gpus N > 1.  The substep itself does not shard within a
-scene (replicas only), so there is no data-path collective to test."""
+round-robin scene sharding of the batched workload when --gpus N > 1 (bench.workload deals one
+seeded list of N x scenes to the ranks).  The substep itself does not shard within a scene, so there
+is no data-path collective to test."""
 import os
 import socket
 
@@ -31,7 +32,8 @@ def _worker(rank, world, port, out):
     try:
         got = bench.max_over_ranks(dist, 10.0 + 5.0 * rank)
         mine = bench.shard(list(range(11)), rank, world)
-        out.put((rank, got, mine))
+        scenes, parts, cfg = bench.workload("batched", rank, 3, world)
+        out.put((rank, got, mine, [p.n for p in parts], cfg["scenes"]))
     finally:
         dist.destroy_process_group()
 
@@ -50,3 +52,12 @@ def test_max_over_ranks_and_scene_sharding_with_two_gloo_ranks():
     assert [r[1] for r in res] == [15.0, 15.0]
     assert res[0][2] == [0, 2, 4, 6, 8, 10] and res[1][2] == [1, 3, 5, 7, 9]
     assert sorted(res[0][2] + res[1][2]) == list(range(11))
+    # the batched workload: each rank holds 3 scenes of one 6-scene population, dealt round-robin
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "ae-engine_b200"))
+    import ae_mpm_scenes as S
+
+    full = [p.n for _, p in S.config4_batched(6, 0xAE04)]
+    assert res[0][4] == res[1][4] == 3
+    assert res[0][3] == full[0::2] and res[1][3] == full[1::2]
