@@ -1166,6 +1166,13 @@ int oracle_run_f64(const ae_mpm_scene_desc* scene, ae_mpm_particles_f64* p, uint
 void oracle_totals_f32(const ae_mpm_particles* p, uint64_t n, double out[5]) { totals_of<float>(p, n, out); }
 void oracle_totals_f64(const ae_mpm_particles_f64* p, uint64_t n, double out[5]) { totals_of<double>(p, n, out); }
 
+int oracle_mpm_step_parallel_with_grid_export(const ae_mpm_particles* buffer, uint64_t capacity,
+                                              const ae_mpm_grid* grid, const ae_mpm_config* config,
+                                              const ae_mpm_material* material_table, uint32_t n_materials,
+                                              const int32_t* model_table, uint32_t n_models, float total_dt,
+                                              const uint64_t* particle_indices, uint64_t n_indices, int32_t threads,
+                                              float* grid_mass, float* grid_vel);
+
 // mpm_step_parallel_with_grid (ae_particle/src/mpm_solver.rs:1063-1084) on the caller's buffer,
 // minus update_lifetimes.  threads > 1 runs the >= 50 000 branch's fold/reduce with that many
 // thread-local grids.
@@ -1174,6 +1181,21 @@ int oracle_mpm_step_parallel_with_grid(const ae_mpm_particles* buffer, uint64_t 
                                        uint32_t n_materials, const int32_t* model_table, uint32_t n_models,
                                        float total_dt, const uint64_t* particle_indices, uint64_t n_indices,
                                        int32_t threads) {
+  return oracle_mpm_step_parallel_with_grid_export(buffer, capacity, grid, config, material_table, n_materials,
+                                                   model_table, n_models, total_dt, particle_indices, n_indices,
+                                                   threads, nullptr, nullptr);
+}
+
+// The same call, and afterwards the Grid the reference leaves behind (mpm_solver.rs:73-86): the
+// node mass and velocity (after Grid::update_parallel of the last substep) in the reference's
+// dense index order i + j*nx + k*nx*ny, when grid_mass / grid_vel are given.  Nodes at or below
+// the 1e-12 mass threshold keep the momentum the update leaves in `vel` (mpm_solver.rs:116).
+int oracle_mpm_step_parallel_with_grid_export(const ae_mpm_particles* buffer, uint64_t capacity,
+                                              const ae_mpm_grid* grid, const ae_mpm_config* config,
+                                              const ae_mpm_material* material_table, uint32_t n_materials,
+                                              const int32_t* model_table, uint32_t n_models, float total_dt,
+                                              const uint64_t* particle_indices, uint64_t n_indices, int32_t threads,
+                                              float* grid_mass, float* grid_vel) {
   if (n_indices == 0) return AE_MPM_OK;
   if (n_materials == 0 || !config || config->substeps == 0) return AE_MPM_EINVAL;
   for (uint64_t k = 0; k < n_indices; ++k)
@@ -1187,6 +1209,8 @@ int oracle_mpm_step_parallel_with_grid(const ae_mpm_particles* buffer, uint64_t 
     ref_substep(g, b, mt, particle_indices, n_indices, sub_dt, config->gravity, config->damping, parallel,
                 parallel ? std::max(threads, 1) : 1);
   }
+  if (grid_mass) std::copy(g.mass.begin(), g.mass.end(), grid_mass);
+  if (grid_vel) std::copy(g.vel.begin(), g.vel.end(), grid_vel);
   return AE_MPM_OK;
 }
 

@@ -56,6 +56,11 @@ def load():
     lib.oracle_mpm_step_parallel_with_grid.argtypes = [
         C.POINTER(M.ParticlesView), C.c_uint64, C.POINTER(M.Grid), C.POINTER(M.Config), C.POINTER(M.Material),
         C.c_uint32, C.POINTER(C.c_int32), C.c_uint32, f, C.POINTER(C.c_uint64), C.c_uint64, C.c_int32]
+    lib.oracle_mpm_step_parallel_with_grid_export.restype = C.c_int
+    lib.oracle_mpm_step_parallel_with_grid_export.argtypes = [
+        C.POINTER(M.ParticlesView), C.c_uint64, C.POINTER(M.Grid), C.POINTER(M.Config), C.POINTER(M.Material),
+        C.c_uint32, C.POINTER(C.c_int32), C.c_uint32, f, C.POINTER(C.c_uint64), C.c_uint64, C.c_int32,
+        C.c_void_p, C.c_void_p]
     lib.oracle_mpm_step_velocity_only_parallel.restype = C.c_int
     lib.oracle_mpm_step_velocity_only_parallel.argtypes = [
         C.POINTER(M.ParticlesView), C.c_uint64, C.POINTER(M.Grid), C.POINTER(M.Config), f,
@@ -116,6 +121,27 @@ def step_parallel_with_grid(p: M.Particles, grid: M.Grid, config: M.Config, mate
     return lib.oracle_mpm_step_parallel_with_grid(C.byref(v), p.n, C.byref(grid), C.byref(config), mats,
                                                   len(materials), mods, len(models), total_dt,
                                                   idx.ctypes.data_as(C.POINTER(C.c_uint64)), idx.size, threads)
+
+
+def step_parallel_with_grid_grid(p: M.Particles, grid: M.Grid, config: M.Config, materials, models, total_dt, indices,
+                                 threads: int = 1):
+    """step_parallel_with_grid, returning the Grid the reference leaves behind: (mass (nx*ny*nz,),
+    vel (nx*ny*nz, 3)) after the last substep's grid update, dense in i + j*nx + k*nx*ny order."""
+    lib = load()
+    mats = (M.Material * max(len(materials), 1))(*materials)
+    mods = (C.c_int32 * max(len(models), 1))(*models)
+    idx = np.ascontiguousarray(np.asarray(indices, np.uint64))
+    nn = int(grid.nx * grid.ny * grid.nz)
+    gm = np.zeros(nn, np.float32)
+    gv = np.zeros((nn, 3), np.float32)
+    v = p.view()
+    rc = lib.oracle_mpm_step_parallel_with_grid_export(C.byref(v), p.n, C.byref(grid), C.byref(config), mats,
+                                                       len(materials), mods, len(models), total_dt,
+                                                       idx.ctypes.data_as(C.POINTER(C.c_uint64)), idx.size, threads,
+                                                       gm.ctypes.data, gv.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("oracle step failed: %d" % rc)
+    return gm, gv
 
 
 def step_velocity_only_parallel(p: M.Particles, grid: M.Grid, config: M.Config, total_dt, indices,

@@ -728,6 +728,37 @@ def test_oracle_steel_rigid_fall():  # mpm_solver.rs:1713-1745
     assert 0.0 <= p.pos[0, 1] < 0.5
 
 
+def test_oracle_grid_export_is_the_reference_grid_after_the_call():
+    # Grid the reference leaves behind after mpm_step_parallel_with_grid (mpm_solver.rs:73-176):
+    # one stress-free particle (F = I) at a known position, one substep.  P2G puts m*N(fx)N(fy)N(fz)
+    # on nodes g..g+2 per axis with g = floor((x-o)/dx - 0.5) (:161-175, :863-875); the update turns
+    # momentum into v + g*dt on nodes above the 1e-12 mass threshold (:112-139).  Everything else is 0.
+    x = np.array([0.537, 0.611, 0.449])
+    p = _ref_buffer([tuple(x)], 2.0)
+    p.vel[0] = (0.3, -0.2, 0.1)
+    n, dx, o = 16, 0.0625, np.array([-0.1, 0.0, -0.05], np.float32)
+    cfg = M.Config(grid_dx=dx, grid_size=(n, n, n), substeps=1, gravity=(0, -9.81, 0), damping=0.995)
+    g = M.Grid(n, n, n, dx, tuple(o))
+    dt = 0.004
+    gm, gv = O.step_parallel_with_grid_grid(p, g, cfg, [M.material(young_modulus=1e4, density=1000)],
+                                            [M.NEO_HOOKEAN], dt, [0])
+    q = (x - o.astype(np.float64)) / dx - 0.5
+    base = np.floor(q).astype(int)
+    fx = q - base
+    want = np.zeros(n ** 3)
+    for di in range(3):
+        for dj in range(3):
+            for dk in range(3):
+                w = np.prod([O.b_spline(float(fx[a] - d)) for a, d in zip(range(3), (di, dj, dk))])
+                i, j, k = base + (di, dj, dk)
+                want[i + j * n + k * n * n] += 2.0 * w
+    assert np.allclose(gm, want, rtol=1e-5, atol=1e-7)
+    live = gm > 1e-12
+    assert live.sum() >= 8 and np.all(gm[~live] == 0) and np.all(gv[~live] == 0)
+    v = np.array([0.3, -0.2 - 9.81 * dt, 0.1])
+    assert np.allclose(gv[live], v, rtol=0, atol=1e-5)
+
+
 def test_oracle_parallel_path_matches_serial_fold_order():
     # thread-local grids merged in order (rayon fold/reduce shape) agree with the serial path
     rng = np.random.default_rng(3)
