@@ -43,6 +43,11 @@ AE_HD bool t_finite(double x) { return isfinite(x); }
 // fmin/fmax return the non-NaN operand, so a NaN position is pulled back onto the domain
 AE_HD float t_fclamp(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
 AE_HD double t_fclamp(double x, double lo, double hi) { return fmin(fmax(x, lo), hi); }
+// a + b * c with the product and the sum each rounded, as the reference's Rust computes it (Rust
+// never contracts to a fused multiply-add); used where the result feeds a branch that exact ties
+// reach, e.g. a wall test on x + v dt after an earlier clamp left x at exactly v dt
+__device__ __forceinline__ float t_add_mul_rn(float a, float b, float c) { return __fadd_rn(a, __fmul_rn(b, c)); }
+__device__ __forceinline__ double t_add_mul_rn(double a, double b, double c) { return __dadd_rn(a, __dmul_rn(b, c)); }
 
 // ---------------------------------------------------------------- quadratic B-spline
 template <class T>

@@ -956,7 +956,7 @@ __device__ __forceinline__ void g2p_reference(const VelTile<T>& vt, const SceneD
   }
 #pragma unroll
   for (int a = 0; a < 3; ++a) nv[a] = t_clamp(nv[a], T(-50), T(50));
-  T np[3] = {pos[0] + nv[0] * sc.dt, pos[1] + nv[1] * sc.dt, pos[2] + nv[2] * sc.dt};
+  T np[3] = {t_add_mul_rn(pos[0], nv[0], sc.dt), t_add_mul_rn(pos[1], nv[1], sc.dt), t_add_mul_rn(pos[2], nv[2], sc.dt)};
   if (!t_finite(np[0]) || !t_finite(np[1]) || !t_finite(np[2])) {
     np[0] = T(6);
     np[1] = T(5);
@@ -1060,7 +1060,7 @@ __device__ __forceinline__ void g2p_velonly(const VelTile<T>& vt, const SceneDev
   if (!t_finite(nv[0]) || !t_finite(nv[1]) || !t_finite(nv[2])) nv[0] = nv[1] = nv[2] = T(0);
 #pragma unroll
   for (int a = 0; a < 3; ++a) nv[a] = t_clamp(nv[a], T(-50), T(50));
-  T np[3] = {pos[0] + nv[0] * sc.dt, pos[1] + nv[1] * sc.dt, pos[2] + nv[2] * sc.dt};
+  T np[3] = {t_add_mul_rn(pos[0], nv[0], sc.dt), t_add_mul_rn(pos[1], nv[1], sc.dt), t_add_mul_rn(pos[2], nv[2], sc.dt)};
   if (!t_finite(np[0]) || !t_finite(np[1]) || !t_finite(np[2])) {
     np[0] = pos[0];
     np[1] = pos[1];

@@ -19,7 +19,12 @@ position moves single-call outputs by up to 5 cm (the oracle against itself).  S
     accumulate) and are held to the oracle's rounding envelope at that state: the oracle run again
     with every selected input position moved by one ulp.  The device's per-particle differences
     must stay within 10x that envelope at the 50th, 90th and 99th percentiles (plus a floor of
-    1e-6 of the field's scale), and the grid likewise.
+    1e-6 of the field's scale), and the grid likewise; grid velocities, which span 15 decades at
+    these settings, are also held per node to 1e-4 relative at the 99th percentile.
+The position update x + v dt is rounded as Rust rounds it (product, then sum): an earlier wall
+clamp leaves particles at exactly 50 dt above the floor, and a fused multiply-add there turns
+the reference's 0 into -4e-9, takes the floor branch and zeroes the velocity that the reference
+keeps (found by this test at call 3).
 Unselected particles must come back bit-unchanged after every call.
 """
 import numpy as np
@@ -95,5 +100,11 @@ def test_engine_near_call_and_grid_readback_match_oracle_call_by_call(ctx):
             _within_envelope(np.abs(gv_dev[both] - gv[both].astype(np.float64)).max(1),
                              np.abs(gv_e[both] - gv[both].astype(np.float64)).max(1),
                              float(np.abs(gv[both]).max()), "call %d grid velocity" % (call + 1))
+            # grid velocities span 15 decades here, so also per node: the 99th percentile of
+            # |v_dev - v_ref| / |v_ref| within 1e-4 (the device's atomic order and folded force)
+            rel_node = (np.abs(gv_dev[both] - gv[both].astype(np.float64)).max(1) /
+                        np.maximum(np.abs(gv[both].astype(np.float64)).max(1), 1e-30))
+            print("call %d grid velocity per-node relative p99 %.3g" % (call + 1, np.percentile(rel_node, 99)))
+            assert np.percentile(rel_node, 99) <= 1e-4
         assert np.isfinite(dev.pos[ii]).all()
         state = ref
