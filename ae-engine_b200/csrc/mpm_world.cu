@@ -671,11 +671,17 @@ __device__ __forceinline__ void block_coords(const SceneDev<T>& sc, uint32_t gb,
 }
 
 template <class T, int MODE>
-__global__ void __launch_bounds__(256) grid_update_kernel(WorldDev<T> w, uint32_t* blk_epoch, const uint32_t* epoch) {
+__global__ void __launch_bounds__(256) grid_update_kernel(WorldDev<T> w, uint32_t* blk_epoch, const uint32_t* epoch,
+                                                          uint32_t* zero_count) {
   using V4 = typename V4T<T>::type;
   const uint32_t count = launch_count(w.touched_count);
   const uint32_t ep = *epoch;
-  if (blockIdx.x == 0 && threadIdx.x == 0) *w.clamp_count = 0u;  // G2P of this substep refills it
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *w.clamp_count = 0u;  // G2P of this substep refills it
+    // the fused G2P + P2G appends the next substep's blocks to the other list, whose previous
+    // contents the grid update of the substep before consumed
+    if (zero_count) *zero_count = 0u;
+  }
   // each 64-thread group takes 4 touched blocks per iteration and issues their 4 accumulator loads
   // before using any, so a long touched list is not one latency-bound load after another
   constexpr int kU = 4;
@@ -1303,6 +1309,335 @@ __global__ void __launch_bounds__(128, 8) snow_clamp_kernel(WorldDev<T> w) {
 }
 
 // ============================================================================================
+// fused G2P + P2G for physics mode (grid -> particle -> grid in one pass over the particles)
+// ============================================================================================
+// G2P of substep s computes each particle's new position, mass-weighted velocity and affine
+// matrix A = m C - k tau; those are exactly the inputs of P2G for substep s + 1, so the same
+// kernel scatters them into the (already cleared) accumulator of the next substep while they are
+// still in registers.  P2G then never re-reads the particle state.  Snow particles whose F left
+// the elastic region get A only after the return mapping: the clamp kernel scatters them.
+//
+// Per-warp shared staging of the column-lane scatter (the layout of p2g_lanes_kernel, one
+// contiguous region per warp): 32 particles x (9 column vectors, x weights + mass, dx times A's x
+// column) and 32 run records.  Per-thread data the warp stages before the scatter (the cp.async
+// prefetch of F, J and the material) lives in the same region.
+template <class T>
+struct WarpStage {
+  using V4 = typename V4T<T>::type;
+  V4* col;   // col[pos * 9 + column]
+  V4* wxm;   // wxm[pos] = (wx0, wx1, wx2, m)
+  V4* acol;  // acol[pos] = dx * A[.][0]
+  int4* gk;  // gk[pos] = (stencil base, cell key)
+};
+template <class T>
+__host__ __device__ constexpr size_t warp_stage_bytes() {
+  return sizeof(typename V4T<T>::type) * 32 * kLaneVecs + sizeof(int4) * 32;
+}
+template <class T>
+__device__ __forceinline__ WarpStage<T> warp_stage(unsigned char* smem, int warp) {
+  using V4 = typename V4T<T>::type;
+  unsigned char* base = smem + size_t(warp) * warp_stage_bytes<T>();
+  WarpStage<T> s;
+  s.col = reinterpret_cast<V4*>(base);
+  s.wxm = s.col + 32 * 9;
+  s.acol = s.wxm + 32;
+  s.gk = reinterpret_cast<int4*>(s.acol + 32);
+  return s;
+}
+
+// The column-lane scatter of one warp (p2g_lanes_kernel's grouping, runs and vector reductions)
+// for particles whose 27 stencil nodes all lie inside their scene's grid, which G2P's domain clamp
+// guarantees.  Every lane of the warp calls it; has = false lanes contribute nothing.  x is the
+// position, mv = m v, A = m C - k tau.  The cell key is the global index of the stencil's base
+// node, unique across scenes.  kMixed: lanes may belong to different scenes (each run looks its
+// scene up from its base node's block); otherwise every lane belongs to scene sc.
+template <class T, bool kMixed>
+__device__ __forceinline__ void p2g_warp_scatter(const WorldDev<T>& w, const SceneDev<T>& sc, bool has, const T* x,
+                                                 T m, const T* mv, const T* A, const WarpStage<T>& st) {
+  using V4 = typename V4T<T>::type;
+  const int lane = threadIdx.x & 31;
+  int g[3] = {0, 0, 0};
+  T fx[3] = {0, 0, 0}, wt[3][3];
+  if (has) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const T X = (x[a] - sc.origin[a]) * sc.inv_dx;
+      const int b = floor_to_int(X - T(0.5));
+      fx[a] = X - T(b);
+      g[a] = b;
+      const T t0 = T(1.5) - fx[a], t1 = fx[a] - T(1), t2 = fx[a] - T(0.5);
+      wt[a][0] = T(0.5) * t0 * t0;
+      wt[a][1] = T(0.75) - t1 * t1;
+      wt[a][2] = T(0.5) * t2 * t2;
+    }
+  }
+  const uint32_t key = has ? node_index(sc, g[0], g[1], g[2]) : 0xffffffffu;
+  // equal keys anywhere in the warp form one group: groups in order of their first lane, lanes
+  // within a group in lane order; pos is this particle's slot in that grouped order
+  const uint32_t peers = __match_any_sync(0xffffffffu, key);
+  const int leader = __ffs(peers) - 1;
+  const uint32_t lead_cnt = lane == leader ? uint32_t(__popc(peers)) : 0u;
+  uint32_t incl = lead_cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t lead_off = incl - lead_cnt;
+  const int pos = int(__shfl_sync(0xffffffffu, lead_off, leader)) + __popc(peers & ((1u << lane) - 1u));
+  uint32_t starts = __reduce_or_sync(0xffffffffu, lane == leader ? (1u << lead_off) : 0u);
+  if (has) {
+    const T dx = sc.dx;
+    T c0[3], c1[3], c2[3], qv[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      c0[r] = dx * A[3 * r + 0];
+      c1[r] = dx * A[3 * r + 1];
+      c2[r] = dx * A[3 * r + 2];
+      qv[r] = mv[r] - (c0[r] * fx[0] + c1[r] * fx[1] + c2[r] * fx[2]);
+    }
+    V4* cq = st.col + pos * 9;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const T ux = qv[0] + T(b) * c1[0] + T(c) * c2[0];
+        const T uy = qv[1] + T(b) * c1[1] + T(c) * c2[1];
+        const T uz = qv[2] + T(b) * c1[2] + T(c) * c2[2];
+        cq[b + 3 * c] = mk4(ux, uy, uz, wt[1][b] * wt[2][c]);
+      }
+    }
+    st.wxm[pos] = mk4(wt[0][0], wt[0][1], wt[0][2], m);
+    st.acol[pos] = mk4(c0[0], c0[1], c0[2], T(0));
+  }
+  st.gk[pos] = make_int4(g[0], g[1], g[2], int(key));
+  __syncwarp();
+  // lanes 0..26 are 3 particle groups x 9 (y,z) columns; lanes 27..31 mirror lanes 22..26
+  // (in-bounds reads, results never used)
+  const int grp = lane < 27 ? lane / 9 : 2;
+  const int jc = lane < 27 ? lane - 9 * grp : lane - 23;
+  const int nb = jc % 3, nc = jc / 3;
+  const V4* colw = st.col + jc;
+  while (starts) {
+    const int s0 = __ffs(starts) - 1;
+    starts &= starts - 1u;
+    const int e0 = starts ? __ffs(starts) - 1 : 32;
+    const int4 run = st.gk[s0];
+    if (uint32_t(run.w) == 0xffffffffu) continue;
+    const SceneDev<T>& rs = kMixed ? w.scenes[w.blk_scene[uint32_t(run.w) >> 6]] : sc;
+    const int X = run.x, Y = run.y + nb, Z = run.z + nc;
+    T m0 = 0, x0 = 0, y0 = 0, z0 = 0, m1 = 0, x1 = 0, y1 = 0, z1 = 0, m2 = 0, x2 = 0, y2 = 0, z2 = 0;
+#pragma unroll 2
+    for (int i = s0 + grp; i < e0; i += 3) {
+      const V4 u = colw[i * 9];
+      const V4 r = st.wxm[i];
+      const V4 a = st.acol[i];
+      const T W0 = r.x * u.w, W1 = r.y * u.w, W2 = r.z * u.w;
+      m0 += W0 * r.w;
+      x0 += W0 * u.x;
+      y0 += W0 * u.y;
+      z0 += W0 * u.z;
+      const T ux = u.x + a.x, uy = u.y + a.y, uz = u.z + a.z;
+      m1 += W1 * r.w;
+      x1 += W1 * ux;
+      y1 += W1 * uy;
+      z1 += W1 * uz;
+      m2 += W2 * r.w;
+      x2 += W2 * (ux + a.x);
+      y2 += W2 * (uy + a.y);
+      z2 += W2 * (uz + a.z);
+    }
+    if (e0 - s0 > 1) {
+      auto groups = [](T v) { return v + __shfl_down_sync(0xffffffffu, v, 9) + __shfl_down_sync(0xffffffffu, v, 18); };
+      m0 = groups(m0), x0 = groups(x0), y0 = groups(y0), z0 = groups(z0);
+      m1 = groups(m1), x1 = groups(x1), y1 = groups(y1), z1 = groups(z1);
+      m2 = groups(m2), x2 = groups(x2), y2 = groups(y2), z2 = groups(z2);
+    }
+    if (lane < 9) {
+      const uint32_t row = ((rs.blk_off + (uint32_t(Z >> 2) * uint32_t(rs.nb[1]) + uint32_t(Y >> 2)) * uint32_t(rs.nb[0])) << 6) |
+                           (uint32_t(Z & 3) << 4) | (uint32_t(Y & 3) << 2);
+      auto node = [row](int xa) { return row + ((uint32_t(xa >> 2) << 6) | uint32_t(xa & 3)); };
+      if (m0 != T(0)) atomic_add4(w.acc + node(X), m0, x0, y0, z0);
+      if (m1 != T(0)) atomic_add4(w.acc + node(X + 1), m1, x1, y1, z1);
+      if (m2 != T(0)) atomic_add4(w.acc + node(X + 2), m2, x2, y2, z2);
+    }
+    if (kMixed && lane >= 9 && lane < 17) {  // the run's stencil blocks (at most 2 per axis)
+      const int o = lane - 9;
+      const int bx = (run.x + 2 * (o & 1)) >> 2, by = (run.y + (o & 2)) >> 2, bz = (run.z + ((o >> 1) & 2)) >> 2;
+      mark_block(w, rs.blk_off + (uint32_t(bz) * uint32_t(rs.nb[1]) + uint32_t(by)) * uint32_t(rs.nb[0]) + uint32_t(bx));
+    }
+  }
+  if (!kMixed) {  // grid blocks of the warp's stencil bounding box (all inside the grid)
+    int B[3], NB[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int l = __reduce_min_sync(0xffffffffu, has ? g[a] : INT_MAX);
+      const int h = __reduce_max_sync(0xffffffffu, has ? g[a] + 2 : INT_MIN);
+      B[a] = l >> 2;
+      NB[a] = l == INT_MAX ? 0 : (h >> 2) - (l >> 2) + 1;
+    }
+    const int nblk = NB[0] * NB[1] * NB[2];
+    for (int t = lane; t < nblk; t += 32) {
+      const int bx = B[0] + t % NB[0], by = B[1] + (t / NB[0]) % NB[1], bz = B[2] + t / (NB[0] * NB[1]);
+      mark_block(w, sc.blk_off + (uint32_t(bz) * uint32_t(sc.nb[1]) + uint32_t(by)) * uint32_t(sc.nb[0]) + uint32_t(bx));
+    }
+  }
+  __syncwarp();  // the staging region is free again
+}
+
+// G2P of substep s and P2G of substep s + 1 (physics mode).  The grid update of substep s ran
+// before; w.touched / w.touched_count are the touched-block list of substep s + 1.
+template <class T>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) g2p2g_kernel(WorldDev<T> w, uint32_t* epoch,
+                                                                              int write_keys) {
+  using V4 = typename V4T<T>::type;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int4 ch = cta_chunk(w);
+  const SceneDev<T>& sc = w.scenes[ch.x];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const WarpStage<T> st = warp_stage<T>(smem, tid >> 5);
+  V4* pre = st.col;  // F, J and the material of the warp's particles (pre[k * 32 + lane]) until the scatter
+  const int j = ch.y + tid;
+  const bool live = j < ch.z;
+  if (blockIdx.x == 0 && tid == 0) *epoch += 1u;
+  uint32_t err = 0;
+  bool cl = false, need = false, has = false;
+  T xs[3] = {0, 0, 0}, m = 0, mv[3] = {0, 0, 0}, A[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (live) {
+    const uint32_t src = w.perm ? w.perm[j] : uint32_t(j);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cp_async_v4(pre + k * 32 + lane, w.in[1 + k] + src);
+    cp_async_commit();
+    const V4 a0 = ld4(w.in[0] + src);
+    const T x0[3] = {a0.x, a0.y, a0.z};
+    G2POut<T> o;
+    T pv[3] = {0, 0, 0};
+    const bool done = g2p_physics_gather_sep<T>(
+        GridRows<T>{w.vel, sc.blk_off, uint32_t(sc.nb[0]), uint32_t(sc.nb[1])}, sc, x0, pv, o.C);
+    if (!done) {  // stencil partly outside the grid (a particle's first substep)
+      VelTile<T> vt;
+      vt.tile = nullptr;
+      vt.vel = w.vel;
+      g2p_physics_gather<T>(vt, sc, x0, pv, o.C);
+    }
+    cp_async_wait_all();
+    const V4 a1 = pre[lane], a2 = pre[32 + lane], a3 = pre[64 + lane];
+    const T F[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
+    const MatDev& md = mat_of(w, sc, Bits<T>::unpack(a3.z) & 0xffffu);
+    g2p_physics_update<T>(sc, md, x0, pv, F, a3.y, a0.w, o);
+    w.out[0][j] = mk4(o.x[0], o.x[1], o.x[2], a0.w);
+    w.out[1][j] = mk4(o.F[0], o.F[1], o.F[2], o.F[3]);
+    w.out[2][j] = mk4(o.F[4], o.F[5], o.F[6], o.F[7]);
+    w.out[3][j] = mk4(o.F[8], o.J, a3.z, a3.w);
+    w.out[4][j] = mk4(o.v[0], o.v[1], o.v[2], o.C[0]);
+    w.out[5][j] = mk4(o.C[1], o.C[2], o.C[3], o.C[4]);
+    w.out[6][j] = mk4(o.C[5], o.C[6], o.C[7], o.C[8]);
+    if (write_keys) w.keys[j] = cell_key(sc, AE_MPM_MODE_PHYSICS, o.x[0], o.x[1], o.x[2]);
+    err = o.err;
+    cl = o.clamped;
+    need = o.needs_clamp;
+    has = !need;
+    m = a0.w;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      xs[a] = o.x[a];
+      mv[a] = m * o.v[a];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) A[k] = o.C[k];
+  } else if (j < ch.w && write_keys) {
+    w.keys[j] = sc.dead_key;
+  }
+  const uint32_t e = __reduce_or_sync(0xffffffffu, err);
+  const uint32_t ncl = __popc(__ballot_sync(0xffffffffu, cl));
+  const uint32_t qmask = __ballot_sync(0xffffffffu, need);
+  uint32_t qbase = 0;
+  if (lane == 0) {
+    if (e) atomicOr(w.err + 4 * ch.x, e);
+    if (ncl) atomicAdd(w.err + 4 * ch.x + 2, ncl);
+    if (qmask) qbase = atomicAdd(w.clamp_count, uint32_t(__popc(qmask)));
+  }
+  qbase = __shfl_sync(0xffffffffu, qbase, 0);
+  if (need) w.clamp_queue[qbase + __popc(qmask & ((1u << lane) - 1u))] = make_uint2(uint32_t(j), uint32_t(ch.x));
+  __syncwarp();  // every lane has read its F, J and material: the scatter may reuse the region
+  p2g_warp_scatter<T, false>(w, sc, has, xs, m, mv, A, st);
+}
+
+// The snow return mapping of snow_clamp_kernel for the particles the fused kernel queued, each
+// then scattered into the next substep's accumulator with its final A.  A warp takes 32
+// consecutive queue entries (possibly of several scenes of a world).
+template <class T>
+__global__ void __launch_bounds__(128, 8) snow_clamp_scatter_kernel(WorldDev<T> w) {
+  using V4 = typename V4T<T>::type;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31;
+  const WarpStage<T> st = warp_stage<T>(smem, threadIdx.x >> 5);
+  V4* pre = st.col;  // position+mass, velocity+A of the queued particle: pre[k * 32 + lane], until the scatter
+  const uint32_t count = launch_count(w.clamp_count);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
+    const uint32_t i = base + lane;
+    const bool valid = i < count;
+    const uint2 q = valid ? w.clamp_queue[i] : make_uint2(0u, 0u);
+    const SceneDev<T>& sc = w.scenes[q.y];
+    T xs[3] = {0, 0, 0}, m = 0, mv[3] = {0, 0, 0}, A[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (valid) {
+      cp_async_v4(pre + lane, w.out[0] + q.x);
+      cp_async_v4(pre + 32 + lane, w.out[4] + q.x);
+      cp_async_v4(pre + 64 + lane, w.out[5] + q.x);
+      cp_async_v4(pre + 96 + lane, w.out[6] + q.x);
+      cp_async_commit();
+      const V4 a1 = w.out[1][q.x], a2 = w.out[2][q.x], a3 = w.out[3][q.x];
+      const MatDev& md = mat_of(w, sc, Bits<T>::unpack(a3.z) & 0xffffu);
+      const T F[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
+      const T lo = T(1) - T(md.theta_c), hi = T(1) + T(md.theta_s);
+      T U[9], sg[3], V[9];
+      const bool fb = svd3_fallback(F, U, sg, V, w.svd_fallback != 0, lo, hi);
+      T scl[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) scl[k] = t_min(t_max(sg[k], lo), hi);
+      const T J = a3.y * ((sg[0] * sg[1] * sg[2]) / (scl[0] * scl[1] * scl[2]));
+      T nF[9];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          nF[r * 3 + c] = U[r * 3 + 0] * scl[0] * V[c * 3 + 0] + U[r * 3 + 1] * scl[1] * V[c * 3 + 1] +
+                          U[r * 3 + 2] * scl[2] * V[c * 3 + 2];
+      w.out[1][q.x] = mk4(nF[0], nF[1], nF[2], nF[3]);
+      w.out[2][q.x] = mk4(nF[4], nF[5], nF[6], nF[7]);
+      w.out[3][q.x] = mk4(nF[8], J, a3.z, a3.w);
+      cp_async_wait_all();
+      const V4 a0 = pre[lane], a4 = pre[32 + lane], a5 = pre[64 + lane], a6 = pre[96 + lane];
+      const T C[9] = {a4.w, a5.x, a5.y, a5.z, a5.w, a6.x, a6.y, a6.z, a6.w};
+      affine_from_c(sc, md, a0.w, C, nF, J, A);
+      w.out[4][q.x] = mk4(a4.x, a4.y, a4.z, A[0]);
+      w.out[5][q.x] = mk4(A[1], A[2], A[3], A[4]);
+      w.out[6][q.x] = mk4(A[5], A[6], A[7], A[8]);
+      if (fb) atomicAdd(w.err + 4 * q.y + 1, 1u);
+      m = a0.w;
+      xs[0] = a0.x, xs[1] = a0.y, xs[2] = a0.z;
+      mv[0] = m * a4.x, mv[1] = m * a4.y, mv[2] = m * a4.z;
+    }
+    __syncwarp();  // prefetched data consumed: the scatter may reuse the region
+    p2g_warp_scatter<T, true>(w, sc, valid, xs, m, mv, A, st);
+  }
+}
+
+// Drops a scatter that was queued for the next substep (the particle state it came from changed):
+// zeroes the accumulator and the flags of the blocks on its touched list.
+template <class T>
+__global__ void discard_scatter_kernel(typename V4T<T>::type* acc, uint32_t* blk_flag, const uint32_t* list,
+                                       const uint32_t* count) {
+  const uint32_t n = launch_count(count);
+  for (uint32_t t = blockIdx.x; t < n; t += gridDim.x) {
+    const uint32_t gb = list[t];
+    if (threadIdx.x < 64) acc[uint64_t(gb) * 64u + threadIdx.x] = mk4(T(0), T(0), T(0), T(0));
+    if (threadIdx.x == 0) blk_flag[gb] = 0u;
+  }
+}
+
+// ============================================================================================
 // deterministic mode: per-cell fixed-order sums, per-node fixed-order gather
 // ============================================================================================
 __global__ void det_heads_kernel(const uint32_t* __restrict__ skeys, uint64_t n, const uint32_t* __restrict__ dead_flag,
@@ -1757,9 +2092,11 @@ class World final : public WorldBase {
     AE_TRY(cudaMemset(blk_flag_, 0, sizeof(uint32_t) * blk));
     AE_TRY(dmalloc(&blk_epoch_, sizeof(uint32_t) * blk));
     AE_TRY(cudaMemset(blk_epoch_, 0xff, sizeof(uint32_t) * blk));
-    AE_TRY(dmalloc(&touched_, sizeof(uint32_t) * blk));
-    AE_TRY(dmalloc(&counters_, sizeof(uint32_t) * 4));
-    AE_TRY(cudaMemset(counters_, 0, sizeof(uint32_t) * 4));
+    // two touched-block lists: the fused G2P + P2G fills the next substep's while the grid update
+    // consumes the current one's
+    AE_TRY(dmalloc(&touched_, sizeof(uint32_t) * 2 * blk));
+    AE_TRY(dmalloc(&counters_, sizeof(uint32_t) * 8));
+    AE_TRY(cudaMemset(counters_, 0, sizeof(uint32_t) * 8));
     AE_TRY(dmalloc(&clamp_queue_, sizeof(uint2) * pc));
     AE_TRY(dmalloc(&err_, sizeof(uint32_t) * 4 * n));
     AE_TRY(cudaMemset(err_, 0, sizeof(uint32_t) * 4 * n));
@@ -1830,6 +2167,7 @@ class World final : public WorldBase {
     scenes_dirty_ = true;
     mats_dirty_ = true;
     keys_stale_ = true;  // dx or origin may have moved the cells
+    scatter_invalid_ = true;
     if (rebase) {
       int rc = sync_tables();
       if (rc) return rc;
@@ -1893,6 +2231,7 @@ class World final : public WorldBase {
                                                                       d_scenes_ + s, d_mats_);
       AE_TRY(cudaGetLastError());
     }
+    scatter_invalid_ = true;
     // the same count keeps the scene table, the chunks and the captured graph (which replays from
     // the upload's buffers); the cell keys are recomputed before the next substep either way
     if (h_scenes_[s].p_count != uint32_t(n)) {
@@ -1947,6 +2286,7 @@ class World final : public WorldBase {
     int rc = prepare();
     if (rc) return rc;
     if (n == 0) return AE_MPM_OK;
+    if ((rc = sync_scatter())) return rc;
     if (keys_stale_) {
       WorldDev<T> w = dev(false);
       launch_init_keys(w);
@@ -2084,6 +2424,7 @@ class World final : public WorldBase {
       for (int k = 0; k < 7; ++k)
         AE_TRY(cudaMemcpyAsync(in_buf()[k], snap_[k], sizeof(V4) * pc, cudaMemcpyDeviceToDevice, stream_));
       keys_stale_ = true;
+      scatter_invalid_ = true;
       AE_TRY(cudaMemsetAsync(err_, 0, sizeof(uint32_t) * 4 * h_scenes_.size(), stream_));
     }
     AE_TRY(cudaStreamSynchronize(stream_));
@@ -2122,7 +2463,7 @@ class World final : public WorldBase {
         AE_TRY(cudaMemcpyAsync(in_buf()[k] + b.p_off, src->in_buf()[k] + a.p_off, sizeof(V4) * a.p_count,
                                cudaMemcpyDeviceToDevice, stream_));
     b.p_count = a.p_count;
-    scenes_dirty_ = chunks_dirty_ = keys_stale_ = true;
+    scenes_dirty_ = chunks_dirty_ = keys_stale_ = scatter_invalid_ = true;
     return AE_MPM_OK;
   }
   uint32_t scene_count(uint32_t s) const override { return s < h_scenes_.size() ? h_scenes_[s].p_count : 0; }
@@ -2133,6 +2474,7 @@ class World final : public WorldBase {
     int rc = prepare();
     if (rc) return rc;
     if (n == 0 || n_chunks_ == 0) return AE_MPM_OK;
+    if ((rc = sync_scatter())) return rc;
     if (keys_stale_) {
       WorldDev<T> w = dev(false);
       launch_init_keys(w);
@@ -2345,7 +2687,7 @@ class World final : public WorldBase {
     } else {
       launch_p2g<MODE>(w);
       mark(2);
-      grid_update_kernel<T, MODE><<<sms * 4, 256, 0, stream_>>>(w, blk_epoch_, counters_ + 2);
+      grid_update_kernel<T, MODE><<<sms * 4, 256, 0, stream_>>>(w, blk_epoch_, counters_ + 2, nullptr);
       launches_ += 2;
     }
     mark(3);
@@ -2361,6 +2703,70 @@ class World final : public WorldBase {
 
   void mark(int k) {
     if (stage_events_) cudaEventRecord(stage_events_[k], stream_);
+  }
+
+  // ---- fused G2P + P2G (physics mode, column-lane P2G, not deterministic) ----
+  // The P2G of substep s + 1 is done by the G2P of substep s, so between substeps the grid
+  // accumulator holds the scatter of the current particle state ("queued"), on touched list
+  // (s + 1) & 1.  Anything that changes the particles or the flow drops it; the next step()
+  // scatters the current state once with the stand-alone P2G before its first substep.
+  bool fused() const {
+    return mode_ == AE_MPM_MODE_PHYSICS && !opts_.deterministic && opts_.p2g_variant == kVarLanes;
+  }
+  uint32_t* touched_list(int par) { return touched_ + size_t(par) * total_blocks_; }
+  uint32_t* touched_count(int par) { return counters_ + (par ? 4 : 0); }
+  WorldDev<T> with_list(WorldDev<T> w, int par) {
+    w.touched = touched_list(par);
+    w.touched_count = touched_count(par);
+    return w;
+  }
+  static size_t fused_smem(int threads) { return warp_stage_bytes<T>() * size_t(threads / 32); }
+
+  int sync_scatter() {
+    const int par = int(substep_ & 1);
+    if (fused() && !fused_smem_set_) {  // sized for the largest block (256 threads) the world accepts
+      AE_TRY(cudaFuncSetAttribute(g2p2g_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(fused_smem(256))));
+      AE_TRY(cudaFuncSetAttribute(snow_clamp_scatter_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(fused_smem(128))));
+      fused_smem_set_ = true;
+    }
+    if (scatter_pending_ && (!fused() || scatter_invalid_)) {
+      discard_scatter_kernel<T><<<device_sm_count() * 8, 64, 0, stream_>>>(acc_, blk_flag_, touched_list(par),
+                                                                            touched_count(par));
+      AE_TRY(cudaMemsetAsync(counters_, 0, sizeof(uint32_t), stream_));
+      AE_TRY(cudaMemsetAsync(counters_ + 4, 0, sizeof(uint32_t), stream_));
+      ++launches_;
+      scatter_pending_ = false;
+    }
+    scatter_invalid_ = false;
+    if (fused() && !scatter_pending_ && n_chunks_ > 0) {
+      AE_TRY(cudaMemsetAsync(touched_count(par), 0, sizeof(uint32_t), stream_));
+      WorldDev<T> w = with_list(dev(false), par);
+      launch_p2g<AE_MPM_MODE_PHYSICS>(w);
+      ++launches_;
+      scatter_pending_ = true;
+    }
+    AE_TRY(cudaGetLastError());
+    return AE_MPM_OK;
+  }
+
+  void substep_fused(WorldDev<T>& w, bool write_keys) {
+    const int sms = device_sm_count();
+    const int par = int(substep_ & 1);
+    mark(2);  // no stand-alone P2G: the previous substep's G2P scattered this one
+    WorldDev<T> wg = with_list(w, par);
+    grid_update_kernel<T, AE_MPM_MODE_PHYSICS><<<sms * 4, 256, 0, stream_>>>(wg, blk_epoch_, counters_ + 2,
+                                                                          touched_count(par ^ 1));
+    mark(3);
+    WorldDev<T> wf = with_list(w, par ^ 1);
+    g2p2g_kernel<T><<<n_chunks_, chunk_threads_, fused_smem(chunk_threads_), stream_>>>(wf, counters_ + 2,
+                                                                                         write_keys ? 1 : 0);
+    launches_ += 2;
+    if (has_snow_) {
+      snow_clamp_scatter_kernel<T><<<sms * 8, 128, fused_smem(128), stream_>>>(wf);
+      ++launches_;
+    }
+    mark(4);
   }
 
   void substep_eager() {
@@ -2381,7 +2787,12 @@ class World final : public WorldBase {
       mark(1);
       WorldDev<T> w = dev(do_sort);
       switch (mode_) {
-        case AE_MPM_MODE_PHYSICS: substep_mode<AE_MPM_MODE_PHYSICS>(w, next_sorts); break;
+        case AE_MPM_MODE_PHYSICS:
+          if (fused())
+            substep_fused(w, next_sorts);
+          else
+            substep_mode<AE_MPM_MODE_PHYSICS>(w, next_sorts);
+          break;
         case AE_MPM_MODE_REFERENCE: substep_mode<AE_MPM_MODE_REFERENCE>(w, next_sorts); break;
         default: substep_mode<AE_MPM_MODE_VELOCITY_ONLY>(w, next_sorts); break;
       }
@@ -2495,7 +2906,9 @@ class World final : public WorldBase {
   cudaGraphExec_t graph_ = nullptr;
   uint64_t graph_period_ = 0, graph_launches_ = 0;
   int graph_variant_ = -1;
-  bool lanes_smem_set_ = false;
+  bool lanes_smem_set_ = false, fused_smem_set_ = false;
+  bool scatter_pending_ = false;  // the accumulator holds the P2G of the current particle state
+  bool scatter_invalid_ = false;  // the particles changed since that scatter
   uint64_t substep_ = 0, snap_substep_ = 0, launches_ = 0;
   cudaEvent_t* stage_events_ = nullptr;
   uint64_t total_cap_ = 0, total_blocks_ = 0, device_bytes_ = 0;

@@ -50,7 +50,17 @@ import numpy as np  # noqa: E402
 # 16 B per active node; the grid update reads and writes 64 B per active node.  (The kernels'
 # own layout moves 64 B per particle in P2G and 180 B in G2P: P2G reads an affine matrix that
 # G2P folds the stress into, instead of F.)
-KERNEL_BYTES = {"p2g": (104, 16), "g2p": (156, 16), "grid": (0, 64)}
+KERNEL_BYTES = {"p2g": (104, 16), "g2p": (156, 16), "grid": (0, 64), "g2p2g": (104 + 156, 16 + 16)}
+
+
+def dominant_kernel(stages):
+    """The kernel the roofline is quoted on, from a world's stage times.  A world whose P2G is
+    fused into G2P (physics mode, column-lane P2G) reports no stand-alone P2G: its G2P stage is the
+    fused kernel (plus the snow clamp), which moves the bytes of both."""
+    if stages["p2g"] < 0.02 * stages["g2p"]:
+        return "g2p2g", stages["g2p"]
+    k = max(("p2g", "g2p", "grid"), key=lambda k: stages[k])
+    return k, stages[k]
 
 
 def l2_note(n_particles):
@@ -1035,10 +1045,10 @@ def run_ours(args, rank, local, world_size, pg):
     stages_end = world.stage_times(STAGE_SUBSTEPS)
 
     # roofline of the dominant kernel (P2G or G2P), from its event-timed mean duration
-    kern = "g2p" if stages["g2p"] >= stages["p2g"] else "p2g"
+    kern, kern_us = dominant_kernel(stages)
     per_p, per_n = KERNEL_BYTES[kern]
     alg_bytes = per_p * n_total + per_n * A
-    achieved = alg_bytes / (stages[kern] * 1e-6) / 1e9
+    achieved = alg_bytes / (kern_us * 1e-6) / 1e9
     peak, peak_kind = peaks()
     traffic = traffic_record(args.workload, kern)
 
@@ -1119,7 +1129,7 @@ def run_ours(args, rank, local, world_size, pg):
                          "frac": achieved / peak, "traffic": traffic["bytes"] if traffic else None,
                          "traffic_source": traffic["source"] if traffic else None, "peak_kind": peak_kind,
                          "algorithmic_bytes": alg_bytes, "bytes_per_particle": per_p, "bytes_per_node": per_n,
-                         "active_nodes": A, "kernel_us": stages[kern],
+                         "active_nodes": A, "kernel_us": kern_us,
                          "kernel_substeps": [t0_sub - STAGE_SUBSTEPS, t0_sub]},
             "stages_us": {k: round(v, 2) for k, v in stages.items()},
             "stages_us_end": dict({k: round(v, 2) for k, v in stages_end.items()},
@@ -1333,10 +1343,10 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
         ref = fp64_run(ctx, scenes, parts, tuned, run)
         err = dict(position_error(scenes, hout, ref), substeps=run)
 
-    kern = max(("p2g", "g2p", "grid"), key=lambda k: stages[k])
+    kern, kern_us = dominant_kernel(stages)
     per_p, per_n = KERNEL_BYTES[kern]
     alg_bytes = per_p * n_total + per_n * A
-    achieved = alg_bytes / (stages[kern] * 1e-6) / 1e9
+    achieved = alg_bytes / (kern_us * 1e-6) / 1e9
     peak, peak_kind = peaks()
     traffic = traffic_record("batched", kern)
 
@@ -1365,7 +1375,7 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
                          "frac": achieved / peak, "traffic": traffic["bytes"] if traffic else None,
                          "traffic_source": traffic["source"] if traffic else None, "peak_kind": peak_kind,
                          "algorithmic_bytes": alg_bytes, "bytes_per_particle": per_p, "bytes_per_node": per_n,
-                         "active_nodes": A, "kernel_us": stages[kern],
+                         "active_nodes": A, "kernel_us": kern_us,
                          "kernel_substeps": [t0_sub - STAGE_SUBSTEPS, t0_sub]},
             "stages_us": {a: round(b, 2) for a, b in stages.items()}, "autotune": tune,
             "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,

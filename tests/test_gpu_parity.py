@@ -215,6 +215,31 @@ def test_batched_world_matches_scenes_alone(ctx):
     w.close()
 
 
+def test_batched_world_with_atomics_matches_fp64_oracle_per_scene(ctx):
+    # the default (fused G2P + P2G) path on a world of several scenes of different grids and
+    # materials, snow included: the clamp kernel's scatter takes queue entries of several scenes in
+    # one warp.  Each scene against the FP64 oracle run alone: 1e-5 of the largest |x|.
+    rng = S.Rng(0xF05E)
+    pairs = [S.batched_scene(rng) for _ in range(9)]
+    pairs.append(S.snow_collision_small(n_box=2048, grid=32))
+    scenes = [sc for sc, _ in pairs]
+    w = M.World(ctx, scenes, M.exec_opts(p2g_variant=M.P2G_LANES, block_threads=128, sort_interval=4))
+    for i, (_, p) in enumerate(pairs):
+        w.upload(i, p)
+    w.step(40)
+    assert w.sync(raise_on_error=False) == M.OK
+    clamped = 0
+    for i, (sc, p) in enumerate(pairs):
+        got = w.download(i, p.n)
+        ref = p.astype(np.float64)
+        cnt = O.run(sc, ref, 40)
+        assert rel(got.pos, ref.pos) <= 1e-5, i
+        assert rel(got.F, ref.F) <= 2e-4, i
+        clamped += int(np.sum(np.abs(ref.J - 1.0) > 1e-9))
+    assert clamped > 1000  # snow particles took the return mapping (and the clamp kernel's scatter)
+    w.close()
+
+
 # ------------------------------------------------------------------ reference mode (drop-in)
 def _ref_setup(n=3000, grid=32, dx=0.05, origin=(0.0, 0.0, 0.0), models=(M.NEO_HOOKEAN,), seed=5):
     rng = np.random.default_rng(seed)
