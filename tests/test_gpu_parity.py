@@ -235,7 +235,8 @@ def test_batched_world_with_atomics_matches_fp64_oracle_per_scene(ctx):
         cnt = O.run(sc, ref, 40)
         assert rel(got.pos, ref.pos) <= 1e-5, i
         assert rel(got.F, ref.F) <= 2e-4, i
-        clamped += int(np.sum(np.abs(ref.J - 1.0) > 1e-9))
+        if sc.materials[0].model == M.PHYS_SNOW:  # J carries the plastic J_p for snow
+            clamped += int(np.sum(np.abs(ref.J - 1.0) > 1e-9))
     assert clamped > 1000  # snow particles took the return mapping (and the clamp kernel's scatter)
     w.close()
 
