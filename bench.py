@@ -57,7 +57,7 @@ def dominant_kernel(stages):
     """The kernel the roofline is quoted on, from a world's stage times.  A world whose P2G is
     fused into G2P (physics mode, column-lane P2G) reports no stand-alone P2G: its G2P stage is the
     fused kernel (plus the snow clamp), which moves the bytes of both."""
-    if stages["p2g"] < 0.02 * stages["g2p"]:
+    if stages["p2g"] < 0.1 * stages["g2p"]:
         return "g2p2g", stages["g2p"]
     k = max(("p2g", "g2p", "grid"), key=lambda k: stages[k])
     return k, stages[k]
@@ -87,6 +87,7 @@ def parse():
                     help="substeps per end-to-end call; default: the workload's run length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 error reference run")
+    ap.add_argument("--no-plain", action="store_true", help="batched: skip the plain (one world per scene) arm")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--variant", choices=["lanes", "tile", "warp_agg", "global"],
                     help="fixed P2G variant (with --block-threads and --sort-interval: no autotune)")
@@ -228,6 +229,31 @@ def workload(name: str, rank: int, n_scenes: int, world_size: int = 1):
                     % n_scenes, "scenes": len(pairs), "particles": n, "l2": l2_note(n),
         "parallelism": "%d scenes per GPU, dealt round-robin from one list of %d" % (len(pairs), n_scenes * world_size)
         if world_size > 1 else "single GPU"}
+
+
+def fixed_options(args) -> dict:
+    """Execution options fixed on the command line (--variant, --block-threads, --sort-interval);
+    any of them turns the autotuner off."""
+    import ae_mpm as M
+
+    fixed = {}
+    if args.variant:
+        fixed["p2g_variant"] = {"tile": M.P2G_TILE, "warp_agg": M.P2G_WARP_AGG, "global": M.P2G_GLOBAL,
+                                "lanes": M.P2G_LANES}[args.variant]
+    if args.block_threads:
+        fixed["block_threads"] = args.block_threads
+    if args.sort_interval:
+        fixed["sort_interval"] = args.sort_interval
+    return fixed
+
+
+def timed_range(torch, begin: bool):
+    """NVTX range "timed" around the timed substeps, so a profiler can select exactly their launches
+    (ncu --nvtx --nvtx-include "timed/")."""
+    if begin:
+        torch.cuda.nvtx.range_push("timed")
+    else:
+        torch.cuda.nvtx.range_pop()
 
 
 def traffic_record(workload_name: str, kernel: str):
@@ -992,14 +1018,7 @@ def run_ours(args, rank, local, world_size, pg):
         return run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg)
     if args.workload == "batched":
         return run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg)
-    fixed = {}
-    if args.variant:
-        fixed["p2g_variant"] = {"tile": M.P2G_TILE, "warp_agg": M.P2G_WARP_AGG, "global": M.P2G_GLOBAL,
-                                "lanes": M.P2G_LANES}[args.variant]
-    if args.block_threads:
-        fixed["block_threads"] = args.block_threads
-    if args.sort_interval:
-        fixed["sort_interval"] = args.sort_interval
+    fixed = fixed_options(args)
     opts = M.exec_opts(**fixed)
     world = M.World(ctx, scenes, opts)
     for i, p in enumerate(parts):
@@ -1030,10 +1049,12 @@ def run_ours(args, rank, local, world_size, pg):
     torch.cuda.synchronize(local)
     clocks.start()
     time.sleep(0.3)
+    timed_range(torch, True)
     e0.record(stream)
     world.step(args.steps)
     e1.record(stream)
     e1.synchronize()
+    timed_range(torch, False)
     torch.cuda.synchronize(local)
     clk = clocks.stop()
     world.sync(raise_on_error=False)
@@ -1236,11 +1257,12 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
     import ae_mpm as M
 
     n_total = sum(p.n for p in parts)
-    world = M.World(ctx, scenes, M.exec_opts())
+    tuned = fixed_options(args)
+    world = M.World(ctx, scenes, M.exec_opts(**tuned))
     for i, p in enumerate(parts):
         world.upload(i, p)
-    tune, tuned = None, {}
-    if not args.no_autotune:
+    tune = {"fixed": {k: int(v) for k, v in tuned.items()}} if tuned else None
+    if not args.no_autotune and not tuned:
         r = world.autotune(8)
         tuned = {"p2g_variant": r.p2g_variant, "block_threads": r.block_threads, "sort_interval": r.sort_interval}
         tune = dict(tuned, p2g_variant={1: "tile", 2: "warp_agg", 3: "global", 4: "lanes"}.get(r.p2g_variant),
@@ -1260,10 +1282,12 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
     torch.cuda.synchronize(local)
     clocks.start()
     time.sleep(0.3)
+    timed_range(torch, True)
     e0.record(stream)
     world.step(args.steps)
     e1.record(stream)
     e1.synchronize()
+    timed_range(torch, False)
     torch.cuda.synchronize(local)
     clk = clocks.stop()
     launches = world.launches()
@@ -1273,13 +1297,13 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
 
     # plain path: every scene in a world of its own (same kernels and options), stepped one scene
     # after another; the same K substeps per scene, each timed with events on that world's stream
-    plain = [M.World(ctx, [sc], M.exec_opts(**tuned)) for sc in scenes]
+    plain = [] if args.no_plain else [M.World(ctx, [sc], M.exec_opts(**tuned)) for sc in scenes]
     t_plain = 0.0
     for w1, p in zip(plain, parts):
         w1.upload(0, p)
         t_plain += time_world(torch, w1, local, args.steps, 3)
     t_plain = max_over_ranks(pg, t_plain)
-    plain_value = n_total * world_size * args.steps / (t_plain / 1e3)
+    plain_value = n_total * world_size * args.steps / (t_plain / 1e3) if plain else None
 
     # end to end through the C ABI: every scene submitted at once from pinned host memory, the
     # config's run length of substeps, every scene downloaded; a scene completes when its results
@@ -1308,7 +1332,7 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
         lat = [ev0.elapsed_time(ev) / 1e3 for ev in done]
         e2e_b.append(max_over_ranks(pg, lat[-1]))
         lat_b.append(lat)
-        if rep == 0 or args.e2e_reps > 1:
+        if plain and (rep == 0 or args.e2e_reps > 1):
             barrier(pg)
             torch.cuda.synchronize(local)
             s0 = torch.cuda.ExternalStream(plain[0].stream(), device=local)
@@ -1327,13 +1351,13 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
             e2e_p.append(max_over_ranks(pg, lat[-1]))
             lat_p.append(lat)
     kb = int(np.argsort(e2e_b)[len(e2e_b) // 2])
-    kp = int(np.argsort(e2e_p)[len(e2e_p) // 2])
+    kp = int(np.argsort(e2e_p)[len(e2e_p) // 2]) if e2e_p else None
     e2e = {"value": n_total * world_size * run / e2e_b[kb], "unit": "particle-updates/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d, "substeps_per_step": run,
            "ms_per_step": 1e3 * e2e_b[kb],
            "call": "ae_mpm_world_upload of every scene from pinned host memory, ae_mpm_world_step(%d), "
                    "ae_mpm_world_download of every scene" % run}
-    plain_e2e = n_total * world_size * run / e2e_p[kp]
+    plain_e2e = n_total * world_size * run / e2e_p[kp] if e2e_p else None
     for w1 in plain:
         w1.close()
 
@@ -1364,10 +1388,12 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
             "batched_vs_plain": {"ratio": value / plain_value, "plain_value": plain_value,
                                  "e2e_ratio": e2e["value"] / plain_e2e, "plain_e2e_value": plain_e2e,
                                  "plain_scenes": len(scenes),
-                                 "plain_kind": "one world per scene (same kernels and options), scenes in turn"},
+                                 "plain_kind": "one world per scene (same kernels and options), scenes in turn"}
+            if plain else None,
             "scene_latency_s": {"substeps": run, "batched_p50": percentile(lat_b[kb], 50),
                                 "batched_p99": percentile(lat_b[kb], 99),
-                                "plain_p50": percentile(lat_p[kp], 50), "plain_p99": percentile(lat_p[kp], 99),
+                                "plain_p50": percentile(lat_p[kp], 50) if plain else None,
+                                "plain_p99": percentile(lat_p[kp], 99) if plain else None,
                                 "definition": "every scene submitted at t=0; done when its results are in the "
                                               "caller's pinned buffer"},
             "error_vs_fp64": err,
