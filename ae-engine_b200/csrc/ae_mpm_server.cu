@@ -1,15 +1,19 @@
 // ae_mpm_server.cu -- continuous-batching MPM server (ae_mpm_server_* in include/ae_mpm.h).
 //
-// One device thread owns a "batch": a world holding every admitted scene.  Each tick it
-//   1. drops cancelled requests and admits waiting ones while their estimated device state fits
-//      the HBM budget (ae_engine/src/vram_manager.rs:4-146 keeps a VRAM budget per subsystem; this
-//      is the device analogue for resident MPM scenes),
-//   2. rebuilds the batch world when membership changed, moving continuing scenes' state
-//      device-to-device (their particles never return to the host mid-run),
-//   3. runs min(substeps_per_tick, smallest remaining substep count) batched substeps,
-//   4. copies finished scenes into their callers' buffers and frees their memory.
-// Requests submitted while a tick runs wait at most one tick before joining the batch, so the
-// device work of old and new requests overlaps in the same launches.
+// One device thread owns a resident world whose scenes are *slots*: each slot was created with a
+// grid, material and particle capacity, and holds one request's scene at a time.  Each tick it
+//   1. drops cancelled requests and admits waiting ones (first come, first served) into free slots
+//      that fit them; when none fits it grows the world by a batch of slots of the request's size
+//      class, as long as the world stays within the HBM budget (ae_engine/src/vram_manager.rs:4-146
+//      keeps a VRAM budget per subsystem; this is the device analogue for resident MPM scenes),
+//   2. uploads the admitted scenes into their slots in place: no other scene moves,
+//   3. runs min(substeps_per_tick, smallest remaining substep count) substeps of every occupied
+//      slot in one batch,
+//   4. copies finished scenes into their callers' buffers and vacates their slots.
+// Requests submitted while a tick runs join at the next tick, so the device work of old and new
+// requests overlaps in the same launches.  Growing is the only step that moves resident scenes
+// (device to device, into a world with more slots); the slot count doubles per size class, so
+// that happens a logarithmic number of times.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,55 +39,6 @@ double now_s() {
   return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
-// Size-class caching allocator: batch rebuilds reuse freed blocks instead of cudaMalloc/cudaFree.
-class CachingAlloc final : public aemp::DevAlloc {
- public:
-  ~CachingAlloc() override { trim(); }
-  cudaError_t alloc(void** p, size_t bytes) override {
-    size_t cls = round(bytes);
-    auto it = free_.find(cls);
-    if (it != free_.end() && !it->second.empty()) {
-      *p = it->second.back();
-      it->second.pop_back();
-      sizes_[*p] = cls;
-      return cudaSuccess;
-    }
-    cudaError_t e = cudaMalloc(p, cls);
-    if (e == cudaErrorMemoryAllocation) {  // give cached blocks back and retry once
-      cudaGetLastError();
-      trim();
-      e = cudaMalloc(p, cls);
-    }
-    if (e == cudaSuccess) sizes_[*p] = cls;
-    return e;
-  }
-  void release(void* p) override {
-    auto it = sizes_.find(p);
-    if (it == sizes_.end()) {
-      cudaFree(p);
-      return;
-    }
-    free_[it->second].push_back(p);
-    sizes_.erase(it);
-  }
-  void trim() {
-    for (auto& kv : free_)
-      for (void* p : kv.second) cudaFree(p);
-    free_.clear();
-  }
-
- private:
-  static size_t round(size_t b) {  // 1/8-octave size classes, >= 512 B
-    if (b < 512) return 512;
-    size_t top = 1;
-    while ((top << 1) <= b) top <<= 1;
-    size_t step = std::max<size_t>(top / 8, 256);
-    return (b + step - 1) / step * step;
-  }
-  std::map<size_t, std::vector<void*>> free_;
-  std::map<void*, size_t> sizes_;
-};
-
 struct Request {
   uint64_t id = 0;
   ae_mpm_scene_desc desc{};
@@ -95,10 +50,38 @@ struct Request {
   uint32_t substeps = 0, done = 0;
   ae_mpm_particles out{};
   double submit_s = 0, admit_s = 0, done_s = 0;
-  uint64_t bytes = 0;
   int status = AE_MPM_OK;
   bool cancelled = false, on_device = false;
-  int slot = -1;  // scene index in the current batch world
+  int slot = -1;  // scene index of its slot in the world
+};
+
+// The size class a request's slot is made with: each grid axis rounded up to 16 nodes, the
+// particle count to a power of two (at least 1024), the material count to a power of two (at
+// least 4).  A request fits any free slot at least that large whose particle capacity is at most
+// twice its class (more would leave most of the slot's chunks empty).
+struct SlotClass {
+  uint32_t n[3];
+  uint64_t particles;
+  uint32_t materials;
+};
+uint64_t pow2_at_least(uint64_t v, uint64_t lo) {
+  uint64_t p = lo;
+  while (p < v) p <<= 1;
+  return p;
+}
+SlotClass class_of(const ae_mpm_scene_desc& d, uint64_t n) {
+  SlotClass c;
+  for (int a = 0; a < 3; ++a) c.n[a] = std::max<uint32_t>(16u, (d.n[a] + 15u) / 16u * 16u);
+  c.particles = pow2_at_least(n, 1024);
+  c.materials = uint32_t(pow2_at_least(d.n_materials, 4));
+  return c;
+}
+uint64_t grid_blocks(const uint32_t* n) { return uint64_t((n[0] + 3) / 4) * ((n[1] + 3) / 4) * ((n[2] + 3) / 4) + 1; }
+
+struct Slot {
+  SlotClass cls{};
+  uint64_t bytes = 0;     // estimated device bytes of the slot
+  Request* r = nullptr;   // occupant
 };
 
 }  // namespace
@@ -114,14 +97,32 @@ struct ae_mpm_server {
   std::deque<Request*> waiting;
   std::vector<Request*> running;
   std::vector<ae_mpm_request_result> finished;
-  uint64_t resident_bytes = 0;
   uint64_t ticks = 0, particle_substeps = 0;
   uint64_t outstanding = 0;  // submitted and not yet finished
   std::string fatal;
+  // slots (guarded by mu; the device thread alone changes them)
+  std::vector<Slot> slots;
+  uint64_t slot_bytes = 0;   // sum of the slots' estimated bytes: the world's footprint
+  size_t world_slots = 0;    // slots the current world was built with (the rest await a rebuild)
+  ae_mpm_material filler{};  // material of the slots' creation descriptors
   // device-thread state
-  std::unique_ptr<CachingAlloc> alloc;
   aemp::WorldBase* world = nullptr;
-  bool rebuild = false;
+  uint64_t worlds_built = 0;
+
+  ae_mpm_scene_desc slot_desc(const Slot& s, std::vector<ae_mpm_material>& mats) const {
+    ae_mpm_scene_desc d{};
+    d.mode = AE_MPM_MODE_PHYSICS;
+    for (int a = 0; a < 3; ++a) d.n[a] = s.cls.n[a];
+    d.dx = 1.0f / float(s.cls.n[0]);
+    d.dt = 0.0f;
+    d.wall_mode = AE_MPM_WALL_STICKY;
+    d.wall_margin = 3;
+    d.n_materials = s.cls.materials;
+    mats.assign(s.cls.materials, filler);
+    d.materials = mats.data();
+    d.max_particles = s.cls.particles;
+    return d;
+  }
 
   void finish(Request* r, int status) {  // mu held
     r->status = status;
@@ -131,9 +132,48 @@ struct ae_mpm_server {
     cv.notify_all();
   }
 
-  int upload_new(aemp::WorldBase* w, Request* r) {
+  // a free slot r fits, the smallest one (mu held); -1 if none
+  int find_slot(const Request* r) const {
+    const SlotClass want = class_of(r->desc, r->n);
+    int best = -1;
+    for (size_t i = 0; i < slots.size(); ++i) {
+      const Slot& s = slots[i];
+      if (s.r || s.cls.particles < r->n || s.cls.particles > 2 * want.particles ||
+          s.cls.materials < r->desc.n_materials || grid_blocks(s.cls.n) < grid_blocks(r->desc.n))
+        continue;
+      if (best < 0 || s.bytes < slots[best].bytes) best = int(i);
+    }
+    return best;
+  }
+
+  // adds slots of r's class within the budget (mu held): as many as that class has already (at
+  // least one), so a class's slot count doubles per growth; false if not even one fits
+  bool grow_for(const Request* r) {
+    Slot s;
+    s.cls = class_of(r->desc, r->n);
+    std::vector<ae_mpm_material> tmp;
+    s.bytes = aemp::scene_device_bytes(slot_desc(s, tmp), 32);
+    uint64_t same = 0;
+    for (const Slot& o : slots)
+      if (std::memcmp(&o.cls, &s.cls, sizeof(SlotClass)) == 0) ++same;
+    uint64_t k = std::max<uint64_t>(1, same);
+    while (k > 0 && slot_bytes + k * s.bytes > opts.hbm_budget_bytes) --k;
+    if (k == 0) return false;
+    for (uint64_t i = 0; i < k; ++i) slots.push_back(s);
+    slot_bytes += k * s.bytes;
+    return true;
+  }
+
+  ae_mpm_scene_desc request_desc(Request* r) const {
+    ae_mpm_scene_desc d = r->desc;
+    d.materials = r->mats.data();
+    d.max_particles = r->n;
+    return d;
+  }
+
+  int upload_new(Request* r) {
     ae_mpm_particles v{r->pos.data(), r->vel.data(), r->F.data(), r->J.data(), r->C.data(), r->mass.data(), r->mat.data()};
-    int rc = w->upload(uint32_t(r->slot), &v, r->n, false);
+    int rc = world->assign_scene(uint32_t(r->slot), request_desc(r), &v, r->n);
     if (rc == AE_MPM_OK) {
       r->on_device = true;
       // the device copy is authoritative from here on
@@ -148,65 +188,76 @@ struct ae_mpm_server {
     return rc;
   }
 
-  // builds a world for `batch`; continuing scenes are copied from the old world
-  int rebuild_world(std::vector<Request*>& batch) {
-    std::vector<ae_mpm_scene_desc> descs(batch.size());
-    for (size_t i = 0; i < batch.size(); ++i) {
-      descs[i] = batch[i]->desc;
-      descs[i].materials = batch[i]->mats.data();
-      descs[i].max_particles = batch[i]->n;
-    }
+  // a world with every slot; resident scenes move over device to device (their particles never
+  // return to the host mid-run)
+  int rebuild_world(size_t n_slots, const std::vector<Request*>& resident) {
+    std::vector<ae_mpm_scene_desc> descs(n_slots);
+    std::vector<std::vector<ae_mpm_material>> mats(n_slots);
+    for (size_t i = 0; i < n_slots; ++i) descs[i] = slot_desc(slots[i], mats[i]);
     std::string why;
     int st = 0;
-    aemp::WorldBase* nw = descs.empty() ? nullptr : aemp::make_world(descs.data(), uint32_t(descs.size()), opts.exec, why, &st, alloc.get());
-    if (!descs.empty() && !nw) {
+    aemp::WorldBase* nw = aemp::make_world(descs.data(), uint32_t(n_slots), opts.exec, why, &st, nullptr);
+    if (!nw) {
       fatal = why;
       return st ? st : AE_MPM_ECUDA;
     }
     if (world) cudaStreamSynchronize(world->stream());
-    for (size_t i = 0; i < batch.size(); ++i) {
-      Request* r = batch[i];
-      int rc;
-      if (r->on_device && world) {
-        // accumulate the old world's error word before it goes away
-        uint32_t word = 0;
-        world->errors(uint32_t(r->slot), &word, nullptr);
-        if (word & aemp::kErrNaN) r->status = AE_MPM_ENAN;
-        else if ((word & aemp::kErrDomain) && r->status == AE_MPM_OK) r->status = AE_MPM_EDOMAIN;
-        rc = nw->copy_scene_from(uint32_t(i), world, uint32_t(r->slot));
-        r->slot = int(i);
-      } else {
-        r->slot = int(i);
-        rc = upload_new(nw, r);
-      }
+    for (Request* r : resident) {
+      if (!r->on_device || !world) continue;
+      uint32_t word = 0;  // the old world's error word goes with the scene
+      world->errors(uint32_t(r->slot), &word, nullptr);
+      if (word & aemp::kErrNaN) r->status = AE_MPM_ENAN;
+      else if ((word & aemp::kErrDomain) && r->status == AE_MPM_OK) r->status = AE_MPM_EDOMAIN;
+      int rc = nw->assign_scene(uint32_t(r->slot), request_desc(r), nullptr, 0);
+      if (rc == AE_MPM_OK) rc = nw->copy_scene_from(uint32_t(r->slot), world, uint32_t(r->slot));
       if (rc) {
         fatal = nw->err;
         delete nw;
         return rc;
       }
     }
-    if (nw) cudaStreamSynchronize(nw->stream());
+    cudaStreamSynchronize(nw->stream());
     delete world;
     world = nw;
+    world_slots = n_slots;
+    ++worlds_built;
     return AE_MPM_OK;
+  }
+
+  void fail_all(int rc) {  // mu held; the world goes too (the next admission builds a new one)
+    for (Request* r : running) {
+      if (r->slot >= 0) slots[size_t(r->slot)].r = nullptr;
+      finish(r, rc);
+      delete r;
+    }
+    running.clear();
+    delete world;
+    world = nullptr;
+    world_slots = 0;
   }
 
   void loop() {
     cudaSetDevice(device);
-    alloc.reset(new CachingAlloc());
+    filler.young_modulus = 1.0e4f;
+    filler.poisson_ratio = 0.2f;
+    filler.density = 1.0f;
+    filler.model = AE_MPM_PHYS_JELLY;
     while (true) {
-      std::vector<Request*> done_now;
+      std::vector<Request*> admitted;
+      std::vector<int> vacate;
+      size_t n_slots = 0;
+      std::vector<Request*> resident;
       {
         std::unique_lock<std::mutex> lk(mu);
         // cancellations
         for (size_t i = 0; i < running.size();) {
           Request* r = running[i];
           if (r->cancelled) {
-            resident_bytes -= r->bytes;
+            if (r->on_device) vacate.push_back(r->slot);
+            slots[size_t(r->slot)].r = nullptr;
             finish(r, AE_MPM_EINVAL);
             delete r;
             running.erase(running.begin() + i);
-            rebuild = true;
           } else {
             ++i;
           }
@@ -220,54 +271,57 @@ struct ae_mpm_server {
             ++i;
           }
         }
-        // admission by HBM budget (FIFO: a request that does not fit blocks later ones)
-        while (!waiting.empty() && running.size() < opts.max_scenes &&
-               resident_bytes + waiting.front()->bytes <= opts.hbm_budget_bytes) {
+        // admission into free slots, growing the world within the HBM budget (first come, first
+        // served: a request that does not fit blocks later ones)
+        while (!waiting.empty() && running.size() < opts.max_scenes) {
           Request* r = waiting.front();
+          int s = find_slot(r);
+          if (s < 0 && grow_for(r)) s = find_slot(r);
+          if (s < 0) break;
           waiting.pop_front();
+          r->slot = s;
+          slots[size_t(s)].r = r;
           r->admit_s = now_s();
-          resident_bytes += r->bytes;
           running.push_back(r);
-          rebuild = true;
+          admitted.push_back(r);
         }
         if (running.empty()) {
           if (stop) break;
           cv.wait_for(lk, std::chrono::milliseconds(1));
-          continue;
+          if (vacate.empty()) continue;
         }
+        n_slots = slots.size();
+        resident = running;
       }
-      if (rebuild) {
-        int rc = rebuild_world(running);
-        rebuild = false;
-        if (rc) {  // the batch cannot run: fail every running request
-          std::lock_guard<std::mutex> lk(mu);
-          for (Request* r : running) {
-            resident_bytes -= r->bytes;
-            finish(r, rc);
-            delete r;
-          }
-          running.clear();
-          delete world;
-          world = nullptr;
-          continue;
+      int rc = AE_MPM_OK;
+      if (world)
+        for (int s : vacate)
+          if (size_t(s) < world_slots) world->vacate_scene(uint32_t(s));
+      if (resident.empty()) continue;
+      if (!world || n_slots != world_slots) rc = rebuild_world(n_slots, resident);
+      for (Request* r : admitted)
+        if (rc == AE_MPM_OK) {
+          rc = upload_new(r);
+          if (rc) fatal = world->err;
         }
+      if (rc) {  // the batch cannot run: fail every running request
+        std::lock_guard<std::mutex> lk(mu);
+        fail_all(rc);
+        continue;
       }
       uint32_t k = opts.substeps_per_tick;
-      for (Request* r : running) k = std::min(k, r->substeps - r->done);
-      int rc = world->step(k);
+      for (Request* r : resident) k = std::min(k, r->substeps - r->done);
+      rc = world->step(k);
       if (rc == AE_MPM_OK) rc = world->sync();
       if (rc == AE_MPM_ENAN || rc == AE_MPM_EDOMAIN) rc = AE_MPM_OK;  // attributed per scene below
       uint64_t parts = 0;
-      for (Request* r : running) {
+      for (Request* r : resident) {
         r->done += k;
         parts += r->n;
       }
-      std::vector<Request*> keep;
-      for (Request* r : running) {
-        if (r->done < r->substeps && rc == AE_MPM_OK) {
-          keep.push_back(r);
-          continue;
-        }
+      std::vector<Request*> done_now;
+      for (Request* r : resident) {
+        if (r->done < r->substeps && rc == AE_MPM_OK) continue;
         int st = rc;
         if (st == AE_MPM_OK) {
           uint32_t word = 0;
@@ -278,6 +332,7 @@ struct ae_mpm_server {
           int d = world->download(uint32_t(r->slot), &r->out, false);
           if (d) st = d;
         }
+        world->vacate_scene(uint32_t(r->slot));
         r->status = st;
         done_now.push_back(r);
       }
@@ -286,17 +341,15 @@ struct ae_mpm_server {
         ticks += 1;
         particle_substeps += parts * k;
         for (Request* r : done_now) {
-          resident_bytes -= r->bytes;
+          slots[size_t(r->slot)].r = nullptr;
+          running.erase(std::find(running.begin(), running.end(), r));
           finish(r, r->status);
           delete r;
         }
-        if (!done_now.empty()) rebuild = true;
-        running.swap(keep);
       }
     }
     delete world;
     world = nullptr;
-    alloc.reset();
   }
 };
 
@@ -317,9 +370,9 @@ int ae_mpm_server_create(ae_mpm_ctx* ctx, const ae_mpm_server_opts* opts, ae_mpm
   if (s->opts.max_scenes == 0) s->opts.max_scenes = 4096;
   if (s->opts.exec.precision != 64) s->opts.exec.precision = 32;
   if (s->opts.exec.p2g_variant == AE_MPM_P2G_AUTO) {
-    // options left to the library: batches are rebuilt whenever membership changes, so graphs
-    // (captured per world) would be re-captured every few ticks; sort every 4th substep as the
-    // autotuner usually picks for batched worlds
+    // options left to the library: slot particle counts change at every admission and completion,
+    // which changes the chunk table a captured graph replays, so substeps are launched eagerly;
+    // sort every 4th substep as the autotuner usually picks for batched worlds
     s->opts.exec.p2g_variant = AE_MPM_P2G_LANES;
     s->opts.exec.use_graph = 0;
     if (s->opts.exec.sort_interval <= 1) s->opts.exec.sort_interval = 4;
@@ -345,6 +398,11 @@ int ae_mpm_server_submit(ae_mpm_server* s, const ae_mpm_scene_desc* scene, const
                          uint32_t substeps, ae_mpm_particles* out, uint64_t* request_id) {
   if (!s || !scene || !in || !out) return AE_MPM_EINVAL;
   if (scene->n_materials == 0 || !scene->materials || substeps == 0 || n == 0) return AE_MPM_EINVAL;
+  // the slots' world steps physics-mode scenes (the reference-mode drop-in is a per-call path)
+  if (scene->mode != AE_MPM_MODE_PHYSICS || scene->wall_margin < 1 || !(scene->dx > 0.0f) || !(scene->dt >= 0.0f))
+    return AE_MPM_EINVAL;
+  for (int a = 0; a < 3; ++a)
+    if (scene->n[a] < 4 || scene->n[a] > 1024) return AE_MPM_EINVAL;
   if (!in->pos || !in->vel || !in->strain || !in->jacobian || !in->c || !in->mass || !in->material_idx) return AE_MPM_EINVAL;
   if (!out->pos || !out->vel || !out->strain || !out->jacobian || !out->c || !out->mass || !out->material_idx)
     return AE_MPM_EINVAL;
@@ -362,12 +420,18 @@ int ae_mpm_server_submit(ae_mpm_server* s, const ae_mpm_scene_desc* scene, const
   r->C.assign(in->c, in->c + 9 * n);
   r->mass.assign(in->mass, in->mass + n);
   r->mat.assign(in->material_idx, in->material_idx + n);
-  r->bytes = aemp::scene_device_bytes(r->desc, 32);
-  std::lock_guard<std::mutex> lk(s->mu);
-  if (r->bytes > s->opts.hbm_budget_bytes) {
-    delete r;
-    return AE_MPM_EBUDGET;
+  // the request's slot class must fit the budget on its own
+  {
+    const SlotClass c = class_of(r->desc, n);
+    ae_mpm_scene_desc cd = r->desc;
+    for (int a = 0; a < 3; ++a) cd.n[a] = c.n[a];
+    cd.max_particles = c.particles;
+    if (aemp::scene_device_bytes(cd, 32) > s->opts.hbm_budget_bytes) {
+      delete r;
+      return AE_MPM_EBUDGET;
+    }
   }
+  std::lock_guard<std::mutex> lk(s->mu);
   r->id = s->next_id++;
   r->submit_s = now_s();
   if (request_id) *request_id = r->id;
@@ -414,7 +478,7 @@ int ae_mpm_server_stats(ae_mpm_server* s, uint64_t* resident_bytes, uint32_t* re
                         uint64_t* particle_substeps) {
   if (!s) return AE_MPM_EINVAL;
   std::lock_guard<std::mutex> lk(s->mu);
-  if (resident_bytes) *resident_bytes = s->resident_bytes;
+  if (resident_bytes) *resident_bytes = s->slot_bytes;
   if (resident_scenes) *resident_scenes = uint32_t(s->running.size());
   if (ticks) *ticks = s->ticks;
   if (particle_substeps) *particle_substeps = s->particle_substeps;

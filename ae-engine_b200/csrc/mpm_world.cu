@@ -2467,6 +2467,58 @@ class World final : public WorldBase {
     return AE_MPM_OK;
   }
   uint32_t scene_count(uint32_t s) const override { return s < h_scenes_.size() ? h_scenes_[s].p_count : 0; }
+
+  int assign_scene(uint32_t s, const ae_mpm_scene_desc& d, const void* host, uint64_t n) override {
+    if (s >= h_scenes_.size()) {
+      err = "unknown scene";
+      return AE_MPM_ENOTFOUND;
+    }
+    SceneDev<T>& h = h_scenes_[s];
+    const uint32_t nmin = mode_ == AE_MPM_MODE_PHYSICS ? 4u : 1u;
+    if (d.mode != mode_ || d.n[0] < nmin || d.n[1] < nmin || d.n[2] < nmin || !(d.dx > 0.0f) || !(d.dt >= 0.0f) ||
+        (mode_ == AE_MPM_MODE_PHYSICS && d.wall_margin < 1) || d.n_materials == 0 || !d.materials) {
+      err = "slot scene needs the world's mode, >= " + std::to_string(nmin) +
+            " nodes per axis, dx > 0, dt >= 0, materials and (physics) wall_margin >= 1";
+      return AE_MPM_EINVAL;
+    }
+    if (blocks_of(d) > blocks_of(descs_[s]) || d.n_materials > descs_[s].n_materials || n > h.p_cap) {
+      err = "scene does not fit slot " + std::to_string(s) + " (grid blocks, materials or particles)";
+      return AE_MPM_EINVAL;
+    }
+    for (int a = 0; a < 3; ++a) {
+      h.n[a] = int(d.n[a]);
+      h.nb[a] = int((d.n[a] + 3) / 4);
+    }
+    h.mode = d.mode;
+    h.n_mat = d.n_materials;  // the out-of-range fallback entry follows the scene's materials
+    fill_scene_params(h, d);
+    for (uint32_t k = 0; k < d.n_materials; ++k) {
+      h_mats_[h.mat_off + k] = mat_dev(d.materials[k], d.materials[k].model);
+      if (d.materials[k].model == kPhysSnow && !has_snow_) {
+        has_snow_ = true;  // the substep gains the clamp kernel: recapture
+        invalidate_graph();
+      }
+    }
+    h_mats_[h.mat_off + d.n_materials] =
+        mat_dev(d.materials[0], mode_ == AE_MPM_MODE_PHYSICS ? d.materials[0].model : kNeoHookean);
+    scenes_dirty_ = mats_dirty_ = chunks_dirty_ = keys_stale_ = true;
+    AE_TRY(cudaMemsetAsync(err_ + 4 * s, 0, sizeof(uint32_t) * 4, stream_));
+    if (host) return upload(s, host, n, sizeof(T) == 8);
+    h.p_count = 0;
+    return AE_MPM_OK;
+  }
+
+  int vacate_scene(uint32_t s) override {
+    if (s >= h_scenes_.size()) {
+      err = "unknown scene";
+      return AE_MPM_ENOTFOUND;
+    }
+    // a scatter queued for the next substep may still hold the scene's contributions: they land in
+    // the slot's own blocks, which the next grid update consumes and no particle reads
+    h_scenes_[s].p_count = 0;
+    scenes_dirty_ = chunks_dirty_ = keys_stale_ = true;
+    return AE_MPM_OK;
+  }
   int precision() const override { return sizeof(T) == 8 ? 64 : 32; }
 
   int stage_times(uint32_t n, double out_us[5]) override {

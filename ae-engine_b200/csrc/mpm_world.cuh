@@ -114,6 +114,13 @@ struct WorldBase {
   // copy scene `src_scene` of `src` (same precision, same grid size) into scene `dst_scene`
   // of this world on the device; the source world's queued work must have finished
   virtual int copy_scene_from(uint32_t dst_scene, WorldBase* src, uint32_t src_scene) = 0;
+  // Continuous batching: scene slot `scene` takes a new scene `d` in place.  The slot keeps the
+  // grid blocks, material entries and particle capacity it was created with, so d's grid must
+  // need no more blocks, d no more materials and n no more particles.  `host` (a particle view as
+  // for upload, or null: particles follow by copy_scene_from) supplies the n particles.
+  virtual int assign_scene(uint32_t scene, const ae_mpm_scene_desc& d, const void* host, uint64_t n) = 0;
+  // The slot holds no particles (and costs the substep nothing but its empty chunks).
+  virtual int vacate_scene(uint32_t scene) = 0;
   virtual uint32_t scene_count(uint32_t scene) const = 0;
   virtual int precision() const = 0;
   virtual int stage_times(uint32_t n, double out_us[5]) = 0;

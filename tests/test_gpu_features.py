@@ -163,6 +163,61 @@ def test_server_results_equal_running_alone(ctx):
     assert stats["particle_substeps"] >= sum(p.n * k for (_, p), k in zip(reqs, substeps))
 
 
+def _served(srv, reqs, substeps):
+    ids = [srv.submit(sc, p, k) for (sc, p), k in zip(reqs, substeps)]
+    assert srv.drain(120.0) == M.OK
+    done = {}
+    for _ in range(100):
+        for rid, st, t0, ta, td, out in srv.poll(1024):
+            done[rid] = (st, out)
+        if len(done) == len(ids):
+            break
+        time.sleep(0.01)
+    assert len(done) == len(ids)
+    return [done[i] for i in ids]
+
+
+def test_server_reuses_slots_in_place_and_results_equal_running_alone(ctx):
+    # at most 3 resident scenes: later requests take the slots that finished ones vacate while the
+    # others keep running; slots are assigned by size class, so scenes of different grids and
+    # particle counts share them.  Deterministic mode: every result bitwise the scene run alone.
+    rng = S.Rng(0x5107)
+    reqs = [S.batched_scene(rng) for _ in range(8)]
+    substeps = [12, 30, 7, 18, 25, 9, 14, 21]
+    srv = M.Server(ctx, hbm_budget_bytes=4 << 30, substeps_per_tick=5, max_scenes=3,
+                   exec_options=M.exec_opts(deterministic=1))
+    res = _served(srv, reqs, substeps)
+    srv.close()
+    for (st, out), (sc, p), k in zip(res, reqs, substeps):
+        assert st == M.OK
+        w = world_of(ctx, [sc], [p], deterministic=1)
+        w.step(k)
+        alone = w.download(0, p.n)
+        w.close()
+        for f in ("pos", "vel", "F", "J", "C"):
+            assert np.array_equal(getattr(out, f), getattr(alone, f)), f
+
+
+def test_server_default_path_results_match_running_alone(ctx):
+    # the default options (fused G2P + P2G with float atomics, snow clamp kernel): a scene's result
+    # in the mix equals the scene run alone up to the order of the atomic sums: positions within
+    # 1e-5 of the largest |x|, F within 1e-4
+    rng = S.Rng(0x5108)
+    reqs = [S.batched_scene(rng) for _ in range(10)]
+    substeps = [15, 40, 8, 22, 31, 12, 17, 26, 9, 35]
+    srv = M.Server(ctx, hbm_budget_bytes=4 << 30, substeps_per_tick=6, max_scenes=4)
+    res = _served(srv, reqs, substeps)
+    srv.close()
+    for (st, out), (sc, p), k in zip(res, reqs, substeps):
+        assert st == M.OK
+        w = world_of(ctx, [sc], [p], p2g_variant=M.P2G_LANES, block_threads=256, sort_interval=4, use_graph=0)
+        w.step(k)
+        alone = w.download(0, p.n)
+        w.close()
+        assert rel(out.pos, alone.pos) <= 1e-5
+        assert rel(out.F, alone.F) <= 1e-4
+
+
 def test_server_budget_and_cancel(ctx):
     sc, p = S.batched_scene(S.Rng(7))
     srv = M.Server(ctx, hbm_budget_bytes=1 << 20, substeps_per_tick=5)
