@@ -52,7 +52,8 @@ struct Request {
   double submit_s = 0, admit_s = 0, done_s = 0;
   int status = AE_MPM_OK;
   bool cancelled = false, on_device = false;
-  int slot = -1;  // scene index of its slot in the world
+  int slot = -1;        // its slot in the server's slot table
+  int world_slot = -1;  // the scene index of that slot in the current world (once on the device)
 };
 
 // The size class a request's slot is made with: each grid axis rounded up to 16 nodes, the
@@ -103,7 +104,8 @@ struct ae_mpm_server {
   // slots (guarded by mu; the device thread alone changes them)
   std::vector<Slot> slots;
   uint64_t slot_bytes = 0;   // sum of the slots' estimated bytes: the world's footprint
-  size_t world_slots = 0;    // slots the current world was built with (the rest await a rebuild)
+  uint64_t layout = 0;       // bumped whenever the slot table grows or is compacted
+  uint64_t world_layout = ~0ull;  // the layout the current world was built with
   ae_mpm_material filler{};  // material of the slots' creation descriptors
   // device-thread state
   aemp::WorldBase* world = nullptr;
@@ -161,6 +163,25 @@ struct ae_mpm_server {
     if (k == 0) return false;
     for (uint64_t i = 0; i < k; ++i) slots.push_back(s);
     slot_bytes += k * s.bytes;
+    ++layout;
+    return true;
+  }
+
+  // drops the vacant slots (mu held): the budget they hold goes back to admission; the occupied
+  // ones are renumbered and move to the next world with it
+  bool compact() {
+    std::vector<Slot> kept;
+    uint64_t bytes = 0;
+    for (Slot& sl : slots)
+      if (sl.r) {
+        sl.r->slot = int(kept.size());
+        kept.push_back(sl);
+        bytes += sl.bytes;
+      }
+    if (kept.size() == slots.size()) return false;
+    slots.swap(kept);
+    slot_bytes = bytes;
+    ++layout;
     return true;
   }
 
@@ -176,6 +197,7 @@ struct ae_mpm_server {
     int rc = world->assign_scene(uint32_t(r->slot), request_desc(r), &v, r->n);
     if (rc == AE_MPM_OK) {
       r->on_device = true;
+      r->world_slot = r->slot;
       // the device copy is authoritative from here on
       std::vector<float>().swap(r->pos);
       std::vector<float>().swap(r->vel);
@@ -190,7 +212,7 @@ struct ae_mpm_server {
 
   // a world with every slot; resident scenes move over device to device (their particles never
   // return to the host mid-run)
-  int rebuild_world(size_t n_slots, const std::vector<Request*>& resident) {
+  int rebuild_world(size_t n_slots, uint64_t lay, const std::vector<Request*>& resident) {
     std::vector<ae_mpm_scene_desc> descs(n_slots);
     std::vector<std::vector<ae_mpm_material>> mats(n_slots);
     for (size_t i = 0; i < n_slots; ++i) descs[i] = slot_desc(slots[i], mats[i]);
@@ -205,11 +227,11 @@ struct ae_mpm_server {
     for (Request* r : resident) {
       if (!r->on_device || !world) continue;
       uint32_t word = 0;  // the old world's error word goes with the scene
-      world->errors(uint32_t(r->slot), &word, nullptr);
+      world->errors(uint32_t(r->world_slot), &word, nullptr);
       if (word & aemp::kErrNaN) r->status = AE_MPM_ENAN;
       else if ((word & aemp::kErrDomain) && r->status == AE_MPM_OK) r->status = AE_MPM_EDOMAIN;
       int rc = nw->assign_scene(uint32_t(r->slot), request_desc(r), nullptr, 0);
-      if (rc == AE_MPM_OK) rc = nw->copy_scene_from(uint32_t(r->slot), world, uint32_t(r->slot));
+      if (rc == AE_MPM_OK) rc = nw->copy_scene_from(uint32_t(r->slot), world, uint32_t(r->world_slot));
       if (rc) {
         fatal = nw->err;
         delete nw;
@@ -219,7 +241,8 @@ struct ae_mpm_server {
     cudaStreamSynchronize(nw->stream());
     delete world;
     world = nw;
-    world_slots = n_slots;
+    world_layout = lay;
+    for (Request* r : resident) r->world_slot = r->slot;
     ++worlds_built;
     return AE_MPM_OK;
   }
@@ -233,7 +256,7 @@ struct ae_mpm_server {
     running.clear();
     delete world;
     world = nullptr;
-    world_slots = 0;
+    world_layout = ~0ull;
   }
 
   void loop() {
@@ -246,6 +269,7 @@ struct ae_mpm_server {
       std::vector<Request*> admitted;
       std::vector<int> vacate;
       size_t n_slots = 0;
+      uint64_t lay = 0;
       std::vector<Request*> resident;
       {
         std::unique_lock<std::mutex> lk(mu);
@@ -253,7 +277,7 @@ struct ae_mpm_server {
         for (size_t i = 0; i < running.size();) {
           Request* r = running[i];
           if (r->cancelled) {
-            if (r->on_device) vacate.push_back(r->slot);
+            if (r->on_device) vacate.push_back(r->world_slot);
             slots[size_t(r->slot)].r = nullptr;
             finish(r, AE_MPM_EINVAL);
             delete r;
@@ -277,6 +301,7 @@ struct ae_mpm_server {
           Request* r = waiting.front();
           int s = find_slot(r);
           if (s < 0 && grow_for(r)) s = find_slot(r);
+          if (s < 0 && compact() && grow_for(r)) s = find_slot(r);
           if (s < 0) break;
           waiting.pop_front();
           r->slot = s;
@@ -291,14 +316,14 @@ struct ae_mpm_server {
           if (vacate.empty()) continue;
         }
         n_slots = slots.size();
+        lay = layout;
         resident = running;
       }
       int rc = AE_MPM_OK;
       if (world)
-        for (int s : vacate)
-          if (size_t(s) < world_slots) world->vacate_scene(uint32_t(s));
+        for (int s : vacate) world->vacate_scene(uint32_t(s));
       if (resident.empty()) continue;
-      if (!world || n_slots != world_slots) rc = rebuild_world(n_slots, resident);
+      if (!world || lay != world_layout) rc = rebuild_world(n_slots, lay, resident);
       for (Request* r : admitted)
         if (rc == AE_MPM_OK) {
           rc = upload_new(r);
@@ -325,14 +350,14 @@ struct ae_mpm_server {
         int st = rc;
         if (st == AE_MPM_OK) {
           uint32_t word = 0;
-          world->errors(uint32_t(r->slot), &word, nullptr);
+          world->errors(uint32_t(r->world_slot), &word, nullptr);
           st = r->status;
           if (word & aemp::kErrNaN) st = AE_MPM_ENAN;
           else if ((word & aemp::kErrDomain) && st == AE_MPM_OK) st = AE_MPM_EDOMAIN;
-          int d = world->download(uint32_t(r->slot), &r->out, false);
+          int d = world->download(uint32_t(r->world_slot), &r->out, false);
           if (d) st = d;
         }
-        world->vacate_scene(uint32_t(r->slot));
+        world->vacate_scene(uint32_t(r->world_slot));
         r->status = st;
         done_now.push_back(r);
       }
