@@ -39,19 +39,68 @@ double now_s() {
   return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
+// Page-locked host blocks, cached by power-of-two size class: request inputs are copied into one at
+// submit and outputs come back through one, so every host<->device copy is one asynchronous DMA.
+class PinnedPool {
+ public:
+  ~PinnedPool() {
+    for (auto& kv : free_)
+      for (void* p : kv.second) cudaFreeHost(p);
+  }
+  void* get(size_t bytes, size_t* cls_out) {
+    size_t cls = size_t(1) << 20;
+    while (cls < bytes) cls <<= 1;
+    *cls_out = cls;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      auto& v = free_[cls];
+      if (!v.empty()) {
+        void* p = v.back();
+        v.pop_back();
+        return p;
+      }
+    }
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, cls, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return p;
+  }
+  void put(void* p, size_t cls) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(mu_);
+    free_[cls].push_back(p);
+  }
+
+ private:
+  std::mutex mu_;
+  std::map<size_t, std::vector<void*>> free_;
+};
+
+// A particle block in the world's upload staging layout (pos 3n | vel 3n | F 9n | J n | C 9n |
+// mass n floats, then n u16 material indices), so it crosses PCIe in one copy.
+ae_mpm_particles staging_view(void* base, uint64_t n) {
+  float* f = static_cast<float*>(base);
+  return ae_mpm_particles{f, f + 3 * n, f + 6 * n, f + 15 * n, f + 16 * n, f + 25 * n,
+                          reinterpret_cast<uint16_t*>(f + 26 * n)};
+}
+size_t staging_bytes(uint64_t n) { return (26 * sizeof(float) + sizeof(uint16_t)) * n; }
+
 struct Request {
   uint64_t id = 0;
   ae_mpm_scene_desc desc{};
   std::vector<ae_mpm_material> mats;
-  // host copy of the input particles (reference layout), kept until the scene is on the device
-  std::vector<float> pos, vel, F, J, C, mass;
-  std::vector<uint16_t> mat;
+  // pinned host block with the input particles (staging layout) until they are on the device,
+  // then with the results on their way to the caller's buffers
+  void* host = nullptr;
+  size_t host_cls = 0;
   uint64_t n = 0;
   uint32_t substeps = 0, done = 0;
   ae_mpm_particles out{};
   double submit_s = 0, admit_s = 0, done_s = 0;
   int status = AE_MPM_OK;
-  bool cancelled = false, on_device = false;
+  bool cancelled = false, on_device = false, uploaded = false;
   int slot = -1;        // its slot in the server's slot table
   int world_slot = -1;  // the scene index of that slot in the current world (once on the device)
 };
@@ -110,6 +159,8 @@ struct ae_mpm_server {
   // device-thread state
   aemp::WorldBase* world = nullptr;
   uint64_t worlds_built = 0;
+  std::shared_ptr<PinnedPool> pool = std::make_shared<PinnedPool>();
+  std::vector<Request*> outgoing;  // results in pinned blocks, copied to callers while the next tick runs
 
   ae_mpm_scene_desc slot_desc(const Slot& s, std::vector<ae_mpm_material>& mats) const {
     ae_mpm_scene_desc d{};
@@ -192,22 +243,43 @@ struct ae_mpm_server {
     return d;
   }
 
+  // queues the request's particles (one DMA from its pinned block) into its slot; the block goes
+  // back to the pool once the tick's work has finished
   int upload_new(Request* r) {
-    ae_mpm_particles v{r->pos.data(), r->vel.data(), r->F.data(), r->J.data(), r->C.data(), r->mass.data(), r->mat.data()};
+    ae_mpm_particles v = staging_view(r->host, r->n);
     int rc = world->assign_scene(uint32_t(r->slot), request_desc(r), &v, r->n);
     if (rc == AE_MPM_OK) {
       r->on_device = true;
+      r->uploaded = true;
       r->world_slot = r->slot;
-      // the device copy is authoritative from here on
-      std::vector<float>().swap(r->pos);
-      std::vector<float>().swap(r->vel);
-      std::vector<float>().swap(r->F);
-      std::vector<float>().swap(r->J);
-      std::vector<float>().swap(r->C);
-      std::vector<float>().swap(r->mass);
-      std::vector<uint16_t>().swap(r->mat);
     }
     return rc;
+  }
+
+  // results of finished scenes: from their pinned blocks into the callers' buffers, then reported
+  // (runs while the device works on the next tick)
+  void deliver() {
+    for (Request* r : outgoing) {
+      if (r->host && r->status == AE_MPM_OK) {
+        const ae_mpm_particles v = staging_view(r->host, r->n);
+        const uint64_t n = r->n;
+        std::memcpy(r->out.pos, v.pos, sizeof(float) * 3 * n);
+        std::memcpy(r->out.vel, v.vel, sizeof(float) * 3 * n);
+        std::memcpy(r->out.strain, v.strain, sizeof(float) * 9 * n);
+        std::memcpy(r->out.jacobian, v.jacobian, sizeof(float) * n);
+        std::memcpy(r->out.c, v.c, sizeof(float) * 9 * n);
+        std::memcpy(r->out.mass, v.mass, sizeof(float) * n);
+        std::memcpy(r->out.material_idx, v.material_idx, sizeof(uint16_t) * n);
+      }
+      pool->put(r->host, r->host_cls);
+      r->host = nullptr;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    for (Request* r : outgoing) {
+      finish(r, r->status);
+      delete r;
+    }
+    outgoing.clear();
   }
 
   // a world with every slot; resident scenes move over device to device (their particles never
@@ -250,6 +322,7 @@ struct ae_mpm_server {
   void fail_all(int rc) {  // mu held; the world goes too (the next admission builds a new one)
     for (Request* r : running) {
       if (r->slot >= 0) slots[size_t(r->slot)].r = nullptr;
+      pool->put(r->host, r->host_cls);
       finish(r, rc);
       delete r;
     }
@@ -279,6 +352,7 @@ struct ae_mpm_server {
           if (r->cancelled) {
             if (r->on_device) vacate.push_back(r->world_slot);
             slots[size_t(r->slot)].r = nullptr;
+            pool->put(r->host, r->host_cls);
             finish(r, AE_MPM_EINVAL);
             delete r;
             running.erase(running.begin() + i);
@@ -288,6 +362,7 @@ struct ae_mpm_server {
         }
         for (size_t i = 0; i < waiting.size();) {
           if (waiting[i]->cancelled) {
+            pool->put(waiting[i]->host, waiting[i]->host_cls);
             finish(waiting[i], AE_MPM_EINVAL);
             delete waiting[i];
             waiting.erase(waiting.begin() + i);
@@ -310,7 +385,7 @@ struct ae_mpm_server {
           running.push_back(r);
           admitted.push_back(r);
         }
-        if (running.empty()) {
+        if (running.empty() && outgoing.empty()) {
           if (stop) break;
           cv.wait_for(lk, std::chrono::milliseconds(1));
           if (vacate.empty()) continue;
@@ -322,7 +397,10 @@ struct ae_mpm_server {
       int rc = AE_MPM_OK;
       if (world)
         for (int s : vacate) world->vacate_scene(uint32_t(s));
-      if (resident.empty()) continue;
+      if (resident.empty()) {
+        deliver();
+        continue;
+      }
       if (!world || lay != world_layout) rc = rebuild_world(n_slots, lay, resident);
       for (Request* r : admitted)
         if (rc == AE_MPM_OK) {
@@ -330,15 +408,23 @@ struct ae_mpm_server {
           if (rc) fatal = world->err;
         }
       if (rc) {  // the batch cannot run: fail every running request
+        deliver();
         std::lock_guard<std::mutex> lk(mu);
         fail_all(rc);
         continue;
       }
       uint32_t k = opts.substeps_per_tick;
       for (Request* r : resident) k = std::min(k, r->substeps - r->done);
-      rc = world->step(k);
+      rc = world->step(k);  // queued: the host copies below overlap the device work
+      deliver();
       if (rc == AE_MPM_OK) rc = world->sync();
       if (rc == AE_MPM_ENAN || rc == AE_MPM_EDOMAIN) rc = AE_MPM_OK;  // attributed per scene below
+      // the uploads of this tick are complete: their input blocks can be reused
+      for (Request* r : admitted)
+        if (r->uploaded && r->host) {
+          pool->put(r->host, r->host_cls);
+          r->host = nullptr;
+        }
       uint64_t parts = 0;
       for (Request* r : resident) {
         r->done += k;
@@ -354,8 +440,15 @@ struct ae_mpm_server {
           st = r->status;
           if (word & aemp::kErrNaN) st = AE_MPM_ENAN;
           else if ((word & aemp::kErrDomain) && st == AE_MPM_OK) st = AE_MPM_EDOMAIN;
-          int d = world->download(uint32_t(r->world_slot), &r->out, false);
-          if (d) st = d;
+          // results into a pinned block (one DMA); the caller's buffers get them next tick
+          r->host = pool->get(staging_bytes(r->n), &r->host_cls);
+          if (!r->host) {
+            st = AE_MPM_ENOMEM;
+          } else {
+            ae_mpm_particles v = staging_view(r->host, r->n);
+            int d = world->download(uint32_t(r->world_slot), &v, false);
+            if (d) st = d;
+          }
         }
         world->vacate_scene(uint32_t(r->world_slot));
         r->status = st;
@@ -368,11 +461,11 @@ struct ae_mpm_server {
         for (Request* r : done_now) {
           slots[size_t(r->slot)].r = nullptr;
           running.erase(std::find(running.begin(), running.end(), r));
-          finish(r, r->status);
-          delete r;
+          outgoing.push_back(r);
         }
       }
     }
+    deliver();
     delete world;
     world = nullptr;
   }
@@ -438,13 +531,6 @@ int ae_mpm_server_submit(ae_mpm_server* s, const ae_mpm_scene_desc* scene, const
   r->n = n;
   r->substeps = substeps;
   r->out = *out;
-  r->pos.assign(in->pos, in->pos + 3 * n);
-  r->vel.assign(in->vel, in->vel + 3 * n);
-  r->F.assign(in->strain, in->strain + 9 * n);
-  r->J.assign(in->jacobian, in->jacobian + n);
-  r->C.assign(in->c, in->c + 9 * n);
-  r->mass.assign(in->mass, in->mass + n);
-  r->mat.assign(in->material_idx, in->material_idx + n);
   // the request's slot class must fit the budget on its own
   {
     const SlotClass c = class_of(r->desc, n);
@@ -455,6 +541,28 @@ int ae_mpm_server_submit(ae_mpm_server* s, const ae_mpm_scene_desc* scene, const
       delete r;
       return AE_MPM_EBUDGET;
     }
+  }
+  // the particles are copied now, into a pinned block in the upload staging layout
+  {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(s->device);
+    r->host = s->pool->get(staging_bytes(n), &r->host_cls);
+    cudaSetDevice(prev);
+  }
+  if (!r->host) {
+    delete r;
+    return AE_MPM_ENOMEM;
+  }
+  {
+    const ae_mpm_particles v = staging_view(r->host, n);
+    std::memcpy(v.pos, in->pos, sizeof(float) * 3 * n);
+    std::memcpy(v.vel, in->vel, sizeof(float) * 3 * n);
+    std::memcpy(v.strain, in->strain, sizeof(float) * 9 * n);
+    std::memcpy(v.jacobian, in->jacobian, sizeof(float) * n);
+    std::memcpy(v.c, in->c, sizeof(float) * 9 * n);
+    std::memcpy(v.mass, in->mass, sizeof(float) * n);
+    std::memcpy(v.material_idx, in->material_idx, sizeof(uint16_t) * n);
   }
   std::lock_guard<std::mutex> lk(s->mu);
   r->id = s->next_id++;
@@ -520,8 +628,14 @@ int ae_mpm_server_destroy(ae_mpm_server* s) {
     s->cv.notify_all();
   }
   if (s->thr.joinable()) s->thr.join();
-  for (Request* r : s->waiting) delete r;
-  for (Request* r : s->running) delete r;
+  for (Request* r : s->waiting) {
+    s->pool->put(r->host, r->host_cls);
+    delete r;
+  }
+  for (Request* r : s->running) {
+    s->pool->put(r->host, r->host_cls);
+    delete r;
+  }
   delete s;
   return AE_MPM_OK;
 }

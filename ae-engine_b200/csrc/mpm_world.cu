@@ -2503,8 +2503,31 @@ class World final : public WorldBase {
         mat_dev(d.materials[0], mode_ == AE_MPM_MODE_PHYSICS ? d.materials[0].model : kNeoHookean);
     scenes_dirty_ = mats_dirty_ = chunks_dirty_ = keys_stale_ = true;
     AE_TRY(cudaMemsetAsync(err_ + 4 * s, 0, sizeof(uint32_t) * 4, stream_));
-    if (host) return upload(s, host, n, sizeof(T) == 8);
-    h.p_count = 0;
+    if (!host) {
+      h.p_count = 0;
+      return AE_MPM_OK;
+    }
+    // with the P2G of the next substep already queued for the other scenes (fused flow), add
+    // only this scene's scatter instead of redoing everyone's
+    const bool keep_queued = scatter_pending_ && !scatter_invalid_ && fused();
+    int rc = upload(s, host, n, sizeof(T) == 8);
+    if (rc || !keep_queued) return rc;
+    scatter_invalid_ = false;
+    // the slot's blocks may hold the last scatter of the scene that vacated it: zero them (their
+    // flags stay set, so the touched list keeps each block once) and scatter the new particles
+    AE_TRY(cudaMemsetAsync(acc_ + uint64_t(h.blk_off) * 64u, 0, sizeof(V4) * 64 * blocks_of(descs_[s]), stream_));
+    if ((rc = prepare())) return rc;
+    if (n == 0) return AE_MPM_OK;
+    WorldDev<T> w = with_list(dev(false), int(substep_ & 1));
+    const int c0 = chunk_first_[s], c1 = chunk_first_[s + 1];
+    if (!w.one_scene) w.chunks = d_chunks_ + c0;
+    const size_t per = sizeof(V4) * kLaneVecs + sizeof(int4);
+    if (!lanes_smem_set_) {
+      AE_TRY(cudaFuncSetAttribute(p2g_lanes_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(per * 256)));
+      lanes_smem_set_ = true;
+    }
+    p2g_lanes_kernel<T><<<unsigned(c1 - c0), chunk_threads_, per * chunk_threads_, stream_>>>(w);
+    AE_TRY(cudaGetLastError());
     return AE_MPM_OK;
   }
 
@@ -2611,7 +2634,9 @@ class World final : public WorldBase {
     if (chunks_dirty_) {
       chunk_threads_ = opts_.block_threads;
       h_chunks_.clear();
+      chunk_first_.assign(h_scenes_.size() + 1, 0);
       for (size_t s = 0; s < h_scenes_.size(); ++s) {
+        chunk_first_[s] = int(h_chunks_.size());
         const SceneDev<T>& h = h_scenes_[s];
         for (uint64_t lo = h.p_off; lo < uint64_t(h.p_off) + h.p_cap; lo += chunk_threads_) {
           uint64_t hl = std::min<uint64_t>(lo + chunk_threads_, uint64_t(h.p_off) + h.p_count);
@@ -2620,6 +2645,7 @@ class World final : public WorldBase {
         }
       }
       n_chunks_ = int(h_chunks_.size());
+      chunk_first_[h_scenes_.size()] = n_chunks_;
       if (n_chunks_ > n_chunks_alloc_) {
         dfree(d_chunks_);
         d_chunks_ = nullptr;
@@ -2928,6 +2954,7 @@ class World final : public WorldBase {
   std::vector<SceneDev<T>> h_scenes_;
   std::vector<MatDev> h_mats_;
   std::vector<int4> h_chunks_;
+  std::vector<int> chunk_first_;  // first chunk of each scene (and the chunk count at the end)
   SceneDev<T>* d_scenes_ = nullptr;
   MatDev* d_mats_ = nullptr;
   int4* d_chunks_ = nullptr;

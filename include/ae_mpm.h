@@ -441,13 +441,19 @@ typedef struct ae_mpm_tune_result {
 int ae_mpm_world_autotune(ae_mpm_world* world, uint32_t substeps_per_trial, ae_mpm_tune_result* out);
 
 /* ---------------------------------------------------------------------------------------------
- * Continuous-batching server.  Requests (a scene plus its particles and a substep count) are
- * admitted while their device state fits the HBM budget, kept resident, and stepped together
- * with every other admitted scene; a finished scene is copied back and its memory freed, which
- * lets waiting requests in.  One host thread per server drives the device.
+ * Continuous-batching server.  Requests (a physics-mode scene plus its particles and a substep
+ * count) run in one resident world of scene *slots*, each made with a grid, material and particle
+ * capacity (the request's size class: axes rounded up to 16 nodes, particles and materials to
+ * powers of two).  A request is admitted, first come first served, into a free slot that fits it;
+ * when none does, the world grows by slots of its class (doubling per class) as long as the
+ * slots' device state fits the HBM budget, dropping vacant slots first if needed.  Admitted
+ * scenes are uploaded into their slots in place and stepped together with every other resident
+ * scene; a finished scene is copied back and vacates its slot for the next request.  Inputs and
+ * results travel through page-locked staging, and results reach the callers' buffers while the
+ * device runs the next batch of substeps.  One host thread per server drives the device.
  * ------------------------------------------------------------------------------------------- */
 typedef struct ae_mpm_server_opts {
-  uint64_t hbm_budget_bytes;   /* admission budget for resident scene state                 */
+  uint64_t hbm_budget_bytes;   /* budget for the slots' device state                         */
   uint32_t substeps_per_tick;  /* substeps run between admission checks (default 10)         */
   uint32_t max_scenes;         /* cap on resident scenes (default 4096)                      */
   ae_mpm_exec_opts exec;
@@ -463,8 +469,9 @@ typedef struct ae_mpm_request_result {
 
 int ae_mpm_server_create(ae_mpm_ctx* ctx, const ae_mpm_server_opts* opts, ae_mpm_server** out);
 /* Submit: the particles are copied at submit time; results are written into `out` (which must
- * stay valid until the request's result has been polled).  Requests larger than the budget are
- * refused with AE_MPM_EBUDGET. */
+ * stay valid until the request's result has been polled).  A request whose slot class alone
+ * exceeds the budget is refused with AE_MPM_EBUDGET; one that is not physics mode, or whose grid
+ * is outside 4..1024 nodes per axis, with AE_MPM_EINVAL. */
 int ae_mpm_server_submit(ae_mpm_server* server, const ae_mpm_scene_desc* scene,
                          const ae_mpm_particles* in, uint64_t n, uint32_t substeps,
                          ae_mpm_particles* out, uint64_t* request_id);
@@ -476,7 +483,7 @@ int ae_mpm_server_poll(ae_mpm_server* server, ae_mpm_request_result* results, ui
                        uint32_t* n_out);
 /* Wait until every submitted request has finished, at most timeout_s seconds. */
 int ae_mpm_server_drain(ae_mpm_server* server, double timeout_s);
-/* Resident bytes and scenes right now; total substeps run (batched ticks). */
+/* Device bytes of the slots and scenes resident right now; ticks run; particle-substeps run. */
 int ae_mpm_server_stats(ae_mpm_server* server, uint64_t* resident_bytes, uint32_t* resident_scenes,
                         uint64_t* ticks, uint64_t* particle_substeps);
 int ae_mpm_server_destroy(ae_mpm_server* server);
