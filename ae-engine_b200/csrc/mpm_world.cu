@@ -2164,8 +2164,8 @@ class World final : public WorldBase {
     }
     h_mats_[h_scenes_[s].mat_off + d.n_materials] =
         mat_dev(d.materials[0], mode_ == AE_MPM_MODE_PHYSICS ? d.materials[0].model : kNeoHookean);
-    scenes_dirty_ = true;
-    mats_dirty_ = true;
+    dirty_scene(s);
+    dirty_mats(s);
     keys_stale_ = true;  // dx or origin may have moved the cells
     scatter_invalid_ = true;
     if (rebase) {
@@ -2236,7 +2236,7 @@ class World final : public WorldBase {
     // the upload's buffers); the cell keys are recomputed before the next substep either way
     if (h_scenes_[s].p_count != uint32_t(n)) {
       h_scenes_[s].p_count = uint32_t(n);
-      scenes_dirty_ = chunks_dirty_ = true;
+      count_changed(s);
     }
     keys_stale_ = true;
     return AE_MPM_OK;
@@ -2463,7 +2463,8 @@ class World final : public WorldBase {
         AE_TRY(cudaMemcpyAsync(in_buf()[k] + b.p_off, src->in_buf()[k] + a.p_off, sizeof(V4) * a.p_count,
                                cudaMemcpyDeviceToDevice, stream_));
     b.p_count = a.p_count;
-    scenes_dirty_ = chunks_dirty_ = keys_stale_ = scatter_invalid_ = true;
+    count_changed(dst);
+    keys_stale_ = scatter_invalid_ = true;
     return AE_MPM_OK;
   }
   uint32_t scene_count(uint32_t s) const override { return s < h_scenes_.size() ? h_scenes_[s].p_count : 0; }
@@ -2501,10 +2502,13 @@ class World final : public WorldBase {
     }
     h_mats_[h.mat_off + d.n_materials] =
         mat_dev(d.materials[0], mode_ == AE_MPM_MODE_PHYSICS ? d.materials[0].model : kNeoHookean);
-    scenes_dirty_ = mats_dirty_ = chunks_dirty_ = keys_stale_ = true;
+    dirty_scene(s);
+    dirty_mats(s);
+    keys_stale_ = true;
     AE_TRY(cudaMemsetAsync(err_ + 4 * s, 0, sizeof(uint32_t) * 4, stream_));
     if (!host) {
       h.p_count = 0;
+      count_changed(s);
       return AE_MPM_OK;
     }
     // with the P2G of the next substep already queued for the other scenes (fused flow), add
@@ -2539,7 +2543,8 @@ class World final : public WorldBase {
     // a scatter queued for the next substep may still hold the scene's contributions: they land in
     // the slot's own blocks, which the next grid update consumes and no particle reads
     h_scenes_[s].p_count = 0;
-    scenes_dirty_ = chunks_dirty_ = keys_stale_ = true;
+    count_changed(s);
+    keys_stale_ = true;
     return AE_MPM_OK;
   }
   int precision() const override { return sizeof(T) == 8 ? 64 : 32; }
@@ -2646,6 +2651,8 @@ class World final : public WorldBase {
       }
       n_chunks_ = int(h_chunks_.size());
       chunk_first_[h_scenes_.size()] = n_chunks_;
+      count_dirty_.assign(h_scenes_.size(), 0);
+      any_count_dirty_ = false;
       if (n_chunks_ > n_chunks_alloc_) {
         dfree(d_chunks_);
         d_chunks_ = nullptr;
@@ -2661,6 +2668,28 @@ class World final : public WorldBase {
         graph_ = nullptr;
       }
       chunks_dirty_ = false;
+    } else if (any_count_dirty_) {
+      // particle counts changed, the chunk layout (by capacity) did not: rewrite those scenes'
+      // slices of the chunk table only
+      for (size_t s = 0; s < h_scenes_.size(); ++s) {
+        if (!count_dirty_[s]) continue;
+        const SceneDev<T>& h = h_scenes_[s];
+        const int c0 = chunk_first_[s], c1 = chunk_first_[s + 1];
+        for (int c = c0; c < c1; ++c) {
+          const uint64_t lo = uint64_t(h_chunks_[c].y);
+          const uint64_t hl = std::min<uint64_t>(lo + chunk_threads_, uint64_t(h.p_off) + h.p_count);
+          h_chunks_[c].z = int(std::max(hl, lo));
+        }
+        if (c1 > c0)
+          AE_TRY(cudaMemcpyAsync(d_chunks_ + c0, h_chunks_.data() + c0, sizeof(int4) * (c1 - c0), cudaMemcpyHostToDevice,
+                                 stream_));
+        count_dirty_[s] = 0;
+      }
+      any_count_dirty_ = false;
+      if (graph_) {  // a one-scene world's graph carries the count in its launch parameters
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+      }
     }
     int rc = sync_tables();
     if (rc) return rc;
@@ -2671,13 +2700,22 @@ class World final : public WorldBase {
   // scene and material tables to the device (copied from pageable memory, staged at the call)
   int sync_tables() {
     if (scenes_dirty_) {
-      AE_TRY(cudaMemcpyAsync(d_scenes_, h_scenes_.data(), sizeof(SceneDev<T>) * h_scenes_.size(), cudaMemcpyHostToDevice,
-                             stream_));
+      const size_t lo = std::min(scene_lo_, h_scenes_.size()), hi = std::min(scene_hi_, h_scenes_.size());
+      if (hi > lo)
+        AE_TRY(cudaMemcpyAsync(d_scenes_ + lo, h_scenes_.data() + lo, sizeof(SceneDev<T>) * (hi - lo),
+                               cudaMemcpyHostToDevice, stream_));
       scenes_dirty_ = false;
+      scene_lo_ = SIZE_MAX;
+      scene_hi_ = 0;
     }
     if (mats_dirty_) {
-      AE_TRY(cudaMemcpyAsync(d_mats_, h_mats_.data(), sizeof(MatDev) * h_mats_.size(), cudaMemcpyHostToDevice, stream_));
+      const size_t lo = std::min(mat_lo_, h_mats_.size()), hi = std::min(mat_hi_, h_mats_.size());
+      if (hi > lo)
+        AE_TRY(cudaMemcpyAsync(d_mats_ + lo, h_mats_.data() + lo, sizeof(MatDev) * (hi - lo), cudaMemcpyHostToDevice,
+                               stream_));
       mats_dirty_ = false;
+      mat_lo_ = SIZE_MAX;
+      mat_hi_ = 0;
     }
     return AE_MPM_OK;
   }
@@ -2781,6 +2819,29 @@ class World final : public WorldBase {
 
   void mark(int k) {
     if (stage_events_) cudaEventRecord(stage_events_[k], stream_);
+  }
+
+  // ranges of the scene and material tables to copy to the device before the next launch
+  void dirty_scene(size_t s) {
+    scene_lo_ = std::min(scene_lo_, s);
+    scene_hi_ = std::max(scene_hi_, s + 1);
+    scenes_dirty_ = true;
+  }
+  void dirty_mats(size_t s) {
+    const size_t lo = h_scenes_[s].mat_off, hi = lo + descs_[s].n_materials + 1;
+    mat_lo_ = std::min(mat_lo_, lo);
+    mat_hi_ = std::max(mat_hi_, hi);
+    mats_dirty_ = true;
+  }
+
+  void count_changed(uint32_t s) {
+    dirty_scene(s);
+    if (count_dirty_.size() != h_scenes_.size()) {
+      chunks_dirty_ = true;  // no table yet: the next prepare() builds it whole
+      return;
+    }
+    count_dirty_[s] = 1;
+    any_count_dirty_ = true;
   }
 
   // ---- fused G2P + P2G (physics mode, column-lane P2G, not deterministic) ----
@@ -2955,6 +3016,8 @@ class World final : public WorldBase {
   std::vector<MatDev> h_mats_;
   std::vector<int4> h_chunks_;
   std::vector<int> chunk_first_;  // first chunk of each scene (and the chunk count at the end)
+  std::vector<uint8_t> count_dirty_;  // scenes whose particle count changed since the table was written
+  bool any_count_dirty_ = false;
   SceneDev<T>* d_scenes_ = nullptr;
   MatDev* d_mats_ = nullptr;
   int4* d_chunks_ = nullptr;
@@ -2993,6 +3056,8 @@ class World final : public WorldBase {
   uint64_t total_cap_ = 0, total_blocks_ = 0, device_bytes_ = 0;
   int key_bits_ = 1;
   bool keys_stale_ = true, chunks_dirty_ = true, scenes_dirty_ = true, mats_dirty_ = false;
+  size_t scene_lo_ = 0, scene_hi_ = SIZE_MAX;  // dirty range of the scene table (all of it at first)
+  size_t mat_lo_ = SIZE_MAX, mat_hi_ = 0;       // dirty range of the material table
   bool keys_fresh_ = false;  // keys_ hold the cell keys of the current positions
 };
 
