@@ -557,8 +557,11 @@ class Server:
         self.h = h
         self._pending = {}
 
-    def submit(self, scene: Scene, p: Particles, substeps: int) -> int:
-        out = Particles.empty(p.n)
+    def submit(self, scene: Scene, p: Particles, substeps: int, out: Particles | None = None) -> int:
+        """Queues `substeps` substeps of `scene` starting from `p`; the results arrive in `out`
+        (allocated here when not given) and are returned by poll()."""
+        if out is None:
+            out = Particles(*(np.empty_like(a) for a in (p.pos, p.vel, p.F, p.J, p.C, p.mass, p.mat)))
         vin, vout = p.view(), out.view()
         d = scene.desc()
         rid = C.c_uint64()

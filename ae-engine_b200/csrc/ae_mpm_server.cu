@@ -18,6 +18,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdio>
+#include <cstdlib>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -41,11 +43,14 @@ double now_s() {
 
 // Page-locked host blocks, cached by power-of-two size class: request inputs are copied into one at
 // submit and outputs come back through one, so every host<->device copy is one asynchronous DMA.
+// Pinning memory is slow (the driver locks every page), so one pool serves every server of the
+// process and keeps up to kPinnedCacheBytes of free blocks for the next requests.
 class PinnedPool {
  public:
-  ~PinnedPool() {
-    for (auto& kv : free_)
-      for (void* p : kv.second) cudaFreeHost(p);
+  static constexpr size_t kPinnedCacheBytes = size_t(8) << 30;
+  static PinnedPool& process() {
+    static PinnedPool* p = new PinnedPool();  // lives until exit: servers may outlive each other
+    return *p;
   }
   void* get(size_t bytes, size_t* cls_out) {
     size_t cls = size_t(1) << 20;
@@ -57,6 +62,7 @@ class PinnedPool {
       if (!v.empty()) {
         void* p = v.back();
         v.pop_back();
+        cached_ -= cls;
         return p;
       }
     }
@@ -69,13 +75,21 @@ class PinnedPool {
   }
   void put(void* p, size_t cls) {
     if (!p) return;
-    std::lock_guard<std::mutex> lk(mu_);
-    free_[cls].push_back(p);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      if (cached_ + cls <= kPinnedCacheBytes) {
+        free_[cls].push_back(p);
+        cached_ += cls;
+        return;
+      }
+    }
+    cudaFreeHost(p);
   }
 
  private:
   std::mutex mu_;
   std::map<size_t, std::vector<void*>> free_;
+  size_t cached_ = 0;
 };
 
 // A particle block in the world's upload staging layout (pos 3n | vel 3n | F 9n | J n | C 9n |
@@ -159,7 +173,11 @@ struct ae_mpm_server {
   // device-thread state
   aemp::WorldBase* world = nullptr;
   uint64_t worlds_built = 0;
-  std::shared_ptr<PinnedPool> pool = std::make_shared<PinnedPool>();
+  PinnedPool* pool = &PinnedPool::process();
+  // host seconds of the device thread per phase, printed at destroy when AE_MPM_SERVER_PROFILE is
+  // set: [admission, world rebuilds, uploads, queueing substeps, deliveries, waiting for the
+  // device, finishing scenes (error words, downloads)]
+  double phase_s[7] = {0, 0, 0, 0, 0, 0, 0};
   std::vector<Request*> outgoing;  // results in pinned blocks, copied to callers while the next tick runs
 
   ae_mpm_scene_desc slot_desc(const Slot& s, std::vector<ae_mpm_material>& mats) const {
@@ -344,6 +362,12 @@ struct ae_mpm_server {
       size_t n_slots = 0;
       uint64_t lay = 0;
       std::vector<Request*> resident;
+      double t = now_s();
+      auto lap = [&](int ph) {
+        const double u = now_s();
+        phase_s[ph] += u - t;
+        t = u;
+      };
       {
         std::unique_lock<std::mutex> lk(mu);
         // cancellations
@@ -401,12 +425,15 @@ struct ae_mpm_server {
         deliver();
         continue;
       }
+      lap(0);
       if (!world || lay != world_layout) rc = rebuild_world(n_slots, lay, resident);
+      lap(1);
       for (Request* r : admitted)
         if (rc == AE_MPM_OK) {
           rc = upload_new(r);
           if (rc) fatal = world->err;
         }
+      lap(2);
       if (rc) {  // the batch cannot run: fail every running request
         deliver();
         std::lock_guard<std::mutex> lk(mu);
@@ -416,8 +443,11 @@ struct ae_mpm_server {
       uint32_t k = opts.substeps_per_tick;
       for (Request* r : resident) k = std::min(k, r->substeps - r->done);
       rc = world->step(k);  // queued: the host copies below overlap the device work
+      lap(3);
       deliver();
+      lap(4);
       if (rc == AE_MPM_OK) rc = world->sync();
+      lap(5);
       if (rc == AE_MPM_ENAN || rc == AE_MPM_EDOMAIN) rc = AE_MPM_OK;  // attributed per scene below
       // the uploads of this tick are complete: their input blocks can be reused
       for (Request* r : admitted)
@@ -454,6 +484,7 @@ struct ae_mpm_server {
         r->status = st;
         done_now.push_back(r);
       }
+      lap(6);
       {
         std::lock_guard<std::mutex> lk(mu);
         ticks += 1;
@@ -468,6 +499,12 @@ struct ae_mpm_server {
     deliver();
     delete world;
     world = nullptr;
+    if (std::getenv("AE_MPM_SERVER_PROFILE"))
+      std::fprintf(stderr,
+                   "ae_mpm_server: %llu ticks, %llu worlds built; seconds: admission %.3f rebuild %.3f upload %.3f "
+                   "queue %.3f deliver %.3f device-wait %.3f finish %.3f\n",
+                   (unsigned long long)ticks, (unsigned long long)worlds_built, phase_s[0], phase_s[1], phase_s[2],
+                   phase_s[3], phase_s[4], phase_s[5], phase_s[6]);
   }
 };
 

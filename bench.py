@@ -1430,9 +1430,9 @@ def run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
     # (module loading, the caching allocator's first blocks) do not land in the first rate's window
     wrng = S.Rng(0xAE05 - 1 - 1000 * rank)
     srv = M.Server(ctx, hbm_budget_bytes=budget, substeps_per_tick=20)
-    for _ in range(8):
+    for _ in range(24):
         sc, p, k = S.config5_request(wrng)
-        srv.submit(sc, p, min(k, 200))
+        srv.submit(sc, p, min(k, 100))
     srv.drain(600.0)
     srv.poll(4096)
     srv.close()
@@ -1442,20 +1442,24 @@ def run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
         n_req = int(min(args.served_max, max(1, rate * args.served_seconds)))
         reqs = [S.config5_request(rng) for _ in range(n_req)]
         gaps = [-math.log(1.0 - rng.scalar()) / rate for _ in range(n_req)]
+        outs = [M.Particles(*(np.empty_like(a) for a in (p.pos, p.vel, p.F, p.J, p.C, p.mass, p.mat)))
+                for _, p, _ in reqs]  # result buffers, allocated before the arrivals start
         srv = M.Server(ctx, hbm_budget_bytes=budget, substeps_per_tick=20)
         lat, work = [], 0
-        done, max_resident = 0, 0
+        done, max_resident, t_submit = 0, 0, 0.0
         t0 = time.perf_counter()
         nxt = t0
-        for (sc, p, k), gap in zip(reqs, gaps):
+        for (sc, p, k), o, gap in zip(reqs, outs, gaps):
             nxt += gap
             while time.perf_counter() < nxt:
                 for rid, st, ts, ta, td, res in srv.poll():
                     done += 1
                     lat.append(td - ts)
-                max_resident = max(max_resident, srv.stats()["resident_scenes"])
                 time.sleep(0.0005)
-            srv.submit(sc, p, k)
+            ts0 = time.perf_counter()
+            srv.submit(sc, p, k, o)
+            t_submit += time.perf_counter() - ts0
+            max_resident = max(max_resident, srv.stats()["resident_scenes"])
             work += p.n * k
         # the busy window: from the first arrival to the last one, the server's throughput while
         # requests keep arriving (the tail after it drains the last, longest requests alone)
@@ -1472,7 +1476,8 @@ def run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
                     "throughput": stats["particle_substeps"] / wall,
                     "throughput_while_arriving": ps_arr / t_arr if t_arr > 0 else None,
                     "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99), "ticks": stats["ticks"],
-                    "max_resident_scenes": max_resident, "arrival_window_s": t_arr, "wall_s": wall})
+                    "max_resident_scenes": max_resident, "arrival_window_s": t_arr, "wall_s": wall,
+                    "submit_ms_mean": 1e3 * t_submit / n_req})
     # the batched path on the same kind of scenes (config 4, one world), for comparison
     bsc, bparts, _ = workload("batched", rank, 512, world_size)
     bw = M.World(ctx, bsc, M.exec_opts(p2g_variant=M.P2G_LANES, sort_interval=8, block_threads=128))
