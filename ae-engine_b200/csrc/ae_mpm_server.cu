@@ -120,9 +120,9 @@ struct Request {
 };
 
 // The size class a request's slot is made with: each grid axis rounded up to 16 nodes, the
-// particle count to a power of two (at least 1024), the material count to a power of two (at
-// least 4).  A request fits any free slot at least that large whose particle capacity is at most
-// twice its class (more would leave most of the slot's chunks empty).
+// particle count to the next of 1024 * 2^(k/4) rounded to 256 (quarter-octave steps: at most 19 %
+// of a slot's chunks stay empty), the material count to a power of two (at least 4).  A request
+// fits any free slot at least that large whose particle capacity is at most 1.5 times its class.
 struct SlotClass {
   uint32_t n[3];
   uint64_t particles;
@@ -133,10 +133,18 @@ uint64_t pow2_at_least(uint64_t v, uint64_t lo) {
   while (p < v) p <<= 1;
   return p;
 }
+uint64_t particle_class(uint64_t n) {
+  static const double kStep[4] = {1.0, 1.189207115002721, 1.414213562373095, 1.681792830507429};  // 2^(k/4)
+  for (uint64_t p2 = 1024;; p2 <<= 1)
+    for (int k = 0; k < 4; ++k) {
+      const uint64_t c = (uint64_t(double(p2) * kStep[k]) + 255) / 256 * 256;
+      if (c >= n) return c;
+    }
+}
 SlotClass class_of(const ae_mpm_scene_desc& d, uint64_t n) {
   SlotClass c;
   for (int a = 0; a < 3; ++a) c.n[a] = std::max<uint32_t>(16u, (d.n[a] + 15u) / 16u * 16u);
-  c.particles = pow2_at_least(n, 1024);
+  c.particles = particle_class(n);
   c.materials = uint32_t(pow2_at_least(d.n_materials, 4));
   return c;
 }
@@ -209,7 +217,7 @@ struct ae_mpm_server {
     int best = -1;
     for (size_t i = 0; i < slots.size(); ++i) {
       const Slot& s = slots[i];
-      if (s.r || s.cls.particles < r->n || s.cls.particles > 2 * want.particles ||
+      if (s.r || s.cls.particles < r->n || 2 * s.cls.particles > 3 * want.particles ||
           s.cls.materials < r->desc.n_materials || grid_blocks(s.cls.n) < grid_blocks(r->desc.n))
         continue;
       if (best < 0 || s.bytes < slots[best].bytes) best = int(i);
@@ -227,7 +235,7 @@ struct ae_mpm_server {
     uint64_t same = 0;
     for (const Slot& o : slots)
       if (std::memcmp(&o.cls, &s.cls, sizeof(SlotClass)) == 0) ++same;
-    uint64_t k = std::max<uint64_t>(1, same);
+    uint64_t k = std::max<uint64_t>(4, same);
     while (k > 0 && slot_bytes + k * s.bytes > opts.hbm_budget_bytes) --k;
     if (k == 0) return false;
     for (uint64_t i = 0; i < k; ++i) slots.push_back(s);
@@ -527,10 +535,10 @@ int ae_mpm_server_create(ae_mpm_ctx* ctx, const ae_mpm_server_opts* opts, ae_mpm
   if (s->opts.exec.p2g_variant == AE_MPM_P2G_AUTO) {
     // options left to the library: slot particle counts change at every admission and completion,
     // which changes the chunk table a captured graph replays, so substeps are launched eagerly;
-    // sort every 4th substep as the autotuner usually picks for batched worlds
+    // sort every 8th substep as the autotuner picks for the batched scene set
     s->opts.exec.p2g_variant = AE_MPM_P2G_LANES;
     s->opts.exec.use_graph = 0;
-    if (s->opts.exec.sort_interval <= 1) s->opts.exec.sort_interval = 4;
+    if (s->opts.exec.sort_interval <= 1) s->opts.exec.sort_interval = 8;
   }
   if (s->opts.exec.block_threads == 0) s->opts.exec.block_threads = 256;
   if (s->opts.exec.sort_interval < 1) s->opts.exec.sort_interval = 1;
