@@ -226,19 +226,42 @@ struct ae_mpm_server {
   }
 
   // adds slots of r's class within the budget (mu held): as many as that class has already (at
-  // least one), so a class's slot count doubles per growth; false if not even one fits
+  // least 4), so a class's slot count doubles per growth; false if not even one fits.  Growing
+  // rebuilds the world, so every other class without a free slot grows in the same rebuild.
   bool grow_for(const Request* r) {
     Slot s;
     s.cls = class_of(r->desc, r->n);
     std::vector<ae_mpm_material> tmp;
     s.bytes = aemp::scene_device_bytes(slot_desc(s, tmp), 32);
+    if (!add_slots(s, 4)) return false;
+    std::vector<Slot> full;  // one representative of each class with no free slot
+    for (const Slot& o : slots) {
+      bool known = false, free_one = false;
+      for (const Slot& f : full) known = known || std::memcmp(&f.cls, &o.cls, sizeof(SlotClass)) == 0;
+      if (known) continue;
+      for (const Slot& q : slots)
+        if (!q.r && std::memcmp(&q.cls, &o.cls, sizeof(SlotClass)) == 0) free_one = true;
+      if (!free_one) full.push_back(o);
+    }
+    for (Slot& f : full) {
+      f.r = nullptr;
+      add_slots(f, 4);
+    }
+    return true;
+  }
+
+  // adds max(at_least, slots of that class already) slots of s's class, fewer if the budget says
+  // so; false if not even one fits
+  bool add_slots(const Slot& s, uint64_t at_least) {
     uint64_t same = 0;
     for (const Slot& o : slots)
       if (std::memcmp(&o.cls, &s.cls, sizeof(SlotClass)) == 0) ++same;
-    uint64_t k = std::max<uint64_t>(4, same);
+    uint64_t k = std::max<uint64_t>(at_least, same);
     while (k > 0 && slot_bytes + k * s.bytes > opts.hbm_budget_bytes) --k;
     if (k == 0) return false;
-    for (uint64_t i = 0; i < k; ++i) slots.push_back(s);
+    Slot add = s;
+    add.r = nullptr;
+    for (uint64_t i = 0; i < k; ++i) slots.push_back(add);
     slot_bytes += k * s.bytes;
     ++layout;
     return true;
