@@ -616,6 +616,134 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) p2g_lanes_kernel(
   }
 }
 
+// Column-lane P2G of the velocity-only mode (mpm_substep_velocity_only, mpm_solver.rs:1377-1449):
+// per node w m and w m v, w = wx (wy wz), skipping a (y,z) column whose wy or wz is below 1e-10
+// and a node whose w is, and nodes past the grid's upper faces.  The structure is
+// p2g_lanes_kernel's: the warp groups its particles by cell, stages per particle the nine
+// w_y w_z column products, the x weights with the mass and the velocity, and lanes 0..26
+// (3 particle groups x 9 columns) sum the three x nodes of their column over each cell's run,
+// one vector reduction per node and run.
+template <class T>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) p2g_lanes_velonly_kernel(WorldDev<T> w) {
+  using V4 = typename V4T<T>::type;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int nt = blockDim.x;
+  V4* wxm = reinterpret_cast<V4*>(smem);          // wxm[q] = (wx0, wx1, wx2, m)
+  V4* vel = wxm + nt;                             // vel[q] = (vx, vy, vz, -)
+  int4* gk = reinterpret_cast<int4*>(vel + nt);   // gk[q] = (stencil base, cell key)
+  T* cw = reinterpret_cast<T*>(gk + nt);          // cw[q * 9 + column] = w_y w_z, 0 when skipped
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int4 ch = cta_chunk(w);
+  const SceneDev<T>& sc = w.scenes[ch.x];
+  const int n0 = sc.n[0], n1 = sc.n[1], n2 = sc.n[2];
+  const int j = ch.y + tid;
+  const bool live = j < ch.z;
+  bool has = false;
+  P2GPart<T> p;
+  p.g[0] = p.g[1] = p.g[2] = 0;
+  if (live) {
+    const uint32_t src = w.perm ? w.perm[j] : uint32_t(j);
+    p2g_setup<T, AE_MPM_MODE_VELOCITY_ONLY>(w, sc, src, p);
+    has = p.g[0] < n0 && p.g[1] < n1 && p.g[2] < n2;  // some stencil node inside the grid (g >= 0)
+  }
+  const uint32_t key = has ? uint32_t(p.g[0]) + uint32_t(n0) * (uint32_t(p.g[1]) + uint32_t(n1) * uint32_t(p.g[2]))
+                           : 0xffffffffu;
+  const uint32_t peers = __match_any_sync(0xffffffffu, key);
+  const int leader = __ffs(peers) - 1;
+  const uint32_t lead_cnt = lane == leader ? uint32_t(__popc(peers)) : 0u;
+  uint32_t incl = lead_cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t lead_off = incl - lead_cnt;
+  const int pos = int(__shfl_sync(0xffffffffu, lead_off, leader)) + __popc(peers & ((1u << lane) - 1u));
+  uint32_t starts = __reduce_or_sync(0xffffffffu, lane == leader ? (1u << lead_off) : 0u);
+  const int q = warp * 32 + pos;
+  if (has) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+        cw[q * 9 + b + 3 * c] = (p.w[2][c] < T(1e-10) || p.w[1][b] < T(1e-10)) ? T(0) : p.w[1][b] * p.w[2][c];
+    wxm[q] = mk4(p.w[0][0], p.w[0][1], p.w[0][2], p.m);
+    vel[q] = mk4(p.v[0], p.v[1], p.v[2], T(0));
+  }
+  gk[q] = make_int4(p.g[0], p.g[1], p.g[2], int(key));
+  __syncwarp();
+  const int grp = lane < 27 ? lane / 9 : 2;
+  const int jc = lane < 27 ? lane - 9 * grp : lane - 23;
+  const int nb = jc % 3, nc = jc / 3;
+  const T* cww = cw + warp * 32 * 9 + jc;
+  const V4* wxw = wxm + warp * 32;
+  const V4* vw = vel + warp * 32;
+  while (starts) {
+    const int s0 = __ffs(starts) - 1;
+    starts &= starts - 1u;
+    const int e0 = starts ? __ffs(starts) - 1 : 32;
+    const int4 run = gk[warp * 32 + s0];
+    if (uint32_t(run.w) == 0xffffffffu) continue;
+    const int X = run.x, Y = run.y + nb, Z = run.z + nc;
+    T m0 = 0, x0 = 0, y0 = 0, z0 = 0, m1 = 0, x1 = 0, y1 = 0, z1 = 0, m2 = 0, x2 = 0, y2 = 0, z2 = 0;
+    for (int i = s0 + grp; i < e0; i += 3) {
+      const T wyz = cww[i * 9];
+      const V4 r = wxw[i];
+      const V4 v = vw[i];
+      T W0 = r.x * wyz, W1 = r.y * wyz, W2 = r.z * wyz;
+      W0 = W0 < T(1e-10) ? T(0) : W0;
+      W1 = W1 < T(1e-10) ? T(0) : W1;
+      W2 = W2 < T(1e-10) ? T(0) : W2;
+      const T a0 = W0 * r.w, a1 = W1 * r.w, a2 = W2 * r.w;  // w m, as the reference forms it
+      m0 += a0;
+      x0 += a0 * v.x;
+      y0 += a0 * v.y;
+      z0 += a0 * v.z;
+      m1 += a1;
+      x1 += a1 * v.x;
+      y1 += a1 * v.y;
+      z1 += a1 * v.z;
+      m2 += a2;
+      x2 += a2 * v.x;
+      y2 += a2 * v.y;
+      z2 += a2 * v.z;
+    }
+    if (e0 - s0 > 1) {
+      auto groups = [](T v) { return v + __shfl_down_sync(0xffffffffu, v, 9) + __shfl_down_sync(0xffffffffu, v, 18); };
+      m0 = groups(m0), x0 = groups(x0), y0 = groups(y0), z0 = groups(z0);
+      m1 = groups(m1), x1 = groups(x1), y1 = groups(y1), z1 = groups(z1);
+      m2 = groups(m2), x2 = groups(x2), y2 = groups(y2), z2 = groups(z2);
+    }
+    if (lane < 9 && Y < n1 && Z < n2) {
+      const uint32_t row = ((sc.blk_off + (uint32_t(Z >> 2) * uint32_t(sc.nb[1]) + uint32_t(Y >> 2)) * uint32_t(sc.nb[0])) << 6) |
+                           (uint32_t(Z & 3) << 4) | (uint32_t(Y & 3) << 2);
+      auto node = [row](int xa) { return row + ((uint32_t(xa >> 2) << 6) | uint32_t(xa & 3)); };
+      if (m0 != T(0) && X < n0) atomic_add4(w.acc + node(X), m0, x0, y0, z0);
+      if (m1 != T(0) && X + 1 < n0) atomic_add4(w.acc + node(X + 1), m1, x1, y1, z1);
+      if (m2 != T(0) && X + 2 < n0) atomic_add4(w.acc + node(X + 2), m2, x2, y2, z2);
+    }
+  }
+  // grid blocks of this warp's stencil bounding box (inside the grid)
+  int B[3], NB[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int l = __reduce_min_sync(0xffffffffu, has ? p.g[a] : INT_MAX);
+    const int h = __reduce_max_sync(0xffffffffu, has ? min(p.g[a] + 2, sc.n[a] - 1) : INT_MIN);
+    B[a] = l >> 2;
+    NB[a] = l == INT_MAX ? 0 : (h >> 2) - (l >> 2) + 1;
+  }
+  const int nblk = NB[0] * NB[1] * NB[2];
+  for (int t = lane; t < nblk; t += 32) {
+    const int bx = B[0] + t % NB[0], by = B[1] + (t / NB[0]) % NB[1], bz = B[2] + t / (NB[0] * NB[1]);
+    mark_block(w, sc.blk_off + (uint32_t(bz) * uint32_t(sc.nb[1]) + uint32_t(by)) * uint32_t(sc.nb[0]) + uint32_t(bx));
+  }
+}
+// shared bytes per particle of p2g_lanes_velonly_kernel
+template <class T>
+constexpr size_t velonly_lane_bytes() {
+  return 2 * sizeof(typename V4T<T>::type) + sizeof(int4) + 9 * sizeof(T);
+}
+
 // ============================================================================================
 // grid update (momentum -> velocity, gravity, walls); clears accumulator and touched flags
 // ============================================================================================
@@ -2780,6 +2908,10 @@ class World final : public WorldBase {
         lanes_smem_set_ = true;
       }
       p2g_lanes_kernel<T><<<n_chunks_, chunk_threads_, sm2, stream_>>>(w);
+      return;
+    }
+    if (MODE == AE_MPM_MODE_VELOCITY_ONLY && opts_.p2g_variant == kVarLanes) {
+      p2g_lanes_velonly_kernel<T><<<n_chunks_, chunk_threads_, velonly_lane_bytes<T>() * chunk_threads_, stream_>>>(w);
       return;
     }
     switch (opts_.p2g_variant) {

@@ -160,6 +160,109 @@ __global__ void __launch_bounds__(kSortThreads) sort_scatter(const uint32_t* __r
   }
 }
 
+// ---- short lists: the whole sort in one CTA ----------------------------------------------------
+// For up to kSmallSortMax keys the three kernels per pass are launch-bound (the engine's near-field
+// call sorts 16 384 keys).  One CTA of 1024 threads keeps keys and 16-bit indices in shared memory
+// and runs every pass there: each warp ranks its contiguous run of keys row by row (match on the
+// digit, as sort_scatter does), a per-digit prefix over warps and a scan over digits give each
+// key its place, and the keys move between two shared buffers.  Stable, as the multi-kernel path.
+constexpr int kSmallThreads = 1024;
+constexpr int kSmallWarps = kSmallThreads / 32;
+constexpr int kSmallRows = kSmallSortMax / kSmallThreads;  // rows of 32 keys per warp at most
+
+size_t small_sort_smem() {
+  return sizeof(uint32_t) * 2 * kSmallSortMax + sizeof(uint16_t) * 2 * kSmallSortMax +
+         sizeof(uint16_t) * kSmallWarps * kMaxRadix + sizeof(uint32_t) * (kMaxRadix + kSmallWarps);
+}
+
+__global__ void __launch_bounds__(kSmallThreads, 1) sort_small(const uint32_t* __restrict__ keys_in, uint32_t n,
+                                                              SortPlan plan, uint32_t* __restrict__ keys_out,
+                                                              uint32_t* __restrict__ perm_out) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint32_t* kbuf = reinterpret_cast<uint32_t*>(smem);                // [2][kSmallSortMax]
+  uint16_t* vbuf = reinterpret_cast<uint16_t*>(kbuf + 2 * kSmallSortMax);  // [2][kSmallSortMax]
+  uint16_t* wcnt = vbuf + 2 * kSmallSortMax;                         // [kSmallWarps][kMaxRadix]
+  uint32_t* dstart = reinterpret_cast<uint32_t*>(wcnt + kSmallWarps * kMaxRadix);  // [kMaxRadix]
+  uint32_t* wsum = dstart + kMaxRadix;                               // [kSmallWarps]
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const uint32_t lt = lanemask_lt();
+  // each warp owns `seg` consecutive keys, `rows` rows of 32
+  const uint32_t rows = (n + 32u * kSmallWarps - 1) / (32u * kSmallWarps);
+  const uint32_t seg = rows * 32u;
+  for (uint32_t i = tid; i < n; i += kSmallThreads) {
+    kbuf[i] = __ldg(keys_in + i);
+    vbuf[i] = uint16_t(i);
+  }
+  int cur = 0;
+  for (int ps = 0; ps < plan.passes; ++ps) {
+    const int shift = plan.shift[ps];
+    const uint32_t mask = (1u << plan.bits[ps]) - 1u;
+    const uint32_t* kin = kbuf + cur * kSmallSortMax;
+    const uint16_t* vin = vbuf + cur * kSmallSortMax;
+    uint32_t* kout = kbuf + (cur ^ 1) * kSmallSortMax;
+    uint16_t* vout = vbuf + (cur ^ 1) * kSmallSortMax;
+    for (int i = tid; i < kSmallWarps * kMaxRadix; i += kSmallThreads) wcnt[i] = 0;
+    __syncthreads();
+    uint32_t rank[kSmallRows];
+#pragma unroll
+    for (int r = 0; r < kSmallRows; ++r) {
+      rank[r] = 0;
+      if (uint32_t(r) >= rows) continue;  // warp-uniform
+      const uint32_t idx = uint32_t(w) * seg + uint32_t(r) * 32u + uint32_t(lane);
+      const bool valid = idx < n;
+      const uint32_t d = valid ? (kin[idx] >> shift) & mask : 0xffffffffu;
+      const uint32_t peers = __match_any_sync(0xffffffffu, d);
+      const uint32_t c = valid ? wcnt[w * kMaxRadix + d] : 0u;
+      rank[r] = c + __popc(peers & lt);
+      __syncwarp();
+      if (valid && lane == __ffs(peers) - 1) wcnt[w * kMaxRadix + d] = uint16_t(c + __popc(peers));
+      __syncwarp();
+    }
+    __syncthreads();
+    // per digit: exclusive prefix over warps, and the digit's total
+    uint32_t total = 0;
+    if (uint32_t(tid) < uint32_t(kMaxRadix)) {
+      for (int ww = 0; ww < kSmallWarps; ++ww) {
+        const uint32_t c = wcnt[ww * kMaxRadix + tid];
+        wcnt[ww * kMaxRadix + tid] = uint16_t(total);
+        total += c;
+      }
+    }
+    // exclusive scan of the digit totals (digits 0..255 live in warps 0..7)
+    const uint32_t incl = warp_incl_scan(total, lane);
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      const uint32_t ws = lane < kSmallWarps ? wsum[lane] : 0u;
+      const uint32_t wi = warp_incl_scan(ws, lane);
+      if (lane < kSmallWarps) wsum[lane] = wi - ws;
+    }
+    __syncthreads();
+    if (uint32_t(tid) < uint32_t(kMaxRadix)) dstart[tid] = wsum[w] + incl - total;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSmallRows; ++r) {
+      if (uint32_t(r) >= rows) continue;
+      const uint32_t idx = uint32_t(w) * seg + uint32_t(r) * 32u + uint32_t(lane);
+      if (idx < n) {
+        const uint32_t k = kin[idx];
+        const uint32_t d = (k >> shift) & mask;
+        const uint32_t pos = dstart[d] + wcnt[w * kMaxRadix + d] + rank[r];
+        kout[pos] = k;
+        vout[pos] = vin[idx];
+      }
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+  const uint32_t* kf = kbuf + cur * kSmallSortMax;
+  const uint16_t* vf = vbuf + cur * kSmallSortMax;
+  for (uint32_t i = tid; i < n; i += kSmallThreads) {
+    keys_out[i] = kf[i];
+    perm_out[i] = vf[i];
+  }
+}
+
 }  // namespace
 
 cudaError_t sort_scratch_alloc(SortScratch& s, uint64_t n, SortAllocFn alloc, void* user) {
@@ -202,6 +305,19 @@ int radix_sort_pairs(uint32_t* keys, uint64_t n, int key_bits, SortScratch& s, c
     return 0;
   }
   const SortPlan p = make_sort_plan(key_bits);
+  if (n <= uint64_t(kSmallSortMax)) {
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+      cudaFuncSetAttribute(sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize, int(small_sort_smem()));
+      attr_set[dev] = true;
+    }
+    sort_small<<<1, kSmallThreads, small_sort_smem(), stream>>>(keys, uint32_t(n), p, s.keys_alt, s.vals_a);
+    *sorted_keys_out = s.keys_alt;
+    *perm_out = s.vals_a;
+    return 1;
+  }
   const uint32_t tiles = uint32_t(sort_tiles(n));
   cudaMemsetAsync(s.totals, 0, sizeof(uint32_t) * 4 * kMaxRadix, stream);
   uint32_t* kin = keys;

@@ -24,6 +24,7 @@ constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per block
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kMaxRadix = 256;
+constexpr int kSmallSortMax = 16384;  // radix_sort_pairs sorts up to this many keys in one CTA
 
 struct SortPlan {
   int passes;
@@ -70,7 +71,8 @@ void sort_scratch_free(SortScratch& s, SortFreeFn release = nullptr, void* user 
 // Sorts keys[0..n) (only bits [0, key_bits) compared).  On return *perm_out points to the
 // permutation (perm[i] = input index of the i-th smallest key) and *sorted_keys_out to the sorted
 // keys; both live in `keys` / scratch buffers and are valid until the next sort.  `keys` is
-// clobbered.  Queues 3 kernels per pass plus one memset on `stream`; returns the launch count.
+// clobbered.  Queues 3 kernels per pass plus one memset on `stream` (one kernel when n <=
+// kSmallSortMax); returns the launch count.
 int radix_sort_pairs(uint32_t* keys, uint64_t n, int key_bits, SortScratch& s, cudaStream_t stream,
                      const uint32_t** sorted_keys_out, const uint32_t** perm_out);
 
