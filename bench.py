@@ -188,6 +188,17 @@ def max_over_ranks(pg, x: float) -> float:
     return float(t.item())
 
 
+def sum_over_ranks(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
 def barrier(pg):
     if pg is not None:
         pg.barrier()
@@ -1257,6 +1268,7 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
     import ae_mpm as M
 
     n_total = sum(p.n for p in parts)
+    n_job = int(sum_over_ranks(pg, n_total))  # the ranks hold different scenes of one list
     tuned = fixed_options(args)
     world = M.World(ctx, scenes, M.exec_opts(**tuned))
     for i, p in enumerate(parts):
@@ -1293,7 +1305,7 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
     launches = world.launches()
     world.sync(raise_on_error=False)
     ms = max_over_ranks(pg, e0.elapsed_time(e1))
-    value = n_total * world_size * args.steps / (ms / 1e3)
+    value = n_job * args.steps / (ms / 1e3)
 
     # plain path: every scene in a world of its own (same kernels and options), stepped one scene
     # after another; the same K substeps per scene, each timed with events on that world's stream
@@ -1303,7 +1315,7 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
         w1.upload(0, p)
         t_plain += time_world(torch, w1, local, args.steps, 3)
     t_plain = max_over_ranks(pg, t_plain)
-    plain_value = n_total * world_size * args.steps / (t_plain / 1e3) if plain else None
+    plain_value = n_job * args.steps / (t_plain / 1e3) if plain else None
 
     # end to end through the C ABI: every scene submitted at once from pinned host memory, the
     # config's run length of substeps, every scene downloaded; a scene completes when its results
@@ -1352,12 +1364,12 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
             lat_p.append(lat)
     kb = int(np.argsort(e2e_b)[len(e2e_b) // 2])
     kp = int(np.argsort(e2e_p)[len(e2e_p) // 2]) if e2e_p else None
-    e2e = {"value": n_total * world_size * run / e2e_b[kb], "unit": "particle-updates/s",
+    e2e = {"value": n_job * run / e2e_b[kb], "unit": "particle-updates/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d, "substeps_per_step": run,
            "ms_per_step": 1e3 * e2e_b[kb],
            "call": "ae_mpm_world_upload of every scene from pinned host memory, ae_mpm_world_step(%d), "
                    "ae_mpm_world_download of every scene" % run}
-    plain_e2e = n_total * world_size * run / e2e_p[kp] if e2e_p else None
+    plain_e2e = n_job * run / e2e_p[kp] if e2e_p else None
     for w1 in plain:
         w1.close()
 

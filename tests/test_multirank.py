@@ -31,9 +31,10 @@ def _worker(rank, world, port, out):
                             timeout=datetime.timedelta(seconds=60))
     try:
         got = bench.max_over_ranks(dist, 10.0 + 5.0 * rank)
+        total = bench.sum_over_ranks(dist, 1.0 + rank)
         mine = bench.shard(list(range(11)), rank, world)
         scenes, parts, cfg = bench.workload("batched", rank, 3, world)
-        out.put((rank, got, mine, [p.n for p in parts], cfg["scenes"]))
+        out.put((rank, got, mine, [p.n for p in parts], cfg["scenes"], total))
     finally:
         dist.destroy_process_group()
 
@@ -50,6 +51,7 @@ def test_max_over_ranks_and_scene_sharding_with_two_gloo_ranks():
         p.join(60)
         assert p.exitcode == 0
     assert [r[1] for r in res] == [15.0, 15.0]
+    assert [r[5] for r in res] == [3.0, 3.0]  # job-wide particle counts: the sum over ranks
     assert res[0][2] == [0, 2, 4, 6, 8, 10] and res[1][2] == [1, 3, 5, 7, 9]
     assert sorted(res[0][2] + res[1][2]) == list(range(11))
     # the batched workload: each rank holds 3 scenes of one 6-scene population, dealt round-robin
