@@ -167,6 +167,8 @@ SIGNATURES = {
     "ae_mpm_world_sync": (C.c_int, [_P]),
     "ae_mpm_world_download": (C.c_int, [_P, C.c_uint32, C.POINTER(ParticlesView)]),
     "ae_mpm_world_download_f64": (C.c_int, [_P, C.c_uint32, C.POINTER(ParticlesView)]),
+    "ae_mpm_world_upload_many": (C.c_int, [_P, C.c_uint32, _P, _P, _P]),
+    "ae_mpm_world_download_many": (C.c_int, [_P, C.c_uint32, _P, _P]),
     "ae_mpm_world_totals": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_double)]),
     "ae_mpm_world_errors": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
     "ae_mpm_world_launch_count": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
@@ -496,6 +498,23 @@ class World:
         v = p.view()
         fn = self.ctx.lib.ae_mpm_world_download_f64 if self.f64 else self.ctx.lib.ae_mpm_world_download
         self.ctx.check(fn(self.h, scene, C.byref(v)))
+
+    def upload_many(self, scenes, parts) -> None:
+        """ae_mpm_world_upload_many: parts[i] (float32 Particles) into scene scenes[i]."""
+        k = len(parts)
+        views = (ParticlesView * max(k, 1))(*[p.view() for p in parts])
+        ids = np.ascontiguousarray(scenes, np.uint32)
+        counts = np.ascontiguousarray([p.n for p in parts], np.uint64)
+        self._keep_many = parts
+        self.ctx.check(self.ctx.lib.ae_mpm_world_upload_many(self.h, k, ids.ctypes.data, C.addressof(views),
+                                                             counts.ctypes.data))
+
+    def download_many(self, scenes, parts) -> None:
+        """ae_mpm_world_download_many: scene scenes[i] into parts[i] (float32 Particles)."""
+        k = len(parts)
+        views = (ParticlesView * max(k, 1))(*[p.view() for p in parts])
+        ids = np.ascontiguousarray(scenes, np.uint32)
+        self.ctx.check(self.ctx.lib.ae_mpm_world_download_many(self.h, k, ids.ctypes.data, C.addressof(views)))
 
     def step(self, n: int) -> None:
         self.ctx.check(self.ctx.lib.ae_mpm_world_step(self.h, n))

@@ -596,6 +596,13 @@ int ae_mpm_world_download_f64(ae_mpm_world* world, uint32_t scene, ae_mpm_partic
   if (world && !host) return fail(world->ctx, AE_MPM_EINVAL, "null particle view");
   AE_WORLD_CALL(world->w->download(scene, host, true));
 }
+int ae_mpm_world_upload_many(ae_mpm_world* world, uint32_t n, const uint32_t* scenes, const ae_mpm_particles* views,
+                             const uint64_t* counts) {
+  AE_WORLD_CALL(world->w->upload_many(n, scenes, views, counts));
+}
+int ae_mpm_world_download_many(ae_mpm_world* world, uint32_t n, const uint32_t* scenes, ae_mpm_particles* views) {
+  AE_WORLD_CALL(world->w->download_many(n, scenes, views));
+}
 int ae_mpm_world_totals(ae_mpm_world* world, uint32_t scene, double out[5]) {
   if (world && !out) return fail(world->ctx, AE_MPM_EINVAL, "null output");
   AE_WORLD_CALL(world->w->totals(scene, out));

@@ -2409,6 +2409,146 @@ class World final : public WorldBase {
     return AE_MPM_OK;
   }
 
+  // byte offset of each scene's region in a many-scene staging area (16-byte aligned regions in the
+  // staging layout of upload)
+  static uint64_t stage_region(uint64_t n) { return (sizeof(T) * 26 * n + sizeof(uint16_t) * n + 15) / 16 * 16; }
+
+  int upload_many(uint32_t k, const uint32_t* scenes, const ae_mpm_particles* views, const uint64_t* counts) override {
+    if (sizeof(T) != 4) {
+      err = "many-scene transfers are for f32 worlds";
+      return AE_MPM_EINVAL;
+    }
+    if (k == 0) return AE_MPM_OK;
+    if (!scenes || !views || !counts) {
+      err = "null scene, view or count array";
+      return AE_MPM_EINVAL;
+    }
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < k; ++i) {
+      const uint32_t s = scenes[i];
+      if (s >= h_scenes_.size()) {
+        err = "unknown scene";
+        return AE_MPM_ENOTFOUND;
+      }
+      if (counts[i] > h_scenes_[s].p_cap) {
+        err = "scene " + std::to_string(s) + ": " + std::to_string(counts[i]) + " particles exceed max_particles " +
+              std::to_string(h_scenes_[s].p_cap);
+        return AE_MPM_EINVAL;
+      }
+      const ae_mpm_particles& v = views[i];
+      if (counts[i] > 0 && (!v.pos || !v.vel || !v.strain || !v.jacobian || !v.c || !v.mass || !v.material_idx)) {
+        err = "particle view has a null array";
+        return AE_MPM_EINVAL;
+      }
+      total += stage_region(counts[i]);
+    }
+    {
+      const int rs = ensure_stage_bytes(total);
+      if (rs) return rs;
+    }
+    // all copies first, back to back on the stream, then the packs
+    uint64_t off = 0;
+    for (uint32_t i = 0; i < k; ++i) {
+      const uint64_t n = counts[i];
+      T* st = reinterpret_cast<T*>(reinterpret_cast<char*>(stage_) + off);
+      HostView<T> hv = host_view<T>(&views[i]);
+      if (n > 0) {
+        if (staging_layout(hv, n)) {
+          AE_TRY(cudaMemcpyAsync(st, hv.f[0], sizeof(T) * 26 * n + sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+        } else {
+          const uint64_t at[6] = {0, 3, 6, 15, 16, 25}, len[6] = {3, 3, 9, 1, 9, 1};
+          for (int f = 0; f < 6; ++f)
+            AE_TRY(cudaMemcpyAsync(st + at[f] * n, hv.f[f], sizeof(T) * len[f] * n, cudaMemcpyDefault, stream_));
+          AE_TRY(cudaMemcpyAsync(st + 26 * n, hv.mat, sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+        }
+      }
+      off += stage_region(n);
+    }
+    for (uint32_t i = 0; i < k; ++i) {
+      const uint32_t s = scenes[i];
+      if (h_scenes_[s].p_count != uint32_t(counts[i])) {
+        h_scenes_[s].p_count = uint32_t(counts[i]);
+        count_changed(s);
+      }
+    }
+    int rc = sync_tables();
+    if (rc) return rc;
+    off = 0;
+    for (uint32_t i = 0; i < k; ++i) {
+      const uint64_t n = counts[i];
+      const T* st = reinterpret_cast<const T*>(reinterpret_cast<const char*>(stage_) + off);
+      if (n > 0)
+        pack_kernel<T><<<unsigned((n + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), st, n, h_scenes_[scenes[i]].p_off,
+                                                                        d_scenes_ + scenes[i], d_mats_);
+      off += stage_region(n);
+    }
+    AE_TRY(cudaGetLastError());
+    keys_stale_ = true;
+    scatter_invalid_ = true;
+    return AE_MPM_OK;
+  }
+
+  int download_many(uint32_t k, const uint32_t* scenes, ae_mpm_particles* views) override {
+    if (sizeof(T) != 4) {
+      err = "many-scene transfers are for f32 worlds";
+      return AE_MPM_EINVAL;
+    }
+    if (k == 0) return AE_MPM_OK;
+    if (!scenes || !views) {
+      err = "null scene or view array";
+      return AE_MPM_EINVAL;
+    }
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < k; ++i) {
+      if (scenes[i] >= h_scenes_.size()) {
+        err = "unknown scene";
+        return AE_MPM_ENOTFOUND;
+      }
+      const ae_mpm_particles& v = views[i];
+      if (h_scenes_[scenes[i]].p_count > 0 &&
+          (!v.pos || !v.vel || !v.strain || !v.jacobian || !v.c || !v.mass || !v.material_idx)) {
+        err = "particle view has a null array";
+        return AE_MPM_EINVAL;
+      }
+      total += stage_region(h_scenes_[scenes[i]].p_count);
+    }
+    {
+      const int rs = ensure_stage_bytes(total);
+      if (rs) return rs;
+    }
+    int rc = sync_tables();
+    if (rc) return rc;
+    uint64_t off = 0;
+    for (uint32_t i = 0; i < k; ++i) {
+      const SceneDev<T>& h = h_scenes_[scenes[i]];
+      T* st = reinterpret_cast<T*>(reinterpret_cast<char*>(stage_) + off);
+      if (h.p_count > 0)
+        unpack_kernel<T><<<unsigned((h.p_count + 255) / 256), 256, 0, stream_>>>(in_ptrs_dev(), st, h.p_count, h.p_off,
+                                                                                 d_scenes_ + scenes[i], d_mats_);
+      off += stage_region(h.p_count);
+    }
+    AE_TRY(cudaGetLastError());
+    off = 0;
+    for (uint32_t i = 0; i < k; ++i) {
+      const uint64_t n = h_scenes_[scenes[i]].p_count;
+      const T* st = reinterpret_cast<const T*>(reinterpret_cast<const char*>(stage_) + off);
+      HostView<T> hv = host_view<T>(&views[i]);
+      if (n > 0) {
+        if (staging_layout(hv, n)) {
+          AE_TRY(cudaMemcpyAsync(hv.f[0], st, sizeof(T) * 26 * n + sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+        } else {
+          const uint64_t at[6] = {0, 3, 6, 15, 16, 25}, len[6] = {3, 3, 9, 1, 9, 1};
+          for (int f = 0; f < 6; ++f)
+            AE_TRY(cudaMemcpyAsync(hv.f[f], st + at[f] * n, sizeof(T) * len[f] * n, cudaMemcpyDefault, stream_));
+          AE_TRY(cudaMemcpyAsync(hv.mat, st + 26 * n, sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+        }
+      }
+      off += stage_region(n);
+    }
+    AE_TRY(cudaStreamSynchronize(stream_));
+    return AE_MPM_OK;
+  }
+
   int step(uint32_t n) override {
     launches_ = 0;
     int rc = prepare();
@@ -2748,9 +2888,11 @@ class World final : public WorldBase {
   V4** out_buf() { return a_in_ ? bufB_ : bufA_; }
   V4* const* in_ptrs_dev() { return a_in_ ? d_ptrA_ : d_ptrB_; }
 
-  int ensure_stage(uint64_t n) {
-    size_t need = sizeof(T) * 26 * n + sizeof(uint16_t) * n + 64;
+  int ensure_stage(uint64_t n) { return ensure_stage_bytes(sizeof(T) * 26 * n + sizeof(uint16_t) * n + 64); }
+  int ensure_stage_bytes(size_t need) {
     if (need <= stage_bytes_) return AE_MPM_OK;
+    // queued work may still read the old staging area
+    AE_TRY(cudaStreamSynchronize(stream_));
     dfree(stage_);
     stage_ = nullptr;
     stage_bytes_ = 0;

@@ -98,6 +98,11 @@ struct WorldBase {
   virtual ~WorldBase() {}
   virtual int upload(uint32_t scene, const void* host, uint64_t n, bool f64) = 0;
   virtual int download(uint32_t scene, void* host, bool f64) = 0;
+  // Many scenes per call (f32 worlds): every host<->device copy is queued back to back through one
+  // staging area, so the copies run at link speed instead of one scene, one wait at a time.
+  // upload_many is asynchronous like upload; download_many waits once, at the end.
+  virtual int upload_many(uint32_t n, const uint32_t* scenes, const ae_mpm_particles* views, const uint64_t* counts) = 0;
+  virtual int download_many(uint32_t n, const uint32_t* scenes, ae_mpm_particles* views) = 0;
   virtual int step(uint32_t n) = 0;
   virtual int sync() = 0;
   virtual int totals(uint32_t scene, double out[5]) = 0;

@@ -258,6 +258,17 @@ int ae_mpm_world_sync(ae_mpm_world* world);
 /* Copy scene particles back in their upload order (into host memory or memory of the world's device). */
 int ae_mpm_world_download(ae_mpm_world* world, uint32_t scene, ae_mpm_particles* host);
 int ae_mpm_world_download_f64(ae_mpm_world* world, uint32_t scene, ae_mpm_particles_f64* host);
+/* Many scenes in one call (f32 worlds; no counterpart in the reference, whose engine moves one
+ * MpssBuffer per call).  upload_many copies counts[i] particles of views[i] into scene scenes[i]
+ * for i < n, as n calls of ae_mpm_world_upload would, but queues every host-to-device copy back
+ * to back through one device staging area before unpacking, so pinned views (best laid out as
+ * pos 3n | vel 3n | strain 9n | jacobian n | c 9n | mass n floats, then n u16 material indices,
+ * which travels in one copy) stream at link speed; asynchronous like ae_mpm_world_upload.
+ * download_many copies scene scenes[i] back into views[i] the same way and returns once all of
+ * them are in place. */
+int ae_mpm_world_upload_many(ae_mpm_world* world, uint32_t n, const uint32_t* scenes,
+                             const ae_mpm_particles* views, const uint64_t* counts);
+int ae_mpm_world_download_many(ae_mpm_world* world, uint32_t n, const uint32_t* scenes, ae_mpm_particles* views);
 /* FP64 totals of a scene: [mass, px, py, pz, kinetic energy] of its particles, now. */
 int ae_mpm_world_totals(ae_mpm_world* world, uint32_t scene, double out[5]);
 /* Per-scene error word (bit 0 NaN, bit 1 domain clamp) and counters
