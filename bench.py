@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """MPM particle-updates/s on B200, batched vs plain, with p50/p99 scene latency.
 
-Default workload (config 4, "batched"): 512 independent scenes, grid per scene drawn from
+Default workload ("batched"): 512 independent scenes, grid per scene drawn from
 {32,48,64}^3, particle count log-uniform in [2k, 64k] (9.7 M particles in all), material jelly,
 snow or water, box velocities in [-1,1]^3 m/s, f32.  One bench step = one MPM substep of every
 scene (radix sort by cell key, P2G, grid update, G2P), all scenes in one world: one launch of each
@@ -1261,8 +1261,9 @@ def fp64_run(ctx, scenes, parts, opts_kw, substeps):
 
 
 def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
-    """Config 4: every scene in one world (one launch per kernel per substep for all scenes) against
-    the plain path, the same kernels stepping one world per scene, one scene at a time."""
+    """The batched workload (512 scenes, grids 32^3-64^3, 2k-64k particles): every scene in one world
+    (one launch per kernel per substep for all scenes) against the plain path, the same kernels
+    stepping one world per scene, one scene at a time."""
     import torch
 
     import ae_mpm as M
@@ -1421,7 +1422,7 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
 
 
 def run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
-    """Config 5: Poisson arrivals of config-4 scenes plus 5% large 1M-particle snow scenes, each
+    """Served: Poisson arrivals of batched-workload scenes plus 5% large 1M-particle snow scenes, each
     with 100..2000 substeps, into the continuous-batching server; per rate the throughput and the
     p50/p99 completion latency (submit -> results in the caller's buffers)."""
     import ae_mpm as M
@@ -1488,7 +1489,7 @@ def run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
                     "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99), "ticks": stats["ticks"],
                     "max_resident_scenes": max_resident, "arrival_window_s": t_arr, "wall_s": wall,
                     "submit_ms_mean": 1e3 * t_submit / n_req})
-    # the batched path on the same kind of scenes (config 4, one world), for comparison
+    # the batched path on the same kind of scenes (the 512-scene batched workload, one world), for comparison
     bsc, bparts, _ = workload("batched", rank, 512, world_size)
     bw = M.World(ctx, bsc, M.exec_opts(p2g_variant=M.P2G_LANES, sort_interval=8, block_threads=128))
     for i, q in enumerate(bparts):

@@ -46,13 +46,13 @@ def test_config2_full_size_fp32_against_fp64_through_the_collision(ctx):
     assert w32.sync(raise_on_error=False) == M.OK and w64.sync(raise_on_error=False) == M.OK
     a, b = w32.download(0, p.n), w64.download(0, p.n)
     r200 = per_particle_rel(a, b)
-    print("config 2, 200 substeps: per-particle rel error max %.3g p99 %.3g" % (r200.max(), np.percentile(r200, 99)))
+    print("snow 1M, 200 substeps: per-particle rel error max %.3g p99 %.3g" % (r200.max(), np.percentile(r200, 99)))
     assert r200.max() <= 1e-4
     # the FP64 kernels against the FP64 oracle on the whole scene, same 200 substeps
     ref = p.astype(np.float64)
     O.run(sc, ref, 200, threads=os.cpu_count() or 1)
     err64 = float(np.abs(b.pos - ref.pos).max() / np.abs(ref.pos).max())
-    print("config 2, 200 substeps: FP64 kernels vs FP64 oracle %.3g" % err64)
+    print("snow 1M, 200 substeps: FP64 kernels vs FP64 oracle %.3g" % err64)
     assert err64 <= 1e-9
     # through the plastic flow to the configuration's full length
     w32.step(300)
@@ -61,7 +61,7 @@ def test_config2_full_size_fp32_against_fp64_through_the_collision(ctx):
     a, b = w32.download(0, p.n), w64.download(0, p.n)
     r500 = per_particle_rel(a, b)
     yielded = float(np.mean(np.abs(b.J - 1.0) > 1e-6))  # plastic J_p leaves 1 once a particle yields
-    print("config 2, 500 substeps: per-particle rel error max %.3g p99 %.3g; %.0f%% of particles yielded"
+    print("snow 1M, 500 substeps: per-particle rel error max %.3g p99 %.3g; %.0f%% of particles yielded"
           % (r500.max(), np.percentile(r500, 99), 100 * yielded))
     assert yielded > 0.2  # the collision drove the plastic flow
     assert np.percentile(r500, 99) <= 1e-4
