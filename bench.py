@@ -1506,7 +1506,7 @@ def run_served(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
         line = {"metric": "MPM particle-updates/s", "value": best["throughput"], "unit": "particle-updates/s",
                 "n_gpus": world_size, "steps": None, "warmup": None, "ms_per_step": None, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64 scenes)",
-                "config": {"workload": "served: Poisson arrivals of config-4 scenes + 5% 128^3 1M-particle snow, "
+                "config": {"workload": "served: Poisson arrivals of batched-workload scenes + 5% 128^3 1M-particle snow, "
                                        "100-2000 substeps each", "hbm_budget_bytes": budget},
                 "batched_value": batched_value, "served": out}
         print(json.dumps(line), flush=True)
