@@ -225,46 +225,60 @@ struct ae_mpm_server {
     return best;
   }
 
-  // adds slots of r's class within the budget (mu held): as many as that class has already (at
-  // least 4), so a class's slot count doubles per growth; false if not even one fits.  Growing
-  // rebuilds the world, so every other class without a free slot grows in the same rebuild.
+  // grows the slot table within the budget (mu held); false if not even one slot of r's class
+  // fits.  Growing rebuilds the world, so one growth sizes every class for what is waiting: each
+  // class present in the queue (r's included) gets slots for all its waiting requests plus half
+  // as many again, at least 4 and at least as many as it has (so a class at least doubles), and
+  // every other class without a free slot doubles too.
   bool grow_for(const Request* r) {
-    Slot s;
-    s.cls = class_of(r->desc, r->n);
-    std::vector<ae_mpm_material> tmp;
-    s.bytes = aemp::scene_device_bytes(slot_desc(s, tmp), 32);
-    if (!add_slots(s, 4)) return false;
-    std::vector<Slot> full;  // one representative of each class with no free slot
-    for (const Slot& o : slots) {
-      bool known = false, free_one = false;
-      for (const Slot& f : full) known = known || std::memcmp(&f.cls, &o.cls, sizeof(SlotClass)) == 0;
-      if (known) continue;
-      for (const Slot& q : slots)
-        if (!q.r && std::memcmp(&q.cls, &o.cls, sizeof(SlotClass)) == 0) free_one = true;
-      if (!free_one) full.push_back(o);
+    std::vector<std::pair<Slot, uint64_t>> want;  // class representative, slots to add
+    auto index_of = [&](const SlotClass& c) {
+      for (size_t i = 0; i < want.size(); ++i)
+        if (std::memcmp(&want[i].first.cls, &c, sizeof(SlotClass)) == 0) return int(i);
+      return -1;
+    };
+    auto count_class = [&](const SlotClass& c, bool free_only) {
+      uint64_t k = 0;
+      for (const Slot& o : slots)
+        if (std::memcmp(&o.cls, &c, sizeof(SlotClass)) == 0 && (!free_only || !o.r)) ++k;
+      return k;
+    };
+    auto add_want = [&](const SlotClass& c) {
+      int i = index_of(c);
+      if (i < 0) {
+        Slot s;
+        s.cls = c;
+        std::vector<ae_mpm_material> tmp;
+        s.bytes = aemp::scene_device_bytes(slot_desc(s, tmp), 32);
+        want.emplace_back(s, 0);
+        i = int(want.size()) - 1;
+      }
+      return i;
+    };
+    add_want(class_of(r->desc, r->n));
+    for (const Request* q : waiting) want[size_t(add_want(class_of(q->desc, q->n)))].second += 1;
+    for (auto& w : want) {
+      const uint64_t have = count_class(w.first.cls, false), free_now = count_class(w.first.cls, true);
+      const uint64_t need = w.second > free_now ? w.second - free_now : 0;
+      w.second = std::max<uint64_t>({4, have, need + need / 2});
     }
-    for (Slot& f : full) {
-      f.r = nullptr;
-      add_slots(f, 4);
-    }
-    return true;
-  }
-
-  // adds max(at_least, slots of that class already) slots of s's class, fewer if the budget says
-  // so; false if not even one fits
-  bool add_slots(const Slot& s, uint64_t at_least) {
-    uint64_t same = 0;
     for (const Slot& o : slots)
-      if (std::memcmp(&o.cls, &s.cls, sizeof(SlotClass)) == 0) ++same;
-    uint64_t k = std::max<uint64_t>(at_least, same);
-    while (k > 0 && slot_bytes + k * s.bytes > opts.hbm_budget_bytes) --k;
-    if (k == 0) return false;
-    Slot add = s;
-    add.r = nullptr;
-    for (uint64_t i = 0; i < k; ++i) slots.push_back(add);
-    slot_bytes += k * s.bytes;
-    ++layout;
-    return true;
+      if (index_of(o.cls) < 0 && count_class(o.cls, true) == 0) {
+        const int i = add_want(o.cls);
+        want[size_t(i)].second = std::max<uint64_t>(4, count_class(o.cls, false));
+      }
+    bool first = true, ok = false;
+    for (auto& w : want) {  // r's class first: if even one of it does not fit, nothing grows
+      uint64_t k = w.second;
+      while (k > 0 && slot_bytes + k * w.first.bytes > opts.hbm_budget_bytes) --k;
+      if (first && k == 0) return false;
+      first = false;
+      for (uint64_t i = 0; i < k; ++i) slots.push_back(w.first);
+      slot_bytes += k * w.first.bytes;
+      ok = ok || k > 0;
+    }
+    if (ok) ++layout;
+    return ok;
   }
 
   // drops the vacant slots (mu held): the budget they hold goes back to admission; the occupied
