@@ -738,6 +738,144 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) p2g_lanes_velonly
     mark_block(w, sc.blk_off + (uint32_t(bz) * uint32_t(sc.nb[1]) + uint32_t(by)) * uint32_t(sc.nb[0]) + uint32_t(bx));
   }
 }
+// Column-lane P2G of the reference mode (mpm_substep_serial_active / parallel_with_indices P2G,
+// mpm_solver.rs:831-903, 1108-1193).  Per node (a,b,c) of a particle: w = (wx wy) wz, skipped below
+// 1e-10 (mass, momentum and force alike); momentum w m (v + C d) with d the node minus the particle;
+// the force sv . (N'(a), N'(b), N'(c)) / dx, not weighted by w, folded into momentum as dt sv (the
+// grid update's v = p/m + g dt then equals the reference's p/m + (g + f/m) dt up to rounding).
+// The particle's owner thread stages per (y,z) column u = v + C[.][1] d_y + C[.][2] d_z with wy,
+// and f = sv[.][1] N'_y + sv[.][2] N'_z with wz; lanes 0..26 (3 particle groups x 9 columns) add
+// the x part of each of their column's three nodes and sum over each cell's run, one vector
+// reduction per node and run.
+constexpr int kRefLaneVecs = 2 * 9 + 5;  // shared vectors per particle
+template <class T>
+__global__ void __launch_bounds__(256, 1) p2g_lanes_ref_kernel(WorldDev<T> w) {
+  using V4 = typename V4T<T>::type;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int nt = blockDim.x;
+  V4* cu = reinterpret_cast<V4*>(smem);  // cu[q * 9 + j] = (u, wy)
+  V4* cf = cu + 9 * nt;                  // cf[q * 9 + j] = (f, wz)
+  V4* pw = cf + 9 * nt;                  // pw[q] = (wx0, wx1, wx2, m)
+  V4* pc = pw + nt;                      // pc[q] = C[.][0]
+  V4* po = pc + nt;                      // po[q] = (d_x of the three x nodes)
+  V4* ps = po + nt;                      // ps[q] = dt sv[.][0]
+  V4* pe = ps + nt;                      // pe[q] = (N'_x of the three x nodes) / dx
+  int4* gk = reinterpret_cast<int4*>(pe + nt);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int4 ch = cta_chunk(w);
+  const SceneDev<T>& sc = w.scenes[ch.x];
+  const int n0 = sc.n[0], n1 = sc.n[1], n2 = sc.n[2];
+  const int j = ch.y + tid;
+  const bool live = j < ch.z;
+  bool has = false;
+  P2GPart<T> p;
+  p.g[0] = p.g[1] = p.g[2] = 0;
+  if (live) {
+    const uint32_t src = w.perm ? w.perm[j] : uint32_t(j);
+    p2g_setup<T, AE_MPM_MODE_REFERENCE>(w, sc, src, p);
+    has = p.g[0] < n0 && p.g[1] < n1 && p.g[2] < n2;  // some stencil node inside the grid (g >= 0)
+  }
+  const uint32_t key = has ? uint32_t(p.g[0]) + uint32_t(n0) * (uint32_t(p.g[1]) + uint32_t(n1) * uint32_t(p.g[2]))
+                           : 0xffffffffu;
+  const uint32_t peers = __match_any_sync(0xffffffffu, key);
+  const int leader = __ffs(peers) - 1;
+  const uint32_t lead_cnt = lane == leader ? uint32_t(__popc(peers)) : 0u;
+  uint32_t incl = lead_cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t lead_off = incl - lead_cnt;
+  const int pos = int(__shfl_sync(0xffffffffu, lead_off, leader)) + __popc(peers & ((1u << lane) - 1u));
+  uint32_t starts = __reduce_or_sync(0xffffffffu, lane == leader ? (1u << lead_off) : 0u);
+  const int q = warp * 32 + pos;
+  if (has) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const T dy = p.o[1][b], dz = p.o[2][c], ey = p.dw[1][b], ez = p.dw[2][c];
+        const T ux = p.v[0] + p.A[1] * dy + p.A[2] * dz;
+        const T uy = p.v[1] + p.A[4] * dy + p.A[5] * dz;
+        const T uz = p.v[2] + p.A[7] * dy + p.A[8] * dz;
+        cu[q * 9 + b + 3 * c] = mk4(ux, uy, uz, p.w[1][b]);
+        cf[q * 9 + b + 3 * c] =
+            mk4(p.sv[1] * ey + p.sv[2] * ez, p.sv[4] * ey + p.sv[5] * ez, p.sv[7] * ey + p.sv[8] * ez, p.w[2][c]);
+      }
+    pw[q] = mk4(p.w[0][0], p.w[0][1], p.w[0][2], p.m);
+    pc[q] = mk4(p.A[0], p.A[3], p.A[6], T(0));
+    po[q] = mk4(p.o[0][0], p.o[0][1], p.o[0][2], T(0));
+    ps[q] = mk4(p.sv[0], p.sv[3], p.sv[6], T(0));
+    pe[q] = mk4(p.dw[0][0], p.dw[0][1], p.dw[0][2], T(0));
+  }
+  gk[q] = make_int4(p.g[0], p.g[1], p.g[2], int(key));
+  __syncwarp();
+  const int grp = lane < 27 ? lane / 9 : 2;
+  const int jc = lane < 27 ? lane - 9 * grp : lane - 23;
+  const int nb = jc % 3, nc = jc / 3;
+  const int wb = warp * 32;
+  while (starts) {
+    const int s0 = __ffs(starts) - 1;
+    starts &= starts - 1u;
+    const int e0 = starts ? __ffs(starts) - 1 : 32;
+    const int4 run = gk[wb + s0];
+    if (uint32_t(run.w) == 0xffffffffu) continue;
+    const int X = run.x, Y = run.y + nb, Z = run.z + nc;
+    T acc[3][4];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) acc[a][0] = acc[a][1] = acc[a][2] = acc[a][3] = T(0);
+    for (int i = s0 + grp; i < e0; i += 3) {
+      const V4 u = cu[(wb + i) * 9 + jc], f = cf[(wb + i) * 9 + jc];
+      const V4 r = pw[wb + i], cx = pc[wb + i], dx = po[wb + i], sx = ps[wb + i], ex = pe[wb + i];
+      const T wxs[3] = {r.x, r.y, r.z}, dxs[3] = {dx.x, dx.y, dx.z}, exs[3] = {ex.x, ex.y, ex.z};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const T wn = (wxs[a] * u.w) * f.w;  // (wx wy) wz, as the reference multiplies
+        if (wn < T(1e-10)) continue;
+        const T wm = wn * r.w;
+        acc[a][0] += wm;
+        acc[a][1] += wm * (u.x + cx.x * dxs[a]) + (f.x + sx.x * exs[a]);
+        acc[a][2] += wm * (u.y + cx.y * dxs[a]) + (f.y + sx.y * exs[a]);
+        acc[a][3] += wm * (u.z + cx.z * dxs[a]) + (f.z + sx.z * exs[a]);
+      }
+    }
+    if (e0 - s0 > 1) {
+      auto groups = [](T v) { return v + __shfl_down_sync(0xffffffffu, v, 9) + __shfl_down_sync(0xffffffffu, v, 18); };
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[a][k] = groups(acc[a][k]);
+    }
+    if (lane < 9 && Y < n1 && Z < n2) {
+      const uint32_t row = ((sc.blk_off + (uint32_t(Z >> 2) * uint32_t(sc.nb[1]) + uint32_t(Y >> 2)) * uint32_t(sc.nb[0])) << 6) |
+                           (uint32_t(Z & 3) << 4) | (uint32_t(Y & 3) << 2);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int xa = X + a;
+        // a node every particle skipped has mass 0; one with a (skipped-weight) force only does not
+        // exist: the force is added exactly where the mass is
+        if (acc[a][0] != T(0) && xa < n0)
+          atomic_add4(w.acc + (row + ((uint32_t(xa >> 2) << 6) | uint32_t(xa & 3))), acc[a][0], acc[a][1], acc[a][2],
+                      acc[a][3]);
+      }
+    }
+  }
+  int B[3], NB[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int l = __reduce_min_sync(0xffffffffu, has ? p.g[a] : INT_MAX);
+    const int h = __reduce_max_sync(0xffffffffu, has ? min(p.g[a] + 2, sc.n[a] - 1) : INT_MIN);
+    B[a] = l >> 2;
+    NB[a] = l == INT_MAX ? 0 : (h >> 2) - (l >> 2) + 1;
+  }
+  const int nblk = NB[0] * NB[1] * NB[2];
+  for (int t = lane; t < nblk; t += 32) {
+    const int bx = B[0] + t % NB[0], by = B[1] + (t / NB[0]) % NB[1], bz = B[2] + t / (NB[0] * NB[1]);
+    mark_block(w, sc.blk_off + (uint32_t(bz) * uint32_t(sc.nb[1]) + uint32_t(by)) * uint32_t(sc.nb[0]) + uint32_t(bx));
+  }
+}
+
 // shared bytes per particle of p2g_lanes_velonly_kernel
 template <class T>
 constexpr size_t velonly_lane_bytes() {
@@ -3052,6 +3190,15 @@ class World final : public WorldBase {
       p2g_lanes_kernel<T><<<n_chunks_, chunk_threads_, sm2, stream_>>>(w);
       return;
     }
+    if (MODE == AE_MPM_MODE_REFERENCE && opts_.p2g_variant == kVarLanes) {
+      const size_t per = sizeof(V4) * kRefLaneVecs + sizeof(int4);
+      if (!ref_lanes_smem_set_) {  // sized for the largest block (256 threads) the world accepts
+        cudaFuncSetAttribute(p2g_lanes_ref_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(per * 256));
+        ref_lanes_smem_set_ = true;
+      }
+      p2g_lanes_ref_kernel<T><<<n_chunks_, chunk_threads_, per * chunk_threads_, stream_>>>(w);
+      return;
+    }
     if (MODE == AE_MPM_MODE_VELOCITY_ONLY && opts_.p2g_variant == kVarLanes) {
       p2g_lanes_velonly_kernel<T><<<n_chunks_, chunk_threads_, velonly_lane_bytes<T>() * chunk_threads_, stream_>>>(w);
       return;
@@ -3322,7 +3469,7 @@ class World final : public WorldBase {
   cudaGraphExec_t graph_ = nullptr;
   uint64_t graph_period_ = 0, graph_launches_ = 0;
   int graph_variant_ = -1;
-  bool lanes_smem_set_ = false, fused_smem_set_ = false;
+  bool lanes_smem_set_ = false, fused_smem_set_ = false, ref_lanes_smem_set_ = false;
   bool scatter_pending_ = false;  // the accumulator holds the P2G of the current particle state
   bool scatter_invalid_ = false;  // the particles changed since that scatter
   uint64_t substep_ = 0, snap_substep_ = 0, launches_ = 0;
