@@ -539,6 +539,16 @@ struct ae_mpm_server {
           running.erase(std::find(running.begin(), running.end(), r));
           outgoing.push_back(r);
         }
+        // A world whose slots stand mostly empty still sorts its whole capacity and launches a CTA
+        // per chunk of every slot each substep: with nothing waiting and under a quarter of the
+        // particle capacity in use, drop the vacant slots (the next tick rebuilds the world from
+        // the occupied ones).
+        if (!done_now.empty() && waiting.empty() && !running.empty()) {
+          uint64_t live = 0, cap = 0;
+          for (const Slot& sl : slots) cap += sl.cls.particles;
+          for (const Request* r : running) live += r->n;
+          if (4 * live < cap) compact();
+        }
       }
     }
     deliver();
