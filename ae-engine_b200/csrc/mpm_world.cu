@@ -1617,6 +1617,9 @@ __device__ __forceinline__ WarpStage<T> warp_stage(unsigned char* smem, int warp
 // position, mv = m v, A = m C - k tau.  The cell key is the global index of the stencil's base
 // node, unique across scenes.  kMixed: lanes may belong to different scenes (each run looks its
 // scene up from its base node's block); otherwise every lane belongs to scene sc.
+// runs of at most this many particles are summed one node per lane; longer ones by the column lanes
+constexpr int kShortRun = 10;
+
 template <class T, bool kMixed>
 __device__ __forceinline__ void p2g_warp_scatter(const WorldDev<T>& w, const SceneDev<T>& sc, bool has, const T* x,
                                                  T m, const T* mv, const T* A, const WarpStage<T>& st) {
@@ -1691,6 +1694,41 @@ __device__ __forceinline__ void p2g_warp_scatter(const WorldDev<T>& w, const Sce
     const int4 run = st.gk[s0];
     if (uint32_t(run.w) == 0xffffffffu) continue;
     const SceneDev<T>& rs = kMixed ? w.scenes[w.blk_scene[uint32_t(run.w) >> 6]] : sc;
+    if (e0 - s0 <= kShortRun) {
+      // a short run: one lane per stencil node (27 lanes), each summing every particle of the run
+      // for its node; no combine across lane groups, one vector reduction per lane
+      const int ln = lane < 27 ? lane : 26;
+      const int xa = ln % 3, jn = ln / 3;
+      const T fa = T(xa);
+      const V4* cn = st.col + jn;
+      T m = 0, px = 0, py = 0, pz = 0;
+      for (int i = s0; i < e0; ++i) {
+        const V4 u = cn[i * 9];
+        const V4 r = st.wxm[i];
+        const V4 a = st.acol[i];
+        const T W = (xa == 0 ? r.x : (xa == 1 ? r.y : r.z)) * u.w;
+        m += W * r.w;
+        px += W * (u.x + fa * a.x);
+        py += W * (u.y + fa * a.y);
+        pz += W * (u.z + fa * a.z);
+      }
+      if (lane < 27 && m != T(0)) {
+        const int Xn = run.x + xa, Yn = run.y + jn % 3, Zn = run.z + jn / 3;
+        const uint32_t node =
+            ((rs.blk_off + (uint32_t(Zn >> 2) * uint32_t(rs.nb[1]) + uint32_t(Yn >> 2)) * uint32_t(rs.nb[0]) +
+              uint32_t(Xn >> 2))
+             << 6) |
+            (uint32_t(Zn & 3) << 4) | (uint32_t(Yn & 3) << 2) | uint32_t(Xn & 3);
+        atomic_add4(w.acc + node, m, px, py, pz);
+      }
+      if (kMixed && lane >= 27) {  // the run's stencil blocks (at most 2 per axis): lanes 27..31 and
+        for (int o = lane - 27; o < 8; o += 5) {  // 27..29 again
+          const int bx = (run.x + 2 * (o & 1)) >> 2, by = (run.y + (o & 2)) >> 2, bz = (run.z + ((o >> 1) & 2)) >> 2;
+          mark_block(w, rs.blk_off + (uint32_t(bz) * uint32_t(rs.nb[1]) + uint32_t(by)) * uint32_t(rs.nb[0]) + uint32_t(bx));
+        }
+      }
+      continue;
+    }
     const int X = run.x, Y = run.y + nb, Z = run.z + nc;
     T m0 = 0, x0 = 0, y0 = 0, z0 = 0, m1 = 0, x1 = 0, y1 = 0, z1 = 0, m2 = 0, x2 = 0, y2 = 0, z2 = 0;
 #pragma unroll 2
@@ -2336,11 +2374,11 @@ class World final : public WorldBase {
     AE_TRY(cudaMemcpy(dead_blk_, dead.data(), sizeof(uint32_t) * blk, cudaMemcpyHostToDevice));
     // particles
     const uint64_t pc = std::max<uint64_t>(cap, 1);
+    // particle slots past a scene's count are never read (every kernel gates on the live range),
+    // so the particle arrays need no clearing
     for (int k = 0; k < 7; ++k) {
       AE_TRY(dmalloc(&bufA_[k], sizeof(V4) * pc));
       AE_TRY(dmalloc(&bufB_[k], sizeof(V4) * pc));
-      AE_TRY(cudaMemset(bufA_[k], 0, sizeof(V4) * pc));
-      AE_TRY(cudaMemset(bufB_[k], 0, sizeof(V4) * pc));
     }
     AE_TRY(dmalloc(&d_ptrA_, sizeof(V4*) * 7));
     AE_TRY(dmalloc(&d_ptrB_, sizeof(V4*) * 7));
@@ -2868,6 +2906,8 @@ class World final : public WorldBase {
       if (a.p_count)
         AE_TRY(cudaMemcpyAsync(in_buf()[k] + b.p_off, src->in_buf()[k] + a.p_off, sizeof(V4) * a.p_count,
                                cudaMemcpyDeviceToDevice, stream_));
+    // the scene's error word and counters move with it
+    AE_TRY(cudaMemcpyAsync(err_ + 4 * dst, src->err_ + 4 * s, sizeof(uint32_t) * 4, cudaMemcpyDeviceToDevice, stream_));
     b.p_count = a.p_count;
     count_changed(dst);
     keys_stale_ = scatter_invalid_ = true;
