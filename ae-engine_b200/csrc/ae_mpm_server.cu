@@ -101,60 +101,6 @@ ae_mpm_particles staging_view(void* base, uint64_t n) {
 }
 size_t staging_bytes(uint64_t n) { return (26 * sizeof(float) + sizeof(uint16_t)) * n; }
 
-// Device memory of the server's worlds, from a pool of its own that keeps what a replaced world
-// gave back: rebuilding the world (growth, compaction) then reuses that memory instead of mapping
-// new pages for every array.  The pool is the server's; destroying the server returns it all.
-class PoolAlloc final : public aemp::DevAlloc {
- public:
-  explicit PoolAlloc(int device) {
-    cudaMemPoolProps props{};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.handleTypes = cudaMemHandleTypeNone;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = device;
-    ok_ = cudaMemPoolCreate(&pool_, &props) == cudaSuccess &&
-          cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking) == cudaSuccess;
-    if (ok_) {
-      uint64_t keep = UINT64_MAX;
-      cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep);
-    } else {
-      cudaGetLastError();
-    }
-  }
-  ~PoolAlloc() override {
-    if (s_) {
-      cudaStreamSynchronize(s_);
-      cudaStreamDestroy(s_);
-    }
-    if (pool_) cudaMemPoolDestroy(pool_);
-  }
-  cudaError_t alloc(void** p, size_t bytes) override {
-    if (!ok_) return cudaMalloc(p, bytes);
-    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool_, s_);
-    if (e == cudaErrorMemoryAllocation) {  // memory the pool kept but cannot fit: give it back, retry
-      cudaGetLastError();
-      cudaStreamSynchronize(s_);
-      cudaMemPoolTrimTo(pool_, 0);
-      e = cudaMallocFromPoolAsync(p, bytes, pool_, s_);
-    }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s_);  // usable from every stream from here on
-    return e;
-  }
-  void release(void* p) override {
-    if (!p) return;
-    if (!ok_) {
-      cudaFree(p);
-      return;
-    }
-    cudaFreeAsync(p, s_);  // the world released it after its own stream went idle
-  }
-
- private:
-  cudaMemPool_t pool_ = nullptr;
-  cudaStream_t s_ = nullptr;
-  bool ok_ = false;
-};
-
 struct Request {
   uint64_t id = 0;
   ae_mpm_scene_desc desc{};
@@ -236,7 +182,6 @@ struct ae_mpm_server {
   aemp::WorldBase* world = nullptr;
   uint64_t worlds_built = 0;
   PinnedPool* pool = &PinnedPool::process();
-  std::unique_ptr<PoolAlloc> dev_pool;  // device memory of the worlds (device thread)
   // host seconds of the device thread per phase, printed at destroy when AE_MPM_SERVER_PROFILE is
   // set: [admission, world rebuilds, uploads, queueing substeps, deliveries, waiting for the
   // device, finishing scenes (error words, downloads)]
@@ -408,8 +353,7 @@ struct ae_mpm_server {
     for (size_t i = 0; i < n_slots; ++i) descs[i] = slot_desc(slots[i], mats[i]);
     std::string why;
     int st = 0;
-    if (!dev_pool) dev_pool.reset(new PoolAlloc(device));
-    aemp::WorldBase* nw = aemp::make_world(descs.data(), uint32_t(n_slots), opts.exec, why, &st, dev_pool.get());
+    aemp::WorldBase* nw = aemp::make_world(descs.data(), uint32_t(n_slots), opts.exec, why, &st, nullptr);
     if (!nw) {
       fatal = why;
       return st ? st : AE_MPM_ECUDA;
@@ -607,7 +551,6 @@ struct ae_mpm_server {
     deliver();
     delete world;
     world = nullptr;
-    dev_pool.reset();
     if (std::getenv("AE_MPM_SERVER_PROFILE"))
       std::fprintf(stderr,
                    "ae_mpm_server: %llu ticks, %llu worlds built; seconds: admission %.3f rebuild %.3f upload %.3f "

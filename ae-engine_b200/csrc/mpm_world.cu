@@ -1080,6 +1080,81 @@ __device__ __forceinline__ bool g2p_physics_gather_sep(const Rows& rows, const S
   return true;
 }
 
+// The same separable gather in f32 with Blackwell's packed FMA (two lanes of a float2 per
+// instruction): the x and y components of each column sum and accumulator travel as one pair, z
+// alone.  Every pair op rounds like the scalar fused multiply-adds it replaces.
+template <class Rows>
+__device__ __forceinline__ bool g2p_physics_gather_sep_f2(const Rows& rows, const SceneDev<float>& sc, const float* x0,
+                                                          float* v, float* C) {
+  int b[3];
+  float w[3][3], e[3][3];
+  bool inside = true;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float X = (x0[a] - sc.origin[a]) * sc.inv_dx;
+    const int bb = floor_to_int(X - 0.5f);
+    const float fx = X - float(bb);
+    b[a] = bb;
+    inside = inside && bb >= 0 && bb + 2 < sc.n[a];
+    const float t0 = 1.5f - fx, t1 = fx - 1.0f, t2 = fx - 0.5f;
+    w[a][0] = 0.5f * t0 * t0;
+    w[a][1] = 0.75f - t1 * t1;
+    w[a][2] = 0.5f * t2 * t2;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) e[a][k] = w[a][k] * ((float(k) - fx) * sc.dx);
+  }
+  if (!inside) return false;
+  float2 wx[3], ex[3], wy[3], ey[3], wz[3], ez[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    wx[k] = make_float2(w[0][k], w[0][k]);
+    ex[k] = make_float2(e[0][k], e[0][k]);
+    wy[k] = make_float2(w[1][k], w[1][k]);
+    ey[k] = make_float2(e[1][k], e[1][k]);
+    wz[k] = make_float2(w[2][k], w[2][k]);
+    ez[k] = make_float2(e[2][k], e[2][k]);
+  }
+  float2 vxy = make_float2(0.f, 0.f), b0xy = vxy, b1xy = vxy, b2xy = vxy;
+  float vz = 0.f, b0z = 0.f, b1z = 0.f, b2z = 0.f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+#pragma unroll
+    for (int bb = 0; bb < 3; ++bb) {
+      const uint32_t r = rows.row(b[1] + bb, b[2] + c);
+      const float4 g0 = rows.at(r, b[0]), g1 = rows.at(r, b[0] + 1), g2 = rows.at(r, b[0] + 2);
+      const float2 g0xy = make_float2(g0.x, g0.y), g1xy = make_float2(g1.x, g1.y), g2xy = make_float2(g2.x, g2.y);
+      const float2 s0xy = __ffma2_rn(wx[2], g2xy, __ffma2_rn(wx[1], g1xy, __fmul2_rn(wx[0], g0xy)));
+      const float2 s1xy = __ffma2_rn(ex[2], g2xy, __ffma2_rn(ex[1], g1xy, __fmul2_rn(ex[0], g0xy)));
+      const float s0z = w[0][0] * g0.z + w[0][1] * g1.z + w[0][2] * g2.z;
+      const float s1z = e[0][0] * g0.z + e[0][1] * g1.z + e[0][2] * g2.z;
+      const float2 wbc = __fmul2_rn(wy[bb], wz[c]), ebc = __fmul2_rn(ey[bb], wz[c]), fbc = __fmul2_rn(wy[bb], ez[c]);
+      vxy = __ffma2_rn(wbc, s0xy, vxy);
+      b0xy = __ffma2_rn(wbc, s1xy, b0xy);
+      b1xy = __ffma2_rn(ebc, s0xy, b1xy);
+      b2xy = __ffma2_rn(fbc, s0xy, b2xy);
+      vz += wbc.x * s0z;
+      b0z += wbc.x * s1z;
+      b1z += ebc.x * s0z;
+      b2z += fbc.x * s0z;
+    }
+  }
+  const float cs = 4.0f * sc.inv_dx * sc.inv_dx;
+  v[0] = vxy.x;
+  v[1] = vxy.y;
+  v[2] = vz;
+  // B[k][col]: column col of the affine sum for velocity component k
+  C[0] = cs * b0xy.x;
+  C[1] = cs * b1xy.x;
+  C[2] = cs * b2xy.x;
+  C[3] = cs * b0xy.y;
+  C[4] = cs * b1xy.y;
+  C[5] = cs * b2xy.y;
+  C[6] = cs * b0z;
+  C[7] = cs * b1z;
+  C[8] = cs * b2z;
+  return true;
+}
+
 // gather half of the physics G2P: grid velocity and APIC C at the particle
 template <class T>
 __device__ __forceinline__ void g2p_physics_gather(const VelTile<T>& vt, const SceneDev<T>& sc, const T* x0, T* v,
@@ -1816,8 +1891,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) g2p2g_kernel(Worl
     const T x0[3] = {a0.x, a0.y, a0.z};
     G2POut<T> o;
     T pv[3] = {0, 0, 0};
-    const bool done = g2p_physics_gather_sep<T>(
-        GridRows<T>{w.vel, sc.blk_off, uint32_t(sc.nb[0]), uint32_t(sc.nb[1])}, sc, x0, pv, o.C);
+    bool done;
+    if constexpr (sizeof(T) == 4)
+      done = g2p_physics_gather_sep_f2(GridRows<T>{w.vel, sc.blk_off, uint32_t(sc.nb[0]), uint32_t(sc.nb[1])}, sc, x0,
+                                       pv, o.C);
+    else
+      done = g2p_physics_gather_sep<T>(GridRows<T>{w.vel, sc.blk_off, uint32_t(sc.nb[0]), uint32_t(sc.nb[1])}, sc, x0,
+                                       pv, o.C);
     if (!done) {  // stencil partly outside the grid (a particle's first substep)
       VelTile<T> vt;
       vt.tile = nullptr;
