@@ -150,6 +150,8 @@ SlotClass class_of(const ae_mpm_scene_desc& d, uint64_t n) {
 }
 uint64_t grid_blocks(const uint32_t* n) { return uint64_t((n[0] + 3) / 4) * ((n[1] + 3) / 4) * ((n[2] + 3) / 4) + 1; }
 
+constexpr uint64_t kCompactMin = uint64_t(1) << 22;  // particle capacity below which a world is not compacted
+
 struct Slot {
   SlotClass cls{};
   uint64_t bytes = 0;     // estimated device bytes of the slot
@@ -536,15 +538,16 @@ struct ae_mpm_server {
           running.erase(std::find(running.begin(), running.end(), r));
           outgoing.push_back(r);
         }
-        // A world whose slots stand mostly empty still sorts its whole capacity and launches a CTA
-        // per chunk of every slot each substep: with nothing waiting and under a quarter of the
-        // particle capacity in use, drop the vacant slots (the next tick rebuilds the world from
-        // the occupied ones).
+        // A large world whose slots stand mostly empty still sorts its whole capacity and launches
+        // a CTA per chunk of every slot each substep: with nothing waiting, a capacity above
+        // kCompactMin particles and under a quarter of it in use, drop the vacant slots (the next
+        // tick rebuilds the world from the occupied ones).  Small worlds are left alone: their
+        // empty slots cost less than the rebuild, and arrivals would grow them again.
         if (!done_now.empty() && waiting.empty() && !running.empty()) {
           uint64_t live = 0, cap = 0;
           for (const Slot& sl : slots) cap += sl.cls.particles;
           for (const Request* r : running) live += r->n;
-          if (4 * live < cap) compact();
+          if (cap > kCompactMin && 4 * live < cap) compact();
         }
       }
     }
