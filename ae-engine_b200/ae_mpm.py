@@ -177,6 +177,7 @@ SIGNATURES = {
     "ae_mpm_world_particles": (C.c_uint64, [_P]),
     "ae_mpm_radix_sort_keys": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, _P, _P]),
     "ae_mpm_radix_sort_keys_noalloc": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, _P, _P, _P]),
+    "ae_mpm_counting_sort_keys": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, _P, _P]),
     "ae_mpm_lod_classify": (C.c_int, [_P, _P, _P, C.c_uint64, _P, C.c_float, C.c_float, C.c_uint64, _P,
                                       C.POINTER(C.c_uint64), _P, C.POINTER(C.c_uint64), _P, C.POINTER(C.c_uint64)]),
     "ae_mpm_far_field_update": (C.c_int, [_P, _P, _P, _P, C.c_uint64, _P, C.c_uint64, _P, C.c_uint32, C.c_float, _P,
@@ -450,6 +451,15 @@ class Context:
         perm = np.empty_like(keys)
         self.check(self.lib.ae_mpm_radix_sort_keys(self.h, keys.ctypes.data, keys.size, key_bits,
                                                    sk.ctypes.data, perm.ctypes.data))
+        return sk, perm
+
+    def counting_sort(self, keys: np.ndarray, key_bits: int):
+        """Grouping sort of keys of at most 16 bits: ascending keys, equal keys in no defined order."""
+        keys = np.ascontiguousarray(keys, np.uint32)
+        sk = np.empty_like(keys)
+        perm = np.empty_like(keys)
+        self.check(self.lib.ae_mpm_counting_sort_keys(self.h, keys.ctypes.data, keys.size, key_bits,
+                                                      sk.ctypes.data, perm.ctypes.data))
         return sk, perm
 
 

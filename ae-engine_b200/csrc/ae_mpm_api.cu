@@ -626,12 +626,13 @@ void* ae_mpm_world_stream(ae_mpm_world* world) { return world ? static_cast<void
 
 uint64_t ae_mpm_world_particles(const ae_mpm_world* world) { return world ? world->w->particles() : 0; }
 
-int ae_mpm_radix_sort_keys(ae_mpm_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t key_bits,
-                           uint32_t* sorted_keys_out, uint32_t* perm_out) {
+static int host_sort(ae_mpm_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t key_bits, uint32_t* sorted_keys_out,
+                     uint32_t* perm_out, bool counting) {
   if (!ctx) return AE_MPM_EINVAL;
   if (n == 0) return AE_MPM_OK;
-  if (!keys || !sorted_keys_out || !perm_out || key_bits == 0 || key_bits > 32 || n >= (1ull << 32))
-    return fail(ctx, AE_MPM_EINVAL, "bad radix sort arguments");
+  if (!keys || !sorted_keys_out || !perm_out || key_bits == 0 || key_bits > (counting ? 16u : 32u) ||
+      n >= (1ull << 32))
+    return fail(ctx, AE_MPM_EINVAL, counting ? "bad counting sort arguments" : "bad radix sort arguments");
   int rc = set_device(ctx);
   if (rc) return rc;
   if (ctx->sort.n_cap < n) {
@@ -649,12 +650,25 @@ int ae_mpm_radix_sort_keys(ae_mpm_ctx* ctx, const uint32_t* keys, uint64_t n, ui
   cudaError_t e = cudaMemcpy(ctx->sort_keys, keys, sizeof(uint32_t) * n, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, cudaGetErrorString(e));
   const uint32_t *sk = nullptr, *pm = nullptr;
-  aemp::radix_sort_pairs(ctx->sort_keys, n, int(key_bits), ctx->sort, 0, &sk, &pm);
+  if (counting)
+    aemp::counting_sort_pairs(ctx->sort_keys, n, int(key_bits), ctx->sort, 0, &sk, &pm);
+  else
+    aemp::radix_sort_pairs(ctx->sort_keys, n, int(key_bits), ctx->sort, 0, &sk, &pm);
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpy(sorted_keys_out, sk, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(perm_out, pm, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, cudaGetErrorString(e));
   return AE_MPM_OK;
+}
+
+int ae_mpm_radix_sort_keys(ae_mpm_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t key_bits,
+                           uint32_t* sorted_keys_out, uint32_t* perm_out) {
+  return host_sort(ctx, keys, n, key_bits, sorted_keys_out, perm_out, false);
+}
+
+int ae_mpm_counting_sort_keys(ae_mpm_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t key_bits,
+                              uint32_t* sorted_keys_out, uint32_t* perm_out) {
+  return host_sort(ctx, keys, n, key_bits, sorted_keys_out, perm_out, true);
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -558,6 +558,29 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) p2g_lanes_kernel(
     if (uint32_t(run.w) == 0xffffffffu) continue;
     const int X = run.x, Y = run.y + nb, Z = run.z + nc;
     T m0 = 0, x0 = 0, y0 = 0, z0 = 0, m1 = 0, x1 = 0, y1 = 0, z1 = 0, m2 = 0, x2 = 0, y2 = 0, z2 = 0;
+    if constexpr (sizeof(T) == 4) {  // x and y of each node as one packed pair
+      float2 q0 = make_float2(0.f, 0.f), q1 = q0, q2 = q0;
+#pragma unroll 2
+      for (int i = s0 + grp; i < e0; i += 3) {
+        const float4 u = colw[i * 9];
+        const float4 r = wxw[i];
+        const float4 a = acw[i];
+        const float W0 = r.x * u.w, W1 = r.y * u.w, W2 = r.z * u.w;
+        const float2 axy = make_float2(a.x, a.y), u0 = make_float2(u.x, u.y);
+        const float2 u1 = __fadd2_rn(u0, axy), u2 = __fadd2_rn(u1, axy);
+        m0 += W0 * r.w;
+        m1 += W1 * r.w;
+        m2 += W2 * r.w;
+        q0 = __ffma2_rn(make_float2(W0, W0), u0, q0);
+        q1 = __ffma2_rn(make_float2(W1, W1), u1, q1);
+        q2 = __ffma2_rn(make_float2(W2, W2), u2, q2);
+        const float uz1 = u.z + a.z;
+        z0 += W0 * u.z;
+        z1 += W1 * uz1;
+        z2 += W2 * (uz1 + a.z);
+      }
+      x0 = q0.x, y0 = q0.y, x1 = q1.x, y1 = q1.y, x2 = q2.x, y2 = q2.y;
+    } else
 #pragma unroll 2
     for (int i = s0 + grp; i < e0; i += 3) {
       const V4 u = colw[i * 9];
@@ -1021,6 +1044,15 @@ struct GridRows {
   __device__ __forceinline__ V4 at(uint32_t r, int X) const {
     return ld4(vel + (r + ((uint32_t(X >> 2) << 6) | uint32_t(X & 3))));
   }
+  // row(Y, Z) == zpart(Z) + ypart(Y), and the node index of (X, Y, Z) == row + xpart(X)
+  __device__ __forceinline__ uint32_t xpart(int X) const { return (uint32_t(X >> 2) << 6) | uint32_t(X & 3); }
+  __device__ __forceinline__ uint32_t ypart(int Y) const {
+    return ((uint32_t(Y >> 2) * nb0) << 6) | (uint32_t(Y & 3) << 2);
+  }
+  __device__ __forceinline__ uint32_t zpart(int Z) const {
+    return ((blk_off + uint32_t(Z >> 2) * nb1 * nb0) << 6) | (uint32_t(Z & 3) << 4);
+  }
+  __device__ __forceinline__ V4 at_part(uint32_t r, uint32_t xp) const { return ld4(vel + (r + xp)); }
 };
 // Physics gather for a particle whose 27 stencil nodes are all inside the grid (every particle
 // after its first substep: positions are clamped to [1, n-2] dx).  Separable: each (y,z) column
@@ -1116,12 +1148,21 @@ __device__ __forceinline__ bool g2p_physics_gather_sep_f2(const Rows& rows, cons
   }
   float2 vxy = make_float2(0.f, 0.f), b0xy = vxy, b1xy = vxy, b2xy = vxy;
   float vz = 0.f, b0z = 0.f, b1z = 0.f, b2z = 0.f;
+  // node index = z part + y part + x part: the three bit fields of the block-major index are
+  // disjoint, so the 27 indexes come from 3 + 3 + 3 parts with one add each
+  uint32_t xp[3], yp[3], zp[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    xp[k] = rows.xpart(b[0] + k);
+    yp[k] = rows.ypart(b[1] + k);
+    zp[k] = rows.zpart(b[2] + k);
+  }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
 #pragma unroll
     for (int bb = 0; bb < 3; ++bb) {
-      const uint32_t r = rows.row(b[1] + bb, b[2] + c);
-      const float4 g0 = rows.at(r, b[0]), g1 = rows.at(r, b[0] + 1), g2 = rows.at(r, b[0] + 2);
+      const uint32_t r = zp[c] + yp[bb];
+      const float4 g0 = rows.at_part(r, xp[0]), g1 = rows.at_part(r, xp[1]), g2 = rows.at_part(r, xp[2]);
       const float2 g0xy = make_float2(g0.x, g0.y), g1xy = make_float2(g1.x, g1.y), g2xy = make_float2(g2.x, g2.y);
       const float2 s0xy = __ffma2_rn(wx[2], g2xy, __ffma2_rn(wx[1], g1xy, __fmul2_rn(wx[0], g0xy)));
       const float2 s1xy = __ffma2_rn(ex[2], g2xy, __ffma2_rn(ex[1], g1xy, __fmul2_rn(ex[0], g0xy)));
@@ -1777,15 +1818,31 @@ __device__ __forceinline__ void p2g_warp_scatter(const WorldDev<T>& w, const Sce
       const T fa = T(xa);
       const V4* cn = st.col + jn;
       T m = 0, px = 0, py = 0, pz = 0;
-      for (int i = s0; i < e0; ++i) {
-        const V4 u = cn[i * 9];
-        const V4 r = st.wxm[i];
-        const V4 a = st.acol[i];
-        const T W = (xa == 0 ? r.x : (xa == 1 ? r.y : r.z)) * u.w;
-        m += W * r.w;
-        px += W * (u.x + fa * a.x);
-        py += W * (u.y + fa * a.y);
-        pz += W * (u.z + fa * a.z);
+      if constexpr (sizeof(T) == 4) {  // x and y as one packed pair
+        float2 pxy = make_float2(0.f, 0.f);
+        const float2 fa2 = make_float2(fa, fa);
+        for (int i = s0; i < e0; ++i) {
+          const float4 u = cn[i * 9];
+          const float4 r = st.wxm[i];
+          const float4 a = st.acol[i];
+          const float W = (xa == 0 ? r.x : (xa == 1 ? r.y : r.z)) * u.w;
+          m += W * r.w;
+          pxy = __ffma2_rn(make_float2(W, W), __ffma2_rn(fa2, make_float2(a.x, a.y), make_float2(u.x, u.y)), pxy);
+          pz += W * (u.z + fa * a.z);
+        }
+        px = pxy.x;
+        py = pxy.y;
+      } else {
+        for (int i = s0; i < e0; ++i) {
+          const V4 u = cn[i * 9];
+          const V4 r = st.wxm[i];
+          const V4 a = st.acol[i];
+          const T W = (xa == 0 ? r.x : (xa == 1 ? r.y : r.z)) * u.w;
+          m += W * r.w;
+          px += W * (u.x + fa * a.x);
+          py += W * (u.y + fa * a.y);
+          pz += W * (u.z + fa * a.z);
+        }
       }
       if (lane < 27 && m != T(0)) {
         const int Xn = run.x + xa, Yn = run.y + jn % 3, Zn = run.z + jn / 3;
@@ -1806,6 +1863,29 @@ __device__ __forceinline__ void p2g_warp_scatter(const WorldDev<T>& w, const Sce
     }
     const int X = run.x, Y = run.y + nb, Z = run.z + nc;
     T m0 = 0, x0 = 0, y0 = 0, z0 = 0, m1 = 0, x1 = 0, y1 = 0, z1 = 0, m2 = 0, x2 = 0, y2 = 0, z2 = 0;
+    if constexpr (sizeof(T) == 4) {  // x and y of each node as one packed pair
+      float2 q0 = make_float2(0.f, 0.f), q1 = q0, q2 = q0;
+#pragma unroll 2
+      for (int i = s0 + grp; i < e0; i += 3) {
+        const float4 u = colw[i * 9];
+        const float4 r = st.wxm[i];
+        const float4 a = st.acol[i];
+        const float W0 = r.x * u.w, W1 = r.y * u.w, W2 = r.z * u.w;
+        const float2 axy = make_float2(a.x, a.y), u0 = make_float2(u.x, u.y);
+        const float2 u1 = __fadd2_rn(u0, axy), u2 = __fadd2_rn(u1, axy);
+        m0 += W0 * r.w;
+        m1 += W1 * r.w;
+        m2 += W2 * r.w;
+        q0 = __ffma2_rn(make_float2(W0, W0), u0, q0);
+        q1 = __ffma2_rn(make_float2(W1, W1), u1, q1);
+        q2 = __ffma2_rn(make_float2(W2, W2), u2, q2);
+        const float uz1 = u.z + a.z;
+        z0 += W0 * u.z;
+        z1 += W1 * uz1;
+        z2 += W2 * (uz1 + a.z);
+      }
+      x0 = q0.x, y0 = q0.y, x1 = q1.x, y1 = q1.y, x2 = q2.x, y2 = q2.y;
+    } else
 #pragma unroll 2
     for (int i = s0 + grp; i < e0; i += 3) {
       const V4 u = colw[i * 9];
@@ -3462,7 +3542,12 @@ class World final : public WorldBase {
           WorldDev<T> wk = dev(false);
           launch_init_keys(wk);
         }
-        launches_ += radix_sort_pairs(keys_, total_cap_, key_bits_, sort_, stream_, &sorted_keys_, &perm_);
+        // keys of a small grid in a mode whose results do not depend on the order of equal keys:
+        // one counting pass instead of two radix passes
+        if (!opts_.deterministic && key_bits_ <= kCountingSortBits && total_cap_ > uint64_t(kSmallSortMax))
+          launches_ += counting_sort_pairs(keys_, total_cap_, key_bits_, sort_, stream_, &sorted_keys_, &perm_);
+        else
+          launches_ += radix_sort_pairs(keys_, total_cap_, key_bits_, sort_, stream_, &sorted_keys_, &perm_);
       }
       mark(1);
       WorldDev<T> w = dev(do_sort);

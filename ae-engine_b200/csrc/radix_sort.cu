@@ -263,6 +263,94 @@ __global__ void __launch_bounds__(kSmallThreads, 1) sort_small(const uint32_t* _
   }
 }
 
+// ---- one-pass counting sort (keys of at most kCountingSortBits bits) ------------------------------
+constexpr int kCountThreads = 256;
+
+__global__ void __launch_bounds__(kCountThreads) count_hist(const uint32_t* __restrict__ keys, uint64_t n, uint32_t mask,
+                                                            uint32_t* __restrict__ bins) {
+  const int lane = threadIdx.x & 31;
+  for (uint64_t base = uint64_t(blockIdx.x) * kCountThreads; base < n; base += uint64_t(gridDim.x) * kCountThreads) {
+    const uint64_t i = base + threadIdx.x;
+    const bool valid = i < n;
+    const uint32_t k = valid ? (__ldg(keys + i) & mask) : 0xffffffffu;
+    const uint32_t peers = __match_any_sync(0xffffffffu, k);  // one atomic per key per warp
+    if (valid && lane == __ffs(peers) - 1) atomicAdd(bins + k, uint32_t(__popc(peers)));
+  }
+}
+
+// exclusive scan of nb bins in place, one CTA of 1024 threads.  Warp w owns the contiguous
+// segment [w*seg, w*seg + seg) (seg a multiple of 32); a pass of coalesced loads sums each segment,
+// a scan over the 32 segment sums gives each warp its carry, and a second pass scans the segment
+// 32 bins at a time.  Loads go in batches of kScanBatch rows so that many are in flight at once
+// (the bins are in L2, just written by the histogram).
+constexpr int kScanBatch = 16;
+
+__global__ void __launch_bounds__(1024) count_scan(uint32_t* bins, uint32_t nb) {
+  __shared__ uint32_t wsum[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t seg = ((nb + 1023u) / 1024u) * 32u;
+  const uint32_t lo = uint32_t(w) * seg, hi = lo + seg < nb ? lo + seg : nb;
+  uint32_t s = 0;
+  for (uint32_t base = lo; base < hi; base += 32u * kScanBatch) {
+    uint32_t x[kScanBatch];
+#pragma unroll
+    for (int k = 0; k < kScanBatch; ++k) {
+      const uint32_t i = base + 32u * k + lane;
+      x[k] = i < hi ? bins[i] : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kScanBatch; ++k) s += x[k];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) wsum[w] = s;
+  __syncthreads();
+  if (w == 0) {
+    const uint32_t ws = wsum[lane];
+    wsum[lane] = warp_incl_scan(ws, lane) - ws;
+  }
+  __syncthreads();
+  uint32_t carry = wsum[w];
+  for (uint32_t base = lo; base < hi; base += 32u * kScanBatch) {
+    uint32_t x[kScanBatch];
+#pragma unroll
+    for (int k = 0; k < kScanBatch; ++k) {
+      const uint32_t i = base + 32u * k + lane;
+      x[k] = i < hi ? bins[i] : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kScanBatch; ++k) {
+      const uint32_t i = base + 32u * k + lane;
+      const uint32_t incl = warp_incl_scan(x[k], lane);
+      if (i < hi) bins[i] = carry + incl - x[k];
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kCountThreads) count_scatter(const uint32_t* __restrict__ keys, uint64_t n,
+                                                               uint32_t mask, uint32_t* __restrict__ bins,
+                                                               uint32_t* __restrict__ keys_out,
+                                                               uint32_t* __restrict__ perm_out) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t lt = lanemask_lt();
+  for (uint64_t base = uint64_t(blockIdx.x) * kCountThreads; base < n; base += uint64_t(gridDim.x) * kCountThreads) {
+    const uint64_t i = base + threadIdx.x;
+    const bool valid = i < n;
+    const uint32_t k = valid ? __ldg(keys + i) : 0xffffffffu;
+    const uint32_t d = valid ? (k & mask) : 0xffffffffu;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const int leader = __ffs(peers) - 1;
+    uint32_t pos = 0;
+    if (valid && lane == leader) pos = atomicAdd(bins + d, uint32_t(__popc(peers)));
+    pos = __shfl_sync(0xffffffffu, pos, leader) + __popc(peers & lt);
+    if (valid) {
+      keys_out[pos] = k;
+      perm_out[pos] = uint32_t(i);
+    }
+  }
+}
+
 }  // namespace
 
 cudaError_t sort_scratch_alloc(SortScratch& s, uint64_t n, SortAllocFn alloc, void* user) {
@@ -281,12 +369,13 @@ cudaError_t sort_scratch_alloc(SortScratch& s, uint64_t n, SortAllocFn alloc, vo
   if ((e = A(&s.keys_alt, sizeof(uint32_t) * m)) != cudaSuccess) return e;
   if ((e = A(&s.vals_a, sizeof(uint32_t) * m)) != cudaSuccess) return e;
   if ((e = A(&s.vals_b, sizeof(uint32_t) * m)) != cudaSuccess) return e;
+  if (n > uint64_t(kSmallSortMax) && (e = A(&s.bins, sizeof(uint32_t) << kCountingSortBits)) != cudaSuccess) return e;
   s.n_cap = n;
   return cudaSuccess;
 }
 
 void sort_scratch_free(SortScratch& s, SortFreeFn release, void* user) {
-  uint32_t* ps[6] = {s.hist, s.offsets, s.totals, s.keys_alt, s.vals_a, s.vals_b};
+  uint32_t* ps[7] = {s.hist, s.offsets, s.totals, s.keys_alt, s.vals_a, s.vals_b, s.bins};
   for (uint32_t* p : ps)
     if (p) {
       if (release)
@@ -372,6 +461,32 @@ int radix_sort_pairs_into(const uint32_t* keys_in, uint64_t n, int key_bits, uin
     vin = vout;
   }
   return launches;
+}
+
+}  // namespace aemp
+
+namespace aemp {
+
+int counting_sort_pairs(uint32_t* keys, uint64_t n, int key_bits, SortScratch& s, cudaStream_t stream,
+                        const uint32_t** sorted_keys_out, const uint32_t** perm_out) {
+  *sorted_keys_out = s.keys_alt;
+  *perm_out = s.vals_a;
+  if (n == 0) return 0;
+  // short lists sort in one CTA (stable and cheaper); wide keys need the radix passes
+  if (n <= uint64_t(kSmallSortMax) || key_bits > kCountingSortBits || !s.bins)
+    return radix_sort_pairs(keys, n, key_bits, s, stream, sorted_keys_out, perm_out);
+  if (key_bits < 1) key_bits = 1;
+  const uint32_t nb = 1u << key_bits, mask = nb - 1u;
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint64_t want = (n + kCountThreads - 1) / kCountThreads;
+  const unsigned grid = unsigned(want < uint64_t(sms) * 8 ? want : uint64_t(sms) * 8);
+  cudaMemsetAsync(s.bins, 0, sizeof(uint32_t) * nb, stream);
+  count_hist<<<grid, kCountThreads, 0, stream>>>(keys, n, mask, s.bins);
+  count_scan<<<1, 1024, 0, stream>>>(s.bins, nb);
+  count_scatter<<<grid, kCountThreads, 0, stream>>>(keys, n, mask, s.bins, s.keys_alt, s.vals_a);
+  return 3;
 }
 
 }  // namespace aemp

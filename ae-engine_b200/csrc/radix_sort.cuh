@@ -25,6 +25,7 @@ constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per block
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kMaxRadix = 256;
 constexpr int kSmallSortMax = 16384;  // radix_sort_pairs sorts up to this many keys in one CTA
+constexpr int kCountingSortBits = 16;  // counting_sort_pairs takes keys of at most this many bits
 
 struct SortPlan {
   int passes;
@@ -56,6 +57,7 @@ struct SortScratch {
   uint32_t* keys_alt = nullptr; // [n]
   uint32_t* vals_a = nullptr;   // [n]
   uint32_t* vals_b = nullptr;   // [n]
+  uint32_t* bins = nullptr;     // [1 << kCountingSortBits] (counting sort; allocated for n > kSmallSortMax)
   uint64_t n_cap = 0;
 };
 
@@ -75,6 +77,16 @@ void sort_scratch_free(SortScratch& s, SortFreeFn release = nullptr, void* user 
 // kSmallSortMax); returns the launch count.
 int radix_sort_pairs(uint32_t* keys, uint64_t n, int key_bits, SortScratch& s, cudaStream_t stream,
                      const uint32_t** sorted_keys_out, const uint32_t** perm_out);
+
+// Groups keys[0..n) by key in one pass (key_bits <= kCountingSortBits): a histogram, one scan
+// over the 2^key_bits bins and a scatter that claims places with atomics.  The keys come out
+// sorted, but equal keys in no defined order (the order atomics give them), so only callers whose
+// results do not depend on that order may use it.  Same outputs and lifetime rules as
+// radix_sort_pairs.  n <= kSmallSortMax, wider keys or scratch without bins go to
+// radix_sort_pairs (which clobbers `keys`); the counting pass itself only reads them.  Returns the
+// launch count.
+int counting_sort_pairs(uint32_t* keys, uint64_t n, int key_bits, SortScratch& s, cudaStream_t stream,
+                        const uint32_t** sorted_keys_out, const uint32_t** perm_out);
 
 // Same sort with every buffer supplied by the caller: keys_in is only read; the result lands in
 // keys_out / vals_out; keys_alt / vals_alt (n entries each), hist and offsets (kMaxRadix *

@@ -552,10 +552,12 @@ def run_midfield(args, rank, local, world_size, pg, reference=False):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(pg)
     torch.cuda.synchronize(local)
+    timed_range(torch, True)
     e0.record(stream)
     world.step(args.steps)
     e1.record(stream)
     e1.synchronize()
+    timed_range(torch, False)
     world.sync(raise_on_error=False)
     launches = world.launches()
     ms = max_over_ranks(pg, e0.elapsed_time(e1))

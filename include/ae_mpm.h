@@ -293,6 +293,14 @@ uint64_t ae_mpm_world_particles(const ae_mpm_world* world);
 int ae_mpm_radix_sort_keys(ae_mpm_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t key_bits,
                            uint32_t* sorted_keys_out, uint32_t* perm_out);
 
+/* The grouping sort that non-deterministic worlds with keys of at most 16 bits use (a 32^3 grid):
+ * one histogram, one scan and one scatter instead of radix passes.  Same buffers as
+ * ae_mpm_radix_sort_keys; sorted_keys_out comes out ascending, but equal keys in no defined order,
+ * and perm_out is a permutation with keys[perm_out[i]] == sorted_keys_out[i].  Up to 16384 keys the
+ * call sorts stably in one CTA.  key_bits above 16 is AE_MPM_EINVAL.  No reference counterpart. */
+int ae_mpm_counting_sort_keys(ae_mpm_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t key_bits,
+                              uint32_t* sorted_keys_out, uint32_t* perm_out);
+
 /* The same sort for callers that cannot allocate GPU memory: an engine frame loop living on
  * memory it reserved up front, work queued during CUDA stream capture, a host whose own pool owns
  * all of HBM.  This entry point has no counterpart in the reference.  keys_dev, sorted_keys_dev

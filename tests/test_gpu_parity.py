@@ -76,6 +76,34 @@ def test_radix_sort_empty(ctx):
     assert sk.size == 0 and perm.size == 0
 
 
+# the grouping sort of non-deterministic worlds with keys of at most 16 bits: keys ascending and
+# bit-exact, the permutation a permutation that reproduces them (equal keys in any order)
+@pytest.mark.parametrize("n,bits,kind", [
+    (1, 4, "random"), (16384, 15, "random"), (16385, 15, "random"), (490045, 15, "random"), (490045, 15, "sorted"),
+    (100000, 16, "random"), (100003, 16, "equal"), (200000, 1, "random"), (65536, 9, "random"),
+    (2000001, 16, "sorted"), (30000, 3, "random"),
+])
+def test_counting_sort_groups_keys(ctx, n, bits, kind):
+    rng = np.random.default_rng(3 * n + bits)
+    if kind == "equal":
+        keys = np.full(n, 54321 & ((1 << bits) - 1), np.uint32)
+    else:
+        keys = rng.integers(0, 1 << bits, n, dtype=np.uint64).astype(np.uint32)
+        if kind == "sorted":
+            keys = np.sort(keys)
+    keys |= np.uint32(0xA5A50000)  # bits above key_bits are carried, not compared
+    sk, perm = ctx.counting_sort(keys, bits)
+    mask = np.uint32((1 << bits) - 1)
+    assert np.array_equal(np.sort(perm), np.arange(n, dtype=np.uint32))
+    assert np.array_equal(sk, keys[perm])
+    assert np.array_equal(sk & mask, np.sort(keys & mask))
+
+
+def test_counting_sort_rejects_wide_keys(ctx):
+    with pytest.raises(M.MpmError):
+        ctx.counting_sort(np.zeros(100000, np.uint32), 17)
+
+
 # ------------------------------------------------------------------ physics mode parity
 @pytest.mark.parametrize("variant", [M.P2G_TILE, M.P2G_WARP_AGG, M.P2G_GLOBAL, M.P2G_LANES])
 def test_physics_jelly_matches_fp64_oracle(ctx, variant):
@@ -87,6 +115,20 @@ def test_physics_jelly_matches_fp64_oracle(ctx, variant):
     assert rel(g.vel, ref.vel) <= 1e-3
     assert rel(g.F, ref.F) <= 1e-4
     assert np.array_equal(g.mat, p.mat) and np.array_equal(g.mass, p.mass)
+
+
+def test_physics_dense_small_grid_matches_fp64_oracle(ctx):
+    # 40 000 particles on a 32^3 grid: 15-bit cell keys over more than one CTA's worth of particles,
+    # so the non-deterministic world groups them with the counting sort (the deterministic one
+    # keeps the stable radix sort); both held to the FP64 oracle
+    sc, p = S.tiny_scene(40000, 32, S.jelly(), v=(0.7, -0.2, 0.3))
+    ref = p.astype(np.float64)
+    O.run(sc, ref, 20)
+    for det in (0, 1):
+        g = run_gpu(ctx, sc, p, 20, deterministic=det)
+        assert rel(g.pos, ref.pos) <= 1e-5, det
+        assert rel(g.vel, ref.vel) <= 1e-3, det
+        assert rel(g.F, ref.F) <= 1e-4, det
 
 
 def test_physics_fp64_kernels_match_fp64_oracle(ctx):
@@ -309,6 +351,22 @@ def test_dropin_velocity_only_matches_oracle(ctx, pattern):
     assert np.array_equal(a.F, p.F) and np.array_equal(a.C, p.C) and np.array_equal(a.J, p.J)
     untouched = np.setdiff1d(np.arange(p.n), idx.astype(np.int64))
     assert np.array_equal(a.pos[untouched], p.pos[untouched]) and np.array_equal(a.vel[untouched], p.vel[untouched])
+
+
+def test_dropin_velocity_only_at_mid_field_size_matches_oracle(ctx):
+    # the engine's mid-field call at full size: 490 045 mid particles of a 1 000 055-particle buffer
+    # on a 32^3 grid (15-bit keys: the call groups particles with the counting sort)
+    import bench as B
+
+    p, idx, g, cfg = B.midfield_setup(0xAE06)
+    a, b = p.copy(), p.copy()
+    ctx.step_velocity_only_parallel(a, g, cfg, 0.2, idx)
+    assert O.step_velocity_only_parallel(b, g, cfg, 0.2, idx, threads=os.cpu_count() or 1) == 0
+    ii = idx.astype(np.int64)
+    assert rel(a.pos[ii], b.pos[ii]) <= 2e-5
+    assert rel(a.vel[ii], b.vel[ii]) <= 1e-4
+    rest = np.setdiff1d(np.arange(p.n), ii)
+    assert np.array_equal(a.pos[rest], p.pos[rest]) and np.array_equal(a.vel[rest], p.vel[rest])
 
 
 @pytest.mark.parametrize("pattern", ["every_other", "sparse", "descending"])
