@@ -169,6 +169,11 @@ SIGNATURES = {
     "ae_mpm_world_download_f64": (C.c_int, [_P, C.c_uint32, C.POINTER(ParticlesView)]),
     "ae_mpm_world_upload_many": (C.c_int, [_P, C.c_uint32, _P, _P, _P]),
     "ae_mpm_world_download_many": (C.c_int, [_P, C.c_uint32, _P, _P]),
+    "ae_mpm_batch_create": (C.c_int, [_P, C.POINTER(SceneDesc), C.c_uint32, C.POINTER(ExecOpts), C.c_uint32,
+                                      C.POINTER(_P)]),
+    "ae_mpm_batch_run": (C.c_int, [_P, _P, _P, _P, C.c_uint32]),
+    "ae_mpm_batch_groups": (C.c_uint32, [_P, _P]),
+    "ae_mpm_batch_destroy": (C.c_int, [_P]),
     "ae_mpm_world_totals": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_double)]),
     "ae_mpm_world_errors": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
     "ae_mpm_world_launch_count": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
@@ -572,6 +577,67 @@ class World:
         r = TuneResult()
         self.ctx.check(self.ctx.lib.ae_mpm_world_autotune(self.h, substeps_per_trial, C.byref(r)))
         return r
+
+
+class ViewArray:
+    """Views of a list of float32 Particles for the many-scene calls, built once: callers that
+    pass the same buffers call after call save rebuilding them.  Holds the particles alive; the
+    views stay valid while their arrays are not replaced (in-place writes are fine)."""
+
+    def __init__(self, parts):
+        self.parts = list(parts)
+        k = len(self.parts)
+        self.arr = (ParticlesView * max(k, 1))(*[p.view() for p in self.parts])
+        self.counts = np.ascontiguousarray([p.n for p in self.parts], np.uint64)
+
+    def __len__(self):
+        return len(self.parts)
+
+
+class Batch:
+    """Pipelined batch (ae_mpm_batch_*): scenes in host memory advanced n substeps per run, in
+    `groups` consecutive groups whose PCIe copies overlap the other groups' substeps."""
+
+    def __init__(self, ctx: Context, scenes, opts: ExecOpts | None = None, groups: int = 4):
+        self.ctx = ctx
+        self.scenes = list(scenes)
+        descs = (SceneDesc * len(self.scenes))(*[s.desc() for s in self.scenes])
+        h = C.c_void_p()
+        ctx.check(ctx.lib.ae_mpm_batch_create(ctx.h, descs, len(self.scenes),
+                                              C.byref(opts) if opts is not None else None, groups, C.byref(h)))
+        self.h = h
+
+    def groups(self):
+        """First scene of every group, then the scene count."""
+        n = self.ctx.lib.ae_mpm_batch_groups(self.h, None)
+        first = np.zeros(n + 1, np.uint32)
+        self.ctx.lib.ae_mpm_batch_groups(self.h, first.ctypes.data)
+        return [int(x) for x in first]
+
+    def run(self, parts, n_substeps: int, out=None, raise_on_error: bool = True) -> int:
+        """Scene i takes parts[i] (float32 Particles, or a ViewArray of them), runs n_substeps and
+        lands in out[i] (parts itself when out is None).  Returns the status code (raises on
+        errors unless told not to; every result is written either way)."""
+        vin = parts if isinstance(parts, ViewArray) else ViewArray(parts)
+        vout = vin if out is None else (out if isinstance(out, ViewArray) else ViewArray(out))
+        if len(vin) != len(self.scenes) or len(vout) != len(self.scenes):
+            raise ValueError("one input and one output per scene")
+        rc = self.ctx.lib.ae_mpm_batch_run(self.h, C.addressof(vin.arr), vin.counts.ctypes.data,
+                                           C.addressof(vout.arr), n_substeps)
+        if rc != OK and (raise_on_error or rc not in (ENAN, EDOMAIN)):
+            self.ctx.check(rc)
+        return rc
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.ae_mpm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Server:

@@ -9,6 +9,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <omp.h>
 #include <map>
@@ -527,13 +529,9 @@ int ae_mpm_grid_download(ae_mpm_ctx* ctx, float* mass, float* vel, uint64_t n_no
   return rc ? fail(ctx, rc, ctx->dropin->err) : AE_MPM_OK;
 }
 
-int ae_mpm_world_create(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32_t n_scenes,
-                        const ae_mpm_exec_opts* opts, ae_mpm_world** out) {
-  if (!ctx || !out) return AE_MPM_EINVAL;
-  *out = nullptr;
-  if (!scenes || n_scenes == 0) return fail(ctx, AE_MPM_EINVAL, "no scenes");
-  int rc = set_device(ctx);
-  if (rc) return rc;
+// the caller's options (or the defaults) with the autotuner's choice for this workload, if any
+static ae_mpm_exec_opts resolve_opts(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32_t n_scenes,
+                                     const ae_mpm_exec_opts* opts) {
   ae_mpm_exec_opts o;
   if (opts)
     o = *opts;
@@ -548,6 +546,17 @@ int ae_mpm_world_create(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32
   }
   if (o.p2g_variant == AE_MPM_P2G_AUTO) o.p2g_variant = AE_MPM_P2G_LANES;
   if (o.block_threads == 0) o.block_threads = 256;
+  return o;
+}
+
+int ae_mpm_world_create(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32_t n_scenes,
+                        const ae_mpm_exec_opts* opts, ae_mpm_world** out) {
+  if (!ctx || !out) return AE_MPM_EINVAL;
+  *out = nullptr;
+  if (!scenes || n_scenes == 0) return fail(ctx, AE_MPM_EINVAL, "no scenes");
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  const ae_mpm_exec_opts o = resolve_opts(ctx, scenes, n_scenes, opts);
   std::string why;
   int st = 0;
   WorldBase* w = aemp::make_world(scenes, n_scenes, o, why, &st);
@@ -603,6 +612,185 @@ int ae_mpm_world_upload_many(ae_mpm_world* world, uint32_t n, const uint32_t* sc
 int ae_mpm_world_download_many(ae_mpm_world* world, uint32_t n, const uint32_t* scenes, ae_mpm_particles* views) {
   AE_WORLD_CALL(world->w->download_many(n, scenes, views));
 }
+// ---------------------------------------------------------------------------------------------
+// pipelined batch: the scenes of one call in consecutive groups, one world per group
+// ---------------------------------------------------------------------------------------------
+struct ae_mpm_batch {
+  ae_mpm_ctx* ctx = nullptr;
+  std::vector<WorldBase*> worlds;
+  std::vector<uint32_t> first;  // group g holds scenes [first[g], first[g + 1])
+  cudaStream_t up = nullptr, down = nullptr;
+  std::vector<cudaEvent_t> done;  // group g's substeps have finished
+  ~ae_mpm_batch() {
+    if (down) cudaStreamSynchronize(down);
+    for (WorldBase* w : worlds) delete w;
+    for (cudaEvent_t e : done)
+      if (e) cudaEventDestroy(e);
+    if (up) cudaStreamDestroy(up);
+    if (down) cudaStreamDestroy(down);
+  }
+};
+
+int ae_mpm_batch_create(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32_t n_scenes,
+                        const ae_mpm_exec_opts* opts, uint32_t n_groups, ae_mpm_batch** out) {
+  if (!ctx || !out) return AE_MPM_EINVAL;
+  *out = nullptr;
+  if (!scenes || n_scenes == 0) return fail(ctx, AE_MPM_EINVAL, "no scenes");
+  if (opts && opts->precision == 64) return fail(ctx, AE_MPM_EINVAL, "a batch runs f32 worlds");
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  const uint32_t g_n = n_groups == 0 ? 1u : (n_groups > n_scenes ? n_scenes : n_groups);
+  // consecutive groups of about equal particle capacity, none empty
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < n_scenes; ++i) total += scenes[i].max_particles;
+  std::vector<uint32_t> first(1, 0u);
+  uint64_t acc = 0;
+  for (uint32_t i = 0; i < n_scenes && first.size() < g_n; ++i) {
+    acc += scenes[i].max_particles;
+    const uint32_t g = uint32_t(first.size());  // the boundary after group g - 1
+    const bool left_enough = n_scenes - (i + 1) >= g_n - g;
+    if (left_enough && acc * g_n >= total * g) first.push_back(i + 1);
+  }
+  while (first.size() < g_n) first.push_back(first.back() + 1);  // capacity-free tail scenes
+  first.push_back(n_scenes);
+  auto* b = new ae_mpm_batch;
+  b->ctx = ctx;
+  b->first = first;
+  cudaError_t e = cudaStreamCreateWithFlags(&b->up, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->down, cudaStreamNonBlocking);
+  b->done.assign(g_n, nullptr);
+  for (uint32_t g = 0; g < g_n && e == cudaSuccess; ++g) e = cudaEventCreateWithFlags(&b->done[g], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    delete b;
+    return fail(ctx, AE_MPM_ECUDA, cudaGetErrorString(e));
+  }
+  int least = 0, greatest = 0;  // numerically: greatest <= least
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  for (uint32_t g = 0; g < g_n; ++g) {
+    const uint32_t k = first[g + 1] - first[g];
+    const ae_mpm_exec_opts o = resolve_opts(ctx, scenes + first[g], k, opts);
+    std::string why;
+    int st = 0;
+    WorldBase* w = aemp::make_world(scenes + first[g], k, o, why, &st);
+    if (!w) {
+      delete b;
+      return fail(ctx, st ? st : AE_MPM_ECUDA, "batch group " + std::to_string(g) + ": " + why);
+    }
+    b->worlds.push_back(w);
+    // earlier groups on higher stream priorities: the GPU serves group g first and fills its
+    // kernels' launch gaps and tails with later groups' work, so group g finishes (and its
+    // results start across PCIe) while later groups still compute
+    const int prio = greatest + int(g) < least ? greatest + int(g) : least;
+    if ((rc = w->set_stream_priority(prio))) {
+      const std::string why2 = w->err;
+      delete b;
+      return fail(ctx, rc, "batch group " + std::to_string(g) + ": " + why2);
+    }
+  }
+  *out = b;
+  return AE_MPM_OK;
+}
+
+int ae_mpm_batch_destroy(ae_mpm_batch* batch) {
+  if (!batch) return AE_MPM_EINVAL;
+  cudaSetDevice(batch->ctx->device);
+  delete batch;
+  return AE_MPM_OK;
+}
+
+uint32_t ae_mpm_batch_groups(const ae_mpm_batch* batch, uint32_t* first_scene) {
+  if (!batch) return 0;
+  const uint32_t g_n = uint32_t(batch->worlds.size());
+  if (first_scene)
+    for (uint32_t g = 0; g <= g_n; ++g) first_scene[g] = batch->first[g];
+  return g_n;
+}
+
+int ae_mpm_batch_run(ae_mpm_batch* batch, const ae_mpm_particles* in, const uint64_t* counts, ae_mpm_particles* out,
+                     uint32_t n_substeps) {
+  if (!batch) return AE_MPM_EINVAL;
+  ae_mpm_ctx* ctx = batch->ctx;
+  if (!in || !counts || !out) return fail(ctx, AE_MPM_EINVAL, "null view or count array");
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  const uint32_t g_n = uint32_t(batch->worlds.size());
+  std::vector<uint32_t> ids;
+  for (uint32_t i = 0; i < batch->first.back(); ++i) ids.push_back(i);
+  // AE_MPM_BATCH_PROFILE: a timeline of the call on stderr (device events per group and stream,
+  // host time after each queueing call), in ms from the start of the call
+  const bool prof = std::getenv("AE_MPM_BATCH_PROFILE") != nullptr;
+  std::vector<cudaEvent_t> pev;
+  std::vector<double> host_ms;
+  const auto h0 = std::chrono::steady_clock::now();
+  auto host_mark = [&]() {
+    if (prof) host_ms.push_back(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count());
+  };
+  auto mark = [&](cudaStream_t st) {
+    if (!prof) return;
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) == cudaSuccess) cudaEventRecord(e, st);
+    pev.push_back(e);
+  };
+  mark(batch->up);
+  // every group's inputs queue on the upload stream in group order; group g's substeps start
+  // when its inputs are in (served before later groups' by stream priority), and its results
+  // leave on the download stream while later groups compute
+  auto group_fail = [&](uint32_t g, int code) {
+    cudaStreamSynchronize(batch->down);
+    for (WorldBase* w : batch->worlds) cudaStreamSynchronize(w->stream());
+    return fail(ctx, code, "batch group " + std::to_string(g) + ": " + batch->worlds[g]->err);
+  };
+  for (uint32_t g = 0; g < g_n; ++g) {
+    const uint32_t f = batch->first[g], k = batch->first[g + 1] - f;
+    if ((rc = batch->worlds[g]->upload_many(k, ids.data(), in + f, counts + f, batch->up))) return group_fail(g, rc);
+    mark(batch->up);
+    host_mark();
+  }
+  for (uint32_t g = 0; g < g_n; ++g) {
+    WorldBase* w = batch->worlds[g];
+    mark(w->stream());
+    if ((rc = w->step(n_substeps))) return group_fail(g, rc);
+    if (cudaEventRecord(batch->done[g], w->stream()) != cudaSuccess)
+      return fail(ctx, AE_MPM_ECUDA, "batch: event record failed");
+    mark(w->stream());
+    host_mark();
+  }
+  for (uint32_t g = 0; g < g_n; ++g) {
+    const uint32_t f = batch->first[g], k = batch->first[g + 1] - f;
+    if ((rc = batch->worlds[g]->download_many(k, ids.data(), out + f, batch->down))) return group_fail(g, rc);
+    mark(batch->down);
+    host_mark();
+  }
+  cudaError_t e = cudaStreamSynchronize(batch->down);
+  if (e != cudaSuccess) return fail(ctx, AE_MPM_ECUDA, cudaGetErrorString(e));
+  if (prof) {
+    host_mark();
+    for (cudaEvent_t ev : pev)
+      if (ev) cudaEventSynchronize(ev);
+    auto at = [&](size_t i) {
+      float ms = 0.f;
+      if (pev[0] && pev[i]) cudaEventElapsedTime(&ms, pev[0], pev[i]);
+      return double(ms);
+    };
+    std::fprintf(stderr, "ae_mpm_batch: %u groups, %u substeps\n", g_n, n_substeps);
+    for (uint32_t g = 0; g < g_n; ++g)
+      std::fprintf(stderr, "  group %u: inputs in %.2f, substeps %.2f-%.2f, results out %.2f ms\n", g, at(1 + g),
+                   at(1 + g_n + 2 * g), at(2 + g_n + 2 * g), at(1 + 3 * g_n + g));
+    std::fprintf(stderr, "  host after each call:");
+    for (double h : host_ms) std::fprintf(stderr, " %.2f", h);
+    std::fprintf(stderr, " ms\n");
+    for (cudaEvent_t ev : pev)
+      if (ev) cudaEventDestroy(ev);
+  }
+  // error words of every group (the first reported wins; every group's results are in place)
+  int first_rc = AE_MPM_OK;
+  for (uint32_t g = 0; g < g_n; ++g) {
+    rc = batch->worlds[g]->sync();
+    if (rc && !first_rc) first_rc = fail(ctx, rc, "batch group " + std::to_string(g) + ": " + batch->worlds[g]->err);
+  }
+  return first_rc;
+}
+
 int ae_mpm_world_totals(ae_mpm_world* world, uint32_t scene, double out[5]) {
   if (world && !out) return fail(world->ctx, AE_MPM_EINVAL, "null output");
   AE_WORLD_CALL(world->w->totals(scene, out));

@@ -2749,7 +2749,16 @@ class World final : public WorldBase {
   // staging layout of upload)
   static uint64_t stage_region(uint64_t n) { return (sizeof(T) * 26 * n + sizeof(uint16_t) * n + 15) / 16 * 16; }
 
-  int upload_many(uint32_t k, const uint32_t* scenes, const ae_mpm_particles* views, const uint64_t* counts) override {
+  // orders `later` after the work queued so far on `earlier`
+  int stream_after(cudaStream_t later, cudaStream_t earlier) {
+    if (!xfer_ev_) AE_TRY(cudaEventCreateWithFlags(&xfer_ev_, cudaEventDisableTiming));
+    AE_TRY(cudaEventRecord(xfer_ev_, earlier));
+    AE_TRY(cudaStreamWaitEvent(later, xfer_ev_, 0));
+    return AE_MPM_OK;
+  }
+
+  int upload_many(uint32_t k, const uint32_t* scenes, const ae_mpm_particles* views, const uint64_t* counts,
+                  cudaStream_t copy) override {
     if (sizeof(T) != 4) {
       err = "many-scene transfers are for f32 worlds";
       return AE_MPM_EINVAL;
@@ -2782,7 +2791,12 @@ class World final : public WorldBase {
       const int rs = ensure_stage_bytes(total);
       if (rs) return rs;
     }
-    // all copies first, back to back on the stream, then the packs
+    // all copies first, back to back on the copy stream (the world's own by default), then the packs
+    const cudaStream_t cs = copy ? copy : stream_;
+    if (copy) {  // the staging area is free once the world's queued work is done with it
+      const int r = stream_after(cs, stream_);
+      if (r) return r;
+    }
     uint64_t off = 0;
     for (uint32_t i = 0; i < k; ++i) {
       const uint64_t n = counts[i];
@@ -2790,15 +2804,19 @@ class World final : public WorldBase {
       HostView<T> hv = host_view<T>(&views[i]);
       if (n > 0) {
         if (staging_layout(hv, n)) {
-          AE_TRY(cudaMemcpyAsync(st, hv.f[0], sizeof(T) * 26 * n + sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+          AE_TRY(cudaMemcpyAsync(st, hv.f[0], sizeof(T) * 26 * n + sizeof(uint16_t) * n, cudaMemcpyDefault, cs));
         } else {
           const uint64_t at[6] = {0, 3, 6, 15, 16, 25}, len[6] = {3, 3, 9, 1, 9, 1};
           for (int f = 0; f < 6; ++f)
-            AE_TRY(cudaMemcpyAsync(st + at[f] * n, hv.f[f], sizeof(T) * len[f] * n, cudaMemcpyDefault, stream_));
-          AE_TRY(cudaMemcpyAsync(st + 26 * n, hv.mat, sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+            AE_TRY(cudaMemcpyAsync(st + at[f] * n, hv.f[f], sizeof(T) * len[f] * n, cudaMemcpyDefault, cs));
+          AE_TRY(cudaMemcpyAsync(st + 26 * n, hv.mat, sizeof(uint16_t) * n, cudaMemcpyDefault, cs));
         }
       }
       off += stage_region(n);
+    }
+    if (copy) {
+      const int r = stream_after(stream_, cs);
+      if (r) return r;
     }
     for (uint32_t i = 0; i < k; ++i) {
       const uint32_t s = scenes[i];
@@ -2824,7 +2842,7 @@ class World final : public WorldBase {
     return AE_MPM_OK;
   }
 
-  int download_many(uint32_t k, const uint32_t* scenes, ae_mpm_particles* views) override {
+  int download_many(uint32_t k, const uint32_t* scenes, ae_mpm_particles* views, cudaStream_t copy) override {
     if (sizeof(T) != 4) {
       err = "many-scene transfers are for f32 worlds";
       return AE_MPM_EINVAL;
@@ -2864,6 +2882,11 @@ class World final : public WorldBase {
       off += stage_region(h.p_count);
     }
     AE_TRY(cudaGetLastError());
+    const cudaStream_t cs = copy ? copy : stream_;
+    if (copy) {
+      const int r = stream_after(cs, stream_);
+      if (r) return r;
+    }
     off = 0;
     for (uint32_t i = 0; i < k; ++i) {
       const uint64_t n = h_scenes_[scenes[i]].p_count;
@@ -2871,15 +2894,20 @@ class World final : public WorldBase {
       HostView<T> hv = host_view<T>(&views[i]);
       if (n > 0) {
         if (staging_layout(hv, n)) {
-          AE_TRY(cudaMemcpyAsync(hv.f[0], st, sizeof(T) * 26 * n + sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+          AE_TRY(cudaMemcpyAsync(hv.f[0], st, sizeof(T) * 26 * n + sizeof(uint16_t) * n, cudaMemcpyDefault, cs));
         } else {
           const uint64_t at[6] = {0, 3, 6, 15, 16, 25}, len[6] = {3, 3, 9, 1, 9, 1};
           for (int f = 0; f < 6; ++f)
-            AE_TRY(cudaMemcpyAsync(hv.f[f], st + at[f] * n, sizeof(T) * len[f] * n, cudaMemcpyDefault, stream_));
-          AE_TRY(cudaMemcpyAsync(hv.mat, st + 26 * n, sizeof(uint16_t) * n, cudaMemcpyDefault, stream_));
+            AE_TRY(cudaMemcpyAsync(hv.f[f], st + at[f] * n, sizeof(T) * len[f] * n, cudaMemcpyDefault, cs));
+          AE_TRY(cudaMemcpyAsync(hv.mat, st + 26 * n, sizeof(uint16_t) * n, cudaMemcpyDefault, cs));
         }
       }
       off += stage_region(n);
+    }
+    if (copy) {  // the next use of the staging area on the world's stream waits for these reads
+      const int r = stream_after(stream_, cs);
+      if (r) return r;
+      return AE_MPM_OK;
     }
     AE_TRY(cudaStreamSynchronize(stream_));
     return AE_MPM_OK;
@@ -3042,6 +3070,18 @@ class World final : public WorldBase {
     return s;
   }
   cudaStream_t stream() const override { return stream_; }
+  int set_stream_priority(int priority) override {
+    if (graph_) {
+      cudaGraphExecDestroy(graph_);
+      graph_ = nullptr;
+    }
+    AE_TRY(cudaStreamSynchronize(stream_));
+    cudaStream_t s = nullptr;
+    AE_TRY(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, priority));
+    cudaStreamDestroy(stream_);
+    stream_ = s;
+    return AE_MPM_OK;
+  }
   ae_mpm_exec_opts& opts() override { return opts_; }
   void invalidate_graph() override {
     if (graph_) cudaGraphExecDestroy(graph_);
@@ -3602,6 +3642,7 @@ class World final : public WorldBase {
   void release() {
     if (graph_) cudaGraphExecDestroy(graph_);
     if (stream_) cudaStreamSynchronize(stream_);
+    if (xfer_ev_) cudaEventDestroy(xfer_ev_);
     for (int k = 0; k < 7; ++k) {
       dfree(bufA_[k]);
       dfree(bufB_[k]);
@@ -3679,6 +3720,7 @@ class World final : public WorldBase {
   bool scatter_invalid_ = false;  // the particles changed since that scatter
   uint64_t substep_ = 0, snap_substep_ = 0, launches_ = 0;
   cudaEvent_t* stage_events_ = nullptr;
+  cudaEvent_t xfer_ev_ = nullptr;  // orders copy streams against the world's stream
   uint64_t total_cap_ = 0, total_blocks_ = 0, device_bytes_ = 0;
   int key_bits_ = 1;
   bool keys_stale_ = true, chunks_dirty_ = true, scenes_dirty_ = true, mats_dirty_ = false;

@@ -101,8 +101,13 @@ struct WorldBase {
   // Many scenes per call (f32 worlds): every host<->device copy is queued back to back through one
   // staging area, so the copies run at link speed instead of one scene, one wait at a time.
   // upload_many is asynchronous like upload; download_many waits once, at the end.
-  virtual int upload_many(uint32_t n, const uint32_t* scenes, const ae_mpm_particles* views, const uint64_t* counts) = 0;
-  virtual int download_many(uint32_t n, const uint32_t* scenes, ae_mpm_particles* views) = 0;
+  // With a copy stream, the host<->device copies go on that stream instead (ordered against the
+  // world's own stream by events), so that they overlap another world's substeps; download_many
+  // then returns without waiting and the results are in place once `copy` has drained.
+  virtual int upload_many(uint32_t n, const uint32_t* scenes, const ae_mpm_particles* views, const uint64_t* counts,
+                          cudaStream_t copy = nullptr) = 0;
+  virtual int download_many(uint32_t n, const uint32_t* scenes, ae_mpm_particles* views,
+                            cudaStream_t copy = nullptr) = 0;
   virtual int step(uint32_t n) = 0;
   virtual int sync() = 0;
   virtual int totals(uint32_t scene, double out[5]) = 0;
@@ -113,6 +118,9 @@ struct WorldBase {
   virtual uint64_t last_launches() const = 0;
   virtual uint64_t particles() const = 0;
   virtual cudaStream_t stream() const = 0;
+  // replaces the world's stream by one of CUDA stream priority `priority` (lower = served first);
+  // the world's queued work finishes first
+  virtual int set_stream_priority(int priority) = 0;
   virtual ae_mpm_exec_opts& opts() = 0;
   virtual void invalidate_graph() = 0;
   virtual uint64_t device_bytes() const = 0;

@@ -269,6 +269,29 @@ int ae_mpm_world_download_f64(ae_mpm_world* world, uint32_t scene, ae_mpm_partic
 int ae_mpm_world_upload_many(ae_mpm_world* world, uint32_t n, const uint32_t* scenes,
                              const ae_mpm_particles* views, const uint64_t* counts);
 int ae_mpm_world_download_many(ae_mpm_world* world, uint32_t n, const uint32_t* scenes, ae_mpm_particles* views);
+
+/* ---------------------------------------------------------------------------------------------
+ * Pipelined batch (no counterpart in the reference): scenes that live in host memory, advanced
+ * n_substeps per call with the PCIe copies hidden behind the substeps.  ae_mpm_batch_create
+ * splits the n_scenes scenes into n_groups consecutive groups of about equal particle capacity
+ * (max_particles), one f32 world each (opts as for ae_mpm_world_create; precision 64 is
+ * AE_MPM_EINVAL; n_groups is clamped to 1..n_scenes).  ae_mpm_batch_run copies counts[i]
+ * particles of in[i] into scene i, runs every group n_substeps substeps and writes each scene's
+ * particles into out[i] (out may be in): group g's inputs cross while group g - 1 computes, and
+ * its results cross back while group g + 1 computes, so a call costs about the substeps of all
+ * groups plus one group's copies each way.  Host views should be pinned (page-locked) memory
+ * for the copies to overlap.  Groups compute one after another, each scene's results the same
+ * as in one world of all scenes (bitwise so in deterministic mode).  Returns once every result
+ * is in place; an error word of any group (AE_MPM_ENAN, AE_MPM_EDOMAIN) is returned after all
+ * results are written.  ae_mpm_batch_groups writes the first scene of every group and then
+ * n_scenes into first_scene (n_groups + 1 entries) when it is not null, and returns n_groups. */
+typedef struct ae_mpm_batch ae_mpm_batch;
+int ae_mpm_batch_create(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32_t n_scenes,
+                        const ae_mpm_exec_opts* opts, uint32_t n_groups, ae_mpm_batch** out);
+int ae_mpm_batch_run(ae_mpm_batch* batch, const ae_mpm_particles* in, const uint64_t* counts, ae_mpm_particles* out,
+                     uint32_t n_substeps);
+uint32_t ae_mpm_batch_groups(const ae_mpm_batch* batch, uint32_t* first_scene);
+int ae_mpm_batch_destroy(ae_mpm_batch* batch);
 /* FP64 totals of a scene: [mass, px, py, pz, kinetic energy] of its particles, now. */
 int ae_mpm_world_totals(ae_mpm_world* world, uint32_t scene, double out[5]);
 /* Per-scene error word (bit 0 NaN, bit 1 domain clamp) and counters

@@ -166,6 +166,49 @@ def test_upload_many_and_download_many_equal_scene_by_scene(ctx):
         w.close()
 
 
+def test_pipelined_batch_equals_one_world_of_all_scenes(ctx):
+    # the pipelined batch (groups of scenes in worlds of their own, copies on their own streams,
+    # groups computing one after another) gives every scene the results one world of all scenes
+    # gives it: deterministic mode, bitwise, over two runs (the second in place)
+    rng = S.Rng(0xBA7C)
+    pairs = [S.batched_scene(rng) for _ in range(11)]
+    scenes = [sc for sc, _ in pairs]
+    parts = [p for _, p in pairs]
+    det = M.exec_opts(deterministic=1)
+    b = M.Batch(ctx, scenes, det, groups=3)
+    first = b.groups()
+    assert len(first) == 4 and first[0] == 0 and first[-1] == len(scenes)
+    assert all(x < y for x, y in zip(first, first[1:]))
+    w = M.World(ctx, scenes, det)
+    ids = list(range(len(parts)))
+    outs = [M.Particles.empty(p.n) for p in parts]
+    assert b.run(parts, 12, out=outs, raise_on_error=False) == M.OK
+    w.upload_many(ids, parts)
+    w.step(12)
+    ref = [M.Particles.empty(p.n) for p in parts]
+    w.download_many(ids, ref)
+    for i in ids:
+        for f in ("pos", "vel", "F", "J", "C", "mass", "mat"):
+            assert np.array_equal(getattr(outs[i], f), getattr(ref[i], f)), (i, f)
+    assert not np.array_equal(outs[0].pos, parts[0].pos)
+    # in place; the world takes the same host state (C crosses the boundary as m C - k tau and
+    # back, so a round trip through the host is not the resident state to the last bit)
+    assert b.run(outs, 5, raise_on_error=False) == M.OK
+    w.upload_many(ids, ref)
+    w.step(5)
+    w.download_many(ids, ref)
+    for i in ids:
+        assert np.array_equal(outs[i].pos, ref[i].pos) and np.array_equal(outs[i].F, ref[i].F), i
+    b.close()
+    w.close()
+    # more groups than scenes: one scene per group; FP64 batches are refused
+    b2 = M.Batch(ctx, scenes[:2], M.exec_opts(), groups=8)
+    assert b2.groups() == [0, 1, 2]
+    b2.close()
+    with pytest.raises(M.MpmError):
+        M.Batch(ctx, scenes[:2], M.exec_opts(precision=64), groups=2)
+
+
 # ------------------------------------------------------------------ server
 def test_server_results_equal_running_alone(ctx):
     rng = S.Rng(0x5E4E)
