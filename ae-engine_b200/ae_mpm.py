@@ -174,6 +174,7 @@ SIGNATURES = {
     "ae_mpm_batch_run": (C.c_int, [_P, _P, _P, _P, C.c_uint32]),
     "ae_mpm_batch_groups": (C.c_uint32, [_P, _P]),
     "ae_mpm_batch_destroy": (C.c_int, [_P]),
+    "ae_mpm_batch_partition": (C.c_uint32, [_P, C.c_uint32, C.c_uint32, _P]),
     "ae_mpm_world_totals": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_double)]),
     "ae_mpm_world_errors": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
     "ae_mpm_world_launch_count": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
@@ -226,6 +227,15 @@ def load(path: str = LIB_PATH):
         f.argtypes = args
     _lib = lib
     return lib
+
+
+def batch_partition(capacities, groups: int):
+    """ae_mpm_batch_partition: the first scene of every group of a pipelined batch, then the
+    scene count (host only)."""
+    caps = np.ascontiguousarray(capacities, np.uint64)
+    first = np.zeros(caps.size + 1, np.uint32)
+    g = load().ae_mpm_batch_partition(caps.ctypes.data, caps.size, groups, first.ctypes.data)
+    return [int(x) for x in first[:g + 1]] if g else []
 
 
 def exec_opts(**kw) -> ExecOpts:

@@ -631,6 +631,32 @@ struct ae_mpm_batch {
   }
 };
 
+uint32_t ae_mpm_batch_partition(const uint64_t* capacities, uint32_t n_scenes, uint32_t n_groups,
+                                uint32_t* first_scene) {
+  if (!capacities || !first_scene || n_scenes == 0) return 0;
+  const uint32_t g_n = n_groups == 0 ? 1u : (n_groups > n_scenes ? n_scenes : n_groups);
+  // consecutive groups of about equal capacity, none empty: boundary g goes after the first scene
+  // at which the running capacity reaches g / g_n of the total, as long as every later group can
+  // still have a scene of its own
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < n_scenes; ++i) total += capacities[i];
+  uint32_t nb = 0;  // boundaries written
+  first_scene[nb++] = 0;
+  uint64_t acc = 0;
+  for (uint32_t i = 0; i < n_scenes && nb < g_n; ++i) {
+    acc += capacities[i];
+    const uint32_t g = nb;
+    const bool left_enough = n_scenes - (i + 1) >= g_n - g;
+    if (left_enough && (unsigned __int128)acc * g_n >= (unsigned __int128)total * g) first_scene[nb++] = i + 1;
+  }
+  while (nb < g_n) {  // capacity-free tail scenes: one scene per remaining group
+    first_scene[nb] = first_scene[nb - 1] + 1;
+    ++nb;
+  }
+  first_scene[g_n] = n_scenes;
+  return g_n;
+}
+
 int ae_mpm_batch_create(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32_t n_scenes,
                         const ae_mpm_exec_opts* opts, uint32_t n_groups, ae_mpm_batch** out) {
   if (!ctx || !out) return AE_MPM_EINVAL;
@@ -639,20 +665,11 @@ int ae_mpm_batch_create(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32
   if (opts && opts->precision == 64) return fail(ctx, AE_MPM_EINVAL, "a batch runs f32 worlds");
   int rc = set_device(ctx);
   if (rc) return rc;
-  const uint32_t g_n = n_groups == 0 ? 1u : (n_groups > n_scenes ? n_scenes : n_groups);
-  // consecutive groups of about equal particle capacity, none empty
-  uint64_t total = 0;
-  for (uint32_t i = 0; i < n_scenes; ++i) total += scenes[i].max_particles;
-  std::vector<uint32_t> first(1, 0u);
-  uint64_t acc = 0;
-  for (uint32_t i = 0; i < n_scenes && first.size() < g_n; ++i) {
-    acc += scenes[i].max_particles;
-    const uint32_t g = uint32_t(first.size());  // the boundary after group g - 1
-    const bool left_enough = n_scenes - (i + 1) >= g_n - g;
-    if (left_enough && acc * g_n >= total * g) first.push_back(i + 1);
-  }
-  while (first.size() < g_n) first.push_back(first.back() + 1);  // capacity-free tail scenes
-  first.push_back(n_scenes);
+  std::vector<uint64_t> caps(n_scenes);
+  for (uint32_t i = 0; i < n_scenes; ++i) caps[i] = scenes[i].max_particles;
+  std::vector<uint32_t> first(n_scenes + 1);
+  const uint32_t g_n = ae_mpm_batch_partition(caps.data(), n_scenes, n_groups, first.data());
+  first.resize(g_n + 1);
   auto* b = new ae_mpm_batch;
   b->ctx = ctx;
   b->first = first;

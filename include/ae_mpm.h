@@ -291,6 +291,12 @@ int ae_mpm_batch_create(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32
 int ae_mpm_batch_run(ae_mpm_batch* batch, const ae_mpm_particles* in, const uint64_t* counts, ae_mpm_particles* out,
                      uint32_t n_substeps);
 uint32_t ae_mpm_batch_groups(const ae_mpm_batch* batch, uint32_t* first_scene);
+/* The grouping ae_mpm_batch_create uses, on the host (no device needed): writes the first scene
+ * of each of the min(max(n_groups, 1), n_scenes) groups and then n_scenes into first_scene
+ * (n_scenes + 1 entries suffice) for scenes of the given particle capacities, and returns the
+ * group count (0 for no scenes or null arrays). */
+uint32_t ae_mpm_batch_partition(const uint64_t* capacities, uint32_t n_scenes, uint32_t n_groups,
+                                uint32_t* first_scene);
 int ae_mpm_batch_destroy(ae_mpm_batch* batch);
 /* FP64 totals of a scene: [mass, px, py, pz, kinetic energy] of its particles, now. */
 int ae_mpm_world_totals(ae_mpm_world* world, uint32_t scene, double out[5]);
