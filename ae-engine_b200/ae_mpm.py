@@ -179,6 +179,7 @@ SIGNATURES = {
     "ae_mpm_world_errors": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
     "ae_mpm_world_launch_count": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "ae_mpm_world_stage_times": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_double)]),
+    "ae_mpm_world_stage_times_split": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_double)]),
     "ae_mpm_world_stream": (_P, [_P]),
     "ae_mpm_world_particles": (C.c_uint64, [_P]),
     "ae_mpm_radix_sort_keys": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, _P, _P]),
@@ -572,10 +573,11 @@ class World:
         return int(n.value)
 
     def stage_times(self, n: int) -> dict:
-        """Mean per-substep device time of each stage (us), measured with CUDA events."""
-        out = (C.c_double * 5)()
-        self.ctx.check(self.ctx.lib.ae_mpm_world_stage_times(self.h, n, out))
-        return dict(zip(("sort", "p2g", "grid", "g2p", "substep"), out[:]))
+        """Mean per-substep device time of each stage (us), measured with CUDA events; "g2p" includes
+        the snow clamp, "g2p_kernel" is the G2P (or fused G2P + P2G) kernel alone."""
+        out = (C.c_double * 6)()
+        self.ctx.check(self.ctx.lib.ae_mpm_world_stage_times_split(self.h, n, out))
+        return dict(zip(("sort", "p2g", "grid", "g2p", "substep", "g2p_kernel"), out[:]))
 
     def stream(self) -> int:
         return int(self.ctx.lib.ae_mpm_world_stream(self.h) or 0)

@@ -818,6 +818,18 @@ int ae_mpm_world_errors(ae_mpm_world* world, uint32_t scene, uint32_t* error_wor
 
 int ae_mpm_world_stage_times(ae_mpm_world* world, uint32_t n_substeps, double out_us[5]) {
   if (world && !out_us) return fail(world->ctx, AE_MPM_EINVAL, "null output");
+  double six[6];
+  if (!world) return AE_MPM_EINVAL;
+  int rc = set_device(world->ctx);
+  if (rc) return rc;
+  rc = world->w->stage_times(n_substeps, six);
+  if (rc) return fail(world->ctx, rc, world->w->err);
+  for (int k = 0; k < 5; ++k) out_us[k] = six[k];
+  return AE_MPM_OK;
+}
+
+int ae_mpm_world_stage_times_split(ae_mpm_world* world, uint32_t n_substeps, double out_us[6]) {
+  if (world && !out_us) return fail(world->ctx, AE_MPM_EINVAL, "null output");
   AE_WORLD_CALL(world->w->stage_times(n_substeps, out_us));
 }
 

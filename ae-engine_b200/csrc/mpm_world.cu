@@ -3195,8 +3195,8 @@ class World final : public WorldBase {
   }
   int precision() const override { return sizeof(T) == 8 ? 64 : 32; }
 
-  int stage_times(uint32_t n, double out_us[5]) override {
-    for (int k = 0; k < 5; ++k) out_us[k] = 0;
+  int stage_times(uint32_t n, double out_us[6]) override {
+    for (int k = 0; k < 6; ++k) out_us[k] = 0;
     int rc = prepare();
     if (rc) return rc;
     if (n == 0 || n_chunks_ == 0) return AE_MPM_OK;
@@ -3209,23 +3209,25 @@ class World final : public WorldBase {
     }
     // all substeps are queued before the one wait, so that (past the first) the stream is never
     // idle waiting for the host and the events measure device time, not launch latency
-    std::vector<cudaEvent_t> ev(5 * size_t(n), nullptr);
+    // per substep: start, after the sort, after P2G, after the grid update, end, and after the
+    // G2P (or fused) kernel alone, before the snow clamp (recorded between the last two)
+    std::vector<cudaEvent_t> ev(6 * size_t(n), nullptr);
     int rc2 = AE_MPM_OK;
     for (auto& e : ev)
       if (cudaEventCreate(&e) != cudaSuccess) rc2 = AE_MPM_ECUDA;
     if (rc2 == AE_MPM_OK) {
       for (uint32_t i = 0; i < n; ++i) {
-        stage_events_ = ev.data() + 5 * size_t(i);
+        stage_events_ = ev.data() + 6 * size_t(i);
         substep_eager();
       }
       stage_events_ = nullptr;
-      if (cudaEventSynchronize(ev.back()) != cudaSuccess) rc2 = AE_MPM_ECUDA;
+      if (cudaEventSynchronize(ev[6 * size_t(n - 1) + 4]) != cudaSuccess) rc2 = AE_MPM_ECUDA;
     }
-    double acc[5] = {0, 0, 0, 0, 0};
+    double acc[6] = {0, 0, 0, 0, 0, 0};
     // the first substep starts on an idle stream: skip it when there is more than one
     const uint32_t first = n > 1 ? 1u : 0u;
     for (uint32_t i = first; i < n && rc2 == AE_MPM_OK; ++i) {
-      const cudaEvent_t* e = ev.data() + 5 * size_t(i);
+      const cudaEvent_t* e = ev.data() + 6 * size_t(i);
       float ms;
       for (int k = 0; k < 4; ++k) {
         cudaEventElapsedTime(&ms, e[k], e[k + 1]);
@@ -3233,6 +3235,8 @@ class World final : public WorldBase {
       }
       cudaEventElapsedTime(&ms, e[0], e[4]);
       acc[4] += ms;
+      cudaEventElapsedTime(&ms, e[3], e[5]);
+      acc[5] += ms;
     }
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
@@ -3240,7 +3244,7 @@ class World final : public WorldBase {
       err = "stage timing events failed";
       return rc2;
     }
-    for (int k = 0; k < 5; ++k) out_us[k] = 1000.0 * acc[k] / (n - first);
+    for (int k = 0; k < 6; ++k) out_us[k] = 1000.0 * acc[k] / (n - first);
     return AE_MPM_OK;
   }
 
@@ -3471,6 +3475,7 @@ class World final : public WorldBase {
     const size_t g2p_smem = sizeof(V4) * ((MODE == AE_MPM_MODE_PHYSICS ? 0 : max_tile_nodes()) + 3 * chunk_threads_);
     g2p_kernel<T, MODE><<<n_chunks_, chunk_threads_, g2p_smem, stream_>>>(w, counters_ + 2, write_keys ? 1 : 0);
     ++launches_;
+    mark(5);  // the G2P kernel alone ends here
     if (MODE == AE_MPM_MODE_PHYSICS && has_snow_) {
       snow_clamp_kernel<T><<<sms * 8, 128, 0, stream_>>>(w);
       ++launches_;
@@ -3562,6 +3567,7 @@ class World final : public WorldBase {
     g2p2g_kernel<T><<<n_chunks_, chunk_threads_, fused_smem(chunk_threads_), stream_>>>(wf, counters_ + 2,
                                                                                          write_keys ? 1 : 0);
     launches_ += 2;
+    mark(5);  // the fused kernel alone ends here
     if (has_snow_) {
       snow_clamp_scatter_kernel<T><<<sms * 8, 128, fused_smem(128), stream_>>>(wf);
       ++launches_;

@@ -136,7 +136,8 @@ struct WorldBase {
   virtual int vacate_scene(uint32_t scene) = 0;
   virtual uint32_t scene_count(uint32_t scene) const = 0;
   virtual int precision() const = 0;
-  virtual int stage_times(uint32_t n, double out_us[5]) = 0;
+  // [sort, P2G, grid update, G2P (+ snow clamp), whole substep, the G2P or fused kernel alone]
+  virtual int stage_times(uint32_t n, double out_us[6]) = 0;
   std::string err;
 };
 

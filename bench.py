@@ -56,11 +56,12 @@ KERNEL_BYTES = {"p2g": (104, 16), "g2p": (156, 16), "grid": (0, 64), "g2p2g": (1
 def dominant_kernel(stages):
     """The kernel the roofline is quoted on, from a world's stage times.  A world whose P2G is
     fused into G2P (physics mode, column-lane P2G) reports no stand-alone P2G: its G2P stage is the
-    fused kernel (plus the snow clamp), which moves the bytes of both."""
+    fused kernel, which moves the bytes of both; "g2p_kernel" times it without the snow clamp."""
+    g2p = stages.get("g2p_kernel") or stages["g2p"]  # the kernel alone, without the snow clamp
     if stages["p2g"] < 0.1 * stages["g2p"]:
-        return "g2p2g", stages["g2p"]
+        return "g2p2g", g2p
     k = max(("p2g", "g2p", "grid"), key=lambda k: stages[k])
-    return k, stages[k]
+    return k, (g2p if k == "g2p" else stages[k])
 
 
 def l2_note(n_particles):

@@ -309,6 +309,10 @@ int ae_mpm_world_launch_count(const ae_mpm_world* world, uint64_t* launches);
  * the mean device time per substep of each stage in microseconds:
  * out_us = [sort, P2G (deterministic: cell sums + gather), grid update, G2P, whole substep]. */
 int ae_mpm_world_stage_times(ae_mpm_world* world, uint32_t n_substeps, double out_us[5]);
+/* The same measurement with a sixth entry: out_us[5] = the G2P kernel alone (in physics mode with
+ * the column-lane P2G, the fused G2P + P2G kernel alone), without the snow clamp that out_us[3]
+ * includes. */
+int ae_mpm_world_stage_times_split(ae_mpm_world* world, uint32_t n_substeps, double out_us[6]);
 /* CUDA stream the world queues on (cudaStream_t), so callers can time it with events. */
 void* ae_mpm_world_stream(ae_mpm_world* world);
 /* Particle count of every scene summed. */

@@ -130,6 +130,16 @@ def test_autotune_picks_a_valid_choice_and_restores_state(ctx):
     assert np.array_equal(before.pos, after.pos) and np.array_equal(before.F, after.F)
 
 
+def test_stage_times_split_the_g2p_kernel_from_the_snow_clamp(ctx):
+    sc, p = S.tiny_scene(8192, 32, S.snow(), v=(1.5, 0.0, -1.0))
+    w = world_of(ctx, [sc], [p])
+    w.step(3)
+    t = w.stage_times(6)
+    assert all(t[k] >= 0 for k in t) and t["substep"] > 0
+    assert 0 < t["g2p_kernel"] <= t["g2p"] + 1e-3
+    assert t["sort"] + t["p2g"] + t["grid"] + t["g2p"] <= t["substep"] + 1e-3
+
+
 # ------------------------------------------------------------------ many-scene transfers
 def test_upload_many_and_download_many_equal_scene_by_scene(ctx):
     # the batched transfer calls (every copy through one staging area, one wait) move the same
