@@ -1734,7 +1734,7 @@ __device__ __forceinline__ WarpStage<T> warp_stage(unsigned char* smem, int warp
 // node, unique across scenes.  kMixed: lanes may belong to different scenes (each run looks its
 // scene up from its base node's block); otherwise every lane belongs to scene sc.
 // runs of at most this many particles are summed one node per lane; longer ones by the column lanes
-constexpr int kShortRun = 10;
+constexpr int kShortRun = 6;
 
 template <class T, bool kMixed>
 __device__ __forceinline__ void p2g_warp_scatter(const WorldDev<T>& w, const SceneDev<T>& sc, bool has, const T* x,
