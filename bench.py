@@ -60,8 +60,9 @@ def dominant_kernel(stages):
     g2p = stages.get("g2p_kernel") or stages["g2p"]  # the kernel alone, without the snow clamp
     if stages["p2g"] < 0.1 * stages["g2p"]:
         return "g2p2g", g2p
-    k = max(("p2g", "g2p", "grid"), key=lambda k: stages[k])
-    return k, (g2p if k == "g2p" else stages[k])
+    alone = {"p2g": stages["p2g"], "g2p": g2p, "grid": stages["grid"]}
+    k = max(alone, key=lambda k: alone[k])
+    return k, alone[k]
 
 
 def l2_note(n_particles):

@@ -31,3 +31,24 @@ def test_near_population_is_the_lod_cap_of_the_same_buffer():
     half = grid.nx * grid.dx / 2
     assert np.all(np.abs(sel) < half)
     assert len(mats) == len(models) == 4 and set(np.unique(p.mat)) <= {0, 1, 2, 3}
+
+
+def test_dominant_kernel_times_the_fused_kernel_without_the_snow_clamp():
+    import bench as B
+
+    fused = {"sort": 6.0, "p2g": 2.6, "grid": 9.0, "g2p": 98.0, "substep": 116.0, "g2p_kernel": 91.0}
+    assert B.dominant_kernel(fused) == ("g2p2g", 91.0)
+    plain = {"sort": 6.0, "p2g": 58.0, "grid": 9.0, "g2p": 60.0, "substep": 133.0, "g2p_kernel": 56.0}
+    assert B.dominant_kernel(plain) == ("p2g", 58.0)
+    old = {"sort": 6.0, "p2g": 2.6, "grid": 9.0, "g2p": 98.0, "substep": 116.0}  # five-stage timings
+    assert B.dominant_kernel(old) == ("g2p2g", 98.0)
+    assert B.KERNEL_BYTES["g2p2g"] == (260, 32)  # P2G 104 + G2P 156 B per particle, 16 + 16 B per node
+
+
+def test_batched_shards_deal_one_scene_list():
+    import bench as B
+
+    a = B.shard(list(range(10)), 0, 3)
+    b = B.shard(list(range(10)), 1, 3)
+    c = B.shard(list(range(10)), 2, 3)
+    assert sorted(a + b + c) == list(range(10)) and a == [0, 3, 6, 9]
