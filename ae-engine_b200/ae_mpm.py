@@ -182,6 +182,7 @@ SIGNATURES = {
     "ae_mpm_world_stage_times_split": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_double)]),
     "ae_mpm_world_stream": (_P, [_P]),
     "ae_mpm_world_particles": (C.c_uint64, [_P]),
+    "ae_mpm_world_scene_particles": (C.c_uint64, [_P, C.c_uint32]),
     "ae_mpm_radix_sort_keys": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, _P, _P]),
     "ae_mpm_radix_sort_keys_noalloc": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, _P, _P, _P]),
     "ae_mpm_counting_sort_keys": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, _P, _P]),
@@ -513,7 +514,16 @@ class World:
         self.ctx.check(fn(self.h, scene, C.byref(v), p.n))
         self._keep = p
 
+    def scene_particles(self, scene: int) -> int:
+        return int(self.ctx.lib.ae_mpm_world_scene_particles(self.h, scene))
+
+    def _room(self, scene: int, n: int) -> None:
+        have = self.scene_particles(scene)
+        if n < have:
+            raise ValueError("scene %d holds %d particles; room for %d" % (scene, have, n))
+
     def download(self, scene: int, n: int) -> Particles:
+        self._room(scene, n)
         p = Particles.empty(n, np.float64 if self.f64 else np.float32)
         v = p.view()
         fn = self.ctx.lib.ae_mpm_world_download_f64 if self.f64 else self.ctx.lib.ae_mpm_world_download
@@ -521,6 +531,7 @@ class World:
         return p
 
     def download_into(self, scene: int, p: Particles) -> None:
+        self._room(scene, p.n)
         v = p.view()
         fn = self.ctx.lib.ae_mpm_world_download_f64 if self.f64 else self.ctx.lib.ae_mpm_world_download
         self.ctx.check(fn(self.h, scene, C.byref(v)))
@@ -537,6 +548,8 @@ class World:
 
     def download_many(self, scenes, parts) -> None:
         """ae_mpm_world_download_many: scene scenes[i] into parts[i] (float32 Particles)."""
+        for sc, p in zip(scenes, parts):
+            self._room(sc, p.n)
         k = len(parts)
         views = (ParticlesView * max(k, 1))(*[p.view() for p in parts])
         ids = np.ascontiguousarray(scenes, np.uint32)
@@ -634,6 +647,10 @@ class Batch:
         vout = vin if out is None else (out if isinstance(out, ViewArray) else ViewArray(out))
         if len(vin) != len(self.scenes) or len(vout) != len(self.scenes):
             raise ValueError("one input and one output per scene")
+        if vout is not vin and any(o.n < i.n for i, o in zip(vin.parts, vout.parts)):
+            raise ValueError("an output holds fewer particles than its input")
+        if any(p.dtype != np.float32 for p in vin.parts + vout.parts):
+            raise TypeError("a batch moves float32 particles")
         rc = self.ctx.lib.ae_mpm_batch_run(self.h, C.addressof(vin.arr), vin.counts.ctypes.data,
                                            C.addressof(vout.arr), n_substeps)
         if rc != OK and (raise_on_error or rc not in (ENAN, EDOMAIN)):

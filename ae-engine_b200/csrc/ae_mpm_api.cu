@@ -842,6 +842,9 @@ int ae_mpm_world_launch_count(const ae_mpm_world* world, uint64_t* launches) {
 void* ae_mpm_world_stream(ae_mpm_world* world) { return world ? static_cast<void*>(world->w->stream()) : nullptr; }
 
 uint64_t ae_mpm_world_particles(const ae_mpm_world* world) { return world ? world->w->particles() : 0; }
+uint64_t ae_mpm_world_scene_particles(const ae_mpm_world* world, uint32_t scene) {
+  return world ? world->w->scene_count(scene) : 0;
+}
 
 static int host_sort(ae_mpm_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t key_bits, uint32_t* sorted_keys_out,
                      uint32_t* perm_out, bool counting) {

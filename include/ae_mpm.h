@@ -317,6 +317,9 @@ int ae_mpm_world_stage_times_split(ae_mpm_world* world, uint32_t n_substeps, dou
 void* ae_mpm_world_stream(ae_mpm_world* world);
 /* Particle count of every scene summed. */
 uint64_t ae_mpm_world_particles(const ae_mpm_world* world);
+/* Particle count of scene `scene` (0 for an unknown scene): the number of particles a download
+ * of it writes, so the caller's arrays must hold at least that many. */
+uint64_t ae_mpm_world_scene_particles(const ae_mpm_world* world, uint32_t scene);
 
 /* ---------------------------------------------------------------------------------------------
  * Radix sort by cell key, exposed for parity testing: stable ascending sort of n 32-bit keys
