@@ -560,6 +560,7 @@ def run_midfield(args, rank, local, world_size, pg, reference=False):
     world.step(max(args.warmup, 3))
     world.sync()
     stages = world.stage_times(STAGE_SUBSTEPS)
+    graph_warm(world)
     stream = torch.cuda.ExternalStream(world.stream(), device=local)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(pg)
@@ -1023,6 +1024,15 @@ def run_ck(args, rank, local, world_size, pg, reference=False):
 
 
 STAGE_SUBSTEPS = 20
+# untimed substeps run just before each timed region: at least one full CUDA-graph period (at most
+# 32 substeps: lcm(2, sort interval <= 32)), so the graph is captured and instantiated outside
+# the timing; stage_times steps eagerly and builds none
+GRAPH_WARM = 64
+
+
+def graph_warm(world) -> None:
+    world.step(GRAPH_WARM)
+    world.sync(raise_on_error=False)
 
 
 def run_ours(args, rank, local, world_size, pg):
@@ -1062,11 +1072,12 @@ def run_ours(args, rank, local, world_size, pg):
     world.sync()
     # per-kernel event times over the next STAGE_SUBSTEPS substeps (eager, one event per stage)
     stages = world.stage_times(STAGE_SUBSTEPS)
-    t0_sub = max(args.warmup, 3) + STAGE_SUBSTEPS  # the timed substeps start here, counted from the initial state
+    t0_sub = max(args.warmup, 3) + STAGE_SUBSTEPS + GRAPH_WARM  # the timed substeps start here, from the initial state
     # active grid nodes of the state the kernel times were taken on (for the roofline's node bytes)
     A = sum(active_nodes(s, world.download(i, p.n)) for i, (s, p) in enumerate(zip(scenes[:64], parts[:64])))
     if len(scenes) > 64:
         A = int(A * len(scenes) / 64)
+    graph_warm(world)
     stream = torch.cuda.ExternalStream(world.stream(), device=local)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -1199,9 +1210,10 @@ def percentile(xs, q):
 
 
 def time_world(torch, world, local, steps, warmup):
-    """CUDA-event time (ms) of `steps` substeps on the world's stream after `warmup` untimed ones."""
+    """CUDA-event time (ms) of `steps` substeps on the world's stream after `warmup` untimed ones
+    and a graph warm-up."""
     world.step(warmup)
-    world.sync()
+    graph_warm(world)
     stream = torch.cuda.ExternalStream(world.stream(), device=local)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -1301,9 +1313,10 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
     world.step(warm)
     world.sync()
     stages = world.stage_times(STAGE_SUBSTEPS)
-    t0_sub = warm + STAGE_SUBSTEPS
+    t0_sub = warm + STAGE_SUBSTEPS + GRAPH_WARM
     state = [world.download(i, p.n) for i, p in enumerate(parts)]
     A = sum(active_nodes(s, q) for s, q in zip(scenes, state))
+    graph_warm(world)
     stream = torch.cuda.ExternalStream(world.stream(), device=local)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -1392,7 +1405,7 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
     batch = M.Batch(ctx, scenes, M.exec_opts(**tuned), groups=groups)
     own_bt, hbt = pinned_staging(torch, parts, fill=False)
     vin, vbt = M.ViewArray(hin), M.ViewArray(hbt)  # the caller's view arrays, built once
-    batch.run(vin, 2, out=vbt, raise_on_error=False)  # first call: graphs, tables, staging
+    batch.run(vin, GRAPH_WARM, out=vbt, raise_on_error=False)  # first call: graphs, tables, staging
     e2e_t = []
     for rep in range(max(1, args.e2e_reps)):
         barrier(pg)
