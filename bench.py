@@ -65,6 +65,16 @@ def dominant_kernel(stages):
     return k, alone[k]
 
 
+def substep_roofline(n_particles, active_nodes, stages, peak):
+    """The whole substep against HBM with the scope's per-substep bytes: 260 B per particle (P2G
+    104, G2P 156) and 80 B per active node (clear 16, P2G write 16, update 32, G2P read 16), over
+    the event-timed substep of the same state as the kernel figures."""
+    b = 260 * n_particles + 80 * active_nodes
+    us = stages["substep"]
+    ach = b / (us * 1e-6) / 1e9
+    return {"substep_bytes": b, "substep_us": us, "substep_achieved": ach, "substep_frac": ach / peak}
+
+
 def l2_note(n_particles):
     """How the timed region relates to the 126 MB L2: the particle state (two 112-byte copies per
     particle, read and written every substep) either exceeds it, or the scene is L2-resident."""
@@ -1189,7 +1199,8 @@ def run_ours(args, rank, local, world_size, pg):
                          "traffic_source": traffic["source"] if traffic else None, "peak_kind": peak_kind,
                          "algorithmic_bytes": alg_bytes, "bytes_per_particle": per_p, "bytes_per_node": per_n,
                          "active_nodes": A, "kernel_us": kern_us,
-                         "kernel_substeps": [t0_sub - STAGE_SUBSTEPS, t0_sub]},
+                         "kernel_substeps": [t0_sub - STAGE_SUBSTEPS, t0_sub],
+                         **substep_roofline(n_total, A, stages, peak)},
             "stages_us": {k: round(v, 2) for k, v in stages.items()},
             "stages_us_end": dict({k: round(v, 2) for k, v in stages_end.items()},
                                   substeps=[t0_sub + args.steps, t0_sub + args.steps + STAGE_SUBSTEPS]),
@@ -1469,7 +1480,8 @@ def run_batched(args, rank, local, world_size, pg, ctx, scenes, parts, cfg):
                          "traffic_source": traffic["source"] if traffic else None, "peak_kind": peak_kind,
                          "algorithmic_bytes": alg_bytes, "bytes_per_particle": per_p, "bytes_per_node": per_n,
                          "active_nodes": A, "kernel_us": kern_us,
-                         "kernel_substeps": [t0_sub - STAGE_SUBSTEPS, t0_sub]},
+                         "kernel_substeps": [t0_sub - STAGE_SUBSTEPS, t0_sub],
+                         **substep_roofline(n_total, A, stages, peak)},
             "stages_us": {a: round(b, 2) for a, b in stages.items()}, "autotune": tune,
             "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,
         }

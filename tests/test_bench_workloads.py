@@ -52,3 +52,11 @@ def test_batched_shards_deal_one_scene_list():
     b = B.shard(list(range(10)), 1, 3)
     c = B.shard(list(range(10)), 2, 3)
     assert sorted(a + b + c) == list(range(10)) and a == [0, 3, 6, 9]
+
+
+def test_substep_roofline_counts_the_scope_bytes():
+    import bench as B
+
+    r = B.substep_roofline(1000, 100, {"substep": 1.0}, 1000.0)
+    assert r["substep_bytes"] == 260 * 1000 + 80 * 100
+    assert abs(r["substep_achieved"] - 268.0) < 1e-9 and abs(r["substep_frac"] - 0.268) < 1e-12
