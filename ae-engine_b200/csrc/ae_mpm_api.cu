@@ -752,7 +752,8 @@ int ae_mpm_batch_run(ae_mpm_batch* batch, const ae_mpm_particles* in, const uint
   // every group's inputs queue on the upload stream in group order; group g's substeps start
   // when its inputs are in (served before later groups' by stream priority), and its results
   // leave on the download stream while later groups compute
-  auto group_fail = [&](uint32_t g, int code) {
+  auto group_fail = [&](uint32_t g, int code) {  // nothing may still read or write the caller's buffers
+    cudaStreamSynchronize(batch->up);
     cudaStreamSynchronize(batch->down);
     for (WorldBase* w : batch->worlds) cudaStreamSynchronize(w->stream());
     return fail(ctx, code, "batch group " + std::to_string(g) + ": " + batch->worlds[g]->err);
