@@ -278,62 +278,46 @@ __global__ void __launch_bounds__(kCountThreads) count_hist(const uint32_t* __re
   }
 }
 
-// exclusive scan of nb bins in place, one CTA of 1024 threads.  Warp w owns the contiguous
-// segment [w*seg, w*seg + seg) (seg a multiple of 32); a pass of coalesced loads sums each segment,
-// a scan over the 32 segment sums gives each warp its carry, and a second pass scans the segment
-// 32 bins at a time.  Loads go in batches of kScanBatch rows so that many are in flight at once
-// (the bins are in L2, just written by the histogram).
-constexpr int kScanBatch = 16;
+// exclusive scan of the bins within each segment of 1024 (one CTA per segment, one bin per
+// thread, coalesced), in place; seg_total[b] = the sum of segment b.  The scatter adds the
+// segment's offset, the exclusive scan of seg_total, which each of its CTAs forms itself.
+constexpr int kSegBins = 1024;
+constexpr int kMaxSegs = (1 << kCountingSortBits) / kSegBins;
 
-__global__ void __launch_bounds__(1024) count_scan(uint32_t* bins, uint32_t nb) {
+__global__ void __launch_bounds__(kSegBins) count_scan(uint32_t* __restrict__ bins, uint32_t nb,
+                                                       uint32_t* __restrict__ seg_total) {
   __shared__ uint32_t wsum[32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const uint32_t seg = ((nb + 1023u) / 1024u) * 32u;
-  const uint32_t lo = uint32_t(w) * seg, hi = lo + seg < nb ? lo + seg : nb;
-  uint32_t s = 0;
-  for (uint32_t base = lo; base < hi; base += 32u * kScanBatch) {
-    uint32_t x[kScanBatch];
-#pragma unroll
-    for (int k = 0; k < kScanBatch; ++k) {
-      const uint32_t i = base + 32u * k + lane;
-      x[k] = i < hi ? bins[i] : 0u;
-    }
-#pragma unroll
-    for (int k = 0; k < kScanBatch; ++k) s += x[k];
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane == 0) wsum[w] = s;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const uint32_t i = blockIdx.x * kSegBins + tid;
+  const uint32_t x = i < nb ? bins[i] : 0u;
+  const uint32_t incl = warp_incl_scan(x, lane);
+  if (lane == 31) wsum[w] = incl;
   __syncthreads();
   if (w == 0) {
     const uint32_t ws = wsum[lane];
     wsum[lane] = warp_incl_scan(ws, lane) - ws;
   }
   __syncthreads();
-  uint32_t carry = wsum[w];
-  for (uint32_t base = lo; base < hi; base += 32u * kScanBatch) {
-    uint32_t x[kScanBatch];
-#pragma unroll
-    for (int k = 0; k < kScanBatch; ++k) {
-      const uint32_t i = base + 32u * k + lane;
-      x[k] = i < hi ? bins[i] : 0u;
-    }
-#pragma unroll
-    for (int k = 0; k < kScanBatch; ++k) {
-      const uint32_t i = base + 32u * k + lane;
-      const uint32_t incl = warp_incl_scan(x[k], lane);
-      if (i < hi) bins[i] = carry + incl - x[k];
-      carry += __shfl_sync(0xffffffffu, incl, 31);
-    }
-  }
+  if (i < nb) bins[i] = wsum[w] + incl - x;
+  if (tid == kSegBins - 1) seg_total[blockIdx.x] = wsum[w] + incl;
 }
 
 __global__ void __launch_bounds__(kCountThreads) count_scatter(const uint32_t* __restrict__ keys, uint64_t n,
                                                                uint32_t mask, uint32_t* __restrict__ bins,
-                                                               uint32_t* __restrict__ keys_out,
+                                                               const uint32_t* __restrict__ seg_total,
+                                                               uint32_t n_segs, uint32_t* __restrict__ keys_out,
                                                                uint32_t* __restrict__ perm_out) {
+  __shared__ uint32_t seg_off[kMaxSegs];
   const int lane = threadIdx.x & 31;
   const uint32_t lt = lanemask_lt();
+  if (threadIdx.x < 32) {  // exclusive scan of the segment totals, two per lane
+    const uint32_t a = 2u * lane < n_segs ? seg_total[2 * lane] : 0u;
+    const uint32_t b = 2u * lane + 1u < n_segs ? seg_total[2 * lane + 1] : 0u;
+    const uint32_t incl = warp_incl_scan(a + b, lane);
+    seg_off[2 * lane] = incl - a - b;
+    seg_off[2 * lane + 1] = incl - b;
+  }
+  __syncthreads();
   for (uint64_t base = uint64_t(blockIdx.x) * kCountThreads; base < n; base += uint64_t(gridDim.x) * kCountThreads) {
     const uint64_t i = base + threadIdx.x;
     const bool valid = i < n;
@@ -342,7 +326,7 @@ __global__ void __launch_bounds__(kCountThreads) count_scatter(const uint32_t* _
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     const int leader = __ffs(peers) - 1;
     uint32_t pos = 0;
-    if (valid && lane == leader) pos = atomicAdd(bins + d, uint32_t(__popc(peers)));
+    if (valid && lane == leader) pos = atomicAdd(bins + d, uint32_t(__popc(peers))) + seg_off[d / kSegBins];
     pos = __shfl_sync(0xffffffffu, pos, leader) + __popc(peers & lt);
     if (valid) {
       keys_out[pos] = k;
@@ -482,10 +466,11 @@ int counting_sort_pairs(uint32_t* keys, uint64_t n, int key_bits, SortScratch& s
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const uint64_t want = (n + kCountThreads - 1) / kCountThreads;
   const unsigned grid = unsigned(want < uint64_t(sms) * 8 ? want : uint64_t(sms) * 8);
+  const uint32_t n_segs = (nb + kSegBins - 1) / kSegBins;  // <= kMaxSegs; totals has 4 * kMaxRadix entries
   cudaMemsetAsync(s.bins, 0, sizeof(uint32_t) * nb, stream);
   count_hist<<<grid, kCountThreads, 0, stream>>>(keys, n, mask, s.bins);
-  count_scan<<<1, 1024, 0, stream>>>(s.bins, nb);
-  count_scatter<<<grid, kCountThreads, 0, stream>>>(keys, n, mask, s.bins, s.keys_alt, s.vals_a);
+  count_scan<<<n_segs, kSegBins, 0, stream>>>(s.bins, nb, s.totals);
+  count_scatter<<<grid, kCountThreads, 0, stream>>>(keys, n, mask, s.bins, s.totals, n_segs, s.keys_alt, s.vals_a);
   return 3;
 }
 
