@@ -620,12 +620,9 @@ struct ae_mpm_batch {
   std::vector<WorldBase*> worlds;
   std::vector<uint32_t> first;  // group g holds scenes [first[g], first[g + 1])
   cudaStream_t up = nullptr, down = nullptr;
-  std::vector<cudaEvent_t> done;  // group g's substeps have finished
   ~ae_mpm_batch() {
     if (down) cudaStreamSynchronize(down);
     for (WorldBase* w : worlds) delete w;
-    for (cudaEvent_t e : done)
-      if (e) cudaEventDestroy(e);
     if (up) cudaStreamDestroy(up);
     if (down) cudaStreamDestroy(down);
   }
@@ -675,8 +672,6 @@ int ae_mpm_batch_create(ae_mpm_ctx* ctx, const ae_mpm_scene_desc* scenes, uint32
   b->first = first;
   cudaError_t e = cudaStreamCreateWithFlags(&b->up, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->down, cudaStreamNonBlocking);
-  b->done.assign(g_n, nullptr);
-  for (uint32_t g = 0; g < g_n && e == cudaSuccess; ++g) e = cudaEventCreateWithFlags(&b->done[g], cudaEventDisableTiming);
   if (e != cudaSuccess) {
     delete b;
     return fail(ctx, AE_MPM_ECUDA, cudaGetErrorString(e));
@@ -768,8 +763,6 @@ int ae_mpm_batch_run(ae_mpm_batch* batch, const ae_mpm_particles* in, const uint
     WorldBase* w = batch->worlds[g];
     mark(w->stream());
     if ((rc = w->step(n_substeps))) return group_fail(g, rc);
-    if (cudaEventRecord(batch->done[g], w->stream()) != cudaSuccess)
-      return fail(ctx, AE_MPM_ECUDA, "batch: event record failed");
     mark(w->stream());
     host_mark();
   }
