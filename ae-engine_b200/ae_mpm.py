@@ -210,6 +210,8 @@ SIGNATURES = {
     "ae_mpm_server_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
                                       C.POINTER(C.c_uint64)]),
     "ae_mpm_server_destroy": (C.c_int, [_P]),
+    "ae_mpm_server_slot_class": (C.c_int, [C.POINTER(SceneDesc), C.c_uint64, _P, C.POINTER(C.c_uint64),
+                                           C.POINTER(C.c_uint32)]),
 }
 
 _lib = None
@@ -238,6 +240,18 @@ def batch_partition(capacities, groups: int):
     first = np.zeros(caps.size + 1, np.uint32)
     g = load().ae_mpm_batch_partition(caps.ctypes.data, caps.size, groups, first.ctypes.data)
     return [int(x) for x in first[:g + 1]] if g else []
+
+
+def server_slot_class(scene: "Scene", n_particles: int):
+    """ae_mpm_server_slot_class: (grid axes, particle capacity, material count) of the server slot
+    a request takes (host only)."""
+    d = scene.desc()
+    g = np.zeros(3, np.uint32)
+    cap, mats = C.c_uint64(), C.c_uint32()
+    rc = load().ae_mpm_server_slot_class(C.byref(d), n_particles, g.ctypes.data, C.byref(cap), C.byref(mats))
+    if rc != OK:
+        raise MpmError(rc, "slot class")
+    return tuple(int(x) for x in g), int(cap.value), int(mats.value)
 
 
 def exec_opts(**kw) -> ExecOpts:

@@ -565,6 +565,16 @@ struct ae_mpm_server {
 
 extern "C" {
 
+int ae_mpm_server_slot_class(const ae_mpm_scene_desc* scene, uint64_t n_particles, uint32_t grid_out[3],
+                             uint64_t* particles_out, uint32_t* materials_out) {
+  if (!scene || !grid_out || !particles_out || !materials_out) return AE_MPM_EINVAL;
+  const SlotClass c = class_of(*scene, n_particles);
+  for (int a = 0; a < 3; ++a) grid_out[a] = c.n[a];
+  *particles_out = c.particles;
+  *materials_out = c.materials;
+  return AE_MPM_OK;
+}
+
 int ae_mpm_server_create(ae_mpm_ctx* ctx, const ae_mpm_server_opts* opts, ae_mpm_server** out) {
   if (!ctx || !out) return AE_MPM_EINVAL;
   *out = nullptr;

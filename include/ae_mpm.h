@@ -542,6 +542,12 @@ int ae_mpm_server_drain(ae_mpm_server* server, double timeout_s);
 int ae_mpm_server_stats(ae_mpm_server* server, uint64_t* resident_bytes, uint32_t* resident_scenes,
                         uint64_t* ticks, uint64_t* particle_substeps);
 int ae_mpm_server_destroy(ae_mpm_server* server);
+/* The size class of the slot a request of `scene` with n_particles takes (host only, no device
+ * needed): grid axes rounded up to multiples of 16 nodes (at least 16), a particle capacity of
+ * the first quarter-octave step 2^(k/4) * 2^j >= n_particles (j >= 10, rounded up to 256), and a
+ * power-of-two material count of at least 4. */
+int ae_mpm_server_slot_class(const ae_mpm_scene_desc* scene, uint64_t n_particles, uint32_t grid_out[3],
+                             uint64_t* particles_out, uint32_t* materials_out);
 
 #ifdef __cplusplus
 }
