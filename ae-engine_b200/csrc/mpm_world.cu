@@ -1136,15 +1136,13 @@ __device__ __forceinline__ bool g2p_physics_gather_sep_f2(const Rows& rows, cons
     for (int k = 0; k < 3; ++k) e[a][k] = w[a][k] * ((float(k) - fx) * sc.dx);
   }
   if (!inside) return false;
-  float2 wx[3], ex[3], wy[3], ey[3], wz[3], ez[3];
+  // only the x weights are kept as broadcast pairs; the y/z weight products are formed per
+  // column and paired there (pairs of all six weight sets took 36 registers and spilled)
+  float2 wx[3], ex[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     wx[k] = make_float2(w[0][k], w[0][k]);
     ex[k] = make_float2(e[0][k], e[0][k]);
-    wy[k] = make_float2(w[1][k], w[1][k]);
-    ey[k] = make_float2(e[1][k], e[1][k]);
-    wz[k] = make_float2(w[2][k], w[2][k]);
-    ez[k] = make_float2(e[2][k], e[2][k]);
   }
   float2 vxy = make_float2(0.f, 0.f), b0xy = vxy, b1xy = vxy, b2xy = vxy;
   float vz = 0.f, b0z = 0.f, b1z = 0.f, b2z = 0.f;
@@ -1168,7 +1166,8 @@ __device__ __forceinline__ bool g2p_physics_gather_sep_f2(const Rows& rows, cons
       const float2 s1xy = __ffma2_rn(ex[2], g2xy, __ffma2_rn(ex[1], g1xy, __fmul2_rn(ex[0], g0xy)));
       const float s0z = w[0][0] * g0.z + w[0][1] * g1.z + w[0][2] * g2.z;
       const float s1z = e[0][0] * g0.z + e[0][1] * g1.z + e[0][2] * g2.z;
-      const float2 wbc = __fmul2_rn(wy[bb], wz[c]), ebc = __fmul2_rn(ey[bb], wz[c]), fbc = __fmul2_rn(wy[bb], ez[c]);
+      const float wbs = w[1][bb] * w[2][c], ebs = e[1][bb] * w[2][c], fbs = w[1][bb] * e[2][c];
+      const float2 wbc = make_float2(wbs, wbs), ebc = make_float2(ebs, ebs), fbc = make_float2(fbs, fbs);
       vxy = __ffma2_rn(wbc, s0xy, vxy);
       b0xy = __ffma2_rn(wbc, s1xy, b0xy);
       b1xy = __ffma2_rn(ebc, s0xy, b1xy);
